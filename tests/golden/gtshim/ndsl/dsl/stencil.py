@@ -1,0 +1,39 @@
+"""StencilFactory / GridIndexing over the numpy executor."""
+from _gtexec import Stencil
+
+
+class GridIndexing:
+    def __init__(self, nx, ny, nz, n_halo=3):
+        self.nx, self.ny, self.nz, self.n_halo = nx, ny, nz, n_halo
+        self.domain = (nx, ny, nz)
+
+    def origin_compute(self, add=(0, 0, 0)):
+        return (self.n_halo + add[0], self.n_halo + add[1], add[2])
+
+    def domain_compute(self, add=(0, 0, 0)):
+        return (self.nx + add[0], self.ny + add[1], self.nz + add[2])
+
+    def origin_full(self, add=(0, 0, 0)):
+        return (add[0], add[1], add[2])
+
+    def domain_full(self, add=(0, 0, 0)):
+        h = self.n_halo
+        return (self.nx + 2 * h + add[0], self.ny + 2 * h + add[1], self.nz + add[2])
+
+    @property
+    def max_shape(self):
+        return self.domain_full(add=(1, 1, 1))
+
+
+class _Cfg:
+    dace_config = None
+
+
+class StencilFactory:
+    def __init__(self, grid_indexing):
+        self.grid_indexing = grid_indexing
+        self.config = _Cfg()
+        self.backend = "numpy"
+
+    def from_origin_domain(self, func, origin, domain, externals=None, **kwargs):
+        return Stencil(func, externals=externals, origin=origin, domain=domain)

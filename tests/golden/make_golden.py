@@ -1,0 +1,371 @@
+"""Generate golden fixtures by running the reference's own pySHiELD source.
+
+Usage (in a container where the pySHiELD source tree is available)::
+
+    python tests/golden/make_golden.py [--reference /path/to/pySHiELD-checkout]
+
+gt4py and NDSL are not installable here, so ``gtshim/`` provides the names
+the reference imports, and its ``_gtexec`` module executes the stencil
+definitions with GT4Py's numpy-backend semantics. Everything that runs is the
+reference's code: ``Microphysics.__init__`` / ``setupm`` / ``__call__``, the
+stencils ``fields_init``, ``warm_rain``, ``sedimentation``, ``icloud``,
+``fields_update`` and the pointwise functions of ``microphysics_funcs.py``,
+plus the coupling stencils of ``physics.py``, ``update_atmos_state.py`` and
+``fv_update_phys.py``.
+
+Inputs come from ``pyshield_b200.inputs.make_state`` plus per-case
+perturbations that reach the rarer branches (negative species for
+``fix_negative``, temperatures below ``T_MIN``, pressures below ``P_MIN``,
+non-zero incoming tendencies). Each case is written to ``<case>.npz`` next to
+this script; the tests compare the oracle against these files bit for bit,
+and the CUDA kernels against the oracle.
+"""
+
+import argparse
+import dataclasses
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+MP_OUT = ("pt_dt", "qv_dt", "ql_dt", "qr_dt", "qi_dt", "qs_dt", "qg_dt", "qa_dt", "udt", "vdt")
+
+
+def _setup_paths(reference):
+    sys.path.insert(0, os.path.join(HERE, "gtshim"))
+    sys.path.insert(0, REPO)
+    sys.path.insert(0, reference)
+
+
+def mp_cases():
+    """(name, nx, ny, L, dt, nsteps, config overrides, perturbation) tuples."""
+    return [
+        ("mp_default", 6, 4, 24, 150.0, 2, {}, "none"),
+        ("mp_substeps", 5, 3, 20, 450.0, 1, {}, "stress"),
+        (
+            "mp_flags_a",
+            4,
+            4,
+            18,
+            225.0,
+            2,
+            dict(
+                do_qa=True,
+                fast_sat_adj=False,
+                z_slope_ice=False,
+                z_slope_liq=False,
+                do_sedi_heat=True,
+                hydrostatic=True,
+                de_ice=True,
+                sedi_transport=False,
+            ),
+            "stress",
+        ),
+        (
+            "mp_flags_b",
+            4,
+            3,
+            16,
+            180.0,
+            1,
+            dict(
+                irain_f=1,
+                const_vi=True,
+                const_vs=True,
+                const_vg=True,
+                const_vr=True,
+                vi_fac=0.3333333333333333,
+                vg_fac=2.0,
+                vr_fac=4.0,
+                rad_snow=False,
+                rad_rain=False,
+                do_sedi_heat=True,
+                fix_negative=False,
+            ),
+            "none",
+        ),
+        ("mp_prog_ccn_off_ice", 3, 3, 12, 150.0, 1, dict(vi_fac=1.0e-6), "stress"),
+    ]
+
+
+def perturb(state, kind, seed):
+    """Push some points into the rarer branches of the scheme."""
+    if kind == "none":
+        return
+    rng = np.random.default_rng(seed + 1000)
+    L, n = state["pt"].shape
+    # negative species for fix_negative (fields_init :202-276)
+    for name in ("qice", "qsnow", "qgraupel", "qrain", "qliquid"):
+        m = rng.random((L, n)) < 0.04
+        state[name][m] = -rng.uniform(1e-9, 2e-6, int(m.sum()))
+    # a negative vapour run near the surface and the top
+    m = rng.random(n) < 0.3
+    state["qvapor"][L - 1, m] = -1e-7
+    state["qvapor"][L - 3, m] = -5e-8
+    state["qvapor"][2, m] = -1e-8
+    # very cold tops (T < T_MIN) and thin top layers (p1 < P_MIN)
+    state["pt"][0, : n // 2] = 170.0
+    state["delprsi"][0, : n // 3] = 20.0
+    # non-zero incoming tendencies (they are accumulated)
+    for name in MP_OUT:
+        state[name][...] = rng.normal(0.0, 1e-6, (L, n))
+    state["qi_dt"][...] = rng.normal(0.0, 1e-7, (L, n))
+
+
+def to_storage(arr_ln, nx, ny, h=3):
+    """(L, n) -> NDSL storage (nx+2h+1, ny+2h+1, L+1), column c = j*nx + i."""
+    L = arr_ln.shape[0]
+    out = np.zeros((nx + 2 * h + 1, ny + 2 * h + 1, L + 1))
+    out[h : h + nx, h : h + ny, :L] = arr_ln.reshape(L, ny, nx).transpose(2, 1, 0)
+    return out
+
+
+def to_storage2d(arr_n, nx, ny, h=3):
+    out = np.zeros((nx + 2 * h + 1, ny + 2 * h + 1))
+    out[h : h + nx, h : h + ny] = arr_n.reshape(ny, nx).T
+    return out
+
+
+def from_storage(st, nx, ny, L, h=3):
+    return st[h : h + nx, h : h + ny, :L].transpose(2, 1, 0).reshape(L, nx * ny).copy()
+
+
+def run_mp_case(name, nx, ny, L, dt, nsteps, overrides, kind):
+    import pySHiELD
+    from ndsl.dsl.stencil import GridIndexing, StencilFactory
+    from ndsl.grid import GridData
+    from ndsl.initialization.allocator import QuantityFactory
+    from ndsl.quantity import Quantity
+    from pySHiELD.stencils.microphysics import Microphysics, MicrophysicsState
+
+    from pyshield_b200._config import PhysicsConfig as OurConfig
+    from pyshield_b200.inputs import make_state
+
+    n = nx * ny
+    seed = abs(hash(name)) % (2 ** 31)
+    seed = sum(ord(c) for c in name)
+    state, area = make_state(n, L, seed=seed, n_cube=nx)
+    perturb(state, kind, seed)
+    inputs = {k: v.copy() for k, v in state.items()}
+
+    cfg_kwargs = dict(dt_atmos=dt, npx=nx + 1, npy=ny + 1, npz=L)
+    cfg_kwargs.update(overrides)
+    ref_cfg = pySHiELD.PhysicsConfig(**cfg_kwargs)
+    gi = GridIndexing(nx, ny, L)
+    sf = StencilFactory(gi)
+    qf = QuantityFactory(nx, ny, L)
+    dims3 = ["x", "y", "z"]
+
+    def q3(a):
+        return Quantity(to_storage(a, nx, ny), dims3, "", origin=(3, 3, 0), extent=(nx, ny, L))
+
+    area_q = Quantity(to_storage2d(area, nx, ny), ["x", "y"], "m^2", origin=(3, 3), extent=(nx, ny))
+    grid_data = GridData(area=area_q)
+    mp = Microphysics(sf, qf, grid_data, ref_cfg)
+
+    fields3 = {
+        k: q3(state[k])
+        for k in ("pt", "qvapor", "qliquid", "qrain", "qice", "qsnow", "qgraupel", "qcld", "ua", "va", "delprsi", "delz", "wmp")
+    }
+    zeros = qf.zeros(dims3, "")
+    land_q = Quantity(to_storage2d(state["land"], nx, ny), ["x", "y"], "", origin=(3, 3), extent=(nx, ny))
+    ms = MicrophysicsState(
+        pt=fields3["pt"],
+        qvapor=fields3["qvapor"],
+        qliquid=fields3["qliquid"],
+        qrain=fields3["qrain"],
+        qice=fields3["qice"],
+        qsnow=fields3["qsnow"],
+        qgraupel=fields3["qgraupel"],
+        qcld=fields3["qcld"],
+        ua=fields3["ua"],
+        va=fields3["va"],
+        delp=qf.zeros(dims3, ""),
+        delz=fields3["delz"],
+        omga=qf.zeros(dims3, ""),
+        delprsi=fields3["delprsi"],
+        wmp=fields3["wmp"],
+        dz=qf.zeros(dims3, ""),
+        tendency=zeros,
+        land=land_q,
+    )
+    for t in MP_OUT:
+        getattr(ms, t).data[...] = to_storage(state[t], nx, ny)
+
+    out = {}
+    for step in range(nsteps):
+        mp(ms, timestep=dt)
+        for t in MP_OUT:
+            out[f"s{step}_{t}"] = from_storage(getattr(ms, t).data, nx, ny, L)
+        for f in ("wmp", "qice", "qsnow"):
+            out[f"s{step}_{f}"] = from_storage(getattr(ms, f).data, nx, ny, L)
+        for p, attr in (("rain", "_rain"), ("snow", "_snow"), ("ice", "_ice"), ("graupel", "_graupel")):
+            out[f"s{step}_{p}"] = from_storage(getattr(mp, attr).data, nx, ny, L)[0]
+        out[f"s{step}_qaz"] = from_storage(mp._qaz.data, nx, ny, L)
+
+    our_fields = {f.name for f in dataclasses.fields(OurConfig)}
+    meta = {
+        "name": name,
+        "nx": nx,
+        "ny": ny,
+        "L": L,
+        "dt": dt,
+        "nsteps": nsteps,
+        "config": {k: v for k, v in cfg_kwargs.items() if k in our_fields},
+        "kind": kind,
+    }
+    arrays = {f"in_{k}": v for k, v in inputs.items()}
+    arrays["in_area"] = area
+    arrays.update(out)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), meta=json.dumps(meta), **arrays)
+    return meta
+
+
+def coupling_cases():
+    return [("cpl_small", 5, 4, 16, 225.0, 0), ("cpl_stress", 4, 3, 12, 150.0, 1)]
+
+
+def run_coupling_case(name, nx, ny, L, dt, stress):
+    """Coupling stencils on one synthetic state, each run on its own inputs:
+    update_physics_state_with_tendencies (physics.py:151-194),
+    fill_gfs_delp (update_atmos_state.py:21-37),
+    prepare_tendencies_and_update_tracers (update_atmos_state.py:40-92),
+    moist_cv and update_pressure_and_surface_winds (fv_update_phys.py:32-75).
+    The domains are those the reference constructs them with."""
+    import pySHiELD.stencils.physics as phys
+    import pySHiELD.update.fv_update_phys as fvp
+    import pySHiELD.update.update_atmos_state as uas
+    from ndsl.dsl.stencil import GridIndexing, StencilFactory
+
+    import pyshield_b200.constants as C
+
+    rng = np.random.default_rng(sum(ord(c) for c in name))
+    h = 3
+    gi = GridIndexing(nx, ny, L)
+    sf = StencilFactory(gi)
+    shape = gi.domain_full(add=(1, 1, 1))
+    qn = ("qvapor", "qliquid", "qrain", "qice", "qsnow", "qgraupel")
+    out = {}
+
+    def rnd(lo, hi):
+        return rng.uniform(lo, hi, shape)
+
+    # --- update_physics_state_with_tendencies
+    names_in = qn + ("qcld", "pt", "ua", "va")
+    arrs = {}
+    for nm in names_in:
+        arrs[nm] = rnd(0.0, 1e-3) if nm.startswith("q") else rnd(-20.0, 300.0)
+    tnd = {t: rng.normal(0.0, 1e-5, shape) for t in MP_OUT}
+    upd = {f"u_{nm}": np.zeros(shape) for nm in names_in}
+    st = sf.from_origin_domain(phys.update_physics_state_with_tendencies, origin=gi.origin_compute(), domain=gi.domain_compute())
+    st(
+        arrs["qvapor"], arrs["qliquid"], arrs["qrain"], arrs["qice"], arrs["qsnow"], arrs["qgraupel"],
+        arrs["qcld"], arrs["pt"], arrs["ua"], arrs["va"],
+        tnd["qv_dt"], tnd["ql_dt"], tnd["qr_dt"], tnd["qi_dt"], tnd["qs_dt"], tnd["qg_dt"], tnd["qa_dt"], tnd["pt_dt"], tnd["udt"], tnd["vdt"],
+        upd["u_qvapor"], upd["u_qliquid"], upd["u_qrain"], upd["u_qice"], upd["u_qsnow"], upd["u_qgraupel"],
+        upd["u_qcld"], upd["u_pt"], upd["u_ua"], upd["u_va"], dt,
+    )
+    for nm in names_in:
+        out[f"upd_in_{nm}"] = arrs[nm]
+        out[f"upd_out_{nm}"] = upd[f"u_{nm}"]
+    for t in MP_OUT:
+        out[f"upd_in_{t}"] = tnd[t]
+
+    # --- fill_gfs_delp on the full (halo) domain with L+1 levels
+    delp = rnd(50.0, 2000.0)
+    q = rnd(-2e-9, 5e-3)
+    if stress:
+        q[..., 3:7] = rng.uniform(-1e-6, 2e-9, q[..., 3:7].shape)
+    out["fill_in_delp"] = delp.copy()
+    out["fill_in_q"] = q.copy()
+    st = sf.from_origin_domain(uas.fill_gfs_delp, origin=gi.origin_full(), domain=gi.domain_full(add=(0, 0, 1)))
+    st(delp, q, 1.0e-9)
+    out["fill_out_q"] = q
+
+    # --- prepare_tendencies_and_update_tracers
+    p = {}
+    for nm in ("u_dt", "v_dt", "pt_dt"):
+        p[nm] = rng.normal(0.0, 1e-4, shape)
+    for nm in ("u_t1", "v_t1", "u_t0", "v_t0"):
+        p[nm] = rnd(-30.0, 30.0)
+    p["pu_pt"] = rnd(200.0, 300.0)
+    p["pt_t0"] = rnd(200.0, 300.0)
+    for nm in qn:
+        p[f"pu_{nm}"] = rnd(0.0, 2e-3)
+        p[f"{nm}_t0"] = rnd(0.0, 2e-3)
+    prsi = np.cumsum(rnd(50.0, 2000.0), axis=2)
+    p["prsi"] = prsi
+    p["delp"] = rnd(50.0, 2000.0)
+    for k, v in p.items():
+        out[f"prep_in_{k}"] = v.copy()
+    st = sf.from_origin_domain(
+        uas.prepare_tendencies_and_update_tracers, origin=gi.origin_compute(), domain=gi.domain_compute(add=(0, 0, 1))
+    )
+    st(
+        p["u_dt"], p["v_dt"], p["pt_dt"], p["u_t1"], p["v_t1"], p["pu_pt"],
+        p["pu_qvapor"], p["pu_qliquid"], p["pu_qrain"], p["pu_qsnow"], p["pu_qice"], p["pu_qgraupel"],
+        p["u_t0"], p["v_t0"], p["pt_t0"],
+        p["qvapor_t0"], p["qliquid_t0"], p["qrain_t0"], p["qsnow_t0"], p["qice_t0"], p["qgraupel_t0"],
+        p["prsi"], p["delp"], 1.0 / dt,
+    )
+    for k in ("u_dt", "v_dt", "pt_dt", "delp") + tuple(f"{nm}_t0" for nm in qn):
+        out[f"prep_out_{k}"] = p[k]
+
+    # --- moist_cv + update_pressure_and_surface_winds
+    m = {nm: rnd(0.0, 2e-3) for nm in qn}
+    m["pt"] = rnd(200.0, 300.0)
+    m["t_dt"] = rng.normal(0.0, 1e-4, shape)
+    for k, v in m.items():
+        out[f"mcv_in_{k}"] = v.copy()
+    st = sf.from_origin_domain(fvp.moist_cv, origin=gi.origin_compute(), domain=gi.domain_compute(add=(0, 0, 1)))
+    st(m["qvapor"], m["qliquid"], m["qrain"], m["qsnow"], m["qice"], m["qgraupel"], m["pt"], m["t_dt"], C.CP_AIR, dt)
+    out["mcv_out_pt"] = m["pt"]
+    out["mcv_out_t_dt"] = m["t_dt"]
+
+    pe = np.zeros(shape)
+    pe[..., 0] = 100.0
+    pdelp = rnd(50.0, 2000.0)
+    ua = rnd(-30.0, 30.0)
+    va = rnd(-30.0, 30.0)
+    peln = np.zeros(shape)
+    pk = np.zeros(shape)
+    ps = np.zeros(shape[:2])
+    us = np.zeros(shape[:2])
+    vs = np.zeros(shape[:2])
+    for k, v in (("pe", pe), ("delp", pdelp), ("ua", ua), ("va", va)):
+        out[f"ups_in_{k}"] = v.copy()
+    st = sf.from_origin_domain(
+        fvp.update_pressure_and_surface_winds, origin=gi.origin_compute(), domain=gi.domain_compute(add=(0, 0, 1))
+    )
+    st(pe, pdelp, peln, pk, C.KAPPA, ua, va, ps, us, vs)
+    for k, v in (("pe", pe), ("peln", peln), ("pk", pk), ("ps", ps), ("u_srf", us), ("v_srf", vs)):
+        out[f"ups_out_{k}"] = v
+    meta = {"name": name, "nx": nx, "ny": ny, "L": L, "dt": dt, "halo": h}
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), meta=json.dumps(meta), **out)
+    return meta
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("PYSHIELD_REFERENCE", "/root/reference"))
+    ap.add_argument("--only", default=None)
+    args = ap.parse_args()
+    _setup_paths(args.reference)
+    for case in mp_cases():
+        if args.only and args.only != case[0]:
+            continue
+        meta = run_mp_case(*case)
+        print("wrote", meta["name"])
+    for case in coupling_cases():
+        if args.only and args.only != case[0]:
+            continue
+        meta = run_coupling_case(*case)
+        print("wrote", meta["name"])
+
+
+if __name__ == "__main__":
+    main()

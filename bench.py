@@ -1,0 +1,430 @@
+"""Benchmark of the GFDL microphysics step (column-steps/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--levels 79] [--form plain|mixed]
+
+Workload: C96 (6 x 96 x 96 = 55,296 columns) x 79 levels, one
+``Microphysics.__call__`` of 180 s per step, on a seeded synthetic state
+(no public dataset exists for this path; the distributions are those of
+``pyshield_b200.inputs``). The arrays are NDSL-layout storages (halo 3,
+i-fastest), as a GT4Py GPU backend would hand them over. One step moves
+1.26 GB, far more than the 126 MB L2, so no L2 flush is needed between
+steps.
+
+Reported (one JSON line, rank 0):
+  value      column-steps/s over all ranks, inputs resident in HBM, timed with
+             CUDA events on the launching stream (max over ranks);
+  e2e        the same metric through the public API with host buffers: the
+             step's inputs copied from pinned host memory to the device and
+             its outputs copied back, inside the timed region;
+  roofline   HBM roofline of the dominant kernel: algorithmic bytes
+             (36 fields x L x 8 B + 48 B per column-step) per launch / mean
+             launch time, against the measured copy bandwidth;
+  cpu_baseline  the FP64 numpy oracle (the restatement of the reference's numpy
+             backend) on the host cores, on a bounded sample of columns.
+
+--impl reference times that CPU implementation on the workload's metric
+(each step a bounded sample of the columns, all host cores).
+Multi-GPU: one process per GPU under torchrun; the columns are independent,
+so every rank advances its own C96 domain (weak scaling, no collective on
+the data path); the timing is the max over ranks.
+"""
+
+import argparse
+import json
+import multiprocessing as mp_
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+N_CUBE = 96
+DT = 180.0
+HALO = 3
+
+
+def algorithmic_bytes_per_column_step(nlev):
+    """Reads: 13 state fields, 10 tendencies (accumulated) and the persistent
+    cloud-fraction accumulator; writes: 10 tendencies, wmp and the
+    accumulator (36 fields x L x 8 B); per column: land, area read and four
+    precipitation totals written (48 B)."""
+    return 36 * nlev * 8 + 48
+
+
+# ------------------------------------------------------------ CPU baseline
+def _oracle_chunk(args):
+    n, nlev, seed, reps = args
+    sys.path.insert(0, REPO)
+    from oracle.microphysics import OracleMicrophysics
+    from pyshield_b200._config import PhysicsConfig
+    from pyshield_b200.inputs import copy_state, make_state
+
+    state, area = make_state(n, nlev, seed=seed, n_cube=N_CUBE)
+    m = OracleMicrophysics(PhysicsConfig(dt_atmos=DT), n, nlev, area)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        m(copy_state(state), DT)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(nlev, cores, cols_per_core=3456, reps=1, pool=None):
+    """Time the numpy oracle on ``cores`` processes x ``cols_per_core``
+    columns; returns (column-steps/s, seconds, sample description)."""
+    work = [(cols_per_core, nlev, 100 + i, reps) for i in range(cores)]
+    t0 = time.perf_counter()
+    if cores == 1:
+        _oracle_chunk(work[0])
+    else:
+        pool.map(_oracle_chunk, work)
+    wall = time.perf_counter() - t0
+    cs = cores * cols_per_core * reps / wall
+    sample = f"{cores} x {cols_per_core} columns x {nlev} levels, {reps} step(s) of {DT:g} s, numpy FP64 oracle"
+    return cs, wall, sample
+
+
+# ------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = (
+        "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+        "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+        "clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True,
+            )
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(smax) if smax else None,
+            "samples": len(sm),
+            "reasons": sorted(reasons),
+        }
+
+
+def peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------ GPU arm
+def build_state(nlev, device, seed):
+    """Synthetic C96 state as NDSL-layout torch storages on ``device``."""
+    import numpy as np
+    import torch
+
+    from pyshield_b200.grid import GridData, GridIndexing, QuantityFactory, StencilFactory
+    from pyshield_b200.inputs import make_state
+    from pyshield_b200.microphysics import MicrophysicsState
+    from pyshield_b200.quantity import Quantity
+
+    nx, ny = N_CUBE, 6 * N_CUBE  # the six tiles side by side
+    n = nx * ny
+    state, area = make_state(n, nlev, seed=seed, n_cube=N_CUBE)
+    gi = GridIndexing(nx, ny, nlev, HALO)
+    qf = QuantityFactory(gi, device=device)
+    host = {}
+
+    def put(name, arr_ln):
+        q = qf.zeros(["x", "y", "z"], "")
+        v = q.view  # (nx, ny, nlev) view of i-fastest storage
+        src = torch.from_numpy(np.ascontiguousarray(arr_ln.reshape(nlev, ny, nx)))
+        v.copy_(src.permute(2, 1, 0).to(device))
+        host[name] = src
+        return q
+
+    qs = {k: put(k, v) for k, v in state.items() if k != "land"}
+    land = qf.zeros(["x", "y"], "")
+    land.view.copy_(torch.from_numpy(state["land"].reshape(ny, nx).T.copy()).to(device))
+    area_q = qf.zeros(["x", "y"], "")
+    area_q.view.copy_(torch.from_numpy(area.reshape(ny, nx).T.copy()).to(device))
+    tend = qf.zeros(["x", "y", "z"], "")
+    ms = MicrophysicsState(
+        qs["pt"], qs["qvapor"], qs["qliquid"], qs["qrain"], qs["qice"], qs["qsnow"], qs["qgraupel"], qs["qcld"],
+        qs["ua"], qs["va"], qf.zeros(["x", "y", "z"], ""), qs["delz"], qf.zeros(["x", "y", "z"], ""), qs["delprsi"],
+        qs["wmp"], qf.zeros(["x", "y", "z"], ""), tend, land,
+    )
+    for t in ("pt_dt", "qv_dt", "ql_dt", "qr_dt", "qi_dt", "qs_dt", "qg_dt", "qa_dt", "udt", "vdt"):
+        setattr(ms, t, qs[t])
+    return ms, StencilFactory(gi), qf, GridData(area_q), host, land, (nx, ny, n)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from pyshield_b200._config import PhysicsConfig
+    from pyshield_b200.microphysics import Microphysics
+
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+    nlev = args.levels
+    ms, sf, qf, gd, host, land, (nx, ny, n) = build_state(nlev, device, seed=1234 + rank)
+    cfg = PhysicsConfig(dt_atmos=DT)
+    mp = Microphysics(sf, qf, gd, cfg, precision=args.form)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        mp(ms, DT)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for s in range(args.steps):
+        ev[s][0].record(stream)
+        mp(ms, DT)
+        ev[s][1].record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    total_ms = t_start.elapsed_time(t_end)
+    launch_ms = [a.elapsed_time(b) for a, b in ev]
+    mean_launch_ms = sum(launch_ms) / len(launch_ms)
+
+    # ---- end to end through the public API with pinned host buffers
+    fields_in = ("pt", "qvapor", "qliquid", "qrain", "qice", "qsnow", "qgraupel", "qcld", "ua", "va", "delprsi",
+                 "delz", "wmp", "pt_dt", "qv_dt", "ql_dt", "qr_dt", "qi_dt", "qs_dt", "qg_dt", "qa_dt", "udt", "vdt")
+    fields_out = ("pt_dt", "qv_dt", "ql_dt", "qr_dt", "qi_dt", "qs_dt", "qg_dt", "qa_dt", "udt", "vdt", "wmp")
+    h_in = {f: host[f].pin_memory() for f in fields_in}
+    h_land = torch.from_numpy(land.view.cpu().numpy().T.copy()).pin_memory()
+    h_out = {f: torch.empty_like(h_in[f]).pin_memory() for f in fields_out}
+    h_precip = torch.empty((4, ny, nx), dtype=torch.float64).pin_memory()
+    h2d = sum(h_in[f].numel() * 8 for f in fields_in) + h_land.numel() * 8
+    d2h = sum(h_out[f].numel() * 8 for f in fields_out) + h_precip.numel() * 8
+
+    def e2e_step():
+        for f in fields_in:
+            getattr(ms, f).view.copy_(h_in[f].permute(2, 1, 0), non_blocking=True)
+        land.view.copy_(h_land.t(), non_blocking=True)
+        mp(ms, DT)
+        for f in fields_out:
+            h_out[f].copy_(getattr(ms, f).view.permute(2, 1, 0), non_blocking=True)
+        h_precip.copy_(mp._precip, non_blocking=True)
+
+    e2e_steps = max(2, min(args.steps, 5))
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+
+    times = torch.tensor([total_ms, e2e_ms, mean_launch_ms], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    total_ms, e2e_ms, mean_launch_ms = times.tolist()
+    return {
+        "n": n,
+        "nlev": nlev,
+        "total_ms": total_ms,
+        "mean_launch_ms": mean_launch_ms,
+        "e2e_ms": e2e_ms,
+        "e2e_steps": e2e_steps,
+        "h2d": h2d,
+        "d2h": d2h,
+        "clocks": clk,
+    }
+
+
+def emit(rec):
+    print(json.dumps(rec), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--levels", type=int, default=79)
+    ap.add_argument("--form", default="plain", choices=["plain", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    cores = os.cpu_count() or 1
+    nlev = args.levels
+    ncol = 6 * N_CUBE * N_CUBE
+    config = {
+        "workload": f"GFDL microphysics step, C{N_CUBE} ({ncol} columns) x L{nlev}, dt {DT:g} s",
+        "columns_per_gpu": ncol,
+        "levels": nlev,
+        "dt_s": DT,
+        "form": args.form,
+        "layout": "NDSL storage, halo 3, i-fastest",
+        "l2": "no flush: 1.26 GB moved per step, > 126 MB L2",
+        "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "1 GPU",
+    }
+    metric = "GFDL MP column-steps/s"
+
+    # a process pool for the CPU oracle must start before any CUDA use
+    pool = None
+    want_cpu = (args.impl == "reference" or not args.no_cpu_baseline) and rank == 0 and world == 1
+    if want_cpu and cores > 1:
+        pool = mp_.get_context("spawn").Pool(cores)
+        pool.map(_oracle_chunk, [(24, nlev, 0, 1)] * cores)  # warm the workers
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        vals = []
+        for _ in range(args.warmup if args.warmup < 1 else 1):
+            cpu_baseline(nlev, cores, cols_per_core=256, reps=1, pool=pool)
+        sample = ""
+        t_all = 0.0
+        for _ in range(args.steps):
+            v, wall, sample = cpu_baseline(nlev, cores, cols_per_core=864, reps=1, pool=pool)
+            vals.append(v)
+            t_all += wall
+        value = len(vals) * cores * 864 / t_all
+        rec = {
+            "impl": "reference",
+            "metric": metric,
+            "value": value,
+            "unit": "column-steps/s",
+            "n_gpus": args.gpus,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": 1000.0 * ncol / value,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic",
+            "config": config,
+            "cpu_baseline": {"value": value, "unit": "column-steps/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "column-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference (GT4Py/NDSL) cannot be installed here; this times the FP64 numpy oracle that "
+                    "restates the reference's numpy backend bit for bit, on every host core",
+        }
+        if pool:
+            pool.close()
+        emit(rec)
+        return
+
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    r = run_ours(args, rank, world, local_rank)
+    steps = args.steps
+    value = world * r["n"] * steps / (r["total_ms"] / 1000.0)
+    bytes_launch = algorithmic_bytes_per_column_step(nlev) * r["n"]
+    achieved = bytes_launch / (r["mean_launch_ms"] / 1000.0) / 1e9
+    peak, peak_kind = peaks()
+    e2e_value = world * r["n"] * r["e2e_steps"] / (r["e2e_ms"] / 1000.0)
+
+    cpu = None
+    if want_cpu:
+        v, wall, sample = cpu_baseline(nlev, cores, cols_per_core=3456, reps=1, pool=pool)
+        v1, wall1, _ = cpu_baseline(nlev, 1, cols_per_core=3456, reps=1)
+        cpu = {"value": v, "unit": "column-steps/s", "cores": cores, "kind": "port",
+               "sample": sample + f"; one core alone: {v1:.4g} column-steps/s"}
+    if pool:
+        pool.close()
+
+    if rank == 0:
+        rec = {
+            "metric": metric,
+            "value": value,
+            "unit": "column-steps/s",
+            "n_gpus": world,
+            "steps": steps,
+            "warmup": args.warmup,
+            "ms_per_step": r["total_ms"] / steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64" if args.form == "plain" else "f32+f64",
+            "data": "synthetic",
+            "config": config,
+            "e2e": {"value": e2e_value, "unit": "column-steps/s", "h2d_bytes_per_step": r["h2d"],
+                    "d2h_bytes_per_step": r["d2h"]},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
+                         "bytes_per_launch": bytes_launch},
+            "cpu_baseline": cpu,
+            "gpu_launches": steps,
+            "clocks": r["clocks"],
+        }
+        emit(rec)
+
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,172 @@
+/*
+ * shield_mp.h -- C-ABI of the B200 GFDL cloud-microphysics step and its
+ * physics-to-dynamics column coupling (libshield_mp.so).
+ *
+ * pySHiELD has no native FFI: its interface is the Python object API. Each
+ * entry point below replaces one call of that API:
+ *
+ *   shield_mp_create   Microphysics.__init__(stencil_factory, quantity_factory,
+ *                      grid_data, namelist)     pySHiELD/stencils/microphysics.py:1624-1804
+ *   shield_mp_step     Microphysics.__call__(state, timestep)
+ *                                                pySHiELD/stencils/microphysics.py:1981-2263
+ *   shield_update_physics_state
+ *                      update_physics_state_with_tendencies
+ *                                                pySHiELD/stencils/physics.py:151-194
+ *   shield_update_atmos_state
+ *                      UpdateAtmosphereState.__call__ column stencils:
+ *                      fill_gfs_delp, prepare_tendencies_and_update_tracers
+ *                                                pySHiELD/update/update_atmos_state.py:21-92, 301-349
+ *                      and ApplyPhysicsToDycore's moist_cv and
+ *                      update_pressure_and_surface_winds
+ *                                                pySHiELD/update/fv_update_phys.py:32-75, 152-188
+ *
+ * Conventions
+ *  - All arrays are device pointers to double. A 3-D field is described by
+ *    the address of its compute-domain origin and element strides (i, j, k);
+ *    any layout works, i-fastest (GPU storage) and k-fastest (C-order numpy
+ *    storage) layouts are both read with coalesced loads. k = 0 is the model
+ *    top. Column c of a (nx, ny) domain is (i, j) = (c % nx, c / nx).
+ *  - Return codes: 0 on success, negative on error (see SHIELD_E*); the
+ *    message is kept per handle (shield_mp_last_error) or per thread
+ *    (shield_last_error for the handle-free calls). Nothing throws across the
+ *    ABI. There is no CPU fallback: without a usable CUDA device every call
+ *    fails with SHIELD_ECUDA.
+ *  - Work is enqueued on the given CUDA stream (NULL = legacy default stream)
+ *    and is asynchronous with respect to the host.
+ *  - A handle is not thread safe; use one handle per host thread.
+ */
+#ifndef SHIELD_MP_H
+#define SHIELD_MP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SHIELD_OK 0
+#define SHIELD_EINVAL (-1)   /* bad argument (null pointer, size, timestep) */
+#define SHIELD_ELAYOUT (-2)  /* unsupported size or layout */
+#define SHIELD_ECUDA (-3)    /* CUDA runtime error (launch, allocation, device) */
+#define SHIELD_EDEVICE (-4)  /* the kernel flagged a bad value */
+
+/* precision modes of shield_mp_step */
+#define SHIELD_MP_PLAIN 0 /* everything in FP64 */
+#define SHIELD_MP_MIXED 1 /* process rates in FP32, saturation adjustment, fall and budgets in FP64 */
+
+/* The PhysicsConfig fields the microphysics path reads
+ * (pySHiELD/_config.py:22-109, same names and meaning; booleans as int). */
+typedef struct {
+  double dt_atmos;
+  int hydrostatic;
+  int do_qa;
+  double c_cracw, c_paut, c_pgacs, c_psaci, ccn_l, ccn_o;
+  int const_vg, const_vi, const_vr, const_vs;
+  double vs_fac, vg_fac, vi_fac, vr_fac;
+  int de_ice;
+  double tau_imlt, tau_i2s, tau_g2v, tau_v2g, ql_mlt, qs_mlt, t_sub, qi_gen, qi_lim, qi0_max;
+  int rad_snow, rad_rain;
+  double dw_ocean, dw_land, tau_l2v;
+  int do_sedi_heat, do_sedi_w, fast_sat_adj;
+  double qc_crt;
+  int fix_negative, irain_f;
+  double mp_time;
+  int prog_ccn;
+  double qi0_crt, qs0_crt, rh_inc, rh_inr, rthresh;
+  int sedi_transport, use_ppm;
+  double vg_max, vi_max, vr_max, vs_max;
+  int z_slope_ice, z_slope_liq;
+  double tice, alin, clin;
+} ShieldMpConfig;
+
+typedef struct {
+  double* ptr; /* address of element (i, j, k) = (0, 0, 0) of the compute domain */
+  int64_t si, sj, sk;
+} ShieldField3D;
+
+typedef struct {
+  const double* ptr;
+  int64_t si, sj;
+} ShieldField2D;
+
+/* MicrophysicsState (pySHiELD/stencils/microphysics.py:1556-1620) as
+ * pointers. Inputs: the 13 state fields and land. In/out: the ten
+ * tendencies (accumulated, as the reference does), wmp (updated when
+ * do_sedi_w holds and hydrostatic does not) and, with de_ice, qice/qsnow.
+ * Outputs: the surface precipitation totals of the step in mm/day, ncol
+ * contiguous doubles each (column c = j*nx + i); any of them may be NULL. */
+typedef struct {
+  ShieldField3D pt, qvapor, qliquid, qrain, qice, qsnow, qgraupel, qcld, ua, va, delprsi, delz, wmp;
+  ShieldField3D pt_dt, qv_dt, ql_dt, qr_dt, qi_dt, qs_dt, qg_dt, qa_dt, udt, vdt;
+  ShieldField2D land;
+  double *rain, *snow, *ice, *graupel;
+} ShieldMpFields;
+
+/* Microphysics.__init__: computes the process constants (setupm) and the
+ * sub-step for cfg->dt_atmos, copies grid_data.area (nx*ny cells, strides
+ * in elements) and allocates the persistent cloud-fraction accumulator
+ * (the reference's never-reset self._qaz, zero at construction). */
+int shield_mp_create(const ShieldMpConfig* cfg, int nx, int ny, int nz, ShieldField2D area, void** handle);
+
+/* Microphysics.__call__(state, timestep): one full step. A timestep that
+ * differs from the previous one recomputes the sub-step (_set_timestep). */
+int shield_mp_step(void* handle, const ShieldMpFields* fields, double timestep, int precision, void* stream);
+
+int shield_mp_destroy(void* handle);
+
+/* Copies the handle's last error message (NUL terminated) into buf. */
+int shield_mp_last_error(void* handle, char* buf, size_t n);
+
+/* Test hook: the scalars the step uses for `timestep` (physical constants,
+ * setupm constants, sub-step values) in the order of the internal parameter
+ * block; returns how many doubles were written (at most n). */
+int shield_mp_constants(void* handle, double timestep, double* out, int n);
+
+/* Test hook: copy the persistent cloud-fraction accumulator (nz*nx*ny
+ * doubles, level-major) into / out of device memory at `qaz`. */
+int shield_mp_get_qaz(void* handle, double* qaz, void* stream);
+int shield_mp_set_qaz(void* handle, const double* qaz, void* stream);
+
+/* update_physics_state_with_tendencies (physics.py:151-194):
+ * out_X = X + X_dt * dt for the ten (X, X_dt) pairs in this order:
+ * qvapor/qv_dt, qliquid/ql_dt, qrain/qr_dt, qice/qi_dt, qsnow/qs_dt,
+ * qgraupel/qg_dt, qcld/qa_dt, pt/pt_dt, ua/udt, va/vdt.
+ * The domain is nx x ny x nz. */
+int shield_update_physics_state(int nx, int ny, int nz, const ShieldField3D* state10, const ShieldField3D* tend10,
+                                const ShieldField3D* out10, double dt, void* stream);
+
+/* The column part of UpdateAtmosphereState.__call__ with
+ * dycore_only = False and apply_tendencies = True
+ * (update_atmos_state.py:301-349, fv_update_phys.py:152-188), in the
+ * reference's order and on the reference's domains:
+ *   fill_gfs_delp(delp, physics_updated_specific_humidity, 1e-9)
+ *       on the full (halo) horizontal domain nxf x nyf, nz+1 levels;
+ *   prepare_tendencies_and_update_tracers on the compute domain, nz+1 levels
+ *       (levels 0..nz-1 are written);
+ *   moist_cv and update_pressure_and_surface_winds on the compute domain,
+ *       nz+1 levels.
+ * The horizontal halo exchange of u_dt/v_dt, AGrid2DGridPhysics and
+ * CubedToLatLon are not part of this call.
+ * Field order of `f` (ShieldField3D, all with origin at the compute-domain
+ * corner; fill_gfs_delp reads and writes `hx` halo points on each side):
+ *   0 u_dt 1 v_dt 2 pt_dt 3 u_t1 4 v_t1 5 physics_updated_pt
+ *   6 physics_updated_specific_humidity 7 physics_updated_qliquid
+ *   8 physics_updated_qrain 9 physics_updated_qsnow 10 physics_updated_qice
+ *   11 physics_updated_qgraupel 12 u_t0 (phy ua) 13 v_t0 (phy va)
+ *   14 pt_t0 (phy pt) 15 dycore qvapor 16 qliquid 17 qrain 18 qsnow 19 qice
+ *   20 qgraupel 21 prsi 22 dycore delp 23 dycore pt 24 pe 25 peln 26 pk
+ *   27 dycore ua 28 dycore va
+ * 2-D outputs (nx x ny, ShieldField2D with a writable ptr): ps, u_srf, v_srf. */
+int shield_update_atmos_state(int nx, int ny, int nz, int hx, const ShieldField3D* f, ShieldField3D ps,
+                              ShieldField3D u_srf, ShieldField3D v_srf, double rdt, double dt, double kappa,
+                              double cp_air, void* stream);
+
+/* Message of the last failing handle-free call on this host thread. */
+int shield_last_error(char* buf, size_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SHIELD_MP_H */

@@ -1,0 +1,178 @@
+"""ctypes binding of libshield_mp.so (the C-ABI in include/shield_mp.h).
+
+The library is built in place by ``pyshield_b200.build``; loading fails
+loudly when it is missing. There is no CPU fallback.
+"""
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libshield_mp.so")
+
+SHIELD_OK = 0
+SHIELD_MP_PLAIN = 0
+SHIELD_MP_MIXED = 1
+
+
+class ShieldField3D(ctypes.Structure):
+    _fields_ = [("ptr", ctypes.c_void_p), ("si", ctypes.c_int64), ("sj", ctypes.c_int64), ("sk", ctypes.c_int64)]
+
+
+class ShieldField2D(ctypes.Structure):
+    _fields_ = [("ptr", ctypes.c_void_p), ("si", ctypes.c_int64), ("sj", ctypes.c_int64)]
+
+
+_CFG_FIELDS = [
+    ("dt_atmos", ctypes.c_double),
+    ("hydrostatic", ctypes.c_int),
+    ("do_qa", ctypes.c_int),
+    ("c_cracw", ctypes.c_double),
+    ("c_paut", ctypes.c_double),
+    ("c_pgacs", ctypes.c_double),
+    ("c_psaci", ctypes.c_double),
+    ("ccn_l", ctypes.c_double),
+    ("ccn_o", ctypes.c_double),
+    ("const_vg", ctypes.c_int),
+    ("const_vi", ctypes.c_int),
+    ("const_vr", ctypes.c_int),
+    ("const_vs", ctypes.c_int),
+    ("vs_fac", ctypes.c_double),
+    ("vg_fac", ctypes.c_double),
+    ("vi_fac", ctypes.c_double),
+    ("vr_fac", ctypes.c_double),
+    ("de_ice", ctypes.c_int),
+    ("tau_imlt", ctypes.c_double),
+    ("tau_i2s", ctypes.c_double),
+    ("tau_g2v", ctypes.c_double),
+    ("tau_v2g", ctypes.c_double),
+    ("ql_mlt", ctypes.c_double),
+    ("qs_mlt", ctypes.c_double),
+    ("t_sub", ctypes.c_double),
+    ("qi_gen", ctypes.c_double),
+    ("qi_lim", ctypes.c_double),
+    ("qi0_max", ctypes.c_double),
+    ("rad_snow", ctypes.c_int),
+    ("rad_rain", ctypes.c_int),
+    ("dw_ocean", ctypes.c_double),
+    ("dw_land", ctypes.c_double),
+    ("tau_l2v", ctypes.c_double),
+    ("do_sedi_heat", ctypes.c_int),
+    ("do_sedi_w", ctypes.c_int),
+    ("fast_sat_adj", ctypes.c_int),
+    ("qc_crt", ctypes.c_double),
+    ("fix_negative", ctypes.c_int),
+    ("irain_f", ctypes.c_int),
+    ("mp_time", ctypes.c_double),
+    ("prog_ccn", ctypes.c_int),
+    ("qi0_crt", ctypes.c_double),
+    ("qs0_crt", ctypes.c_double),
+    ("rh_inc", ctypes.c_double),
+    ("rh_inr", ctypes.c_double),
+    ("rthresh", ctypes.c_double),
+    ("sedi_transport", ctypes.c_int),
+    ("use_ppm", ctypes.c_int),
+    ("vg_max", ctypes.c_double),
+    ("vi_max", ctypes.c_double),
+    ("vr_max", ctypes.c_double),
+    ("vs_max", ctypes.c_double),
+    ("z_slope_ice", ctypes.c_int),
+    ("z_slope_liq", ctypes.c_int),
+    ("tice", ctypes.c_double),
+    ("alin", ctypes.c_double),
+    ("clin", ctypes.c_double),
+]
+
+
+class ShieldMpConfig(ctypes.Structure):
+    _fields_ = _CFG_FIELDS
+
+
+MP_STATE_FIELDS = ("pt", "qvapor", "qliquid", "qrain", "qice", "qsnow", "qgraupel", "qcld", "ua", "va", "delprsi", "delz", "wmp")
+MP_TENDENCY_FIELDS = ("pt_dt", "qv_dt", "ql_dt", "qr_dt", "qi_dt", "qs_dt", "qg_dt", "qa_dt", "udt", "vdt")
+
+
+class ShieldMpFields(ctypes.Structure):
+    _fields_ = (
+        [(n, ShieldField3D) for n in MP_STATE_FIELDS]
+        + [(n, ShieldField3D) for n in MP_TENDENCY_FIELDS]
+        + [("land", ShieldField2D)]
+        + [(n, ctypes.c_void_p) for n in ("rain", "snow", "ice", "graupel")]
+    )
+
+
+EXPORTS = (
+    "shield_mp_create",
+    "shield_mp_step",
+    "shield_mp_destroy",
+    "shield_mp_last_error",
+    "shield_mp_constants",
+    "shield_mp_get_qaz",
+    "shield_mp_set_qaz",
+    "shield_update_physics_state",
+    "shield_update_atmos_state",
+    "shield_last_error",
+)
+
+_lib = None
+
+
+class ShieldError(RuntimeError):
+    pass
+
+
+def load():
+    """Load the library (once). Raises when it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ShieldError(
+            f"{LIB_PATH} is missing; build it with `python -m pyshield_b200.build` "
+            "(this package has no CPU fallback)"
+        )
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, i32, dbl = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    lib.shield_mp_create.argtypes = [ctypes.POINTER(ShieldMpConfig), i32, i32, i32, ShieldField2D, ctypes.POINTER(vp)]
+    lib.shield_mp_step.argtypes = [vp, ctypes.POINTER(ShieldMpFields), dbl, i32, vp]
+    lib.shield_mp_destroy.argtypes = [vp]
+    lib.shield_mp_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+    lib.shield_mp_constants.argtypes = [vp, dbl, ctypes.POINTER(ctypes.c_double), i32]
+    lib.shield_mp_get_qaz.argtypes = [vp, vp, vp]
+    lib.shield_mp_set_qaz.argtypes = [vp, vp, vp]
+    lib.shield_update_physics_state.argtypes = [
+        i32, i32, i32, ctypes.POINTER(ShieldField3D), ctypes.POINTER(ShieldField3D), ctypes.POINTER(ShieldField3D), dbl, vp,
+    ]
+    lib.shield_update_atmos_state.argtypes = [
+        i32, i32, i32, i32, ctypes.POINTER(ShieldField3D), ShieldField3D, ShieldField3D, ShieldField3D, dbl, dbl, dbl, dbl, vp,
+    ]
+    lib.shield_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+    for name in EXPORTS:
+        getattr(lib, name).restype = i32
+    _lib = lib
+    return lib
+
+
+def last_error(handle=None):
+    lib = load()
+    buf = ctypes.create_string_buffer(512)
+    if handle is None:
+        lib.shield_last_error(buf, 512)
+    else:
+        lib.shield_mp_last_error(handle, buf, 512)
+    return buf.value.decode(errors="replace")
+
+
+def check(rc, handle=None, what="call"):
+    if rc < 0:
+        raise ShieldError(f"{what} failed ({rc}): {last_error(handle)}")
+    return rc
+
+
+def make_config(cfg):
+    """ShieldMpConfig from a PhysicsConfig-like object."""
+    c = ShieldMpConfig()
+    for name, ctype in _CFG_FIELDS:
+        v = getattr(cfg, name)
+        setattr(c, name, float(v) if ctype is ctypes.c_double else int(bool(v)) if isinstance(v, bool) else int(v))
+    return c

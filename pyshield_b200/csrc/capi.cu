@@ -1,0 +1,393 @@
+// C-ABI entry points of libshield_mp.so (declared in include/shield_mp.h).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/shield_mp.h"
+#include "mp_launch.h"
+#include "mp_params.h"
+
+using namespace shield;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Handle {
+  ShieldMpConfig cfg;
+  int nx, ny, nz;
+  int64_t ncol;
+  int device;
+  double* area = nullptr;  // device copy of grid_data.area (ncol)
+  double* qaz = nullptr;   // persistent accumulator, nz * ncol, level-major
+  int* err = nullptr;
+  MpConst K;
+  bool have_ts = false;
+  std::string last_error;
+};
+
+int fail(Handle* h, int code, const std::string& msg) {
+  if (h) h->last_error = msg;
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_fail(Handle* h, cudaError_t e, const char* what) {
+  return fail(h, SHIELD_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Microphysics.setupm (pySHiELD/stencils/microphysics.py:1813-1953) and the
+// scalars of __init__ / gfdl_cloud_microphys_init (:1643-1658, :1806-1811).
+void setupm(const ShieldMpConfig& c, MpConst& K) {
+  // physical constants: the values of pyshield_b200/constants.py, with the
+  // derived ones computed by the same formulas
+  K.GRAV = 9.80665;
+  K.RGRAV = 1.0 / K.GRAV;
+  K.RDGAS = 287.05;
+  K.RVGAS = 461.50;
+  K.HLV = 2.5e6;
+  K.HLF = 3.3358e5;
+  K.CP_AIR = 1004.6;
+  K.KAPPA = K.RDGAS / K.CP_AIR;
+  K.CP_VAP = 4.0 * K.RVGAS;
+  K.CV_AIR = K.CP_AIR - K.RDGAS;
+  K.CV_VAP = 3.0 * K.RVGAS;
+  K.C_ICE = 1972.0;
+  K.C_LIQ = 4.1855e3;
+  K.TICE = 273.16;
+  K.E00 = 611.21;
+  K.DC_VAP = K.CP_VAP - K.C_LIQ;
+  K.DC_ICE = K.C_LIQ - K.C_ICE;
+  K.D2ICE = K.DC_VAP + K.DC_ICE;
+  K.LV0 = K.HLV - K.DC_VAP * K.TICE;
+  K.LI00 = K.HLF - K.DC_ICE * K.TICE;
+  K.LI2 = K.LV0 + K.LI00;
+  K.EPS = K.RDGAS / K.RVGAS;
+  K.ZVIR = K.RVGAS / K.RDGAS - 1.0;
+  K.T_MIN = 178.0;
+  K.T_SAT_MIN = K.TICE - 160.0;
+  K.LAT2 = std::pow(K.HLV + K.HLF, 2.0);
+
+  const double RHOS = 1.0e2, RHOG = 4.0e2, RHOR = 1.0e3, SFCRHO = 1.2;
+  const double gam263 = 1.456943, gam275 = 1.608355, gam290 = 1.827363, gam325 = 2.54925, gam350 = 3.323363,
+               gam380 = 4.694155;
+  const double rnzs = 3.0e6, rnzr = 8.0e6, rnzg = 4.0e6;
+  const double acc[3] = {5.0, 2.0, 0.5};
+  const double pie = 4.0 * std::atan(1.0);
+  const double fac_rc = (4.0 / 3.0) * pie * RHOR * std::pow(c.rthresh, 3.0);
+  const double vdifu = 2.11e-5, tcond = 2.36e-2, visk = 1.259e-5, hlts = 2.8336e6, hltc = 2.5e6, hltf = 3.336e5,
+               ch2o = 4.1855e3;
+  const double pisq = pie * pie;
+  const double scm3 = std::pow(visk / vdifu, 1.0 / 3.0);
+  K.cracs = pisq * rnzr * rnzs * RHOS;
+  K.csacr = pisq * rnzr * rnzs * RHOR;
+  K.cgacr = pisq * rnzr * rnzg * RHOR;
+  K.cgacs = pisq * rnzg * rnzs * RHOS;
+  K.cgacs = K.cgacs * c.c_pgacs;
+  double act[8];
+  act[0] = pie * rnzs * RHOS;
+  act[1] = pie * rnzr * RHOR;
+  act[5] = pie * rnzg * RHOG;
+  act[2] = act[1];
+  act[3] = act[0];
+  act[4] = act[1];
+  act[6] = act[0];
+  act[7] = act[5];
+  for (int i = 0; i < 3; ++i)
+    for (int k = 0; k < 4; ++k)
+      K.acco[i][k] =
+          acc[i] / (std::pow(act[2 * k], (6 - i) * 0.25) * std::pow(act[2 * k + 1], (i + 1) * 0.25));
+  const double gcon = 40.74 * std::sqrt(SFCRHO);
+  K.csacw = pie * rnzs * c.clin * gam325 / (4.0 * std::pow(act[0], 0.8125));
+  const double craci = pie * rnzr * c.alin * gam380 / (4.0 * std::pow(act[1], 0.95));
+  K.csaci = K.csacw * c.c_psaci;
+  K.cgacw = pie * rnzg * gam350 * gcon / (4.0 * std::pow(act[5], 0.875));
+  K.cgaci = K.cgacw * 0.05;
+  K.cracw = c.c_cracw * craci;
+  K.cssub[0] = 2.0 * pie * vdifu * tcond * K.RVGAS * rnzs;
+  K.cssub[1] = 0.78 / std::sqrt(act[0]);
+  K.cssub[2] = 0.31 * scm3 * gam263 * std::sqrt(c.clin / visk) / std::pow(act[0], 0.65625);
+  K.cssub[3] = tcond * K.RVGAS;
+  K.cssub[4] = std::pow(hlts, 2.0) * vdifu;
+  const double cgsub_1 = 0.78 / std::sqrt(act[5]);
+  const double cgsub_2 = 0.31 * scm3 * gam275 * std::sqrt(gcon / visk) / std::pow(act[5], 0.6875);
+  K.crevp[0] = 2.0 * pie * vdifu * tcond * K.RVGAS * rnzr;
+  K.crevp[1] = 0.78 / std::sqrt(act[1]);
+  K.crevp[2] = 0.31 * scm3 * gam290 * std::sqrt(c.alin / visk) / std::pow(act[1], 0.725);
+  K.crevp[3] = K.cssub[3];
+  K.crevp[4] = std::pow(hltc, 2.0) * vdifu;
+  K.cgfr[0] = 20.0e2 * pisq * rnzr * RHOR / std::pow(act[1], 1.75);
+  K.cgfr[1] = 0.66;
+  K.csmlt[0] = 2.0 * pie * tcond * rnzs / hltf;
+  K.csmlt[1] = 2.0 * pie * vdifu * rnzs * hltc / hltf;
+  K.csmlt[2] = K.cssub[1];
+  K.csmlt[3] = K.cssub[2];
+  K.csmlt[4] = ch2o / hltf;
+  K.cgmlt[0] = 2.0 * pie * tcond * rnzg / hltf;
+  K.cgmlt[1] = 2.0 * pie * vdifu * rnzg * hltc / hltf;
+  K.cgmlt[2] = cgsub_1;
+  K.cgmlt[3] = cgsub_2;
+  K.cgmlt[4] = ch2o / hltf;
+  const double es0 = 6.107799961e2;
+  K.fac_rc = fac_rc;
+  K.ces0 = K.EPS * es0;
+  K.iqs_lo_num = K.E00 * std::exp((K.D2ICE * std::log(1.0 - 160.0 / K.TICE) - K.LI2 * 160.0 / (K.T_SAT_MIN * K.TICE)) /
+                                  K.RVGAS);
+  K.log_10 = std::log(10.0);
+  K.tice0 = c.tice - 0.01;
+  K.t_wfr = c.tice - 40.0;
+  K.c_air = K.CP_AIR;
+  K.c_vap = K.CP_VAP;
+  K.d0_vap = K.c_vap - K.C_LIQ;
+  K.lv00 = K.HLV - K.d0_vap * K.TICE;
+  K.cpaut = c.c_paut * 0.104 * K.GRAV / 1.717e-5;
+  K.so3 = 7.0 / 3.0;
+  K.zs = 0.0;
+  // namelist values baked in as stencil externals
+  K.tice = c.tice;
+  K.ql_mlt = c.ql_mlt;
+  K.qs_mlt = c.qs_mlt;
+  K.t_sub = c.t_sub;
+  K.qi_gen = c.qi_gen;
+  K.qi_lim = c.qi_lim;
+  K.qi0_max = c.qi0_max;
+  K.dw_ocean = c.dw_ocean;
+  K.dw_land = c.dw_land;
+  K.qc_crt = c.qc_crt;
+  K.qi0_crt = c.qi0_crt;
+  K.qs0_crt = c.qs0_crt;
+  K.rh_inc = c.rh_inc;
+  K.rh_inr = c.rh_inr;
+  K.vi_fac = c.vi_fac;
+  K.vs_fac = c.vs_fac;
+  K.vg_fac = c.vg_fac;
+  K.vr_fac = c.vr_fac;
+  K.vi_max = c.vi_max;
+  K.vs_max = c.vs_max;
+  K.vg_max = c.vg_max;
+  K.vr_max = c.vr_max;
+  K.ccn_l = c.ccn_l;
+  K.ccn_o = c.ccn_o;
+  K.do_qa = c.do_qa != 0;
+  K.const_vg = c.const_vg != 0;
+  K.const_vi = c.const_vi != 0;
+  K.const_vr = c.const_vr != 0;
+  K.const_vs = c.const_vs != 0;
+  K.rad_snow = c.rad_snow != 0;
+  K.rad_rain = c.rad_rain != 0;
+  K.do_sedi_heat = c.do_sedi_heat != 0;
+  K.do_sedi_w = c.hydrostatic ? 0 : (c.do_sedi_w != 0);
+  K.fast_sat_adj = c.fast_sat_adj != 0;
+  K.fix_negative = c.fix_negative != 0;
+  K.irain_f = c.irain_f;
+  K.prog_ccn = c.prog_ccn != 0;
+  K.use_ccn = c.prog_ccn ? 0 : 1;
+  K.sedi_transport = c.sedi_transport != 0;
+  K.z_slope_ice = c.z_slope_ice != 0;
+  K.z_slope_liq = c.z_slope_liq != 0;
+  K.de_ice = c.de_ice != 0;
+}
+
+// Microphysics._set_timestep (microphysics.py:1964-1979).
+int set_timestep(const ShieldMpConfig& c, MpConst& K, double timestep, std::string& why) {
+  if (!(timestep > 0.0) || !std::isfinite(timestep)) {
+    why = "timestep must be positive and finite";
+    return SHIELD_EINVAL;
+  }
+  const double mpdt = std::fmin(timestep, c.mp_time);
+  if (!(mpdt > 0.0)) {
+    why = "mp_time must be positive";
+    return SHIELD_EINVAL;
+  }
+  K.rdt = 1.0 / timestep;
+  // Python's round(): halves go to the even neighbour, as nearbyint does in
+  // the default rounding mode
+  const double nt = std::nearbyint(timestep / mpdt);
+  if (nt < 1.0 || nt > 1.0e6) {
+    why = "timestep / mp_time gives an unusable number of sub-steps";
+    return SHIELD_EINVAL;
+  }
+  K.ntimes = (int)nt;
+  K.timestep = timestep;
+  K.dts = timestep / K.ntimes;
+  K.dt_rain = K.dts * 0.5;
+  K.rdts = 1.0 / K.dts;
+  K.dt_evap = c.fast_sat_adj ? 0.5 * K.dts : K.dts;
+  K.fac_i2s = 1.0 - std::exp(-K.dts / c.tau_i2s);
+  K.fac_g2v = 1.0 - std::exp(-K.dts / c.tau_g2v);
+  K.fac_v2g = 1.0 - std::exp(-K.dts / c.tau_v2g);
+  K.fac_imlt = 1.0 - std::exp(-0.5 * K.dts / c.tau_imlt);
+  K.fac_l2v = 1.0 - std::exp(-K.dt_evap / c.tau_l2v);
+  return SHIELD_OK;
+}
+
+Fld3 f3(const ShieldField3D& f) { return Fld3{f.ptr, f.si, f.sj, f.sk}; }
+
+}  // namespace
+
+extern "C" int shield_mp_create(const ShieldMpConfig* cfg, int nx, int ny, int nz, ShieldField2D area,
+                                void** handle) {
+  if (!cfg || !handle) return fail(nullptr, SHIELD_EINVAL, "null config or handle pointer");
+  *handle = nullptr;
+  if (nx < 1 || ny < 1) return fail(nullptr, SHIELD_EINVAL, "nx and ny must be positive");
+  if (nz < 3 || nz > mp_max_levels()) return fail(nullptr, SHIELD_ELAYOUT, "nz must lie in [3, 256]");
+  if (cfg->use_ppm) return fail(nullptr, SHIELD_EINVAL, "use_ppm=True is not supported (incomplete in the reference)");
+  if (!area.ptr) return fail(nullptr, SHIELD_EINVAL, "null area pointer");
+  Handle* h = new Handle();
+  h->cfg = *cfg;
+  h->nx = nx;
+  h->ny = ny;
+  h->nz = nz;
+  h->ncol = (int64_t)nx * ny;
+  cudaError_t e = cudaGetDevice(&h->device);
+  if (e != cudaSuccess) {
+    int rc = cuda_fail(h, e, "cudaGetDevice");
+    delete h;
+    return rc;
+  }
+  setupm(*cfg, h->K);
+  std::string why;
+  if (set_timestep(*cfg, h->K, cfg->dt_atmos, why) != SHIELD_OK) {
+    delete h;
+    return fail(nullptr, SHIELD_EINVAL, "dt_atmos: " + why);
+  }
+  h->have_ts = true;
+  const size_t qbytes = sizeof(double) * (size_t)h->ncol * nz;
+  if ((e = cudaMalloc(&h->qaz, qbytes)) != cudaSuccess || (e = cudaMemset(h->qaz, 0, qbytes)) != cudaSuccess ||
+      (e = cudaMalloc(&h->area, sizeof(double) * h->ncol)) != cudaSuccess ||
+      (e = cudaMalloc(&h->err, sizeof(int))) != cudaSuccess || (e = cudaMemset(h->err, 0, sizeof(int))) != cudaSuccess) {
+    int rc = cuda_fail(nullptr, e, "allocating handle state");
+    cudaFree(h->qaz);
+    cudaFree(h->area);
+    cudaFree(h->err);
+    delete h;
+    return rc;
+  }
+  e = mp_gather_area(area.ptr, area.si, area.sj, nx, ny, h->area);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    int rc = cuda_fail(nullptr, e, "copying area");
+    cudaFree(h->qaz);
+    cudaFree(h->area);
+    cudaFree(h->err);
+    delete h;
+    return rc;
+  }
+  *handle = h;
+  return SHIELD_OK;
+}
+
+extern "C" int shield_mp_step(void* handle, const ShieldMpFields* F, double timestep, int precision, void* stream) {
+  Handle* h = static_cast<Handle*>(handle);
+  if (!h) return fail(nullptr, SHIELD_EINVAL, "null handle");
+  if (!F) return fail(h, SHIELD_EINVAL, "null fields");
+  if (precision != SHIELD_MP_PLAIN && precision != SHIELD_MP_MIXED)
+    return fail(h, SHIELD_EINVAL, "unknown precision mode");
+  if (timestep != h->K.timestep) {
+    std::string why;
+    MpConst K2 = h->K;
+    if (set_timestep(h->cfg, K2, timestep, why) != SHIELD_OK) return fail(h, SHIELD_EINVAL, why);
+    h->K = K2;
+  }
+  const ShieldField3D* ins[] = {&F->pt, &F->qvapor, &F->qliquid, &F->qrain, &F->qice, &F->qsnow, &F->qgraupel,
+                                &F->qcld, &F->ua, &F->va, &F->delprsi, &F->delz, &F->wmp};
+  const ShieldField3D* outs[] = {&F->pt_dt, &F->qv_dt, &F->ql_dt, &F->qr_dt, &F->qi_dt,
+                                 &F->qs_dt, &F->qg_dt, &F->qa_dt, &F->udt,   &F->vdt};
+  MpArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.K = h->K;
+  A.nx = h->nx;
+  A.ny = h->ny;
+  A.nz = h->nz;
+  A.ncol = h->ncol;
+  for (int f = 0; f < 13; ++f) {
+    if (!ins[f]->ptr) return fail(h, SHIELD_EINVAL, "null input field pointer");
+    A.in[f] = f3(*ins[f]);
+  }
+  const Fld3 qaz{h->qaz, 1, h->nx, h->ncol};
+  A.in[IN_QAZ] = qaz;
+  for (int o = 0; o < 10; ++o) {
+    if (!outs[o]->ptr) return fail(h, SHIELD_EINVAL, "null tendency pointer");
+    A.out[o] = f3(*outs[o]);
+  }
+  A.out[OUT_W] = A.in[IN_W];
+  A.out[OUT_QAZ] = qaz;
+  if (!F->land.ptr) return fail(h, SHIELD_EINVAL, "null land pointer");
+  A.land = Fld2{F->land.ptr, F->land.si, F->land.sj};
+  A.area = Fld2{h->area, 1, h->nx};
+  A.rain = F->rain;
+  A.snow = F->snow;
+  A.ice = F->ice;
+  A.graupel = F->graupel;
+  A.err = h->err;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaSuccess;
+  if (h->K.de_ice) {
+    e = mp_launch_de_ice(A, f3(F->qi_dt), f3(F->qs_dt), st);
+    if (e != cudaSuccess) return cuda_fail(h, e, "de_ice launch");
+  }
+  e = mp_launch_step(A, precision, st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "microphysics launch");
+  return SHIELD_OK;
+}
+
+extern "C" int shield_mp_destroy(void* handle) {
+  Handle* h = static_cast<Handle*>(handle);
+  if (!h) return SHIELD_OK;
+  cudaFree(h->qaz);
+  cudaFree(h->area);
+  cudaFree(h->err);
+  delete h;
+  return SHIELD_OK;
+}
+
+extern "C" int shield_mp_last_error(void* handle, char* buf, size_t n) {
+  Handle* h = static_cast<Handle*>(handle);
+  const std::string& m = h ? h->last_error : g_last_error;
+  if (buf && n) {
+    std::strncpy(buf, m.c_str(), n - 1);
+    buf[n - 1] = 0;
+  }
+  return SHIELD_OK;
+}
+
+extern "C" int shield_last_error(char* buf, size_t n) {
+  if (buf && n) {
+    std::strncpy(buf, g_last_error.c_str(), n - 1);
+    buf[n - 1] = 0;
+  }
+  return SHIELD_OK;
+}
+
+extern "C" int shield_mp_constants(void* handle, double timestep, double* out, int n) {
+  Handle* h = static_cast<Handle*>(handle);
+  if (!h || !out) return SHIELD_EINVAL;
+  MpConst K = h->K;
+  std::string why;
+  if (set_timestep(h->cfg, K, timestep, why) != SHIELD_OK) return fail(h, SHIELD_EINVAL, why);
+  const double* src = reinterpret_cast<const double*>(&K);
+  // the leading block of doubles, up to the first int member (ntimes)
+  const int nd = (int)(offsetof(MpConst, ntimes) / sizeof(double));
+  const int m = n < nd ? n : nd;
+  std::memcpy(out, src, sizeof(double) * m);
+  return m;
+}
+
+extern "C" int shield_mp_get_qaz(void* handle, double* qaz, void* stream) {
+  Handle* h = static_cast<Handle*>(handle);
+  if (!h || !qaz) return fail(h, SHIELD_EINVAL, "null argument");
+  cudaError_t e = cudaMemcpyAsync(qaz, h->qaz, sizeof(double) * h->ncol * h->nz, cudaMemcpyDeviceToDevice,
+                                  static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? SHIELD_OK : cuda_fail(h, e, "copying qaz");
+}
+
+extern "C" int shield_mp_set_qaz(void* handle, const double* qaz, void* stream) {
+  Handle* h = static_cast<Handle*>(handle);
+  if (!h || !qaz) return fail(h, SHIELD_EINVAL, "null argument");
+  cudaError_t e = cudaMemcpyAsync(h->qaz, qaz, sizeof(double) * h->ncol * h->nz, cudaMemcpyDeviceToDevice,
+                                  static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? SHIELD_OK : cuda_fail(h, e, "copying qaz");
+}

@@ -1,0 +1,15 @@
+// Launch entry points of the microphysics kernels (host side).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "mp_params.h"
+
+namespace shield {
+
+int mp_max_levels();
+cudaError_t mp_launch_step(const MpArgs& A, int precision, cudaStream_t st);
+cudaError_t mp_launch_de_ice(const MpArgs& A, Fld3 qi_dt, Fld3 qs_dt, cudaStream_t st);
+cudaError_t mp_gather_area(const double* p, int64_t si, int64_t sj, int nx, int ny, double* out);
+
+}  // namespace shield

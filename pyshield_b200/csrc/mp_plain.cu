@@ -1,0 +1,60 @@
+// Plain FP64 form of the microphysics step. Compiled with -fmad=false so
+// that every multiply and add rounds as the reference's numpy expressions do.
+#include "mp_kernel.cuh"
+#include "mp_launch.h"
+
+namespace shield {
+
+namespace {
+
+constexpr int kCPB = 4;  // columns (warps) per block
+
+template <int P>
+cudaError_t launch_p(const MpArgs& A, cudaStream_t st) {
+  const size_t smem = sizeof(double) * (size_t)N_IN * kCPB * Lev<P>::ROW;
+  cudaError_t e = cudaFuncSetAttribute(mp_step_kernel<P, kCPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int64_t nblk = (A.ncol + kCPB - 1) / kCPB;
+  mp_step_kernel<P, kCPB><<<(unsigned)nblk, kCPB * 32, smem, st>>>(A);
+  return cudaGetLastError();
+}
+
+__global__ void gather2d(const double* p, int64_t si, int64_t sj, int nx, int64_t n, double* out) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x)
+    out[c] = p[(c % nx) * si + (c / nx) * sj];
+}
+
+}  // namespace
+
+int mp_max_levels() { return 256; }
+
+cudaError_t mp_launch_plain(const MpArgs& A, cudaStream_t st) {
+  const int L = A.nz;
+  if (L <= 64) return launch_p<2>(A, st);
+  if (L <= 96) return launch_p<3>(A, st);
+  if (L <= 128) return launch_p<4>(A, st);
+  return launch_p<8>(A, st);
+}
+
+cudaError_t mp_launch_mixed(const MpArgs& A, cudaStream_t st);
+
+cudaError_t mp_launch_step(const MpArgs& A, int precision, cudaStream_t st) {
+  if (precision == 1) return mp_launch_mixed(A, st);
+  return mp_launch_plain(A, st);
+}
+
+cudaError_t mp_launch_de_ice(const MpArgs& A, Fld3 qi_dt, Fld3 qs_dt, cudaStream_t st) {
+  const int64_t n = A.ncol * (int64_t)A.nz;
+  const int64_t nb = (n + 255) / 256;
+  de_ice_kernel<<<(unsigned)(nb < 148 * 16 ? nb : 148 * 16), 256, 0, st>>>(A, qi_dt, qs_dt);
+  return cudaGetLastError();
+}
+
+cudaError_t mp_gather_area(const double* p, int64_t si, int64_t sj, int nx, int ny, double* out) {
+  const int64_t n = (int64_t)nx * ny;
+  const int64_t nb = (n + 255) / 256;
+  gather2d<<<(unsigned)(nb < 4096 ? nb : 4096), 256>>>(p, si, sj, nx, n, out);
+  return cudaGetLastError();
+}
+
+}  // namespace shield

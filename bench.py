@@ -149,7 +149,7 @@ def peaks():
 
 
 # ------------------------------------------------------------ GPU arm
-def build_state(nlev, device, seed):
+def build_state(nlev, device, seed, n_cube=N_CUBE):
     """Synthetic C96 state as NDSL-layout torch storages on ``device``."""
     import numpy as np
     import torch
@@ -159,9 +159,9 @@ def build_state(nlev, device, seed):
     from pyshield_b200.microphysics import MicrophysicsState
     from pyshield_b200.quantity import Quantity
 
-    nx, ny = N_CUBE, 6 * N_CUBE  # the six tiles side by side
+    nx, ny = n_cube, 6 * n_cube  # the six tiles side by side
     n = nx * ny
-    state, area = make_state(n, nlev, seed=seed, n_cube=N_CUBE)
+    state, area = make_state(n, nlev, seed=seed, n_cube=n_cube)
     gi = GridIndexing(nx, ny, nlev, HALO)
     qf = QuantityFactory(gi, device=device)
     host = {}
@@ -199,7 +199,7 @@ def run_ours(args, rank, world, local_rank):
     device = torch.device("cuda", local_rank)
     torch.cuda.set_device(device)
     nlev = args.levels
-    ms, sf, qf, gd, host, land, (nx, ny, n) = build_state(nlev, device, seed=1234 + rank)
+    ms, sf, qf, gd, host, land, (nx, ny, n) = build_state(nlev, device, seed=1234 + rank, n_cube=args.ncube)
     cfg = PhysicsConfig(dt_atmos=DT)
     mp = Microphysics(sf, qf, gd, cfg, precision=args.form)
     stream = torch.cuda.current_stream()
@@ -256,6 +256,15 @@ def run_ours(args, rank, world, local_rank):
         h_precip.copy_(mp._precip, non_blocking=True)
 
     e2e_steps = max(2, min(args.steps, 5))
+    if args.no_e2e:
+        e2e_steps = 0
+        times = torch.tensor([total_ms, 0.0, mean_launch_ms], dtype=torch.float64, device=device)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.all_reduce(times, op=dist.ReduceOp.MAX)
+        return {"n": n, "nlev": nlev, "total_ms": times[0].item(), "mean_launch_ms": times[2].item(), "e2e_ms": 0.0,
+                "e2e_steps": 0, "h2d": h2d, "d2h": d2h, "clocks": clk}
     e2e_step()
     torch.cuda.synchronize()
     barrier()
@@ -301,6 +310,8 @@ def main():
     ap.add_argument("--levels", type=int, default=79)
     ap.add_argument("--form", default="plain", choices=["plain", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--ncube", type=int, default=N_CUBE, help="cube size N of the CN workload (default 96)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -310,9 +321,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     cores = os.cpu_count() or 1
     nlev = args.levels
-    ncol = 6 * N_CUBE * N_CUBE
+    ncol = 6 * args.ncube * args.ncube
     config = {
-        "workload": f"GFDL microphysics step, C{N_CUBE} ({ncol} columns) x L{nlev}, dt {DT:g} s",
+        "workload": f"GFDL microphysics step, C{args.ncube} ({ncol} columns) x L{nlev}, dt {DT:g} s",
         "columns_per_gpu": ncol,
         "levels": nlev,
         "dt_s": DT,
@@ -382,7 +393,7 @@ def main():
     bytes_launch = algorithmic_bytes_per_column_step(nlev) * r["n"]
     achieved = bytes_launch / (r["mean_launch_ms"] / 1000.0) / 1e9
     peak, peak_kind = peaks()
-    e2e_value = world * r["n"] * r["e2e_steps"] / (r["e2e_ms"] / 1000.0)
+    e2e_value = world * r["n"] * r["e2e_steps"] / (r["e2e_ms"] / 1000.0) if r["e2e_ms"] > 0 else None
 
     cpu = None
     if want_cpu:
@@ -408,8 +419,8 @@ def main():
             "dtype": "f64" if args.form == "plain" else "f32+f64",
             "data": "synthetic",
             "config": config,
-            "e2e": {"value": e2e_value, "unit": "column-steps/s", "h2d_bytes_per_step": r["h2d"],
-                    "d2h_bytes_per_step": r["d2h"]},
+            "e2e": ({"value": e2e_value, "unit": "column-steps/s", "h2d_bytes_per_step": r["h2d"],
+                     "d2h_bytes_per_step": r["d2h"]} if e2e_value else None),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
                          "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",

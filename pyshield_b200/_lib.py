@@ -8,7 +8,7 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libshield_mp.so")
+LIB_PATH = os.environ.get("SHIELD_MP_LIB") or os.path.join(HERE, "libshield_mp.so")
 
 SHIELD_OK = 0
 SHIELD_MP_PLAIN = 0

@@ -47,6 +47,18 @@ constexpr double QVMIN = 1.0e-20;
 
 #define SHD __device__ __forceinline__
 
+// The FP64 exp/log/pow sequences are large; called through these
+// out-of-line wrappers they exist once in the kernel instead of at every one
+// of their call sites, which keeps the kernel within the instruction cache.
+#ifndef SHIELD_INLINE_MATH
+#define SHIELD_MATH_ATTR __device__ __noinline__
+#else
+#define SHIELD_MATH_ATTR __device__ __forceinline__
+#endif
+SHIELD_MATH_ATTR double xexp(double x) { return exp(x); }
+SHIELD_MATH_ATTR double xlog(double x) { return log(x); }
+SHIELD_MATH_ATTR double xpow(double x, double y) { return pow(x, y); }
+
 SHD double dim(double x, double y) {
   double d = x - y;
   return d > 0.0 ? d : 0.0;
@@ -54,8 +66,8 @@ SHD double dim(double x, double y) {
 SHD double sq(double x) { return x * x; }
 
 // ---------------------------------------------------- microphysics_funcs.py:52-145
-SHD double wqs1(const MpConst& K, double ta, double den) {
-  return (K.E00 * exp((K.DC_VAP * log(ta / K.TICE) + K.LV0 * (ta - K.TICE) / (ta * K.TICE)) / K.RVGAS)) /
+SHIELD_MATH_ATTR double wqs1(const MpConst& K, double ta, double den) {
+  return (K.E00 * xexp((K.DC_VAP * xlog(ta / K.TICE) + K.LV0 * (ta - K.TICE) / (ta * K.TICE)) / K.RVGAS)) /
          (K.RVGAS * ta * den);
 }
 SHD double wqs2(const MpConst& K, double ta, double den, double& dqdt) {
@@ -63,10 +75,10 @@ SHD double wqs2(const MpConst& K, double ta, double den, double& dqdt) {
   dqdt = tmp * (K.DC_VAP + K.LV0 / ta) / (K.RVGAS * ta);
   return tmp;
 }
-SHD double iqs1(const MpConst& K, double ta, double den) {
+SHIELD_MATH_ATTR double iqs1(const MpConst& K, double ta, double den) {
   if (ta < K.TICE) {
     if (ta >= K.T_SAT_MIN) {
-      return (K.E00 * exp((K.D2ICE * log(ta / K.TICE) + K.LI2 * (ta - K.TICE) / (ta * K.TICE)) / K.RVGAS)) /
+      return (K.E00 * xexp((K.D2ICE * xlog(ta / K.TICE) + K.LI2 * (ta - K.TICE) / (ta * K.TICE)) / K.RVGAS)) /
              (K.RVGAS * ta * den);
     }
     return K.iqs_lo_num / (K.RVGAS * K.T_SAT_MIN * den);
@@ -100,12 +112,12 @@ SHD R acr3d(R v1, R v2, R q1, R q2, R c, R cac_ik, R cac_i1k, R cac_i2k, R rho) 
 }
 template <typename R>
 SHD R smlt(R tc, R dqs, R qsrho, R psacw, R psacr, R c_0, R c_1, R c_2, R c_3, R c_4, R rho, R rhofac) {
-  return (c_0 * tc / rho - c_1 * dqs) * (c_2 * sqrt(qsrho) + c_3 * pow(qsrho, R(0.65625)) * sqrt(rhofac)) +
+  return (c_0 * tc / rho - c_1 * dqs) * (c_2 * sqrt(qsrho) + c_3 * xpow(qsrho, R(0.65625)) * sqrt(rhofac)) +
          c_4 * tc * (psacw + psacr);
 }
 template <typename R>
 SHD R gmlt(R tc, R dqs, R qgrho, R pgacw, R pgacr, R c_0, R c_1, R c_2, R c_3, R c_4, R rho) {
-  return (c_0 * tc / rho - c_1 * dqs) * (c_2 * sqrt(qgrho) + c_3 * pow(qgrho, R(0.6875)) / pow(rho, R(0.25))) +
+  return (c_0 * tc / rho - c_1 * dqs) * (c_2 * sqrt(qgrho) + c_3 * xpow(qgrho, R(0.6875)) / xpow(rho, R(0.25))) +
          c_4 * tc * (pgacw + pgacr);
 }
 
@@ -139,7 +151,7 @@ SHD void revap_racc(const MpConst& K, double dt, double h_var, double& qg, doubl
         dq = 0.25 * sq(q_minus - qsat) / dqh;
       double qden = qr * den;
       double t2 = tin * tin;
-      double evap = K.crevp[0] * t2 * dq * (K.crevp[1] * sqrt(qden) + K.crevp[2] * exp(0.725 * log(qden))) /
+      double evap = K.crevp[0] * t2 * dq * (K.crevp[1] * sqrt(qden) + K.crevp[2] * xexp(0.725 * xlog(qden))) /
                     (K.crevp[3] * t2 + K.crevp[4] * qsat * den);
       evap = fmin(qr, fmin(dt * evap, dqv / (1.0 + lcpk * dqsdt)));
       qr = qr - evap;
@@ -149,7 +161,7 @@ SHD void revap_racc(const MpConst& K, double dt, double h_var, double& qg, doubl
       tz = tz - evap * lhl / cvm;
     }
     if ((qr > QRMIN) && (ql > 1.0e-6) && (qsat < q_minus)) {
-      double sink = dt * denfac * K.cracw * exp(0.95 * log(qr * den));
+      double sink = dt * denfac * K.cracw * xexp(0.95 * xlog(qr * den));
       sink = sink / (1.0 + sink) * ql;
       ql = ql - sink;
       qr = qr + sink;
@@ -169,8 +181,8 @@ SHD void fall_speed(const MpConst& K, double qg, double qi, double qs, double tk
       vti = VF_MIN;
     } else {
       double tc = tk - K.tice;
-      vti = (3.0 + log(qi * den) / K.log_10) * (tc * (AA * tc + BB) + CC) + DD_FS * tc + EE;
-      vti = vi0 * exp(K.log_10 * vti) * 0.8;
+      vti = (3.0 + xlog(qi * den) / K.log_10) * (tc * (AA * tc + BB) + CC) + DD_FS * tc + EE;
+      vti = vi0 * xexp(K.log_10 * vti) * 0.8;
       vti = fmin(K.vi_max, fmax(VF_MIN, vti));
     }
   }
@@ -180,7 +192,7 @@ SHD void fall_speed(const MpConst& K, double qg, double qi, double qs, double tk
     if (qs < THS) {
       vts = VF_MIN;
     } else {
-      vts = K.vs_fac * VCONS * rhof * exp(0.0625 * log(qs * den / NORMS));
+      vts = K.vs_fac * VCONS * rhof * xexp(0.0625 * xlog(qs * den / NORMS));
       vts = fmin(K.vs_max, fmax(VF_MIN, vts));
     }
   }
@@ -201,7 +213,7 @@ SHD double rain_fspeed(const MpConst& K, double qrz, double den) {
   if (K.const_vr) return K.vr_fac;
   double qden = qrz * den;
   if (qrz < THR) return VR_MIN;
-  double v = K.vr_fac * VCONR * sqrt(fmin(10.0, SFCRHO / den)) * exp(0.2 * log(qden / NORMR));
+  double v = K.vr_fac * VCONR * sqrt(fmin(10.0, SFCRHO / den)) * xexp(0.2 * xlog(qden / NORMR));
   return fmin(K.vr_max, fmax(VR_MIN, v));
 }
 
@@ -213,7 +225,7 @@ SHD void autoconv_no_subgrid_var(const MpConst& K, double& qlz, double& qrz, dou
     double qc = K.use_ccn ? qc0 : qc0 / den;
     double dq = qlz - qc;
     if (dq > 0.0) {
-      double sink = fmin(dq, K.dt_rain * c_praut * den * exp(K.so3 * log(qlz)));
+      double sink = fmin(dq, K.dt_rain * c_praut * den * xexp(K.so3 * xlog(qlz)));
       qlz = qlz - sink;
       qrz = qrz + sink;
     }
@@ -227,7 +239,7 @@ SHD void autoconv_subgrid_var(const MpConst& K, double& qlz, double& qrz, double
     double qc = K.use_ccn ? qc0 : qc0 / den;
     double dq = 0.5 * (qlz + dl - qc);
     if (dq > 0.0) {
-      double sink = fmin(1.0, dq / dl) * K.dt_rain * c_praut * den * exp(K.so3 * log(qlz));
+      double sink = fmin(1.0, dq / dl) * K.dt_rain * c_praut * den * xexp(K.so3 * xlog(qlz));
       qlz = qlz - sink;
       qrz = qrz + sink;
     }
@@ -318,7 +330,7 @@ SHD void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
     dt_pisub = K.dts;
     double tc = tice - tz;
     if ((qlz > QRMIN) && (tc > 0.0)) {
-      double sink = 3.3333e-10 * K.dts * (exp(0.66 * tc) - 1.0) * den * qlz * qlz;
+      double sink = 3.3333e-10 * K.dts * (xexp(0.66 * tc) - 1.0) * den * qlz * qlz;
       sink = fmin(qlz, fmin(tc / icpk, sink));
       qlz = qlz - sink;
       qiz = qiz + sink;
@@ -341,7 +353,7 @@ SHD void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
     double sink = dq / (1.0 + tcpk * dqsdt);
     double pidep;
     if (qiz > QRMIN) {
-      pidep = dt_pisub * dq * 349138.78 * exp(0.875 * log(qiz * den)) /
+      pidep = dt_pisub * dq * 349138.78 * xexp(0.875 * xlog(qiz * den)) /
               (qsi * den * K.LAT2 / (0.0243 * K.RVGAS * sq(tz)) + 4.42478e4);
     } else {
       pidep = 0.0;
@@ -370,7 +382,7 @@ SHD void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
     double dqsdt;
     double qsi = iqs2(K, tz, den, dqsdt);
     double qden = qsz * den;
-    double tmp = exp(0.65625 * log(qden));
+    double tmp = xexp(0.65625 * xlog(qden));
     double tsq = tz * tz;
     double dq = (qsi - qvz) / (1.0 + tcpk * dqsdt);
     double pssub = K.cssub[0] * tsq * (K.cssub[1] * sqrt(qden) + K.cssub[2] * tmp * sqrt(denfac)) /
@@ -483,7 +495,7 @@ SHD void icloud_processes(const MpConst& K, double& qgz, double& qiz, double& ql
     if (qsz > QCMIN) {
       double psacw, psacr, pracs;
       if (qlz > QRMIN) {
-        double factor = denfac * K.csacw * exp(0.8125 * log(qsz * den));
+        double factor = denfac * K.csacw * xexp(0.8125 * xlog(qsz * den));
         psacw = factor / (1.0 + dts * factor) * qlz;
       } else {
         psacw = 0.0;
@@ -535,13 +547,13 @@ SHD void icloud_processes(const MpConst& K, double& qgz, double& qiz, double& ql
     if (qiz > 3.0e-7) {
       double psaci;
       if (qsz > 1.0e-7) {
-        double factor = dts * denfac * K.csaci * exp(0.05 * tc + 0.8125 * log(qsz * den));
+        double factor = dts * denfac * K.csaci * xexp(0.05 * tc + 0.8125 * xlog(qsz * den));
         psaci = factor / (1.0 + factor) * qiz;
       } else {
         psaci = 0.0;
       }
       double qim = K.qi0_crt / den;
-      double tmp = K.const_vi ? K.fac_i2s : K.fac_i2s * exp(0.025 * tc);
+      double tmp = K.const_vi ? K.fac_i2s : K.fac_i2s * xexp(0.025 * tc);
       di = fmax(di, QRMIN);
       double q_plus = qiz + di;
       double psaut;
@@ -572,7 +584,7 @@ SHD void icloud_processes(const MpConst& K, double& qgz, double& qiz, double& ql
         psacr = dts * acr3d<double>(vtsz, vtrz, qrz, qsz, K.csacr, K.acco[0][1], K.acco[1][1], K.acco[2][1], den);
       else
         psacr = 0.0;
-      double pgfr = dts * K.cgfr[0] / den * (exp(-K.cgfr[1] * tc) - 1.0) * exp(1.75 * log(qrz * den));
+      double pgfr = dts * K.cgfr[0] / den * (xexp(-K.cgfr[1] * tc) - 1.0) * xexp(1.75 * xlog(qrz * den));
       double sink = psacr + pgfr;
       double factor = fmin(sink, fmin(qrz, -tc / icpk)) / fmax(sink, QRMIN);
       psacr = factor * psacr;
@@ -596,7 +608,7 @@ SHD void icloud_processes(const MpConst& K, double& qgz, double& qiz, double& ql
         sink = 0.0;
       double qsm = K.qs0_crt / den;
       if (qsz > qsm) {
-        double factor = dts * 1.0e-3 * exp(0.09 * (tz - tice));
+        double factor = dts * 1.0e-3 * xexp(0.09 * (tz - tice));
         sink = sink + factor / (1.0 + factor) * (qsz - qsm);
       }
       sink = fmin(qsz, sink);

@@ -7,15 +7,14 @@ namespace shield {
 
 namespace {
 
-constexpr int kCPB = 4;  // columns (warps) per block
-
-template <int P>
-cudaError_t launch_p(const MpArgs& A, cudaStream_t st) {
-  const size_t smem = sizeof(double) * (size_t)N_IN * kCPB * Lev<P>::ROW;
-  cudaError_t e = cudaFuncSetAttribute(mp_step_kernel<P, kCPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+template <int NW, int G, int MINB>
+cudaError_t launch_nw(const MpArgs& A, cudaStream_t st) {
+  const size_t smem = Smem<NW, G>::bytes;
+  auto kern = mp_step_kernel<NW, G, MINB>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  const int64_t nblk = (A.ncol + kCPB - 1) / kCPB;
-  mp_step_kernel<P, kCPB><<<(unsigned)nblk, kCPB * 32, smem, st>>>(A);
+  const int64_t nblk = (A.ncol + G - 1) / G;
+  kern<<<(unsigned)nblk, 32 * NW * G, smem, st>>>(A);
   return cudaGetLastError();
 }
 
@@ -30,10 +29,11 @@ int mp_max_levels() { return 256; }
 
 cudaError_t mp_launch_plain(const MpArgs& A, cudaStream_t st) {
   const int L = A.nz;
-  if (L <= 64) return launch_p<2>(A, st);
-  if (L <= 96) return launch_p<3>(A, st);
-  if (L <= 128) return launch_p<4>(A, st);
-  return launch_p<8>(A, st);
+  if (L <= 32) return launch_nw<1, 4, 2>(A, st);
+  if (L <= 64) return launch_nw<2, 2, 2>(A, st);
+  if (L <= 96) return launch_nw<3, 2, 2>(A, st);
+  if (L <= 128) return launch_nw<4, 2, 2>(A, st);
+  return launch_nw<8, 1, 2>(A, st);
 }
 
 cudaError_t mp_launch_mixed(const MpArgs& A, cudaStream_t st);

@@ -136,31 +136,39 @@ int shield_mp_set_qaz(void* handle, const double* qaz, void* stream);
 int shield_update_physics_state(int nx, int ny, int nz, const ShieldField3D* state10, const ShieldField3D* tend10,
                                 const ShieldField3D* out10, double dt, void* stream);
 
-/* The column part of UpdateAtmosphereState.__call__ with
- * dycore_only = False and apply_tendencies = True
+/* The column part of UpdateAtmosphereState.__call__
  * (update_atmos_state.py:301-349, fv_update_phys.py:152-188), in the
  * reference's order and on the reference's domains:
- *   fill_gfs_delp(delp, physics_updated_specific_humidity, 1e-9)
- *       on the full (halo) horizontal domain nxf x nyf, nz+1 levels;
+ *   fill_gfs_delp(delp, q, 1e-9) on the full (halo) horizontal domain,
+ *       nz+1 levels; q is physics_updated_specific_humidity, or the dycore
+ *       qvapor with SHIELD_UAS_DYCORE_ONLY (then nothing else runs);
  *   prepare_tendencies_and_update_tracers on the compute domain, nz+1 levels
- *       (levels 0..nz-1 are written);
- *   moist_cv and update_pressure_and_surface_winds on the compute domain,
- *       nz+1 levels.
+ *       (levels 0..nz-1 written), with rdt = 1 / dt_atmos;
+ *   with SHIELD_UAS_APPLY: moist_cv and update_pressure_and_surface_winds on
+ *       the compute domain, nz+1 levels, with the call's dt.
  * The horizontal halo exchange of u_dt/v_dt, AGrid2DGridPhysics and
  * CubedToLatLon are not part of this call.
- * Field order of `f` (ShieldField3D, all with origin at the compute-domain
- * corner; fill_gfs_delp reads and writes `hx` halo points on each side):
- *   0 u_dt 1 v_dt 2 pt_dt 3 u_t1 4 v_t1 5 physics_updated_pt
- *   6 physics_updated_specific_humidity 7 physics_updated_qliquid
- *   8 physics_updated_qrain 9 physics_updated_qsnow 10 physics_updated_qice
- *   11 physics_updated_qgraupel 12 u_t0 (phy ua) 13 v_t0 (phy va)
- *   14 pt_t0 (phy pt) 15 dycore qvapor 16 qliquid 17 qrain 18 qsnow 19 qice
- *   20 qgraupel 21 prsi 22 dycore delp 23 dycore pt 24 pe 25 peln 26 pk
- *   27 dycore ua 28 dycore va
- * 2-D outputs (nx x ny, ShieldField2D with a writable ptr): ps, u_srf, v_srf. */
-int shield_update_atmos_state(int nx, int ny, int nz, int hx, const ShieldField3D* f, ShieldField3D ps,
+ * Every field must provide nz+1 levels; fill_gfs_delp also reads and
+ * writes `hx` halo points on each side of the compute domain.
+ * Field order of `f` (ShieldField3D, origin at the compute-domain corner):
+ *   0 u_dt 1 v_dt 2 pt_dt 3 u_t1 (physics_updated_ua) 4 v_t1
+ *   5 physics_updated_pt 6 physics_updated_specific_humidity
+ *   7 physics_updated_qliquid 8 physics_updated_qrain 9 physics_updated_qsnow
+ *   10 physics_updated_qice 11 physics_updated_qgraupel 12 u_t0 (physics ua)
+ *   13 v_t0 (physics va) 14 pt_t0 (physics pt) 15 dycore qvapor 16 qliquid
+ *   17 qrain 18 qsnow 19 qice 20 qgraupel 21 prsi 22 dycore delp
+ *   23 dycore pt 24 pe 25 peln 26 pk 27 dycore ua 28 dycore va
+ * Outputs ps, u_srf, v_srf: 2-D fields (their sk is ignored). */
+#define SHIELD_UAS_APPLY 1       /* apply_tendencies = True */
+#define SHIELD_UAS_DYCORE_ONLY 2 /* dycore_only = True */
+int shield_update_atmos_state(int nx, int ny, int nz, int hx, int mode, const ShieldField3D* f, ShieldField3D ps,
                               ShieldField3D u_srf, ShieldField3D v_srf, double rdt, double dt, double kappa,
                               double cp_air, void* stream);
+
+/* Test hook: the scalars shield_mp_step uses for `timestep` (physical
+ * constants, setupm constants, sub-step values), computed on the host
+ * without touching the GPU; returns how many doubles were written. */
+int shield_mp_setup_constants(const ShieldMpConfig* cfg, double timestep, double* out, int n);
 
 /* Message of the last failing handle-free call on this host thread. */
 int shield_last_error(char* buf, size_t n);

@@ -113,3 +113,44 @@ def update_pressure_and_surface_winds(pe, delp, peln, pk, kappa, ua, va):
     peln[..., 1:] = np.log(pe[..., 1:])
     pk[..., 1:] = np.exp(kappa * peln[..., 1:])
     return pe[..., nk - 1].copy(), ua[..., nk - 2].copy(), va[..., nk - 2].copy()
+
+
+def update_atmos_state_columns(f, dt, nx, ny, h, dycore_only=False, apply_tendencies=True):
+    """The column part of ``UpdateAtmosphereState.__call__``
+    (update_atmos_state.py:301-349, fv_update_phys.py:170-186), in place on
+    NDSL storages (ni, nj, L+1) keyed as in tests/golden/make_golden.py:
+    ``pu_*`` physics-updated fields, ``ph_*`` physics-state fields, ``dy_*``
+    dycore fields, ``u_dt``/``v_dt``/``pt_dt``, ``prsi``, ``pe``/``peln``/``pk``.
+    fill_gfs_delp runs on the full domain [0, nx+2h) x [0, ny+2h); the others
+    on the compute domain. Returns (ps, u_srf, v_srf) on the compute domain,
+    or None when the tendencies are not applied."""
+    full = (slice(0, nx + 2 * h), slice(0, ny + 2 * h))
+    cd = (slice(h, h + nx), slice(h, h + ny))
+    if dycore_only:
+        q = f["dy_qvapor"][full]
+        fill_gfs_delp(f["dy_delp"][full], q, 1.0e-9)
+    else:
+        q = f["pu_qvapor"][full]
+        fill_gfs_delp(f["dy_delp"][full], q, 1.0e-9)
+        a = {
+            "u_dt": f["u_dt"][cd], "v_dt": f["v_dt"][cd], "pt_dt": f["pt_dt"][cd],
+            "u_t1": f["pu_ua"][cd], "v_t1": f["pu_va"][cd], "physics_updated_pt": f["pu_pt"][cd],
+            "physics_updated_specific_humidity": f["pu_qvapor"][cd],
+            "physics_updated_qliquid": f["pu_qliquid"][cd], "physics_updated_qrain": f["pu_qrain"][cd],
+            "physics_updated_qsnow": f["pu_qsnow"][cd], "physics_updated_qice": f["pu_qice"][cd],
+            "physics_updated_qgraupel": f["pu_qgraupel"][cd],
+            "u_t0": f["ph_ua"][cd], "v_t0": f["ph_va"][cd], "pt_t0": f["ph_pt"][cd],
+            "qvapor_t0": f["dy_qvapor"][cd], "qliquid_t0": f["dy_qliquid"][cd], "qrain_t0": f["dy_qrain"][cd],
+            "qsnow_t0": f["dy_qsnow"][cd], "qice_t0": f["dy_qice"][cd], "qgraupel_t0": f["dy_qgraupel"][cd],
+            "prsi": f["prsi"][cd], "delp": f["dy_delp"][cd],
+        }
+        prepare_tendencies_and_update_tracers(a, 1.0 / dt)
+    if not apply_tendencies:
+        return None
+    moist_cv(
+        f["dy_qvapor"][cd], f["dy_qliquid"][cd], f["dy_qrain"][cd], f["dy_qsnow"][cd], f["dy_qice"][cd],
+        f["dy_qgraupel"][cd], f["dy_pt"][cd], f["pt_dt"][cd], C.CP_AIR, dt,
+    )
+    return update_pressure_and_surface_winds(
+        f["pe"][cd], f["dy_delp"][cd], f["peln"][cd], f["pk"][cd], C.KAPPA, f["dy_ua"][cd], f["dy_va"][cd]
+    )

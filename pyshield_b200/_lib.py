@@ -13,6 +13,8 @@ LIB_PATH = os.environ.get("SHIELD_MP_LIB") or os.path.join(HERE, "libshield_mp.s
 SHIELD_OK = 0
 SHIELD_MP_PLAIN = 0
 SHIELD_MP_MIXED = 1
+SHIELD_UAS_APPLY = 1
+SHIELD_UAS_DYCORE_ONLY = 2
 
 
 class ShieldField3D(ctypes.Structure):
@@ -112,6 +114,7 @@ EXPORTS = (
     "shield_update_physics_state",
     "shield_update_atmos_state",
     "shield_last_error",
+    "shield_mp_setup_constants",
 )
 
 _lib = None
@@ -144,8 +147,9 @@ def load():
         i32, i32, i32, ctypes.POINTER(ShieldField3D), ctypes.POINTER(ShieldField3D), ctypes.POINTER(ShieldField3D), dbl, vp,
     ]
     lib.shield_update_atmos_state.argtypes = [
-        i32, i32, i32, i32, ctypes.POINTER(ShieldField3D), ShieldField3D, ShieldField3D, ShieldField3D, dbl, dbl, dbl, dbl, vp,
+        i32, i32, i32, i32, i32, ctypes.POINTER(ShieldField3D), ShieldField3D, ShieldField3D, ShieldField3D, dbl, dbl, dbl, dbl, vp,
     ]
+    lib.shield_mp_setup_constants.argtypes = [ctypes.POINTER(ShieldMpConfig), dbl, ctypes.POINTER(ctypes.c_double), i32]
     lib.shield_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
     for name in EXPORTS:
         getattr(lib, name).restype = i32

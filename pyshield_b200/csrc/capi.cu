@@ -228,6 +228,11 @@ Fld3 f3(const ShieldField3D& f) { return Fld3{f.ptr, f.si, f.sj, f.sk}; }
 
 }  // namespace
 
+namespace shield {
+// The handle-free calls (coupling kernels) report through here.
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace shield
+
 extern "C" int shield_mp_create(const ShieldMpConfig* cfg, int nx, int ny, int nz, ShieldField2D area,
                                 void** handle) {
   if (!cfg || !handle) return fail(nullptr, SHIELD_EINVAL, "null config or handle pointer");
@@ -370,6 +375,20 @@ extern "C" int shield_mp_constants(void* handle, double timestep, double* out, i
   if (set_timestep(h->cfg, K, timestep, why) != SHIELD_OK) return fail(h, SHIELD_EINVAL, why);
   const double* src = reinterpret_cast<const double*>(&K);
   // the leading block of doubles, up to the first int member (ntimes)
+  const int nd = (int)(offsetof(MpConst, ntimes) / sizeof(double));
+  const int m = n < nd ? n : nd;
+  std::memcpy(out, src, sizeof(double) * m);
+  return m;
+}
+
+extern "C" int shield_mp_setup_constants(const ShieldMpConfig* cfg, double timestep, double* out, int n) {
+  if (!cfg || !out) return fail(nullptr, SHIELD_EINVAL, "null argument");
+  MpConst K;
+  std::memset(&K, 0, sizeof(K));
+  setupm(*cfg, K);
+  std::string why;
+  if (set_timestep(*cfg, K, timestep, why) != SHIELD_OK) return fail(nullptr, SHIELD_EINVAL, why);
+  const double* src = reinterpret_cast<const double*>(&K);
   const int nd = (int)(offsetof(MpConst, ntimes) / sizeof(double));
   const int m = n < nd ? n : nd;
   std::memcpy(out, src, sizeof(double) * m);

@@ -18,9 +18,11 @@
 
 #include "../../include/shield_mp.h"
 
-namespace {
+namespace shield {
+void set_last_error(const std::string& msg);
+}
 
-thread_local std::string g_err;
+namespace {
 
 struct F3 {
   double* p;
@@ -65,7 +67,7 @@ enum {
 struct AtmArgs {
   F3 f[N_ATM];
   F3 ps, us, vs;
-  int nx, ny, nz, hx;
+  int nx, ny, nz, hx, mode;
   double rdt, dt, kappa, cp_air;
   double CV_AIR, CV_VAP, C_LIQ, C_ICE;
 };
@@ -77,8 +79,9 @@ __global__ void update_atmos_state_kernel(const __grid_constant__ AtmArgs A) {
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncf; c += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = c % nxf - A.hx, j = c / nxf - A.hx;
     // ---- fill_gfs_delp(delp, physics_updated_specific_humidity, 1e-9) on the full domain
+    const bool dycore_only = (A.mode & SHIELD_UAS_DYCORE_ONLY) != 0;
     {
-      const F3& q = A.f[PU_QV];
+      const F3& q = dycore_only ? A.f[D_QV] : A.f[PU_QV];
       const F3& dp = A.f[D_DELP];
       const double q_min = 1.0e-9;
       double qn = q.at(i, j, nk - 2);  // BACKWARD interval(0, -2): reads the updated level below
@@ -105,7 +108,7 @@ __global__ void update_atmos_state_kernel(const __grid_constant__ AtmArgs A) {
         q.at(i, j, k) = (qk < 0.0) ? 0.0 : qk;
       }
     }
-    if (i < 0 || j < 0 || i >= A.nx || j >= A.ny) continue;
+    if (dycore_only || i < 0 || j < 0 || i >= A.nx || j >= A.ny) continue;
     // ---- prepare_tendencies_and_update_tracers, interval(0, -1) of nz + 1 levels
     const F3* f = A.f;
     double p_lo = f[PRSI].at(i, j, 0);
@@ -134,6 +137,7 @@ __global__ void update_atmos_state_kernel(const __grid_constant__ AtmArgs A) {
       f[D_QI].at(i, j, k) = qwat_qi / q0;
       f[D_QG].at(i, j, k) = qwat_qg / q0;
     }
+    if (!(A.mode & SHIELD_UAS_APPLY)) continue;
     // ---- moist_cv(dycore q..., dycore pt, t_dt = pt_dt, CP_AIR, dt) on nz + 1 levels
     for (int k = 0; k < nk; ++k) {
       const double ql = f[D_QL].at(i, j, k) + f[D_QR].at(i, j, k);
@@ -170,13 +174,13 @@ extern "C" int shield_update_physics_state(int nx, int ny, int nz, const ShieldF
                                            const ShieldField3D* tend10, const ShieldField3D* out10, double dt,
                                            void* stream) {
   if (!state10 || !tend10 || !out10 || nx < 1 || ny < 1 || nz < 1) {
-    g_err = "shield_update_physics_state: bad arguments";
+    shield::set_last_error("shield_update_physics_state: bad arguments");
     return SHIELD_EINVAL;
   }
   UpdArgs A;
   for (int p = 0; p < 10; ++p) {
     if (!state10[p].ptr || !tend10[p].ptr || !out10[p].ptr) {
-      g_err = "shield_update_physics_state: null field";
+      shield::set_last_error("shield_update_physics_state: null field");
       return SHIELD_EINVAL;
     }
     A.x[p] = mk(state10[p]);
@@ -192,23 +196,23 @@ extern "C" int shield_update_physics_state(int nx, int ny, int nz, const ShieldF
   update_physics_state_kernel<<<grid_for(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(A);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
-    g_err = std::string("shield_update_physics_state: ") + cudaGetErrorString(e);
+    shield::set_last_error(std::string("shield_update_physics_state: ") + cudaGetErrorString(e));
     return SHIELD_ECUDA;
   }
   return SHIELD_OK;
 }
 
-extern "C" int shield_update_atmos_state(int nx, int ny, int nz, int hx, const ShieldField3D* f, ShieldField3D ps,
+extern "C" int shield_update_atmos_state(int nx, int ny, int nz, int hx, int mode, const ShieldField3D* f, ShieldField3D ps,
                                          ShieldField3D u_srf, ShieldField3D v_srf, double rdt, double dt, double kappa,
                                          double cp_air, void* stream) {
   if (!f || nx < 1 || ny < 1 || nz < 2 || hx < 0 || !ps.ptr || !u_srf.ptr || !v_srf.ptr) {
-    g_err = "shield_update_atmos_state: bad arguments";
+    shield::set_last_error("shield_update_atmos_state: bad arguments");
     return SHIELD_EINVAL;
   }
   AtmArgs A;
   for (int p = 0; p < N_ATM; ++p) {
     if (!f[p].ptr) {
-      g_err = "shield_update_atmos_state: null field " + std::to_string(p);
+      shield::set_last_error("shield_update_atmos_state: null field " + std::to_string(p));
       return SHIELD_EINVAL;
     }
     A.f[p] = mk(f[p]);
@@ -220,6 +224,7 @@ extern "C" int shield_update_atmos_state(int nx, int ny, int nz, int hx, const S
   A.ny = ny;
   A.nz = nz;
   A.hx = hx;
+  A.mode = mode;
   A.rdt = rdt;
   A.dt = dt;
   A.kappa = kappa;
@@ -234,7 +239,7 @@ extern "C" int shield_update_atmos_state(int nx, int ny, int nz, int hx, const S
   update_atmos_state_kernel<<<grid_for(ncf, 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(A);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
-    g_err = std::string("shield_update_atmos_state: ") + cudaGetErrorString(e);
+    shield::set_last_error(std::string("shield_update_atmos_state: ") + cudaGetErrorString(e));
     return SHIELD_ECUDA;
   }
   return SHIELD_OK;

@@ -349,6 +349,83 @@ def run_coupling_case(name, nx, ny, L, dt, stress):
     return meta
 
 
+def run_coupling_chain(name, nx, ny, L, dt, seed):
+    """The column part of UpdateAtmosphereState.__call__ with dycore_only=False
+    and apply_tendencies=True (update_atmos_state.py:301-349,
+    fv_update_phys.py:170-186) on one consistent state: fill_gfs_delp on the
+    physics-updated vapour, prepare_tendencies_and_update_tracers, moist_cv
+    and update_pressure_and_surface_winds, each on the domain the reference
+    builds it with."""
+    import pySHiELD.update.fv_update_phys as fvp
+    import pySHiELD.update.update_atmos_state as uas
+    from ndsl.dsl.stencil import GridIndexing, StencilFactory
+
+    import pyshield_b200.constants as C
+
+    rng = np.random.default_rng(seed)
+    gi = GridIndexing(nx, ny, L)
+    sf = StencilFactory(gi)
+    shape = gi.domain_full(add=(1, 1, 1))
+
+    def rnd(lo, hi):
+        return rng.uniform(lo, hi, shape)
+
+    f = {}
+    for nm in ("u_dt", "v_dt", "pt_dt"):
+        f[nm] = rng.normal(0.0, 1e-4, shape)
+    f["pu_ua"] = rnd(-30.0, 30.0)
+    f["pu_va"] = rnd(-30.0, 30.0)
+    f["pu_pt"] = rnd(200.0, 300.0)
+    for nm in ("qvapor", "qliquid", "qrain", "qsnow", "qice", "qgraupel"):
+        f["pu_" + nm] = rnd(0.0, 2e-3)
+        f["dy_" + nm] = rnd(0.0, 2e-3)
+    # a few small / negative vapour values for fill_gfs_delp
+    m = rng.random(shape) < 0.05
+    f["pu_qvapor"][m] = rng.uniform(-2e-6, 2e-9, int(m.sum()))
+    f["ph_ua"] = rnd(-30.0, 30.0)
+    f["ph_va"] = rnd(-30.0, 30.0)
+    f["ph_pt"] = rnd(200.0, 300.0)
+    f["prsi"] = np.cumsum(rnd(50.0, 2000.0), axis=2)
+    f["dy_delp"] = rnd(50.0, 2000.0)
+    f["dy_pt"] = rnd(200.0, 300.0)
+    f["pe"] = np.zeros(shape)
+    f["pe"][..., 0] = 100.0
+    f["peln"] = np.zeros(shape)
+    f["pk"] = np.zeros(shape)
+    f["dy_ua"] = rnd(-30.0, 30.0)
+    f["dy_va"] = rnd(-30.0, 30.0)
+    out = {f"in_{k}": v.copy() for k, v in f.items()}
+    ps = np.zeros(shape[:2])
+    us = np.zeros(shape[:2])
+    vs = np.zeros(shape[:2])
+    fill = sf.from_origin_domain(uas.fill_gfs_delp, origin=gi.origin_full(), domain=gi.domain_full(add=(0, 0, 1)))
+    prep = sf.from_origin_domain(
+        uas.prepare_tendencies_and_update_tracers, origin=gi.origin_compute(), domain=gi.domain_compute(add=(0, 0, 1))
+    )
+    mcv = sf.from_origin_domain(fvp.moist_cv, origin=gi.origin_compute(), domain=gi.domain_compute(add=(0, 0, 1)))
+    ups = sf.from_origin_domain(
+        fvp.update_pressure_and_surface_winds, origin=gi.origin_compute(), domain=gi.domain_compute(add=(0, 0, 1))
+    )
+    fill(f["dy_delp"], f["pu_qvapor"], 1.0e-9)
+    prep(
+        f["u_dt"], f["v_dt"], f["pt_dt"], f["pu_ua"], f["pu_va"], f["pu_pt"],
+        f["pu_qvapor"], f["pu_qliquid"], f["pu_qrain"], f["pu_qsnow"], f["pu_qice"], f["pu_qgraupel"],
+        f["ph_ua"], f["ph_va"], f["ph_pt"],
+        f["dy_qvapor"], f["dy_qliquid"], f["dy_qrain"], f["dy_qsnow"], f["dy_qice"], f["dy_qgraupel"],
+        f["prsi"], f["dy_delp"], 1.0 / dt,
+    )
+    mcv(f["dy_qvapor"], f["dy_qliquid"], f["dy_qrain"], f["dy_qsnow"], f["dy_qice"], f["dy_qgraupel"], f["dy_pt"], f["pt_dt"], C.CP_AIR, dt)
+    ups(f["pe"], f["dy_delp"], f["peln"], f["pk"], C.KAPPA, f["dy_ua"], f["dy_va"], ps, us, vs)
+    for k, v in f.items():
+        out[f"out_{k}"] = v
+    out["out_ps"] = ps
+    out["out_u_srf"] = us
+    out["out_v_srf"] = vs
+    meta = {"name": name, "nx": nx, "ny": ny, "L": L, "dt": dt, "halo": 3}
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), meta=json.dumps(meta), **out)
+    return meta
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("PYSHIELD_REFERENCE", "/root/reference"))
@@ -364,6 +441,11 @@ def main():
         if args.only and args.only != case[0]:
             continue
         meta = run_coupling_case(*case)
+        print("wrote", meta["name"])
+    for case in (("cpl_chain", 6, 5, 20, 225.0, 7),):
+        if args.only and args.only != case[0]:
+            continue
+        meta = run_coupling_chain(*case)
         print("wrote", meta["name"])
 
 

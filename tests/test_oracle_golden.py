@@ -90,3 +90,26 @@ def test_moist_cv_and_pressure_bitexact(name):
     np.testing.assert_array_equal(ps, z["ups_out_ps"][cs])
     np.testing.assert_array_equal(us, z["ups_out_u_srf"][cs])
     np.testing.assert_array_equal(vs, z["ups_out_v_srf"][cs])
+
+
+def test_update_atmos_state_chain_bitexact():
+    """fill_gfs_delp -> prepare_tendencies_and_update_tracers -> moist_cv ->
+    update_pressure_and_surface_winds on one state, as UpdateAtmosphereState
+    runs them."""
+    z, m = load("cpl_chain")
+    nx, ny, h, dt = m["nx"], m["ny"], m["halo"], m["dt"]
+    f = {k[3:]: np.array(z[k]) for k in z.files if k.startswith("in_")}
+    ps, us, vs = OC.update_atmos_state_columns(f, dt, nx, ny, h)
+    full = (slice(0, nx + 2 * h), slice(0, ny + 2 * h))
+    cd = (slice(h, h + nx), slice(h, h + ny))
+    for k, v in f.items():
+        ref = z["out_" + k]
+        if k == "pu_qvapor":
+            np.testing.assert_array_equal(v[full], ref[full], err_msg=k)
+        elif k in ("peln", "pk"):
+            np.testing.assert_array_equal(v[cd][..., 1:], ref[cd][..., 1:], err_msg=k)
+        else:
+            np.testing.assert_array_equal(v[cd], ref[cd], err_msg=k)
+    np.testing.assert_array_equal(ps, z["out_ps"][cd])
+    np.testing.assert_array_equal(us, z["out_u_srf"][cd])
+    np.testing.assert_array_equal(vs, z["out_v_srf"][cd])

@@ -27,11 +27,21 @@ __global__ void gather2d(const double* p, int64_t si, int64_t sj, int nx, int64_
 
 int mp_max_levels() { return 256; }
 
+// Launch shape for 65-96 levels (the common L79 case): columns per block and
+// the minimum resident blocks per SM given to __launch_bounds__ (which caps
+// the registers per thread).
+#ifndef SHIELD_NW3_G
+#define SHIELD_NW3_G 2
+#endif
+#ifndef SHIELD_NW3_MINB
+#define SHIELD_NW3_MINB 2
+#endif
+
 cudaError_t mp_launch_plain(const MpArgs& A, cudaStream_t st) {
   const int L = A.nz;
   if (L <= 32) return launch_nw<1, 4, 2>(A, st);
   if (L <= 64) return launch_nw<2, 2, 2>(A, st);
-  if (L <= 96) return launch_nw<3, 2, 2>(A, st);
+  if (L <= 96) return launch_nw<3, SHIELD_NW3_G, SHIELD_NW3_MINB>(A, st);
   if (L <= 128) return launch_nw<4, 2, 2>(A, st);
   return launch_nw<8, 1, 2>(A, st);
 }

@@ -271,7 +271,7 @@ def run_ours(args, rank, world, local_rank):
 
             dist.all_reduce(times, op=dist.ReduceOp.MAX)
         return {"n": n, "nlev": nlev, "total_ms": times[0].item(), "mean_launch_ms": times[2].item(), "e2e_ms": 0.0,
-                "e2e_steps": 0, "h2d": h2d, "d2h": d2h, "clocks": clk}
+                "e2e_steps": 0, "h2d": h2d, "d2h": d2h, "clocks": clk, "mixed_ms": 0.0}
     e2e_step()
     torch.cuda.synchronize()
     barrier()
@@ -285,13 +285,30 @@ def run_ours(args, rank, world, local_rank):
     barrier()
     e2e_ms = e0.elapsed_time(e1)
 
-    times = torch.tensor([total_ms, e2e_ms, mean_launch_ms], dtype=torch.float64, device=device)
+    # the mixed form on the same state, for the FP64-vs-mixed comparison
+    mixed_ms = 0.0
+    if args.form == "plain" and not args.no_mixed:
+        mpm = Microphysics(sf, qf, gd, cfg, precision="mixed")
+        for _ in range(args.warmup):
+            mpm(ms, DT)
+        torch.cuda.synchronize()
+        m0 = torch.cuda.Event(enable_timing=True)
+        m1 = torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        for _ in range(args.steps):
+            mpm(ms, DT)
+        m1.record(stream)
+        torch.cuda.synchronize()
+        mixed_ms = m0.elapsed_time(m1) / args.steps
+
+    times = torch.tensor([total_ms, e2e_ms, mean_launch_ms, mixed_ms], dtype=torch.float64, device=device)
     if world > 1:
         import torch.distributed as dist
 
         dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    total_ms, e2e_ms, mean_launch_ms = times.tolist()
+    total_ms, e2e_ms, mean_launch_ms, mixed_ms = times.tolist()
     return {
+        "mixed_ms": mixed_ms,
         "n": n,
         "nlev": nlev,
         "total_ms": total_ms,
@@ -318,6 +335,7 @@ def main():
     ap.add_argument("--form", default="plain", choices=["plain", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--ncube", type=int, default=N_CUBE, help="cube size N of the CN workload (default 96)")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -437,6 +455,10 @@ def main():
                          "bytes_per_launch": bytes_launch},
             "cpu_baseline": cpu,
             "gpu_launches": steps,
+            "mixed": ({"value": world * r["n"] / (r["mixed_ms"] / 1000.0), "unit": "column-steps/s",
+                       "ms_per_step": r["mixed_ms"], "speedup_vs_fp64": r["total_ms"] / steps / r["mixed_ms"],
+                       "dtype": "f32 process rates + f64 saturation adjustment, fall and budgets"}
+                      if r["mixed_ms"] > 0 else None),
             "clocks": r["clocks"],
         }
         emit(rec)

@@ -226,6 +226,49 @@ int set_timestep(const ShieldMpConfig& c, MpConst& K, double timestep, std::stri
 
 Fld3 f3(const ShieldField3D& f) { return Fld3{f.ptr, f.si, f.sj, f.sk}; }
 
+// FP32 copies of the constants used by the mixed form's process rates.
+MpConstF to_float(const MpConst& K) {
+  MpConstF F;
+  F.E00 = (float)K.E00;
+  F.DC_VAP = (float)K.DC_VAP;
+  F.LV0 = (float)K.LV0;
+  F.D2ICE = (float)K.D2ICE;
+  F.LI2 = (float)K.LI2;
+  F.RVGAS = (float)K.RVGAS;
+  F.TICE = (float)K.TICE;
+  F.T_SAT_MIN = (float)K.T_SAT_MIN;
+  F.iqs_lo_num = (float)K.iqs_lo_num;
+  F.LAT2 = (float)K.LAT2;
+  F.cracs = (float)K.cracs;
+  F.csacr = (float)K.csacr;
+  F.cgacr = (float)K.cgacr;
+  F.cgacs = (float)K.cgacs;
+  for (int i = 0; i < 3; ++i)
+    for (int k = 0; k < 4; ++k) F.acco[i][k] = (float)K.acco[i][k];
+  F.csacw = (float)K.csacw;
+  F.csaci = (float)K.csaci;
+  F.cgacw = (float)K.cgacw;
+  F.cgaci = (float)K.cgaci;
+  F.cracw = (float)K.cracw;
+  for (int i = 0; i < 5; ++i) {
+    F.cssub[i] = (float)K.cssub[i];
+    F.crevp[i] = (float)K.crevp[i];
+    F.csmlt[i] = (float)K.csmlt[i];
+    F.cgmlt[i] = (float)K.cgmlt[i];
+  }
+  F.cgfr[0] = (float)K.cgfr[0];
+  F.cgfr[1] = (float)K.cgfr[1];
+  F.ces0 = (float)K.ces0;
+  F.log_10 = (float)K.log_10;
+  F.fac_rc = (float)K.fac_rc;
+  F.so3 = (float)K.so3;
+  F.dt_rain = (float)K.dt_rain;
+  F.dts = (float)K.dts;
+  F.rdts = (float)K.rdts;
+  F.fac_i2s = (float)K.fac_i2s;
+  return F;
+}
+
 }  // namespace
 
 namespace shield {
@@ -304,6 +347,7 @@ extern "C" int shield_mp_step(void* handle, const ShieldMpFields* F, double time
   MpArgs A;
   std::memset(&A, 0, sizeof(A));
   A.K = h->K;
+  A.KF = to_float(h->K);
   A.nx = h->nx;
   A.ny = h->ny;
   A.nz = h->nz;

@@ -25,6 +25,7 @@
 #pragma once
 
 #include "mp_physics.cuh"
+#include "mp_physics_mixed.cuh"
 
 namespace shield {
 
@@ -402,12 +403,15 @@ SHD void stage_out(const MpArgs& A, const double* sm, int64_t c0) {
 }
 
 // ------------------------------------------------------------------ kernel
-template <int NW, int G, int MINB>
+// MIXED selects the mixed-precision process rates (mp_physics_mixed.cuh);
+// everything else is shared by both forms.
+template <int NW, int G, int MINB, bool MIXED>
 __global__ void __launch_bounds__(32 * NW * G, MINB) mp_step_kernel(const __grid_constant__ MpArgs A) {
   using SM = Smem<NW, G>;
   constexpr int RP = Tiles<NW>::RP;
   extern __shared__ double sm[];
   const MpConst& K = A.K;
+  const MpConstF& KF = A.KF;
   const int L = A.nz;
   const int tid = threadIdx.x;
   const int g = tid / (32 * NW);
@@ -575,17 +579,28 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) mp_step_kernel(const __grid
         if (!fall) {
           vtr = VF_MIN;
         } else {
-          vtr = rain_fspeed(K, qr, den);
-          revap_racc(K, dt5, h_var, qg, qi, ql, qr, qs, qv, tz, den, denfac);
+          if constexpr (MIXED) {
+            vtr = rain_fspeed_m(K, qr, den);
+            revap_racc_m(K, KF, dt5, h_var, qg, qi, ql, qr, qs, qv, tz, den, denfac);
+          } else {
+            vtr = rain_fspeed(K, qr, den);
+            revap_racc(K, dt5, h_var, qg, qi, ql, qr, qs, qv, tz, den, denfac);
+          }
           const double dm = dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
           m1_rain = implicit_fall<NW>(C, qr, vtr, dz, dp1, valid, K.dt_rain);
           r1 = C.bcast(m1_rain, L - 1);
           if (K.do_sedi_w) w_transport<NW>(C, w, dm, m1_rain, vtr);
           if (K.do_sedi_heat) sedi_heat<NW>(C, K, tz, dz1, dp1, qv, ql, qr, qi, qs, qg, m1_rain, valid, K.C_LIQ);
-          revap_racc(K, dt5, h_var, qg, qi, ql, qr, qs, qv, tz, den, denfac);
+          if constexpr (MIXED)
+            revap_racc_m(K, KF, dt5, h_var, qg, qi, ql, qr, qs, qv, tz, den, denfac);
+          else
+            revap_racc(K, dt5, h_var, qg, qi, ql, qr, qs, qv, tz, den, denfac);
         }
         if (K.irain_f != 0) {
-          autoconv_no_subgrid_var(K, ql, qr, tz, den, ccn, c_praut);
+          if constexpr (MIXED)
+            autoconv_no_subgrid_var_m(K, KF, ql, qr, tz, den, ccn, c_praut);
+          else
+            autoconv_no_subgrid_var(K, ql, qr, tz, den, ccn, c_praut);
         } else {
           double dl;
           if (K.z_slope_liq) {
@@ -594,7 +609,10 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) mp_step_kernel(const __grid
           } else {
             dl = fmax(QVMIN, h_var * ql);
           }
-          autoconv_subgrid_var(K, ql, qr, tz, den, ccn, c_praut, dl);
+          if constexpr (MIXED)
+            autoconv_subgrid_var_m(K, KF, ql, qr, tz, den, ccn, c_praut, dl);
+          else
+            autoconv_subgrid_var(K, ql, qr, tz, den, ccn, c_praut, dl);
         }
         rain = rain + r1;
         m1 = is_first ? m1 + m1_rain : m1 + m1_rain + m1_sol;
@@ -603,7 +621,10 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) mp_step_kernel(const __grid
 
         // ------------------------------------ sedimentation (:657-1217)
         double vti;
-        fall_speed(K, qg, qi, qs, tz, den, vtg, vti, vts);
+        if constexpr (MIXED)
+          fall_speed_m(K, KF, qg, qi, qs, tz, den, vtg, vti, vts);
+        else
+          fall_speed(K, qg, qi, qs, tz, den, vtg, vti, vts);
         m1_sol = 0.0;
         // cloud ice melting at and below the first level warmer than tice (:702-746)
         const int first = C.min_int((valid && tz > K.tice) ? k : (1 << 30));
@@ -695,7 +716,10 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) mp_step_kernel(const __grid
         di = fmax(QVMIN, h_var * qi);
       }
       if (valid) {
-        icloud_processes(K, qg, qi, ql, qr, qs, qv, tz, den, denfac, vtg, vtr, vts, p1, di, q_liq, q_sol, cvm);
+        if constexpr (MIXED)
+          icloud_processes_m(K, KF, qg, qi, ql, qr, qs, qv, tz, den, denfac, vtg, vtr, vts, p1, di, q_liq, q_sol, cvm);
+        else
+          icloud_processes(K, qg, qi, ql, qr, qs, qv, tz, den, denfac, vtg, vtr, vts, p1, di, q_liq, q_sol, cvm);
         subgrid_z_proc(K, h_var, rh_adj, rh_rain, qa, qg, qi, ql, qr, qs, qv, tz, den, denfac, p1);
       }
     }
@@ -761,29 +785,6 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) mp_step_kernel(const __grid
   }
   __syncthreads();
   stage_out<NW, G>(A, sm, c0);
-}
-
-// de_ice (microphysics.py:110-120): applied in place before the step.
-__global__ void de_ice_kernel(const __grid_constant__ MpArgs A, Fld3 qi_dt, Fld3 qs_dt) {
-  const MpConst& K = A.K;
-  const int64_t n = A.ncol * (int64_t)A.nz;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t c = e % A.ncol, k = e / A.ncol;
-    const int64_t i = c % A.nx, j = c / A.nx;
-    double* qi = A.in[IN_QI].p + i * A.in[IN_QI].si + j * A.in[IN_QI].sj + k * A.in[IN_QI].sk;
-    double* qs = A.in[IN_QS].p + i * A.in[IN_QS].si + j * A.in[IN_QS].sj + k * A.in[IN_QS].sk;
-    double* pqi = qi_dt.p + i * qi_dt.si + j * qi_dt.sj + k * qi_dt.sk;
-    double* pqs = qs_dt.p + i * qs_dt.si + j * qs_dt.sj + k * qs_dt.sk;
-    const double qio = *qi - K.timestep * *pqi;
-    const double qin = fmax(qio, K.qi0_max);
-    if (*qi > qin) {
-      *qs = *qs + *qi - qin;
-      *qi = qin;
-      const double dqi = (qin - qio) * K.rdt;
-      *pqs = *pqs + *pqi - dqi;
-      *pqi = dqi;
-    }
-  }
 }
 
 }  // namespace shield

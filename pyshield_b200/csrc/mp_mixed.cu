@@ -1,7 +1,33 @@
-// Mixed-precision form of the microphysics step: not built yet, so the
-// entry point reports that the mode is unavailable.
+// Mixed-precision form of the microphysics step: process rates in FP32,
+// saturation adjustment, sedimentation, precipitation and every state
+// update in FP64 (see mp_physics_mixed.cuh). FMA contraction is allowed here.
+#include "mp_kernel.cuh"
 #include "mp_launch.h"
 
 namespace shield {
-cudaError_t mp_launch_mixed(const MpArgs&, cudaStream_t) { return cudaErrorNotSupported; }
+
+namespace {
+
+template <int NW, int G, int MINB>
+cudaError_t launch_nw(const MpArgs& A, cudaStream_t st) {
+  const size_t smem = Smem<NW, G>::bytes;
+  auto kern = mp_step_kernel<NW, G, MINB, true>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int64_t nblk = (A.ncol + G - 1) / G;
+  kern<<<(unsigned)nblk, 32 * NW * G, smem, st>>>(A);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t mp_launch_mixed(const MpArgs& A, cudaStream_t st) {
+  const int L = A.nz;
+  if (L <= 32) return launch_nw<1, 4, 2>(A, st);
+  if (L <= 64) return launch_nw<2, 2, 2>(A, st);
+  if (L <= 96) return launch_nw<3, 2, 2>(A, st);
+  if (L <= 128) return launch_nw<4, 2, 2>(A, st);
+  return launch_nw<8, 1, 2>(A, st);
+}
+
 }  // namespace shield

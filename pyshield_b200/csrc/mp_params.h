@@ -29,6 +29,13 @@ struct MpConst {
       fix_negative, irain_f, prog_ccn, use_ccn, sedi_transport, z_slope_ice, z_slope_liq, de_ice;
 };
 
+// FP32 copies of the constants the mixed form's process rates use.
+struct MpConstF {
+  float E00, DC_VAP, LV0, D2ICE, LI2, RVGAS, TICE, T_SAT_MIN, iqs_lo_num, LAT2;
+  float cracs, csacr, cgacr, cgacs, acco[3][4], csacw, csaci, cgacw, cgaci, cracw, cssub[5], crevp[5], cgfr[2],
+      csmlt[5], cgmlt[5], ces0, log_10, fac_rc, so3, dt_rain, dts, rdts, fac_i2s;
+};
+
 // A strided 3-D field; ptr addresses the compute-domain origin.
 struct Fld3 {
   double* p;
@@ -52,6 +59,7 @@ enum OutField {
 
 struct MpArgs {
   MpConst K;
+  MpConstF KF;
   int nx, ny, nz;
   int64_t ncol;
   Fld3 in[N_IN];

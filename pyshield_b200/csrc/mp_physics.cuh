@@ -51,7 +51,7 @@ constexpr double QVMIN = 1.0e-20;
 // out-of-line wrappers they exist once in the kernel instead of at every one
 // of their call sites, which keeps the kernel within the instruction cache.
 #ifndef SHIELD_INLINE_MATH
-#define SHIELD_MATH_ATTR __device__ __noinline__
+#define SHIELD_MATH_ATTR static __device__ __noinline__
 #else
 #define SHIELD_MATH_ATTR __device__ __forceinline__
 #endif

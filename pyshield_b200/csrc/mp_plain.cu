@@ -5,12 +5,36 @@
 
 namespace shield {
 
+// de_ice (microphysics.py:110-120): applied in place before the step.
+__global__ void de_ice_kernel(const __grid_constant__ MpArgs A, Fld3 qi_dt, Fld3 qs_dt) {
+  const MpConst& K = A.K;
+  const int64_t n = A.ncol * (int64_t)A.nz;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = e % A.ncol, k = e / A.ncol;
+    const int64_t i = c % A.nx, j = c / A.nx;
+    double* qi = A.in[IN_QI].p + i * A.in[IN_QI].si + j * A.in[IN_QI].sj + k * A.in[IN_QI].sk;
+    double* qs = A.in[IN_QS].p + i * A.in[IN_QS].si + j * A.in[IN_QS].sj + k * A.in[IN_QS].sk;
+    double* pqi = qi_dt.p + i * qi_dt.si + j * qi_dt.sj + k * qi_dt.sk;
+    double* pqs = qs_dt.p + i * qs_dt.si + j * qs_dt.sj + k * qs_dt.sk;
+    const double qio = *qi - K.timestep * *pqi;
+    const double qin = fmax(qio, K.qi0_max);
+    if (*qi > qin) {
+      *qs = *qs + *qi - qin;
+      *qi = qin;
+      const double dqi = (qin - qio) * K.rdt;
+      *pqs = *pqs + *pqi - dqi;
+      *pqi = dqi;
+    }
+  }
+}
+
+
 namespace {
 
 template <int NW, int G, int MINB>
 cudaError_t launch_nw(const MpArgs& A, cudaStream_t st) {
   const size_t smem = Smem<NW, G>::bytes;
-  auto kern = mp_step_kernel<NW, G, MINB>;
+  auto kern = mp_step_kernel<NW, G, MINB, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int64_t nblk = (A.ncol + G - 1) / G;

@@ -313,38 +313,43 @@ struct Smem {
   static constexpr size_t bytes = total * sizeof(double);
 };
 
+// Each thread moves at most one level of each field (32 NW >= L), so all
+// loads of a stage are issued before any store: one memory round trip per
+// stage instead of one per field.
 template <int NW, int G>
 SHD void stage_in(const MpArgs& A, double* sm, int64_t c0) {
   constexpr int RP = Tiles<NW>::RP;
-  constexpr int NT = 32 * NW * G;
   const int L = A.nz;
   const int tid = threadIdx.x;
   // i-fastest fields: consecutive threads take consecutive columns
   const int g = tid % G;
-  const int kk0 = tid / G;
-  constexpr int KSTEP = NT / G;
+  const int k = tid / G;
   const int64_t col = c0 + g;
-  const bool ok = col < A.ncol;
-  const int64_t i = ok ? col % A.nx : 0, j = ok ? col / A.nx : 0;
+  const bool ok = col < A.ncol && k < L;
+  const int64_t i = (col < A.ncol) ? col % A.nx : 0, j = (col < A.ncol) ? col / A.nx : 0;
   // k-fastest fields: consecutive threads take consecutive levels of a column
-  const int gk = tid / (32 * NW), lk = tid % (32 * NW);
+  const int gk = tid / (32 * NW), kk = tid % (32 * NW);
   const int64_t colk = c0 + gk;
-  const bool okk = colk < A.ncol;
-  const int64_t ik = okk ? colk % A.nx : 0, jk = okk ? colk / A.nx : 0;
-#pragma unroll 1
+  const bool okk = colk < A.ncol && kk < L;
+  const int64_t ik = (colk < A.ncol) ? colk % A.nx : 0, jk = (colk < A.ncol) ? colk / A.nx : 0;
+  double v[N_IN];
+#pragma unroll
+  for (int f = 0; f < N_IN; ++f) {
+    const Fld3 F = A.in[f];
+    v[f] = 0.0;
+    if (F.sk == 1) {
+      if (okk) v[f] = F.p[ik * F.si + jk * F.sj + kk];
+    } else if (ok) {
+      v[f] = F.p[i * F.si + j * F.sj + (int64_t)k * F.sk];
+    }
+  }
+#pragma unroll
   for (int f = 0; f < N_IN; ++f) {
     const Fld3 F = A.in[f];
     if (F.sk == 1) {
-      if (okk) {
-        const double* src = F.p + ik * F.si + jk * F.sj;
-        double* dst = sm + (f * G + gk) * RP;
-        for (int k = lk; k < L; k += 32 * NW) dst[k] = src[k];
-      }
+      if (okk) sm[(f * G + gk) * RP + kk] = v[f];
     } else if (ok) {
-      const double* src = F.p + i * F.si + j * F.sj;
-      double* dst = sm + (f * G + g) * RP;
-#pragma unroll 4
-      for (int k = kk0; k < L; k += KSTEP) dst[k] = src[(int64_t)k * F.sk];
+      sm[(f * G + g) * RP + k] = v[f];
     }
   }
 }
@@ -354,51 +359,42 @@ enum OutMode { OM_SKIP = 0, OM_ADD = 1, OM_ADD_K1 = 2, OM_SET = 3 };
 template <int NW, int G>
 SHD void stage_out(const MpArgs& A, const double* sm, int64_t c0) {
   constexpr int RP = Tiles<NW>::RP;
-  constexpr int NT = 32 * NW * G;
   const MpConst& K = A.K;
   const int L = A.nz;
   const int tid = threadIdx.x;
   const int g = tid % G;
-  const int kk0 = tid / G;
-  constexpr int KSTEP = NT / G;
+  const int k = tid / G;
   const int64_t col = c0 + g;
-  const bool ok = col < A.ncol;
-  const int64_t i = ok ? col % A.nx : 0, j = ok ? col / A.nx : 0;
-  const int gk = tid / (32 * NW), lk = tid % (32 * NW);
+  const bool ok = col < A.ncol && k < L;
+  const int64_t i = (col < A.ncol) ? col % A.nx : 0, j = (col < A.ncol) ? col / A.nx : 0;
+  const int gk = tid / (32 * NW), kk = tid % (32 * NW);
   const int64_t colk = c0 + gk;
-  const bool okk = colk < A.ncol;
-  const int64_t ik = okk ? colk % A.nx : 0, jk = okk ? colk / A.nx : 0;
-#pragma unroll 1
+  const bool okk = colk < A.ncol && kk < L;
+  const int64_t ik = (colk < A.ncol) ? colk % A.nx : 0, jk = (colk < A.ncol) ? colk / A.nx : 0;
+  int mode[N_OUT];
+  double* dst[N_OUT];
+  double old[N_OUT];
+#pragma unroll
   for (int o = 0; o < N_OUT; ++o) {
-    int mode = OM_ADD;
-    if (o == OUT_UDT || o == OUT_VDT) mode = K.sedi_transport ? OM_ADD_K1 : OM_SKIP;
-    if (o == OUT_QA_DT && K.do_qa) mode = OM_SET;
-    if (o == OUT_W) mode = K.do_sedi_w ? OM_SET : OM_SKIP;
-    if (o == OUT_QAZ) mode = OM_SET;
-    if (mode == OM_SKIP) continue;
+    int m = OM_ADD;
+    if (o == OUT_UDT || o == OUT_VDT) m = K.sedi_transport ? OM_ADD_K1 : OM_SKIP;
+    if (o == OUT_QA_DT && K.do_qa) m = OM_SET;
+    if (o == OUT_W) m = K.do_sedi_w ? OM_SET : OM_SKIP;
+    if (o == OUT_QAZ) m = OM_SET;
     const Fld3 F = A.out[o];
-    const int kmin = (mode == OM_ADD_K1) ? 1 : 0;
-    if (F.sk == 1) {
-      if (okk) {
-        double* dst = F.p + ik * F.si + jk * F.sj;
-        const double* src = sm + (o * G + gk) * RP;
-        for (int k = lk; k < L; k += 32 * NW) {
-          if (k < kmin) continue;
-          const double v = src[k];
-          dst[k] = (mode == OM_SET) ? v : dst[k] + v;
-        }
-      }
-    } else if (ok) {
-      double* dst = F.p + i * F.si + j * F.sj;
-      const double* src = sm + (o * G + g) * RP;
-#pragma unroll 4
-      for (int k = kk0; k < L; k += KSTEP) {
-        if (k < kmin) continue;
-        const double v = src[k];
-        double* d = dst + (int64_t)k * F.sk;
-        *d = (mode == OM_SET) ? v : *d + v;
-      }
-    }
+    const bool kf = F.sk == 1;
+    const int lev = kf ? kk : k;
+    if (!(kf ? okk : ok) || (m == OM_ADD_K1 && lev < 1)) m = OM_SKIP;
+    mode[o] = m;
+    dst[o] = kf ? F.p + ik * F.si + jk * F.sj + kk : F.p + i * F.si + j * F.sj + (int64_t)k * F.sk;
+    old[o] = (m == OM_ADD || m == OM_ADD_K1) ? *dst[o] : 0.0;
+  }
+#pragma unroll
+  for (int o = 0; o < N_OUT; ++o) {
+    if (mode[o] == OM_SKIP) continue;
+    const bool kf = A.out[o].sk == 1;
+    const double v = kf ? sm[(o * G + gk) * RP + kk] : sm[(o * G + g) * RP + k];
+    *dst[o] = (mode[o] == OM_SET) ? v : old[o] + v;
   }
 }
 

@@ -170,7 +170,7 @@ SHD void autoconv_subgrid_var_m(const MpConst& K, const MpConstF& F, double& qlz
 SHD void icloud_processes_m(const MpConst& K, const MpConstF& F, double& qgz, double& qiz, double& qlz, double& qrz,
                             double& qsz, double qvz, double& tz, double den, double denfac, double vtgz, double vtrz,
                             double vtsz, double p1, double di, double q_liq, double q_sol, double cvm) {
-  const double tice = K.tice, dts = K.dts, rdts = K.rdts;
+  const double tice = K.tice, dts = K.dts;
   const float denf = (float)den, denfacf = (float)denfac, dtsf = F.dts;
   const float vtg = (float)vtgz, vtr = (float)vtrz, vts = (float)vtsz;
   double lhi = K.LI00 + K.DC_ICE * tz;

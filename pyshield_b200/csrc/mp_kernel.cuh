@@ -34,7 +34,7 @@ namespace shield {
 template <int NW>
 struct Tiles {
   static constexpr int RP = 32 * NW + 1;  // doubles per (field, column) row; odd pitch
-  static constexpr int SCR = 4 * NW + 8;  // per-column scratch doubles per parity
+  static constexpr int SCR = 8 * NW + 8;  // per-column scratch doubles per parity
 };
 
 // Vertical operations of one column group. Every thread of the group calls
@@ -188,6 +188,141 @@ struct Column {
     x1 = A1 + B1 * X1;
     x2 = A2 + B2 * X2;
   }
+  // values at levels k - 1 of N fields with one barrier (undefined at k = 0)
+  template <int N>
+  SHD void prevN(const double (&x)[N], double (&px)[N]) {
+#pragma unroll
+    for (int n = 0; n < N; ++n) px[n] = __shfl_up_sync(FULLMASK, x[n], 1);
+    if (NW == 1) return;
+    double* s = slot();
+    if (lane == 31) {
+#pragma unroll
+      for (int n = 0; n < N; ++n) s[N * w + n] = x[n];
+    }
+    sync();
+    if (lane == 0 && w > 0) {
+#pragma unroll
+      for (int n = 0; n < N; ++n) px[n] = s[N * (w - 1) + n];
+    }
+  }
+  // values at levels k - 1 and k + 1 with one barrier
+  SHD void nbrs(double x, double& xp, double& xn) {
+    xp = __shfl_up_sync(FULLMASK, x, 1);
+    xn = __shfl_down_sync(FULLMASK, x, 1);
+    if (NW == 1) return;
+    double* s = slot();
+    if (lane == 0) s[2 * w] = x;
+    if (lane == 31) s[2 * w + 1] = x;
+    sync();
+    if (lane == 0 && w > 0) xp = s[2 * w - 1];
+    if (lane == 31 && w < NW - 1) xn = s[2 * w + 2];
+  }
+  // three column any() flags with one barrier
+  SHD void any3(bool a, bool b, bool c, bool& ra, bool& rb, bool& rc) {
+    const unsigned m = (__any_sync(FULLMASK, a) ? 1u : 0u) | (__any_sync(FULLMASK, b) ? 2u : 0u) |
+                       (__any_sync(FULLMASK, c) ? 4u : 0u);
+    unsigned r = m;
+    if (NW > 1) {
+      double* s = slot();
+      unsigned* su = reinterpret_cast<unsigned*>(s);
+      if (lane == 0) su[w] = m;
+      sync();
+      r = 0;
+#pragma unroll
+      for (int u = 0; u < NW; ++u) r |= su[u];
+    }
+    ra = (r & 1u) != 0;
+    rb = (r & 2u) != 0;
+    rc = (r & 4u) != 0;
+  }
+  // N independent top-down affine scans with one barrier
+  template <int N>
+  SHD void scanN(const double (&a)[N], const double (&b)[N], double (&x)[N]) {
+    double A[N], B[N];
+#pragma unroll
+    for (int n = 0; n < N; ++n) {
+      A[n] = a[n];
+      B[n] = b[n];
+    }
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+#pragma unroll
+      for (int n = 0; n < N; ++n) {
+        const double pA = __shfl_up_sync(FULLMASK, A[n], d);
+        const double pB = __shfl_up_sync(FULLMASK, B[n], d);
+        if (lane >= d) {
+          A[n] = A[n] + B[n] * pA;
+          B[n] = B[n] * pB;
+        }
+      }
+    }
+    if (NW == 1) {
+#pragma unroll
+      for (int n = 0; n < N; ++n) x[n] = A[n];
+      return;
+    }
+    double* s = slot();
+    if (lane == 31) {
+#pragma unroll
+      for (int n = 0; n < N; ++n) {
+        s[2 * N * w + 2 * n] = A[n];
+        s[2 * N * w + 2 * n + 1] = B[n];
+      }
+    }
+    sync();
+#pragma unroll
+    for (int n = 0; n < N; ++n) {
+      double X = 0.0;
+      for (int u = 0; u < w; ++u) X = s[2 * N * u + 2 * n] + s[2 * N * u + 2 * n + 1] * X;
+      x[n] = A[n] + B[n] * X;
+    }
+  }
+  // values of N fields at level k0 with one barrier
+  template <int N>
+  SHD void bcastN(const double (&x)[N], int k0, double (&x0)[N]) {
+    const int w0 = k0 >> 5, l0 = k0 & 31;
+#pragma unroll
+    for (int n = 0; n < N; ++n) x0[n] = __shfl_sync(FULLMASK, x[n], l0);
+    if (NW == 1) return;
+    double* s = slot();
+    if (w == w0 && lane == 0) {
+#pragma unroll
+      for (int n = 0; n < N; ++n) s[n] = x0[n];
+    }
+    sync();
+#pragma unroll
+    for (int n = 0; n < N; ++n) x0[n] = s[n];
+  }
+  // layer thickness from the BACKWARD height sweep with one barrier:
+  // ze_k = zs + sum_{j >= k} (-dz1_j); dz_k = ze_k - ze_{k+1}, dz_{L-1} = ze_{L-1} - zs
+  SHD double heights(double t, double zs) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      double v = __shfl_down_sync(FULLMASK, t, d);
+      if (lane + d < 32) t = t + v;
+    }
+    double zn_in_warp = __shfl_down_sync(FULLMASK, t, 1);  // suffix at k + 1 within the warp
+    double c = 0.0, cn = 0.0;
+    if (NW > 1) {
+      double* s = slot();
+      if (lane == 0) s[w] = t;
+      sync();
+      for (int u = NW - 1; u > w; --u) c = c + s[u];
+      // for lane 31 the level below is lane 0 of warp w + 1: its suffix is
+      // s[w + 1] plus the carry from the warps below it
+      if (lane == 31 && w < NW - 1) {
+        for (int u = NW - 1; u > w + 1; --u) cn = cn + s[u];
+        zn_in_warp = s[w + 1];
+      }
+    }
+    const double ze = zs + (t + c);
+    double zn;
+    if (lane == 31)
+      zn = zs + (zn_in_warp + cn);
+    else
+      zn = zs + (zn_in_warp + c);
+    return (k == L - 1) ? ze - zs : ze - zn;
+  }
   // inclusive sum from the bottom: sum over levels j >= k
   SHD double suffix_sum(double t) {
 #pragma unroll
@@ -204,17 +339,6 @@ struct Column {
     return t + c;
   }
 };
-
-// Layer thickness from the BACKWARD height sweep ze_k = ze_{k+1} - dz1_k,
-// ze_{L-1} = zs - dz1_{L-1}; dz_k = ze_k - ze_{k+1}, dz_{L-1} = ze_{L-1} - zs
-// (microphysics.py:373-380, 445-452, 756-765, 830-837).
-template <int NW>
-SHD double layer_dz(Column<NW>& C, double dz1, bool valid, double zs) {
-  const double S = C.suffix_sum(valid ? -dz1 : 0.0);
-  const double ze = zs + S;
-  const double zn = C.next(ze);
-  return (C.k == C.L - 1) ? ze - zs : ze - zn;
-}
 
 // Implicit upwind fall of one species (use_ppm = False): q is the dry mixing
 // ratio (updated), dtf the fall time step; returns the cumulative mass flux
@@ -243,23 +367,11 @@ SHD double implicit_fall(Column<NW>& C, double& q, double vt, double dz, double 
   return valid ? dd * r : 0.0;
 }
 
-// Vertical-velocity transport by the falling species (microphysics.py:492-515).
-template <int NW>
-SHD void w_transport(Column<NW>& C, double& w, double dm, double flux, double vt) {
-  double fp, vp;
-  C.prev2(flux, vt, fp, vp);
-  if (C.k == 0)
-    w = (dm * w + flux * vt) / (dm - flux);
-  else
-    w = (dm * w - fp * vp + flux * vt) / (dm + fp - flux);
-}
-
 // Implicit heating by falling condensate (microphysics.py:516-557 with
-// C_LIQ, :1176-1217 with C_ICE).
+// C_LIQ, :1176-1217 with C_ICE); fp is the flux at the level above.
 template <int NW>
 SHD void sedi_heat(Column<NW>& C, const MpConst& K, double& tz, double dz1, double dp1, double qv, double ql,
-                   double qr, double qi, double qs, double qg, double flux, bool valid, double c_cond) {
-  const double fp = C.prev(flux);
+                   double qr, double qi, double qs, double qg, double flux, double fp, bool valid, double c_cond) {
   const double dgz = -0.5 * K.GRAV * dz1;
   const double cvn = dp1 * (K.CV_AIR + qv * K.CV_VAP + (qr + ql) * K.C_LIQ + (qi + qs + qg) * K.C_ICE);
   double a, b;
@@ -279,13 +391,21 @@ SHD void sedi_heat(Column<NW>& C, const MpConst& K, double& tz, double dz1, doub
   tz = C.scan_affine(a, b);
 }
 
+// Vertical-velocity update by one falling species given the flux and fall
+// speed at this level and the level above (microphysics.py:492-515).
+SHD double w_update(int k, double w, double dm, double flux, double vt, double fp, double vp) {
+  if (k == 0) return (dm * w + flux * vt) / (dm - flux);
+  return (dm * w - fp * vp + flux * vt) / (dm + fp - flux);
+}
+
 // Monotone vertical slope for autoconversion (microphysics.py:595-620,
-// 1341-1367), before the h_var floor.
+// 1341-1367), before the h_var floor: dq_k = 0.5 (q_k - q_{k-1}).
 template <int NW>
 SHD double mono_slope(Column<NW>& C, double q) {
-  const double qp = C.prev(q);
+  double qp, qn;
+  C.nbrs(q, qp, qn);
   const double dq = 0.5 * (q - qp);
-  const double dqn = C.next(dq);
+  const double dqn = 0.5 * (qn - q);
   double v = 0.0;
   if (C.k >= 1 && C.k <= C.L - 2) {
     v = 0.5 * fmin(fabs(dq + dqn), 0.5 * q);
@@ -566,7 +686,7 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) mp_step_kernel(const __grid
           dz1 = dz0 * tz / t0;
           den = den0 * dz0 / dz1;
           denfac = sqrt(SFCRHO / den);
-          dz = layer_dz<NW>(C, dz1, valid, K.zs);
+          dz = C.heights(valid ? -dz1 : 0.0, K.zs);
         }
         const double dt5 = 0.5 * K.dt_rain;
         double m1_rain = 0.0;
@@ -584,9 +704,12 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) mp_step_kernel(const __grid
           }
           const double dm = dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
           m1_rain = implicit_fall<NW>(C, qr, vtr, dz, dp1, valid, K.dt_rain);
+          double fv[2] = {m1_rain, vtr}, pv[2];
+          C.prevN<2>(fv, pv);
           r1 = C.bcast(m1_rain, L - 1);
-          if (K.do_sedi_w) w_transport<NW>(C, w, dm, m1_rain, vtr);
-          if (K.do_sedi_heat) sedi_heat<NW>(C, K, tz, dz1, dp1, qv, ql, qr, qi, qs, qg, m1_rain, valid, K.C_LIQ);
+          if (K.do_sedi_w) w = w_update(k, w, dm, m1_rain, vtr, pv[0], pv[1]);
+          if (K.do_sedi_heat)
+            sedi_heat<NW>(C, K, tz, dz1, dp1, qv, ql, qr, qi, qs, qg, m1_rain, pv[0], valid, K.C_LIQ);
           if constexpr (MIXED)
             revap_racc_m(K, KF, dt5, h_var, qg, qi, ql, qr, qs, qv, tz, den, denfac);
           else
@@ -643,32 +766,67 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) mp_step_kernel(const __grid
             tz = tz - sink * lhi / cvm;
           }
         }
-        // ice (:773-900)
-        if ((K.vi_fac >= 1.0e-5) && C.any(valid && (qi > QRMIN))) {
-          const double dm = dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
-          const double flux = implicit_fall<NW>(C, qi, vti, dz, dp1, valid, K.dts);
-          m1_sol = flux;
-          if (K.do_sedi_w) w_transport<NW>(C, w, dm, flux, vti);
-          ice = ice + C.bcast(flux, L - 1);
-        }
-        // snow (:902-1035)
-        if (C.any(valid && (qs > QRMIN))) {
-          const double dm = dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
-          const double flux = implicit_fall<NW>(C, qs, vts, dz, dp1, valid, K.dts);
-          m1_sol = m1_sol + flux;
-          if (K.do_sedi_w) w_transport<NW>(C, w, dm, flux, vts);
-          snow = snow + C.bcast(flux, L - 1);
-        }
-        // graupel (:1037-1168)
-        if (C.any(valid && (qg > QRMIN))) {
-          const double dm = dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
-          const double flux = implicit_fall<NW>(C, qg, vtg, dz, dp1, valid, K.dts);
-          m1_sol = m1_sol + flux;
-          if (K.do_sedi_w) w_transport<NW>(C, w, dm, flux, vtg);
-          graupel = graupel + C.bcast(flux, L - 1);
+        // ice (:773-900), snow (:902-1035) and graupel (:1037-1168): their
+        // implicit falls are independent of one another, so the three share
+        // each column exchange; the vertical-velocity updates, which the
+        // reference applies species after species, stay in that order.
+        bool fi, fs, fg;
+        C.any3(valid && (qi > QRMIN), valid && (qs > QRMIN), valid && (qg > QRMIN), fi, fs, fg);
+        fi = fi && (K.vi_fac >= 1.0e-5);
+        double mp = 0.0;  // m1_sol at the level above, for the heating
+        if (fi || fs || fg) {
+          const double dd[3] = {K.dts * vti, K.dts * vts, K.dts * vtg};
+          double ddp[3];
+          C.prevN<3>(dd, ddp);
+          const double qq[3] = {qi, qs, qg};
+          double ra[3], rb[3], r[3];
+#pragma unroll
+          for (int n = 0; n < 3; ++n) {
+            const double qmass = valid ? qq[n] * dp1 : 0.0;
+            const double D = dz + dd[n];
+            ra[n] = qmass / D;
+            rb[n] = (k == 0) ? 0.0 : ddp[n] / D;
+            if (!valid) {
+              ra[n] = 0.0;
+              rb[n] = 0.0;
+            }
+          }
+          C.scanN<3>(ra, rb, r);
+          double flux[3];
+#pragma unroll
+          for (int n = 0; n < 3; ++n) flux[n] = valid ? dd[n] * r[n] : 0.0;
+          const double dm_i = dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
+          if (fi && valid) qi = r[0] * dz / dp1;
+          const double dm_s = dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
+          if (fs && valid) qs = r[1] * dz / dp1;
+          const double dm_g = dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
+          if (fg && valid) qg = r[2] * dz / dp1;
+          double sfc[3];
+          C.bcastN<3>(flux, L - 1, sfc);
+          const double nv[6] = {flux[0], vti, flux[1], vts, flux[2], vtg};
+          double pv[6];
+          C.prevN<6>(nv, pv);
+          if (fi) {
+            m1_sol = flux[0];
+            mp = pv[0];
+            if (K.do_sedi_w) w = w_update(k, w, dm_i, flux[0], vti, pv[0], pv[1]);
+            ice = ice + sfc[0];
+          }
+          if (fs) {
+            m1_sol = m1_sol + flux[1];
+            mp = mp + pv[2];
+            if (K.do_sedi_w) w = w_update(k, w, dm_s, flux[1], vts, pv[2], pv[3]);
+            snow = snow + sfc[1];
+          }
+          if (fg) {
+            m1_sol = m1_sol + flux[2];
+            mp = mp + pv[4];
+            if (K.do_sedi_w) w = w_update(k, w, dm_g, flux[2], vtg, pv[4], pv[5]);
+            graupel = graupel + sfc[2];
+          }
         }
         rain = rain + 0.0;
-        if (K.do_sedi_heat) sedi_heat<NW>(C, K, tz, dz1, dp1, qv, ql, qr, qi, qs, qg, m1_sol, valid, K.C_ICE);
+        if (K.do_sedi_heat) sedi_heat<NW>(C, K, tz, dz1, dp1, qv, ql, qr, qi, qs, qg, m1_sol, mp, valid, K.C_ICE);
       }
 
       // ------------------------------------------------ icloud (:1220-1449)

@@ -118,6 +118,35 @@ int shield_mp_destroy(void* handle);
 /* Copies the handle's last error message (NUL terminated) into buf. */
 int shield_mp_last_error(void* handle, char* buf, size_t n);
 
+/* ---------------------------------------------------------------------------
+ * Ensembles: many independent domains (members of different sizes and
+ * timesteps, one shared config and level count) advanced by ONE persistent
+ * launch. pySHiELD has no batched call; this replaces a loop of
+ * Microphysics.__call__ over members (microphysics.py:1981-2263), each member
+ * with its own Microphysics instance.
+ *
+ * shield_mp_ensemble_create computes every member's constants, copies its
+ * cell area and allocates its persistent accumulator (zero), and uploads the
+ * member table once. shield_mp_ensemble_step then enqueues a single kernel
+ * and nothing else (no allocation, no copy), so it can be captured in a CUDA
+ * graph and replayed. Supported level counts: 65..128. */
+typedef struct {
+  ShieldMpFields fields; /* the member's fields; its precipitation outputs may be NULL */
+  int nx, ny;            /* the member's horizontal domain */
+  double timestep;       /* the member's step */
+  ShieldField2D area;    /* the member's cell area (grid_data.area) */
+} ShieldMpMember;
+
+int shield_mp_ensemble_create(const ShieldMpConfig* cfg, int nz, int nmembers, const ShieldMpMember* members,
+                              int precision, void** plan);
+/* cols_per_block in {1, 2, 4} (4 only up to 96 levels); the launch has
+ * blocks_per_sm x (number of SMs) persistent blocks. */
+int shield_mp_ensemble_step(void* plan, int cols_per_block, int blocks_per_sm, void* stream);
+/* copy member m's persistent accumulator (nz*nx*ny doubles, level-major)
+ * into device memory at `out`, on `stream` */
+int shield_mp_ensemble_qaz(void* plan, int m, double* out, void* stream);
+int shield_mp_ensemble_destroy(void* plan);
+
 /* Test hook: the scalars the step uses for `timestep` (physical constants,
  * setupm constants, sub-step values) in the order of the internal parameter
  * block; returns how many doubles were written (at most n). */

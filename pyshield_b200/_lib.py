@@ -103,6 +103,16 @@ class ShieldMpFields(ctypes.Structure):
     )
 
 
+class ShieldMpMember(ctypes.Structure):
+    _fields_ = [
+        ("fields", ShieldMpFields),
+        ("nx", ctypes.c_int),
+        ("ny", ctypes.c_int),
+        ("timestep", ctypes.c_double),
+        ("area", ShieldField2D),
+    ]
+
+
 EXPORTS = (
     "shield_mp_create",
     "shield_mp_step",
@@ -115,6 +125,10 @@ EXPORTS = (
     "shield_update_atmos_state",
     "shield_last_error",
     "shield_mp_setup_constants",
+    "shield_mp_ensemble_create",
+    "shield_mp_ensemble_step",
+    "shield_mp_ensemble_qaz",
+    "shield_mp_ensemble_destroy",
 )
 
 _lib = None
@@ -150,6 +164,10 @@ def load():
         i32, i32, i32, i32, i32, ctypes.POINTER(ShieldField3D), ShieldField3D, ShieldField3D, ShieldField3D, dbl, dbl, dbl, dbl, vp,
     ]
     lib.shield_mp_setup_constants.argtypes = [ctypes.POINTER(ShieldMpConfig), dbl, ctypes.POINTER(ctypes.c_double), i32]
+    lib.shield_mp_ensemble_create.argtypes = [ctypes.POINTER(ShieldMpConfig), i32, i32, ctypes.POINTER(ShieldMpMember), i32, ctypes.POINTER(vp)]
+    lib.shield_mp_ensemble_step.argtypes = [vp, i32, i32, vp]
+    lib.shield_mp_ensemble_qaz.argtypes = [vp, i32, vp, vp]
+    lib.shield_mp_ensemble_destroy.argtypes = [vp]
     lib.shield_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
     for name in EXPORTS:
         getattr(lib, name).restype = i32

@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/shield_mp.h"
 #include "mp_launch.h"
@@ -453,4 +454,176 @@ extern "C" int shield_mp_set_qaz(void* handle, const double* qaz, void* stream) 
   cudaError_t e = cudaMemcpyAsync(h->qaz, qaz, sizeof(double) * h->ncol * h->nz, cudaMemcpyDeviceToDevice,
                                   static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? SHIELD_OK : cuda_fail(h, e, "copying qaz");
+}
+
+// ------------------------------------------------------------------ ensembles
+namespace {
+
+struct Plan {
+  int nm = 0, nz = 0, precision = 0, num_sms = 0;
+  MpArgs* d_members = nullptr;
+  int64_t* d_offs[3] = {nullptr, nullptr, nullptr};  // cols_per_block 1, 2, 4
+  double* d_area = nullptr;
+  double* d_qaz = nullptr;
+  std::vector<int64_t> qaz_off;
+  int64_t qaz_total = 0;
+  std::string last_error;
+};
+
+int gindex(int G) { return G == 1 ? 0 : G == 2 ? 1 : G == 4 ? 2 : -1; }
+
+void plan_free(Plan* p) {
+  cudaFree(p->d_members);
+  for (auto& o : p->d_offs) cudaFree(o);
+  cudaFree(p->d_area);
+  cudaFree(p->d_qaz);
+  delete p;
+}
+
+}  // namespace
+
+extern "C" int shield_mp_ensemble_create(const ShieldMpConfig* cfg, int nz, int nm, const ShieldMpMember* mem,
+                                         int precision, void** plan) {
+  if (!cfg || !mem || !plan || nm < 1) return fail(nullptr, SHIELD_EINVAL, "bad ensemble arguments");
+  *plan = nullptr;
+  if (nz <= 64 || nz > 128) return fail(nullptr, SHIELD_ELAYOUT, "ensembles support 65..128 levels");
+  if (precision != SHIELD_MP_PLAIN && precision != SHIELD_MP_MIXED) return fail(nullptr, SHIELD_EINVAL, "precision");
+  if (cfg->use_ppm) return fail(nullptr, SHIELD_EINVAL, "use_ppm=True is not supported");
+  Plan* p = new Plan();
+  p->nm = nm;
+  p->nz = nz;
+  p->precision = precision;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) {
+    int rc = cuda_fail(nullptr, e, "device query");
+    plan_free(p);
+    return rc;
+  }
+  std::vector<MpArgs> host(nm);
+  int64_t area_total = 0, qaz_total = 0;
+  std::vector<int64_t> area_off(nm);
+  p->qaz_off.resize(nm);
+  MpConst base;
+  std::memset(&base, 0, sizeof(base));
+  setupm(*cfg, base);
+  for (int m = 0; m < nm; ++m) {
+    const ShieldMpMember& M = mem[m];
+    if (M.nx < 1 || M.ny < 1 || !M.area.ptr) {
+      plan_free(p);
+      return fail(nullptr, SHIELD_EINVAL, "member " + std::to_string(m) + ": bad domain or area");
+    }
+    MpArgs& A = host[m];
+    std::memset(&A, 0, sizeof(A));
+    A.K = base;
+    std::string why;
+    if (set_timestep(*cfg, A.K, M.timestep, why) != SHIELD_OK) {
+      plan_free(p);
+      return fail(nullptr, SHIELD_EINVAL, "member " + std::to_string(m) + ": " + why);
+    }
+    A.KF = to_float(A.K);
+    A.nx = M.nx;
+    A.ny = M.ny;
+    A.nz = nz;
+    A.ncol = (int64_t)M.nx * M.ny;
+    const ShieldMpFields& F = M.fields;
+    const ShieldField3D* ins[] = {&F.pt, &F.qvapor, &F.qliquid, &F.qrain, &F.qice, &F.qsnow, &F.qgraupel,
+                                  &F.qcld, &F.ua, &F.va, &F.delprsi, &F.delz, &F.wmp};
+    const ShieldField3D* outs[] = {&F.pt_dt, &F.qv_dt, &F.ql_dt, &F.qr_dt, &F.qi_dt,
+                                   &F.qs_dt, &F.qg_dt, &F.qa_dt, &F.udt,   &F.vdt};
+    for (int f = 0; f < 13; ++f) {
+      if (!ins[f]->ptr) {
+        plan_free(p);
+        return fail(nullptr, SHIELD_EINVAL, "member " + std::to_string(m) + ": null field");
+      }
+      A.in[f] = f3(*ins[f]);
+    }
+    for (int o = 0; o < 10; ++o) {
+      if (!outs[o]->ptr) {
+        plan_free(p);
+        return fail(nullptr, SHIELD_EINVAL, "member " + std::to_string(m) + ": null tendency");
+      }
+      A.out[o] = f3(*outs[o]);
+    }
+    if (!F.land.ptr || A.K.de_ice) {
+      plan_free(p);
+      return fail(nullptr, SHIELD_EINVAL, "member " + std::to_string(m) + ": null land, or de_ice (not supported)");
+    }
+    A.out[OUT_W] = A.in[IN_W];
+    A.land = Fld2{F.land.ptr, F.land.si, F.land.sj};
+    A.rain = F.rain;
+    A.snow = F.snow;
+    A.ice = F.ice;
+    A.graupel = F.graupel;
+    area_off[m] = area_total;
+    p->qaz_off[m] = qaz_total;
+    area_total += A.ncol;
+    qaz_total += A.ncol * nz;
+  }
+  p->qaz_total = qaz_total;
+  if ((e = cudaMalloc(&p->d_area, sizeof(double) * area_total)) != cudaSuccess ||
+      (e = cudaMalloc(&p->d_qaz, sizeof(double) * qaz_total)) != cudaSuccess ||
+      (e = cudaMemset(p->d_qaz, 0, sizeof(double) * qaz_total)) != cudaSuccess ||
+      (e = cudaMalloc(&p->d_members, sizeof(MpArgs) * nm)) != cudaSuccess) {
+    int rc = cuda_fail(nullptr, e, "allocating the ensemble plan");
+    plan_free(p);
+    return rc;
+  }
+  for (int m = 0; m < nm; ++m) {
+    MpArgs& A = host[m];
+    A.area = Fld2{p->d_area + area_off[m], 1, A.nx};
+    const Fld3 qaz{p->d_qaz + p->qaz_off[m], 1, A.nx, A.ncol};
+    A.in[IN_QAZ] = qaz;
+    A.out[OUT_QAZ] = qaz;
+    e = mp_gather_area(mem[m].area.ptr, mem[m].area.si, mem[m].area.sj, A.nx, A.ny, p->d_area + area_off[m]);
+    if (e != cudaSuccess) break;
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(p->d_members, host.data(), sizeof(MpArgs) * nm, cudaMemcpyHostToDevice);
+  const int Gs[3] = {1, 2, 4};
+  for (int gi = 0; gi < 3 && e == cudaSuccess; ++gi) {
+    std::vector<int64_t> offs(nm + 1, 0);
+    for (int m = 0; m < nm; ++m) offs[m + 1] = offs[m] + (host[m].ncol + Gs[gi] - 1) / Gs[gi];
+    e = cudaMalloc(&p->d_offs[gi], sizeof(int64_t) * (nm + 1));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(p->d_offs[gi], offs.data(), sizeof(int64_t) * (nm + 1), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    int rc = cuda_fail(nullptr, e, "uploading the ensemble plan");
+    plan_free(p);
+    return rc;
+  }
+  *plan = p;
+  return SHIELD_OK;
+}
+
+extern "C" int shield_mp_ensemble_step(void* plan, int G, int bpsm, void* stream) {
+  Plan* p = static_cast<Plan*>(plan);
+  if (!p) return fail(nullptr, SHIELD_EINVAL, "null plan");
+  const int gi = gindex(G);
+  if (gi < 0 || bpsm < 1 || bpsm > 32 || (G == 4 && p->nz > 96))
+    return fail(nullptr, SHIELD_EINVAL, "cols_per_block must be 1, 2 or 4 (4 up to 96 levels), blocks_per_sm 1..32");
+  const int grid = bpsm * p->num_sms;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e = (p->precision == SHIELD_MP_MIXED)
+                      ? mp_launch_ensemble_mixed(p->d_members, p->d_offs[gi], p->nm, p->nz, G, grid, st)
+                      : mp_launch_ensemble_plain(p->d_members, p->d_offs[gi], p->nm, p->nz, G, grid, st);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "ensemble launch");
+  return SHIELD_OK;
+}
+
+extern "C" int shield_mp_ensemble_qaz(void* plan, int m, double* out, void* stream) {
+  Plan* p = static_cast<Plan*>(plan);
+  if (!p || !out || m < 0 || m >= p->nm) return fail(nullptr, SHIELD_EINVAL, "bad arguments");
+  const int64_t n = (m + 1 < p->nm ? p->qaz_off[m + 1] : p->qaz_total) - p->qaz_off[m];
+  cudaError_t e = cudaMemcpyAsync(out, p->d_qaz + p->qaz_off[m], sizeof(double) * n, cudaMemcpyDeviceToDevice,
+                                  static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? SHIELD_OK : cuda_fail(nullptr, e, "copying qaz");
+}
+
+extern "C" int shield_mp_ensemble_destroy(void* plan) {
+  Plan* p = static_cast<Plan*>(plan);
+  if (p) plan_free(p);
+  return SHIELD_OK;
 }

@@ -519,19 +519,18 @@ SHD void stage_out(const MpArgs& A, const double* sm, int64_t c0) {
 }
 
 // ------------------------------------------------------------------ kernel
+// One block's work: columns c0 .. c0 + G - 1 of the domain described by A.
 // MIXED selects the mixed-precision process rates (mp_physics_mixed.cuh);
 // everything else is shared by both forms.
-template <int NW, int G, int MINB, bool MIXED>
-__global__ void __launch_bounds__(32 * NW * G, MINB) mp_step_kernel(const __grid_constant__ MpArgs A) {
+template <int NW, int G, bool MIXED>
+SHD void mp_block(const MpArgs& A, double* sm, const int64_t c0) {
   using SM = Smem<NW, G>;
   constexpr int RP = Tiles<NW>::RP;
-  extern __shared__ double sm[];
   const MpConst& K = A.K;
   const MpConstF& KF = A.KF;
   const int L = A.nz;
   const int tid = threadIdx.x;
   const int g = tid / (32 * NW);
-  const int64_t c0 = (int64_t)blockIdx.x * G;
 
   stage_in<NW, G>(A, sm, c0);
   __syncthreads();
@@ -939,6 +938,50 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) mp_step_kernel(const __grid
   }
   __syncthreads();
   stage_out<NW, G>(A, sm, c0);
+}
+
+template <int NW, int G, int MINB, bool MIXED>
+__global__ void __launch_bounds__(32 * NW * G, MINB) mp_step_kernel(const __grid_constant__ MpArgs A) {
+  extern __shared__ double sm[];
+  mp_block<NW, G, MIXED>(A, sm, (int64_t)blockIdx.x * G);
+}
+
+// Many domains (ensemble members) in one persistent launch. Work item wi
+// of the flattened index space is block (wi - offs[m]) of member m, where
+// offs[m] <= wi < offs[m + 1] (offs holds nm + 1 prefix sums of each member's
+// ceil(ncol / G)). Each item copies its member's parameter block into shared
+// memory, so the step body reads its constants from there.
+template <int NW, int G, int MINB, bool MIXED>
+__global__ void __launch_bounds__(32 * NW * G, MINB)
+    mp_ensemble_kernel(const MpArgs* __restrict__ members, const int64_t* __restrict__ offs, int nm) {
+  extern __shared__ double sm[];
+  __shared__ MpArgs sargs;
+  __shared__ int smember;
+  const int64_t total = offs[nm];
+  for (int64_t wi = blockIdx.x; wi < total; wi += gridDim.x) {
+    __syncthreads();  // the previous item is done with sargs and the tiles
+    if (threadIdx.x == 0) {
+      int lo = 0, hi = nm - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (offs[mid] <= wi)
+          lo = mid;
+        else
+          hi = mid - 1;
+      }
+      smember = lo;
+    }
+    __syncthreads();
+    const int m = smember;
+    {
+      const int* src = reinterpret_cast<const int*>(members + m);
+      int* dst = reinterpret_cast<int*>(&sargs);
+      constexpr int nwords = (int)(sizeof(MpArgs) / sizeof(int));
+      for (int e = threadIdx.x; e < nwords; e += blockDim.x) dst[e] = src[e];
+    }
+    __syncthreads();
+    mp_block<NW, G, MIXED>(sargs, sm, (wi - offs[m]) * G);
+  }
 }
 
 }  // namespace shield

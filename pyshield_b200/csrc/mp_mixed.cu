@@ -30,4 +30,34 @@ cudaError_t mp_launch_mixed(const MpArgs& A, cudaStream_t st) {
   return launch_nw<8, 1, 2>(A, st);
 }
 
+
+namespace {
+
+template <int NW, int G, int MINB>
+cudaError_t launch_ens(const MpArgs* members, const int64_t* offs, int nm, int grid, cudaStream_t st) {
+  const size_t smem = Smem<NW, G>::bytes;
+  auto kern = mp_ensemble_kernel<NW, G, MINB, true>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<grid, 32 * NW * G, smem, st>>>(members, offs, nm);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+// Ensemble launch over nz in (64, 128]: G columns per block (1, 2 or 4), a
+// persistent grid of `grid` blocks.
+cudaError_t mp_launch_ensemble_mixed(const MpArgs* members, const int64_t* offs, int nm, int nz, int G, int grid,
+                                     cudaStream_t st) {
+  if (nz <= 96) {
+    if (G == 1) return launch_ens<3, 1, 4>(members, offs, nm, grid, st);
+    if (G == 2) return launch_ens<3, 2, 2>(members, offs, nm, grid, st);
+    if (G == 4) return launch_ens<3, 4, 1>(members, offs, nm, grid, st);
+  } else if (nz <= 128) {
+    if (G == 1) return launch_ens<4, 1, 4>(members, offs, nm, grid, st);
+    if (G == 2) return launch_ens<4, 2, 2>(members, offs, nm, grid, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
 }  // namespace shield

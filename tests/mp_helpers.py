@@ -46,6 +46,39 @@ def device_quantity2d(arr_n, nx, ny, h=3):
     return Quantity(torch.from_numpy(st).cuda(), ("x", "y"), "", (h, h), (nx, ny))
 
 
+def device_state(state, area, nx, ny, layout="ifirst"):
+    """MicrophysicsState with NDSL-layout device storages holding ``state``;
+    returns (state, stencil_factory, quantity_factory, grid_data)."""
+    from pyshield_b200.grid import GridData, GridIndexing, QuantityFactory, StencilFactory
+    from pyshield_b200.microphysics import MicrophysicsState
+
+    L = state["pt"].shape[0]
+    gi = GridIndexing(nx, ny, L)
+    qf = QuantityFactory(gi)
+    q = {k: device_quantity(v, nx, ny, layout) for k, v in state.items() if k != "land"}
+    land = device_quantity2d(state["land"], nx, ny)
+    ms = MicrophysicsState(
+        q["pt"], q["qvapor"], q["qliquid"], q["qrain"], q["qice"], q["qsnow"], q["qgraupel"], q["qcld"], q["ua"],
+        q["va"], qf.zeros(["x", "y", "z"], ""), q["delz"], qf.zeros(["x", "y", "z"], ""), q["delprsi"], q["wmp"],
+        qf.zeros(["x", "y", "z"], ""), qf.zeros(["x", "y", "z"], ""), land,
+    )
+    for t in MP_TENDENCIES:
+        setattr(ms, t, q[t])
+    return ms, StencilFactory(gi), qf, GridData(device_quantity2d(area, nx, ny))
+
+
+def read_state(ms, nx, ny, L, layout="ifirst"):
+    o = {}
+    for t in MP_TENDENCIES + ("wmp", "qice", "qsnow"):
+        data = getattr(ms, t).data
+        if layout == "ifirst":
+            arr = data.permute(2, 1, 0).contiguous().cpu().numpy().transpose(2, 1, 0)
+        else:
+            arr = data.cpu().numpy()
+        o[t] = from_storage_np(arr, nx, ny, L)
+    return o
+
+
 def run_gpu(cfg, state, area, nx, ny, dt, nsteps=1, layout="ifirst", precision="plain", qaz0=None):
     """Run the CUDA step ``nsteps`` times; return per-step outputs as (L, n)
     numpy arrays (tendencies, wmp, qice, qsnow, qaz) and (n,) precip."""

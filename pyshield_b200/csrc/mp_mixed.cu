@@ -25,7 +25,7 @@ cudaError_t mp_launch_mixed(const MpArgs& A, cudaStream_t st) {
   const int L = A.nz;
   if (L <= 32) return launch_nw<1, 4, 2>(A, st);
   if (L <= 64) return launch_nw<2, 2, 2>(A, st);
-  if (L <= 96) return launch_nw<3, 2, 2>(A, st);
+  if (L <= 96) return launch_nw<3, 4, 1>(A, st);
   if (L <= 128) return launch_nw<4, 2, 2>(A, st);
   return launch_nw<8, 1, 2>(A, st);
 }

@@ -118,6 +118,32 @@ int shield_mp_destroy(void* handle);
 /* Copies the handle's last error message (NUL terminated) into buf. */
 int shield_mp_last_error(void* handle, char* buf, size_t n);
 
+/* Allocation-free step: one step of shield_mp_step with no handle and no
+ * device allocation. It has no counterpart in the reference. It is meant for
+ * hosts that may not call cudaMalloc: a model whose memory pool owns all of
+ * the GPU's memory, or a caller whose physics interface forbids allocating.
+ * The caller passes every input and output, as for shield_mp_step, plus
+ * what shield_mp_create would have taken (cfg, nx, ny, nz, area); the
+ * constants are recomputed on the host each call.
+ *
+ * The cloud-fraction accumulator that a handle would own lives instead in
+ * one fixed device array of 16 MiB inside the library. Every GPU that loads
+ * the library holds that array until the process exits.
+ *  - Size limit: nx * ny * nz <= 2097152. Larger domains fail with
+ *    SHIELD_ELAYOUT and should use shield_mp_step.
+ *  - The first call on each device finds and clears the array, and
+ *    synchronises that device. Make that first call before any stream
+ *    capture.
+ *  - All calls on a device share the array. It keeps what the last call
+ *    left. Pass first_step != 0 on the first step of a run, or when
+ *    switching to another domain: this zeroes the accumulator, as a new
+ *    handle starts at zero. Calls that overlap on the GPU (other streams,
+ *    threads or domains) race on the array.
+ *  - Errors are reported through shield_last_error. */
+int shield_mp_step_noalloc(const ShieldMpConfig* cfg, int nx, int ny, int nz, ShieldField2D area,
+                           const ShieldMpFields* fields, double timestep, int precision, int first_step,
+                           void* stream);
+
 /* ---------------------------------------------------------------------------
  * Ensembles: many independent domains (members of different sizes and
  * timesteps, one shared config and level count) advanced by ONE persistent

@@ -129,6 +129,7 @@ EXPORTS = (
     "shield_mp_ensemble_step",
     "shield_mp_ensemble_qaz",
     "shield_mp_ensemble_destroy",
+    "shield_mp_step_noalloc",
 )
 
 _lib = None
@@ -169,6 +170,9 @@ def load():
     lib.shield_mp_ensemble_qaz.argtypes = [vp, i32, vp, vp]
     lib.shield_mp_ensemble_destroy.argtypes = [vp]
     lib.shield_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+    lib.shield_mp_step_noalloc.argtypes = [
+        ctypes.POINTER(ShieldMpConfig), i32, i32, i32, ShieldField2D, ctypes.POINTER(ShieldMpFields), dbl, i32, i32, vp,
+    ]
     for name in EXPORTS:
         getattr(lib, name).restype = i32
     _lib = lib

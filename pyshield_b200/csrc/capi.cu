@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -625,5 +626,124 @@ extern "C" int shield_mp_ensemble_qaz(void* plan, int m, double* out, void* stre
 extern "C" int shield_mp_ensemble_destroy(void* plan) {
   Plan* p = static_cast<Plan*>(plan);
   if (p) plan_free(p);
+  return SHIELD_OK;
+}
+
+// ------------------------------------------------------ allocation-free step
+// shield_mp_step_noalloc: the step of shield_mp_step for callers that may not
+// allocate device memory. Some hosts hand every byte of the GPU to their own
+// pool or arena at start-up, and a cudaMalloc made behind its back either
+// fails or breaks its accounting; others call physics from a context whose
+// contract forbids allocation. The step's only scratch, the persistent
+// cloud-fraction accumulator (nz values per column), therefore lives in the
+// file-scope array below instead of a handle: it is part of this module's
+// image, so the driver reserves it when the module loads on a GPU and every
+// GPU that loads the library holds it until the process exits.
+namespace {
+
+// the largest nx * ny * nz the allocation-free step accepts: 16 MiB of
+// accumulator (a 96 x 96 tile at 79 levels needs 0.73 M cells)
+constexpr int64_t kNoAllocMaxCells = int64_t(1) << 21;
+constexpr int kNoAllocMaxDevices = 64;
+
+// accumulator cells, then one word for the kernel's error flag
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxCells + 32];
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Once per device, with that device current: look up the array's device
+// address (its host-side name is only a stand-in) and clear it. Runs inside
+// the first call on each device; it synchronises with the legacy default
+// stream, so that first call should come before any stream capture.
+int noalloc_setup(int dev, double** out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    double* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetSymbolAddress of the allocation-free scratch");
+    e = cudaMemset(p, 0, sizeof(g_noalloc_scratch));
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "clearing the allocation-free scratch");
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return SHIELD_OK;
+}
+
+}  // namespace
+
+extern "C" int shield_mp_step_noalloc(const ShieldMpConfig* cfg, int nx, int ny, int nz, ShieldField2D area,
+                                      const ShieldMpFields* F, double timestep, int precision, int first_step,
+                                      void* stream) {
+  if (!cfg || !F) return fail(nullptr, SHIELD_EINVAL, "null config or fields");
+  if (nx < 1 || ny < 1) return fail(nullptr, SHIELD_EINVAL, "nx and ny must be positive");
+  if (nz < 3 || nz > mp_max_levels()) return fail(nullptr, SHIELD_ELAYOUT, "nz must lie in [3, 256]");
+  const int64_t ncol = (int64_t)nx * ny;
+  if (ncol > kNoAllocMaxCells / nz)
+    return fail(nullptr, SHIELD_ELAYOUT,
+                "nx * ny * nz = " + std::to_string(ncol * nz) + " exceeds the allocation-free step's limit of " +
+                    std::to_string(kNoAllocMaxCells) + " cells (its fixed 16 MiB scratch); use shield_mp_step");
+  if (cfg->use_ppm) return fail(nullptr, SHIELD_EINVAL, "use_ppm=True is not supported (incomplete in the reference)");
+  if (!area.ptr) return fail(nullptr, SHIELD_EINVAL, "null area pointer");
+  if (precision != SHIELD_MP_PLAIN && precision != SHIELD_MP_MIXED)
+    return fail(nullptr, SHIELD_EINVAL, "unknown precision mode");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDevice");
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(nullptr, SHIELD_EINVAL, "device ordinal beyond 63");
+  double* scratch = nullptr;
+  int rc = noalloc_setup(dev, &scratch);
+  if (rc != SHIELD_OK) return rc;
+
+  MpArgs A;
+  std::memset(&A, 0, sizeof(A));
+  setupm(*cfg, A.K);
+  std::string why;
+  if (set_timestep(*cfg, A.K, timestep, why) != SHIELD_OK) return fail(nullptr, SHIELD_EINVAL, why);
+  A.KF = to_float(A.K);
+  A.nx = nx;
+  A.ny = ny;
+  A.nz = nz;
+  A.ncol = ncol;
+  const ShieldField3D* ins[] = {&F->pt, &F->qvapor, &F->qliquid, &F->qrain, &F->qice, &F->qsnow, &F->qgraupel,
+                                &F->qcld, &F->ua, &F->va, &F->delprsi, &F->delz, &F->wmp};
+  const ShieldField3D* outs[] = {&F->pt_dt, &F->qv_dt, &F->ql_dt, &F->qr_dt, &F->qi_dt,
+                                 &F->qs_dt, &F->qg_dt, &F->qa_dt, &F->udt,   &F->vdt};
+  for (int f = 0; f < 13; ++f) {
+    if (!ins[f]->ptr) return fail(nullptr, SHIELD_EINVAL, "null input field pointer");
+    A.in[f] = f3(*ins[f]);
+  }
+  for (int o = 0; o < 10; ++o) {
+    if (!outs[o]->ptr) return fail(nullptr, SHIELD_EINVAL, "null tendency pointer");
+    A.out[o] = f3(*outs[o]);
+  }
+  if (!F->land.ptr) return fail(nullptr, SHIELD_EINVAL, "null land pointer");
+  // the accumulator, level-major over this call's nx * ny columns
+  const Fld3 qaz{scratch, 1, nx, ncol};
+  A.in[IN_QAZ] = qaz;
+  A.out[OUT_W] = A.in[IN_W];
+  A.out[OUT_QAZ] = qaz;
+  A.land = Fld2{F->land.ptr, F->land.si, F->land.sj};
+  A.area = Fld2{area.ptr, area.si, area.sj};
+  A.rain = F->rain;
+  A.snow = F->snow;
+  A.ice = F->ice;
+  A.graupel = F->graupel;
+  A.err = reinterpret_cast<int*>(scratch + kNoAllocMaxCells);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // The array keeps whatever the last call on this device left in it. The
+  // first step of a run (or of another domain) starts from a zero
+  // accumulator, as a freshly constructed handle does.
+  if (first_step) {
+    e = cudaMemsetAsync(scratch, 0, sizeof(double) * (size_t)(ncol * nz), st);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "clearing the accumulator");
+  }
+  if (A.K.de_ice) {
+    e = mp_launch_de_ice(A, f3(F->qi_dt), f3(F->qs_dt), st);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "de_ice launch");
+  }
+  e = mp_launch_step(A, precision, st);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "microphysics launch");
   return SHIELD_OK;
 }

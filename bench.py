@@ -197,6 +197,26 @@ def build_state(nlev, device, seed, n_cube=N_CUBE):
     return ms, StencilFactory(gi), qf, GridData(area_q), host, land, (nx, ny, n)
 
 
+def max_over_ranks(values, world, device):
+    """Each rank's device-measured times -> their maximum over all ranks (the
+    slowest replica sets the job's time). One all-reduce; every rank calls it
+    at the same point."""
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def whole_job_rate(world, columns_per_rank, steps, total_ms):
+    """Column-steps/s of the whole job: every replica advances its own
+    columns ``steps`` times; the time is the max over ranks."""
+    return world * columns_per_rank * steps / (total_ms / 1000.0)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -264,13 +284,8 @@ def run_ours(args, rank, world, local_rank):
 
     e2e_steps = max(2, min(args.steps, 5))
     if args.no_e2e:
-        e2e_steps = 0
-        times = torch.tensor([total_ms, 0.0, mean_launch_ms], dtype=torch.float64, device=device)
-        if world > 1:
-            import torch.distributed as dist
-
-            dist.all_reduce(times, op=dist.ReduceOp.MAX)
-        return {"n": n, "nlev": nlev, "total_ms": times[0].item(), "mean_launch_ms": times[2].item(), "e2e_ms": 0.0,
+        total_ms, _, mean_launch_ms = max_over_ranks([total_ms, 0.0, mean_launch_ms], world, device)
+        return {"n": n, "nlev": nlev, "total_ms": total_ms, "mean_launch_ms": mean_launch_ms, "e2e_ms": 0.0,
                 "e2e_steps": 0, "h2d": h2d, "d2h": d2h, "clocks": clk, "mixed_ms": 0.0}
     e2e_step()
     torch.cuda.synchronize()
@@ -301,12 +316,7 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         mixed_ms = m0.elapsed_time(m1) / args.steps
 
-    times = torch.tensor([total_ms, e2e_ms, mean_launch_ms, mixed_ms], dtype=torch.float64, device=device)
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    total_ms, e2e_ms, mean_launch_ms, mixed_ms = times.tolist()
+    total_ms, e2e_ms, mean_launch_ms, mixed_ms = max_over_ranks([total_ms, e2e_ms, mean_launch_ms, mixed_ms], world, device)
     return {
         "mixed_ms": mixed_ms,
         "n": n,
@@ -496,11 +506,11 @@ def main():
 
     r = run_ours(args, rank, world, local_rank)
     steps = args.steps
-    value = world * r["n"] * steps / (r["total_ms"] / 1000.0)
+    value = whole_job_rate(world, r["n"], steps, r["total_ms"])
     bytes_launch = algorithmic_bytes_per_column_step(nlev) * r["n"]
     achieved = bytes_launch / (r["mean_launch_ms"] / 1000.0) / 1e9
     peak, peak_kind = peaks()
-    e2e_value = world * r["n"] * r["e2e_steps"] / (r["e2e_ms"] / 1000.0) if r["e2e_ms"] > 0 else None
+    e2e_value = whole_job_rate(world, r["n"], r["e2e_steps"], r["e2e_ms"]) if r["e2e_ms"] > 0 else None
 
     cpu = None
     if want_cpu:

@@ -704,7 +704,7 @@ SHD void mp_block(const MpArgs& A, double* sm, const int64_t c0) {
           const double dm = dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
           m1_rain = implicit_fall<NW>(C, qr, vtr, dz, dp1, valid, K.dt_rain);
           double fv[2] = {m1_rain, vtr}, pv[2];
-          C.prevN<2>(fv, pv);
+          C.template prevN<2>(fv, pv);
           r1 = C.bcast(m1_rain, L - 1);
           if (K.do_sedi_w) w = w_update(k, w, dm, m1_rain, vtr, pv[0], pv[1]);
           if (K.do_sedi_heat)
@@ -776,7 +776,7 @@ SHD void mp_block(const MpArgs& A, double* sm, const int64_t c0) {
         if (fi || fs || fg) {
           const double dd[3] = {K.dts * vti, K.dts * vts, K.dts * vtg};
           double ddp[3];
-          C.prevN<3>(dd, ddp);
+          C.template prevN<3>(dd, ddp);
           const double qq[3] = {qi, qs, qg};
           double ra[3], rb[3], r[3];
 #pragma unroll
@@ -790,7 +790,7 @@ SHD void mp_block(const MpArgs& A, double* sm, const int64_t c0) {
               rb[n] = 0.0;
             }
           }
-          C.scanN<3>(ra, rb, r);
+          C.template scanN<3>(ra, rb, r);
           double flux[3];
 #pragma unroll
           for (int n = 0; n < 3; ++n) flux[n] = valid ? dd[n] * r[n] : 0.0;
@@ -801,10 +801,10 @@ SHD void mp_block(const MpArgs& A, double* sm, const int64_t c0) {
           const double dm_g = dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
           if (fg && valid) qg = r[2] * dz / dp1;
           double sfc[3];
-          C.bcastN<3>(flux, L - 1, sfc);
+          C.template bcastN<3>(flux, L - 1, sfc);
           const double nv[6] = {flux[0], vti, flux[1], vts, flux[2], vtg};
           double pv[6];
-          C.prevN<6>(nv, pv);
+          C.template prevN<6>(nv, pv);
           if (fi) {
             m1_sol = flux[0];
             mp = pv[0];

@@ -12,6 +12,9 @@
 #pragma once
 
 #include <cstdint>
+#ifndef __CUDACC__
+#include <cmath>
+#endif
 
 #include "mp_params.h"
 
@@ -45,37 +48,50 @@ constexpr double QCMIN = 1.0e-12;
 constexpr double QRMIN = 1.0e-8;
 constexpr double QVMIN = 1.0e-20;
 
+#ifdef __CUDACC__
 #define SHD __device__ __forceinline__
+// pointwise physics: also compiled for the host, where the adjoint tests
+// instantiate it with a dual-number type
+#define SHP __host__ __device__ __forceinline__
+#else
+#define SHD inline
+#define SHP inline
+#endif
 
 // The FP64 exp/log/pow sequences are large; called through these
 // out-of-line wrappers they exist once in the kernel instead of at every one
 // of their call sites, which keeps the kernel within the instruction cache.
-#ifndef SHIELD_INLINE_MATH
-#define SHIELD_MATH_ATTR static __device__ __noinline__
+#if defined(__CUDACC__) && !defined(SHIELD_INLINE_MATH)
+#define SHIELD_MATH_ATTR static __host__ __device__ __noinline__
+#elif defined(__CUDACC__)
+#define SHIELD_MATH_ATTR __host__ __device__ __forceinline__
 #else
-#define SHIELD_MATH_ATTR __device__ __forceinline__
+#define SHIELD_MATH_ATTR static inline
 #endif
 SHIELD_MATH_ATTR double xexp(double x) { return exp(x); }
 SHIELD_MATH_ATTR double xlog(double x) { return log(x); }
 SHIELD_MATH_ATTR double xpow(double x, double y) { return pow(x, y); }
 
-SHD double dim(double x, double y) {
+SHP double dim(double x, double y) {
   double d = x - y;
   return d > 0.0 ? d : 0.0;
 }
-SHD double sq(double x) { return x * x; }
+SHP double sq(double x) { return x * x; }
 
 // ---------------------------------------------------- microphysics_funcs.py:52-145
-SHIELD_MATH_ATTR double wqs1(const MpConst& K, double ta, double den) {
+template <typename T>
+SHIELD_MATH_ATTR T wqs1(const MpConst& K, T ta, T den) {
   return (K.E00 * xexp((K.DC_VAP * xlog(ta / K.TICE) + K.LV0 * (ta - K.TICE) / (ta * K.TICE)) / K.RVGAS)) /
          (K.RVGAS * ta * den);
 }
-SHD double wqs2(const MpConst& K, double ta, double den, double& dqdt) {
-  double tmp = wqs1(K, ta, den);
+template <typename T>
+SHP T wqs2(const MpConst& K, T ta, T den, T& dqdt) {
+  T tmp = wqs1(K, ta, den);
   dqdt = tmp * (K.DC_VAP + K.LV0 / ta) / (K.RVGAS * ta);
   return tmp;
 }
-SHIELD_MATH_ATTR double iqs1(const MpConst& K, double ta, double den) {
+template <typename T>
+SHIELD_MATH_ATTR T iqs1(const MpConst& K, T ta, T den) {
   if (ta < K.TICE) {
     if (ta >= K.T_SAT_MIN) {
       return (K.E00 * xexp((K.D2ICE * xlog(ta / K.TICE) + K.LI2 * (ta - K.TICE) / (ta * K.TICE)) / K.RVGAS)) /
@@ -83,11 +99,12 @@ SHIELD_MATH_ATTR double iqs1(const MpConst& K, double ta, double den) {
     }
     return K.iqs_lo_num / (K.RVGAS * K.T_SAT_MIN * den);
   }
-  if (ta <= K.TICE + 102.0) return wqs1(K, ta, den);
-  return wqs1(K, K.TICE + 102.0, den);
+  if (ta <= K.TICE + 102.0) return wqs1<T>(K, ta, den);
+  return wqs1<T>(K, T(K.TICE + 102.0), den);
 }
-SHD double iqs2(const MpConst& K, double ta, double den, double& dqdt) {
-  double tmp = iqs1(K, ta, den);
+template <typename T>
+SHP T iqs2(const MpConst& K, T ta, T den, T& dqdt) {
+  T tmp = iqs1(K, ta, den);
   if (ta < K.TICE) {
     if (ta >= K.T_SAT_MIN)
       dqdt = tmp * (K.D2ICE + K.LI2 / ta) / (K.RVGAS * ta);
@@ -104,54 +121,56 @@ SHD double iqs2(const MpConst& K, double ta, double den, double& dqdt) {
 
 // ---------------------------------------------------- microphysics_funcs.py:148-179
 template <typename R>
-SHD R acr3d(R v1, R v2, R q1, R q2, R c, R cac_ik, R cac_i1k, R cac_i2k, R rho) {
+SHP R acr3d(R v1, R v2, R q1, R q2, R c, R cac_ik, R cac_i1k, R cac_i2k, R rho) {
   R t1 = sqrt(q1 * rho);
   R s1 = sqrt(q2 * rho);
   R s2 = sqrt(s1);
   return c * fabs(v1 - v2) * q1 * s2 * (cac_ik * t1 + cac_i1k * sqrt(t1) * s2 + cac_i2k * s1);
 }
 template <typename R>
-SHD R smlt(R tc, R dqs, R qsrho, R psacw, R psacr, R c_0, R c_1, R c_2, R c_3, R c_4, R rho, R rhofac) {
+SHP R smlt(R tc, R dqs, R qsrho, R psacw, R psacr, R c_0, R c_1, R c_2, R c_3, R c_4, R rho, R rhofac) {
   return (c_0 * tc / rho - c_1 * dqs) * (c_2 * sqrt(qsrho) + c_3 * xpow(qsrho, R(0.65625)) * sqrt(rhofac)) +
          c_4 * tc * (psacw + psacr);
 }
 template <typename R>
-SHD R gmlt(R tc, R dqs, R qgrho, R pgacw, R pgacr, R c_0, R c_1, R c_2, R c_3, R c_4, R rho) {
+SHP R gmlt(R tc, R dqs, R qgrho, R pgacw, R pgacr, R c_0, R c_1, R c_2, R c_3, R c_4, R rho) {
   return (c_0 * tc / rho - c_1 * dqs) * (c_2 * sqrt(qgrho) + c_3 * xpow(qgrho, R(0.6875)) / xpow(rho, R(0.25))) +
          c_4 * tc * (pgacw + pgacr);
 }
 
-SHD double cvm_of(const MpConst& K, double qv, double q_liq, double q_sol) {
+template <typename T>
+SHP T cvm_of(const MpConst& K, T qv, T q_liq, T q_sol) {
   return K.c_air + qv * K.c_vap + q_liq * K.C_LIQ + q_sol * K.C_ICE;
 }
 
 // ---------------------------------------------------- microphysics_funcs.py:182-265
-SHD void revap_racc(const MpConst& K, double dt, double h_var, double& qg, double& qi, double& ql, double& qr,
-                    double& qs, double& qv, double& tz, double den, double denfac) {
+template <typename T>
+SHP void revap_racc(const MpConst& K, double dt, double h_var, T& qg, T& qi, T& ql, T& qr, T& qs, T& qv, T& tz,
+                    T den, T denfac) {
   if ((tz > K.t_wfr) && (qr > QRMIN)) {
-    double lhl = K.lv00 + K.d0_vap * tz;
-    double q_liq = ql + qr;
-    double q_sol = qi + qs + qg;
-    double cvm = cvm_of(K, qv, q_liq, q_sol);
-    double lcpk = lhl / cvm;
-    double tin = tz - lcpk * ql;
-    double qpz = qv + ql;
-    double dqsdt;
-    double qsat = wqs2(K, tin, den, dqsdt);
-    double dqh = fmax(ql, h_var * fmax(qpz, QCMIN));
+    T lhl = K.lv00 + K.d0_vap * tz;
+    T q_liq = ql + qr;
+    T q_sol = qi + qs + qg;
+    T cvm = cvm_of(K, qv, q_liq, q_sol);
+    T lcpk = lhl / cvm;
+    T tin = tz - lcpk * ql;
+    T qpz = qv + ql;
+    T dqsdt;
+    T qsat = wqs2(K, tin, den, dqsdt);
+    T dqh = fmax(ql, h_var * fmax(qpz, QCMIN));
     dqh = fmin(dqh, 0.2 * qpz);
-    double dqv = qsat - qv;
-    double q_minus = qpz - dqh;
-    double q_plus = qpz + dqh;
+    T dqv = qsat - qv;
+    T q_minus = qpz - dqh;
+    T q_plus = qpz + dqh;
     if ((dqv > QVMIN) && (qsat > q_minus)) {
-      double dq;
+      T dq;
       if (qsat > q_plus)
         dq = qsat - qpz;
       else
         dq = 0.25 * sq(q_minus - qsat) / dqh;
-      double qden = qr * den;
-      double t2 = tin * tin;
-      double evap = K.crevp[0] * t2 * dq * (K.crevp[1] * sqrt(qden) + K.crevp[2] * xexp(0.725 * xlog(qden))) /
+      T qden = qr * den;
+      T t2 = tin * tin;
+      T evap = K.crevp[0] * t2 * dq * (K.crevp[1] * sqrt(qden) + K.crevp[2] * xexp(0.725 * xlog(qden))) /
                     (K.crevp[3] * t2 + K.crevp[4] * qsat * den);
       evap = fmin(qr, fmin(dt * evap, dqv / (1.0 + lcpk * dqsdt)));
       qr = qr - evap;
@@ -161,7 +180,7 @@ SHD void revap_racc(const MpConst& K, double dt, double h_var, double& qg, doubl
       tz = tz - evap * lhl / cvm;
     }
     if ((qr > QRMIN) && (ql > 1.0e-6) && (qsat < q_minus)) {
-      double sink = dt * denfac * K.cracw * xexp(0.95 * xlog(qr * den));
+      T sink = dt * denfac * K.cracw * xexp(0.95 * xlog(qr * den));
       sink = sink / (1.0 + sink) * ql;
       ql = ql - sink;
       qr = qr + sink;
@@ -170,17 +189,17 @@ SHD void revap_racc(const MpConst& K, double dt, double h_var, double& qg, doubl
 }
 
 // ---------------------------------------------------- microphysics_funcs.py:268-341
-SHD void fall_speed(const MpConst& K, double qg, double qi, double qs, double tk, double den, double& vtg,
-                    double& vti, double& vts) {
-  double rhof = sqrt(fmin(10.0, SFCRHO / den));
+template <typename T>
+SHP void fall_speed(const MpConst& K, T qg, T qi, T qs, T tk, T den, T& vtg, T& vti, T& vts) {
+  T rhof = sqrt(fmin(10.0, SFCRHO / den));
   if (K.const_vi) {
     vti = K.vi_fac;
   } else {
-    double vi0 = 0.01 * K.vi_fac;
+    T vi0 = 0.01 * K.vi_fac;
     if (qi < THI) {
       vti = VF_MIN;
     } else {
-      double tc = tk - K.tice;
+      T tc = tk - K.tice;
       vti = (3.0 + xlog(qi * den) / K.log_10) * (tc * (AA * tc + BB) + CC) + DD_FS * tc + EE;
       vti = vi0 * xexp(K.log_10 * vti) * 0.8;
       vti = fmin(K.vi_max, fmax(VF_MIN, vti));
@@ -209,37 +228,38 @@ SHD void fall_speed(const MpConst& K, double qg, double qi, double qs, double tk
 }
 
 // microphysics_funcs.py:344-372 (the no_fall == 0 branch)
-SHD double rain_fspeed(const MpConst& K, double qrz, double den) {
+template <typename T>
+SHP T rain_fspeed(const MpConst& K, T qrz, T den) {
   if (K.const_vr) return K.vr_fac;
-  double qden = qrz * den;
+  T qden = qrz * den;
   if (qrz < THR) return VR_MIN;
-  double v = K.vr_fac * VCONR * sqrt(fmin(10.0, SFCRHO / den)) * xexp(0.2 * xlog(qden / NORMR));
+  T v = K.vr_fac * VCONR * sqrt(fmin(10.0, SFCRHO / den)) * xexp(0.2 * xlog(qden / NORMR));
   return fmin(K.vr_max, fmax(VR_MIN, v));
 }
 
 // ---------------------------------------------------- microphysics_funcs.py:375-428
-SHD void autoconv_no_subgrid_var(const MpConst& K, double& qlz, double& qrz, double tz, double den, double ccn,
-                                 double c_praut) {
-  double qc0 = K.fac_rc * ccn;
+template <typename T>
+SHP void autoconv_no_subgrid_var(const MpConst& K, T& qlz, T& qrz, T tz, T den, T ccn, T c_praut) {
+  T qc0 = K.fac_rc * ccn;
   if (tz > K.t_wfr) {
-    double qc = K.use_ccn ? qc0 : qc0 / den;
-    double dq = qlz - qc;
+    T qc = K.use_ccn ? qc0 : qc0 / den;
+    T dq = qlz - qc;
     if (dq > 0.0) {
-      double sink = fmin(dq, K.dt_rain * c_praut * den * xexp(K.so3 * xlog(qlz)));
+      T sink = fmin(dq, K.dt_rain * c_praut * den * xexp(K.so3 * xlog(qlz)));
       qlz = qlz - sink;
       qrz = qrz + sink;
     }
   }
 }
-SHD void autoconv_subgrid_var(const MpConst& K, double& qlz, double& qrz, double tz, double den, double ccn,
-                              double c_praut, double dl) {
-  double qc0 = K.fac_rc * ccn;
+template <typename T>
+SHP void autoconv_subgrid_var(const MpConst& K, T& qlz, T& qrz, T tz, T den, T ccn, T c_praut, T dl) {
+  T qc0 = K.fac_rc * ccn;
   if (tz > K.t_wfr + DT_FR) {
     dl = fmin(fmax(1.0e-6, dl), 0.5 * qlz);
-    double qc = K.use_ccn ? qc0 : qc0 / den;
-    double dq = 0.5 * (qlz + dl - qc);
+    T qc = K.use_ccn ? qc0 : qc0 / den;
+    T dq = 0.5 * (qlz + dl - qc);
     if (dq > 0.0) {
-      double sink = fmin(1.0, dq / dl) * K.dt_rain * c_praut * den * xexp(K.so3 * xlog(qlz));
+      T sink = fmin(1.0, dq / dl) * K.dt_rain * c_praut * den * xexp(K.so3 * xlog(qlz));
       qlz = qlz - sink;
       qrz = qrz + sink;
     }
@@ -247,23 +267,23 @@ SHD void autoconv_subgrid_var(const MpConst& K, double& qlz, double& qrz, double
 }
 
 // ---------------------------------------------------- microphysics_funcs.py:431-850
-SHD void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh_rain, double& qaz, double& qgz,
-                        double& qiz, double& qlz, double& qrz, double& qsz, double& qvz, double& tz, double den,
-                        double denfac, double p1) {
-  const double tice = K.tice, t_wfr = K.t_wfr, t_sub = K.t_sub;
-  double lhl = K.lv00 + K.d0_vap * tz;
-  double lhi = K.LI00 + K.DC_ICE * tz;
-  double q_liq = qlz + qrz;
-  double q_sol = qiz + qsz + qgz;
-  double cvm = cvm_of(K, qvz, q_liq, q_sol);
-  double lcpk = lhl / cvm;
-  double icpk = lhi / cvm;
-  double tcpk = lcpk + icpk;
-  double tcp3 = lcpk + icpk * fmin(1.0, dim(tice, tz) / (tice - t_wfr));
+template <typename T>
+SHP void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh_rain, T& qaz, T& qgz, T& qiz,
+                        T& qlz, T& qrz, T& qsz, T& qvz, T& tz, T den, T denfac, T p1) {
+  const T tice = K.tice, t_wfr = K.t_wfr, t_sub = K.t_sub;
+  T lhl = K.lv00 + K.d0_vap * tz;
+  T lhi = K.LI00 + K.DC_ICE * tz;
+  T q_liq = qlz + qrz;
+  T q_sol = qiz + qsz + qgz;
+  T cvm = cvm_of(K, qvz, q_liq, q_sol);
+  T lcpk = lhl / cvm;
+  T icpk = lhi / cvm;
+  T tcpk = lcpk + icpk;
+  T tcp3 = lcpk + icpk * fmin(1.0, dim(tice, tz) / (tice - t_wfr));
   (void)tcpk;
   if (!(p1 >= P_MIN)) return;
   if (tz < K.T_MIN) {
-    double sink = dim(1.0e-7, qvz);
+    T sink = dim(1.0e-7, qvz);
     qvz = qvz - sink;
     qiz = qiz + sink;
     q_sol = q_sol + sink;
@@ -278,11 +298,11 @@ SHD void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
   icpk = lhi / cvm;
   tcpk = lcpk + icpk;
   tcp3 = lcpk + icpk * fmin(1.0, dim(tice, tz) / (tice - t_wfr));
-  double qpz = qvz + qlz + qiz;
-  double tin = tz - (lhl * (qlz + qiz) + lhi * qiz) / (K.c_air + qpz * K.c_vap + qrz * K.C_LIQ + (qsz + qgz) * K.C_ICE);
+  T qpz = qvz + qlz + qiz;
+  T tin = tz - (lhl * (qlz + qiz) + lhi * qiz) / (K.c_air + qpz * K.c_vap + qrz * K.C_LIQ + (qsz + qgz) * K.C_ICE);
   bool warm = tin > t_sub + 6.0;
   if (warm) {
-    double rh = qpz / iqs1(K, tin, den);
+    T rh = qpz / iqs1(K, tin, den);
     if (rh < rh_adj) {
       tz = tin;
       qvz = qpz;
@@ -292,12 +312,12 @@ SHD void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
     }
   }
   // cloud water <-> vapour adjustment (:531-554)
-  double dwsdt;
-  double qsw = wqs2(K, tz, den, dwsdt);
-  double dq0 = qsw - qvz;
-  double evap;
+  T dwsdt;
+  T qsw = wqs2(K, tz, den, dwsdt);
+  T dq0 = qsw - qvz;
+  T evap;
   if (dq0 > 0.0) {
-    double factor = fmin(1.0, K.fac_l2v * (10.0 * dq0 / qsw));
+    T factor = fmin(1.0, K.fac_l2v * (10.0 * dq0 / qsw));
     evap = fmin(qlz, factor * dq0 / (1.0 + tcp3 * dwsdt));
   } else {
     evap = dq0 / (1.0 + tcp3 * dwsdt);
@@ -310,9 +330,9 @@ SHD void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
   lhi = K.LI00 + K.DC_ICE * tz;
   icpk = lhi / cvm;
   // forced freezing below t_wfr (:560-575)
-  double dtmp = t_wfr - tz;
+  T dtmp = t_wfr - tz;
   if ((dtmp > 0.0) && (qlz > QCMIN)) {
-    double sink = fmin(qlz, fmin(qlz * dtmp * 0.125, dtmp / icpk));
+    T sink = fmin(qlz, fmin(qlz * dtmp * 0.125, dtmp / icpk));
     qlz = qlz - sink;
     qiz = qiz + sink;
     q_liq = q_liq - sink;
@@ -323,14 +343,14 @@ SHD void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
   lhi = K.LI00 + K.DC_ICE * tz;
   icpk = lhi / cvm;
   // Bigg mechanism (:581-605)
-  double dt_pisub;
+  T dt_pisub;
   if (K.fast_sat_adj) {
     dt_pisub = 0.5 * K.dts;
   } else {
     dt_pisub = K.dts;
-    double tc = tice - tz;
+    T tc = tice - tz;
     if ((qlz > QRMIN) && (tc > 0.0)) {
-      double sink = 3.3333e-10 * K.dts * (xexp(0.66 * tc) - 1.0) * den * qlz * qlz;
+      T sink = 3.3333e-10 * K.dts * (xexp(0.66 * tc) - 1.0) * den * qlz * qlz;
       sink = fmin(qlz, fmin(tc / icpk, sink));
       qlz = qlz - sink;
       qiz = qiz + sink;
@@ -347,11 +367,11 @@ SHD void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
   tcpk = lcpk + icpk;
   // ice deposition / sublimation (:614-661)
   if (tz < tice) {
-    double dqsdt;
-    double qsi = iqs2(K, tz, den, dqsdt);
-    double dq = qvz - qsi;
-    double sink = dq / (1.0 + tcpk * dqsdt);
-    double pidep;
+    T dqsdt;
+    T qsi = iqs2(K, tz, den, dqsdt);
+    T dq = qvz - qsi;
+    T sink = dq / (1.0 + tcpk * dqsdt);
+    T pidep;
     if (qiz > QRMIN) {
       pidep = dt_pisub * dq * 349138.78 * xexp(0.875 * xlog(qiz * den)) /
               (qsi * den * K.LAT2 / (0.0243 * K.RVGAS * sq(tz)) + 4.42478e4);
@@ -359,8 +379,8 @@ SHD void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
       pidep = 0.0;
     }
     if (dq > 0.0) {
-      double tmp = tice - tz;
-      double qi_crt = K.qi_gen * fmin(K.qi_lim, 0.1 * tmp) / den;
+      T tmp = tice - tz;
+      T qi_crt = K.qi_gen * fmin(K.qi_lim, 0.1 * tmp) / den;
       sink = fmin(sink, fmin(fmax(qi_crt - qiz, pidep), tmp / tcpk));
     } else {
       pidep = pidep * fmin(1.0, dim(tz, t_sub) * 0.2);
@@ -379,13 +399,13 @@ SHD void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
   tcpk = lcpk + icpk;
   // snow sublimation / deposition (:670-706)
   if (qsz > QRMIN) {
-    double dqsdt;
-    double qsi = iqs2(K, tz, den, dqsdt);
-    double qden = qsz * den;
-    double tmp = xexp(0.65625 * xlog(qden));
-    double tsq = tz * tz;
-    double dq = (qsi - qvz) / (1.0 + tcpk * dqsdt);
-    double pssub = K.cssub[0] * tsq * (K.cssub[1] * sqrt(qden) + K.cssub[2] * tmp * sqrt(denfac)) /
+    T dqsdt;
+    T qsi = iqs2(K, tz, den, dqsdt);
+    T qden = qsz * den;
+    T tmp = xexp(0.65625 * xlog(qden));
+    T tsq = tz * tz;
+    T dq = (qsi - qvz) / (1.0 + tcpk * dqsdt);
+    T pssub = K.cssub[0] * tsq * (K.cssub[1] * sqrt(qden) + K.cssub[2] * tmp * sqrt(denfac)) /
                    (K.cssub[3] * tsq + K.cssub[4] * qsi * den);
     pssub = (qsi - qvz) * K.dts * pssub;
     if (pssub > 0.0) {
@@ -409,10 +429,10 @@ SHD void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
   tcpk = lcpk + icpk;
   // graupel sublimation / deposition (:715-746)
   if (qgz > QRMIN) {
-    double dqsdt;
-    double qsi = iqs2(K, tz, den, dqsdt);
-    double dq = (qvz - qsi) / (1.0 + tcpk * dqsdt);
-    double pgsub = (qvz / qsi - 1.0) * qgz;
+    T dqsdt;
+    T qsi = iqs2(K, tz, den, dqsdt);
+    T dq = (qvz - qsi) / (1.0 + tcpk * dqsdt);
+    T pgsub = (qvz / qsi - 1.0) * qgz;
     if (pgsub > 0.0) {
       if (tz > tice)
         pgsub = 0.0;
@@ -431,9 +451,9 @@ SHD void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
   lhl = K.lv00 + K.d0_vap * tz;
   lcpk = lhl / cvm;
   if (qrz > QCMIN) {
-    double dqsdt;
-    double qsw2 = wqs2(K, tz, den, dqsdt);
-    double sink = fmin(qrz, dim(rh_rain * qsw2, qvz) / (1.0 + lcpk * dqsdt));
+    T dqsdt;
+    T qsw2 = wqs2(K, tz, den, dqsdt);
+    T sink = fmin(qrz, dim(rh_rain * qsw2, qvz) / (1.0 + lcpk * dqsdt));
     qvz = qvz + sink;
     qrz = qrz - sink;
     q_liq = q_liq - sink;
@@ -447,18 +467,18 @@ SHD void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
   if (!K.do_qa) {
     q_sol = K.rad_snow ? qiz + qsz : qiz;
     q_liq = K.rad_rain ? qlz + qrz : qlz;
-    double q_cond = q_liq + q_sol;
-    double qpz2 = qvz + q_cond;
-    double tin2 = tz - (lcpk * q_cond + icpk * q_sol);
-    double qstar;
+    T q_cond = q_liq + q_sol;
+    T qpz2 = qvz + q_cond;
+    T tin2 = tz - (lcpk * q_cond + icpk * q_sol);
+    T qstar;
     if (tin2 <= t_wfr) {
       qstar = iqs1(K, tin2, den);
     } else if (tin2 >= tice) {
       qstar = wqs1(K, tin2, den);
     } else {
-      double qsi = iqs1(K, tin2, den);
-      double qsw3 = wqs1(K, tin2, den);
-      double rqi;
+      T qsi = iqs1(K, tin2, den);
+      T qsw3 = wqs1(K, tin2, den);
+      T rqi;
       if (q_cond > 3.0e-6)
         rqi = q_sol / q_cond;
       else
@@ -466,9 +486,9 @@ SHD void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
       qstar = rqi * qsi + (1.0 - rqi) * qsw3;
     }
     if (qpz2 > QRMIN) {
-      double dq = fmax(QCMIN, h_var * qpz2);
-      double q_plus = qpz2 + dq;
-      double q_minus = qpz2 - dq;
+      T dq = fmax(QCMIN, h_var * qpz2);
+      T q_plus = qpz2 + dq;
+      T q_minus = qpz2 - dq;
       if (qstar < q_minus)
         qaz = qaz + 1.0;
       else if ((qstar < q_plus) && (q_cond > K.qc_crt))
@@ -480,39 +500,39 @@ SHD void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
 // ---------------------------------------------------- microphysics_funcs.py:853-1227
 // Ice-phase processes before the saturation adjustment; the caller runs
 // subgrid_z_proc afterwards (icloud_main's tail call, :1229-1258).
-SHD void icloud_processes(const MpConst& K, double& qgz, double& qiz, double& qlz, double& qrz, double& qsz,
-                          double qvz, double& tz, double den, double denfac, double vtgz, double vtrz, double vtsz,
-                          double p1, double di, double q_liq, double q_sol, double cvm) {
-  const double tice = K.tice, dts = K.dts, rdts = K.rdts;
-  double lhi = K.LI00 + K.DC_ICE * tz;
-  double icpk = lhi / cvm;
+template <typename T>
+SHP void icloud_processes(const MpConst& K, T& qgz, T& qiz, T& qlz, T& qrz, T& qsz, T qvz, T& tz, T den, T denfac,
+                          T vtgz, T vtrz, T vtsz, T p1, T di, T q_liq, T q_sol, T cvm) {
+  const T tice = K.tice, dts = K.dts, rdts = K.rdts;
+  T lhi = K.LI00 + K.DC_ICE * tz;
+  T icpk = lhi / cvm;
   if (!(p1 >= P_MIN)) return;
-  double pgacr = 0.0;
-  double pgacw = 0.0;
-  double tc = tz - tice;
+  T pgacr = 0.0;
+  T pgacw = 0.0;
+  T tc = tz - tice;
   if (tc >= 0.0) {
-    double dqs0 = K.ces0 / p1 - qvz;
+    T dqs0 = K.ces0 / p1 - qvz;
     if (qsz > QCMIN) {
-      double psacw, psacr, pracs;
+      T psacw, psacr, pracs;
       if (qlz > QRMIN) {
-        double factor = denfac * K.csacw * xexp(0.8125 * xlog(qsz * den));
+        T factor = denfac * K.csacw * xexp(0.8125 * xlog(qsz * den));
         psacw = factor / (1.0 + dts * factor) * qlz;
       } else {
         psacw = 0.0;
       }
       if (qrz > QRMIN) {
-        psacr = fmin(acr3d<double>(vtsz, vtrz, qrz, qsz, K.csacr, K.acco[0][1], K.acco[1][1], K.acco[2][1], den),
+        psacr = fmin(acr3d<T>(vtsz, vtrz, qrz, qsz, K.csacr, K.acco[0][1], K.acco[1][1], K.acco[2][1], den),
                      qrz * rdts);
-        pracs = acr3d<double>(vtrz, vtsz, qsz, qrz, K.cracs, K.acco[0][0], K.acco[1][0], K.acco[2][0], den);
+        pracs = acr3d<T>(vtrz, vtsz, qsz, qrz, K.cracs, K.acco[0][0], K.acco[1][0], K.acco[2][0], den);
       } else {
         psacr = 0.0;
         pracs = 0.0;
       }
-      double psmlt = fmax(0.0, smlt<double>(tc, dqs0, qsz * den, psacw, psacr, K.csmlt[0], K.csmlt[1], K.csmlt[2],
+      T psmlt = fmax(0.0, smlt<T>(tc, dqs0, qsz * den, psacw, psacr, K.csmlt[0], K.csmlt[1], K.csmlt[2],
                                              K.csmlt[3], K.csmlt[4], den, denfac));
-      double sink = fmin(qsz, fmin(dts * (psmlt + pracs), tc / icpk));
+      T sink = fmin(qsz, fmin(dts * (psmlt + pracs), tc / icpk));
       qsz = qsz - sink;
-      double tmp = fmin(sink, dim(K.qs_mlt, qlz));
+      T tmp = fmin(sink, dim(K.qs_mlt, qlz));
       qlz = qlz + tmp;
       qrz = qrz + sink - tmp;
       q_liq = q_liq + sink;
@@ -525,15 +545,15 @@ SHD void icloud_processes(const MpConst& K, double& qgz, double& qiz, double& ql
     icpk = lhi / cvm;
     if ((qgz > QCMIN) && (tc > 0.0)) {
       if (qrz > QRMIN) {
-        pgacr = fmin(acr3d<double>(vtgz, vtrz, qrz, qgz, K.cgacr, K.acco[0][2], K.acco[1][2], K.acco[2][2], den),
+        pgacr = fmin(acr3d<T>(vtgz, vtrz, qrz, qgz, K.cgacr, K.acco[0][2], K.acco[1][2], K.acco[2][2], den),
                      rdts * qrz);
       }
-      double qden = qgz * den;
+      T qden = qgz * den;
       if (qlz > QRMIN) {
-        double factor = K.cgacw * qden / sqrt(den * sqrt(sqrt(qden)));
+        T factor = K.cgacw * qden / sqrt(den * sqrt(sqrt(qden)));
         pgacw = factor / (1.0 + dts * factor) * qlz;
       }
-      double pgmlt = dts * gmlt<double>(tc, dqs0, qden, pgacw, pgacr, K.cgmlt[0], K.cgmlt[1], K.cgmlt[2],
+      T pgmlt = dts * gmlt<T>(tc, dqs0, qden, pgacw, pgacr, K.cgmlt[0], K.cgmlt[1], K.cgmlt[2],
                                         K.cgmlt[3], K.cgmlt[4], den);
       pgmlt = fmin(fmax(0.0, pgmlt), fmin(qgz, tc / icpk));
       qgz = qgz - pgmlt;
@@ -545,20 +565,20 @@ SHD void icloud_processes(const MpConst& K, double& qgz, double& qiz, double& ql
     }
   } else {
     if (qiz > 3.0e-7) {
-      double psaci;
+      T psaci;
       if (qsz > 1.0e-7) {
-        double factor = dts * denfac * K.csaci * xexp(0.05 * tc + 0.8125 * xlog(qsz * den));
+        T factor = dts * denfac * K.csaci * xexp(0.05 * tc + 0.8125 * xlog(qsz * den));
         psaci = factor / (1.0 + factor) * qiz;
       } else {
         psaci = 0.0;
       }
-      double qim = K.qi0_crt / den;
-      double tmp = K.const_vi ? K.fac_i2s : K.fac_i2s * xexp(0.025 * tc);
+      T qim = K.qi0_crt / den;
+      T tmp = K.const_vi ? K.fac_i2s : K.fac_i2s * xexp(0.025 * tc);
       di = fmax(di, QRMIN);
-      double q_plus = qiz + di;
-      double psaut;
+      T q_plus = qiz + di;
+      T psaut;
       if (q_plus > (qim + QRMIN)) {
-        double dq;
+        T dq;
         if (qim > (qiz - di))
           dq = (0.25 * sq(q_plus - qim)) / di;
         else
@@ -567,26 +587,26 @@ SHD void icloud_processes(const MpConst& K, double& qgz, double& qiz, double& ql
       } else {
         psaut = 0.0;
       }
-      double sink = fmin(0.75 * qiz, psaci + psaut);
+      T sink = fmin(0.75 * qiz, psaci + psaut);
       qiz = qiz - sink;
       qsz = qsz + sink;
       if (qgz > 1.0e-6) {
-        double factor = dts * K.cgaci * sqrt(den) * qgz;
-        double pgaci = factor / (1.0 + factor) * qiz;
+        T factor = dts * K.cgaci * sqrt(den) * qgz;
+        T pgaci = factor / (1.0 + factor) * qiz;
         qiz = qiz - pgaci;
         qgz = qgz + pgaci;
       }
     }
     tc = tz - tice;
     if ((qrz > 1e-7) && (tc < 0.0)) {
-      double psacr;
+      T psacr;
       if (qsz > 1.0e-7)
-        psacr = dts * acr3d<double>(vtsz, vtrz, qrz, qsz, K.csacr, K.acco[0][1], K.acco[1][1], K.acco[2][1], den);
+        psacr = dts * acr3d<T>(vtsz, vtrz, qrz, qsz, K.csacr, K.acco[0][1], K.acco[1][1], K.acco[2][1], den);
       else
         psacr = 0.0;
-      double pgfr = dts * K.cgfr[0] / den * (xexp(-K.cgfr[1] * tc) - 1.0) * xexp(1.75 * xlog(qrz * den));
-      double sink = psacr + pgfr;
-      double factor = fmin(sink, fmin(qrz, -tc / icpk)) / fmax(sink, QRMIN);
+      T pgfr = dts * K.cgfr[0] / den * (xexp(-K.cgfr[1] * tc) - 1.0) * xexp(1.75 * xlog(qrz * den));
+      T sink = psacr + pgfr;
+      T factor = fmin(sink, fmin(qrz, -tc / icpk)) / fmax(sink, QRMIN);
       psacr = factor * psacr;
       pgfr = factor * pgfr;
       sink = psacr + pgfr;
@@ -601,14 +621,14 @@ SHD void icloud_processes(const MpConst& K, double& qgz, double& qiz, double& ql
     lhi = K.LI00 + K.DC_ICE * tz;
     icpk = lhi / cvm;
     if (qsz > 1.0e-7) {
-      double sink;
+      T sink;
       if (qgz > QRMIN)
-        sink = dts * acr3d<double>(vtgz, vtsz, qsz, qgz, K.cgacs, K.acco[0][3], K.acco[1][3], K.acco[2][3], den);
+        sink = dts * acr3d<T>(vtgz, vtsz, qsz, qgz, K.cgacs, K.acco[0][3], K.acco[1][3], K.acco[2][3], den);
       else
         sink = 0.0;
-      double qsm = K.qs0_crt / den;
+      T qsm = K.qs0_crt / den;
       if (qsz > qsm) {
-        double factor = dts * 1.0e-3 * xexp(0.09 * (tz - tice));
+        T factor = dts * 1.0e-3 * xexp(0.09 * (tz - tice));
         sink = sink + factor / (1.0 + factor) * (qsz - qsm);
       }
       sink = fmin(qsz, sink);
@@ -617,20 +637,20 @@ SHD void icloud_processes(const MpConst& K, double& qgz, double& qiz, double& ql
     }
     if ((qgz > 1.0e-7) && (tz < K.tice0)) {
       if (qlz > 1.0e-6) {
-        double qden = qgz * den;
-        double factor = dts * K.cgacw * qden / sqrt(den * sqrt(sqrt(qden)));
+        T qden = qgz * den;
+        T factor = dts * K.cgacw * qden / sqrt(den * sqrt(sqrt(qden)));
         pgacw = factor / (1.0 + factor) * qlz;
       } else {
         pgacw = 0.0;
       }
       if (qrz > 1.0e-6) {
-        pgacr = fmin(dts * acr3d<double>(vtgz, vtrz, qrz, qgz, K.cgacr, K.acco[0][2], K.acco[1][2], K.acco[2][2], den),
+        pgacr = fmin(dts * acr3d<T>(vtgz, vtrz, qrz, qgz, K.cgacr, K.acco[0][2], K.acco[1][2], K.acco[2][2], den),
                      qrz);
       } else {
         pgacr = 0.0;
       }
-      double sink = pgacr + pgacw;
-      double factor = fmin(sink, dim(tice, tz) / icpk) / fmax(sink, QRMIN);
+      T sink = pgacr + pgacw;
+      T factor = fmin(sink, dim(tice, tz) / icpk) / fmax(sink, QRMIN);
       pgacr = factor * pgacr;
       pgacw = factor * pgacw;
       sink = pgacr + pgacw;

@@ -118,6 +118,38 @@ int shield_mp_destroy(void* handle);
 /* Copies the handle's last error message (NUL terminated) into buf. */
 int shield_mp_last_error(void* handle, char* buf, size_t n);
 
+/* ---------------------------------------------------------------------------
+ * Adjoint of the step. pySHiELD has no adjoint; this is the vector-Jacobian
+ * product (VJP) of one Microphysics.__call__ (microphysics.py:1981-2263),
+ * evaluated in FP64 by a hand-written reverse kernel that replays the step
+ * from its inputs.
+ *
+ * Outputs of the step, whose cotangents are given: the ten tendencies
+ * (as written by the step: udt and vdt for levels k >= 1 only), wmp (when
+ * do_sedi_w), and the four surface totals. Inputs, whose adjoints are
+ * written (assigned): the 13 state fields of ShieldMpFields (pt, the six
+ * species, qcld, ua, va, delprsi, delz, wmp). The incoming tendencies only
+ * add to the outputs and are not differentiated; the persistent
+ * cloud-fraction accumulator only adds a constant to qa_dt.
+ *
+ * Branches follow the forward at the given input. Supported: the plain form
+ * and configurations without do_sedi_heat and de_ice, with at most 4
+ * sub-steps (SHIELD_ELAYOUT otherwise). */
+typedef struct {
+  ShieldField3D pt_dt, qv_dt, ql_dt, qr_dt, qi_dt, qs_dt, qg_dt, qa_dt, udt, vdt, wmp;
+  const double *rain, *snow, *ice, *graupel; /* ncol each (column c = j*nx + i), or NULL for zero */
+} ShieldMpCotangents;
+
+typedef struct {
+  ShieldField3D pt, qvapor, qliquid, qrain, qice, qsnow, qgraupel, qcld, ua, va, delprsi, delz, wmp;
+} ShieldMpGradients;
+
+/* state: the step's input state (its 13 state fields and land are read; its
+ * tendency and precipitation pointers are ignored). A gradient pointer may
+ * be NULL to skip that field. */
+int shield_mp_step_vjp(void* handle, const ShieldMpFields* state, const ShieldMpCotangents* cot,
+                       const ShieldMpGradients* grad, double timestep, void* stream);
+
 /* Allocation-free step: one step of shield_mp_step with no handle and no
  * device allocation. It has no counterpart in the reference. It is meant for
  * hosts that may not call cudaMalloc: a model whose memory pool owns all of

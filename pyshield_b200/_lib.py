@@ -103,6 +103,16 @@ class ShieldMpFields(ctypes.Structure):
     )
 
 
+class ShieldMpCotangents(ctypes.Structure):
+    _fields_ = [(n, ShieldField3D) for n in MP_TENDENCY_FIELDS + ("wmp",)] + [
+        (n, ctypes.c_void_p) for n in ("rain", "snow", "ice", "graupel")
+    ]
+
+
+class ShieldMpGradients(ctypes.Structure):
+    _fields_ = [(n, ShieldField3D) for n in MP_STATE_FIELDS]
+
+
 class ShieldMpMember(ctypes.Structure):
     _fields_ = [
         ("fields", ShieldMpFields),
@@ -130,6 +140,7 @@ EXPORTS = (
     "shield_mp_ensemble_qaz",
     "shield_mp_ensemble_destroy",
     "shield_mp_step_noalloc",
+    "shield_mp_step_vjp",
 )
 
 _lib = None
@@ -170,6 +181,9 @@ def load():
     lib.shield_mp_ensemble_qaz.argtypes = [vp, i32, vp, vp]
     lib.shield_mp_ensemble_destroy.argtypes = [vp]
     lib.shield_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+    lib.shield_mp_step_vjp.argtypes = [
+        vp, ctypes.POINTER(ShieldMpFields), ctypes.POINTER(ShieldMpCotangents), ctypes.POINTER(ShieldMpGradients), dbl, vp,
+    ]
     lib.shield_mp_step_noalloc.argtypes = [
         ctypes.POINTER(ShieldMpConfig), i32, i32, i32, ShieldField2D, ctypes.POINTER(ShieldMpFields), dbl, i32, i32, vp,
     ]

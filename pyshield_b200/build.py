@@ -28,6 +28,7 @@ UNITS = [
     ("mp_plain.cu", ["-fmad=false"]),
     ("mp_mixed.cu", []),
     ("coupling.cu", ["-fmad=false"]),
+    ("mp_vjp.cu", ["-fmad=false"]),
 ]
 
 

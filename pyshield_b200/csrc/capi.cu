@@ -158,6 +158,57 @@ extern "C" int shield_mp_step(void* handle, const ShieldMpFields* F, double time
   return SHIELD_OK;
 }
 
+extern "C" int shield_mp_step_vjp(void* handle, const ShieldMpFields* F, const ShieldMpCotangents* cot,
+                                  const ShieldMpGradients* grad, double timestep, void* stream) {
+  Handle* h = static_cast<Handle*>(handle);
+  if (!h) return fail(nullptr, SHIELD_EINVAL, "null handle");
+  if (!F || !cot || !grad) return fail(h, SHIELD_EINVAL, "null fields, cotangents or gradients");
+  if (h->cfg.do_sedi_heat || h->cfg.de_ice)
+    return fail(h, SHIELD_ELAYOUT, "the adjoint does not support do_sedi_heat or de_ice");
+  MpConst K = h->K;
+  if (timestep != K.timestep) {
+    std::string why;
+    if (set_timestep(h->cfg, K, timestep, why) != SHIELD_OK) return fail(h, SHIELD_EINVAL, why);
+  }
+  if (K.ntimes > mp_vjp_max_substeps())
+    return fail(h, SHIELD_ELAYOUT, "the adjoint supports at most " + std::to_string(mp_vjp_max_substeps()) +
+                                       " sub-steps (timestep / mp_time)");
+  VjpArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.K = K;
+  A.KF = to_float(K);
+  A.nx = h->nx;
+  A.ny = h->ny;
+  A.nz = h->nz;
+  A.ncol = h->ncol;
+  const ShieldField3D* ins[] = {&F->pt, &F->qvapor, &F->qliquid, &F->qrain, &F->qice, &F->qsnow, &F->qgraupel,
+                                &F->qcld, &F->ua, &F->va, &F->delprsi, &F->delz, &F->wmp};
+  const ShieldField3D* cots[] = {&cot->pt_dt, &cot->qv_dt, &cot->ql_dt, &cot->qr_dt, &cot->qi_dt, &cot->qs_dt,
+                                 &cot->qg_dt, &cot->qa_dt, &cot->udt,   &cot->vdt,   &cot->wmp};
+  const ShieldField3D* grads[] = {&grad->pt,   &grad->qvapor, &grad->qliquid, &grad->qrain, &grad->qice,
+                                  &grad->qsnow, &grad->qgraupel, &grad->qcld,  &grad->ua,    &grad->va,
+                                  &grad->delprsi, &grad->delz,  &grad->wmp};
+  for (int f = 0; f < N_VJP_IN; ++f) {
+    if (!ins[f]->ptr) return fail(h, SHIELD_EINVAL, "null input field pointer");
+    A.in[f] = f3(*ins[f]);
+    A.grad[f] = f3(*grads[f]);
+  }
+  for (int f = 0; f < N_VJP_COT; ++f) {
+    if (!cots[f]->ptr) return fail(h, SHIELD_EINVAL, "null cotangent pointer");
+    A.cot[f] = f3(*cots[f]);
+  }
+  if (!F->land.ptr) return fail(h, SHIELD_EINVAL, "null land pointer");
+  A.land = Fld2{F->land.ptr, F->land.si, F->land.sj};
+  A.area = Fld2{h->area, 1, h->nx};
+  A.rain_b = cot->rain;
+  A.snow_b = cot->snow;
+  A.ice_b = cot->ice;
+  A.graupel_b = cot->graupel;
+  cudaError_t e = mp_launch_vjp(A, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return cuda_fail(h, e, "adjoint launch");
+  return SHIELD_OK;
+}
+
 extern "C" int shield_mp_destroy(void* handle) {
   Handle* h = static_cast<Handle*>(handle);
   if (!h) return SHIELD_OK;

@@ -1801,4 +1801,189 @@ SHP void subgrid_z_proc_b(const MpConst& K, double h_var, double rh_adj, double 
   tz_b = Zb.tz;
 }
 
+// ------------------------------------------ pointwise blocks of the step
+// sedi_ice_melt: state (qv ql qr qi qs qg tz); qv qs qg are read only
+SHP void sedi_ice_melt_b(const MpConst& K, double qv, double ql, double qr, double qi, double qs, double qg, double tz,
+                         double& qv_b, double& ql_b, double& qr_b, double& qi_b, double& qs_b, double& qg_b,
+                         double& tz_b) {
+  const double lhi = K.LI00 + K.DC_ICE * tz;
+  const double q_liq = ql + qr;
+  const double q_sol = qi + qs + qg;
+  const double cvm = K.c_air + qv * K.c_vap + q_liq * K.C_LIQ + q_sol * K.C_ICE;
+  const double icpk = lhi / cvm;
+  const double tc = tz - K.tice;
+  if (!((qi > QCMIN) && (tc > 0.0))) return;
+  const double r = K.fac_imlt * tc / icpk;
+  const double sink = fmin(qi, r);
+  const double dm = dim(K.ql_mlt, ql);
+  const double q_liq1 = q_liq + sink, q_sol1 = q_sol - sink;
+  const double cvm1 = K.c_air + qv * K.c_vap + q_liq1 * K.C_LIQ + q_sol1 * K.C_ICE;
+  // tz' = tz - sink lhi / cvm1
+  double sink_b = -tz_b * lhi / cvm1;
+  double lhi_b = -tz_b * sink / cvm1;
+  const double cvm1_b = tz_b * sink * lhi / (cvm1 * cvm1);
+  qv_b += cvm1_b * K.c_vap;
+  const double q_liq_b = cvm1_b * K.C_LIQ, q_sol_b = cvm1_b * K.C_ICE;  // q_liq1, q_sol1 adjoints
+  sink_b += q_liq_b - q_sol_b;
+  sink_b -= qi_b;
+  sink_b += qr_b;
+  const double tmp_b = ql_b - qr_b;
+  if (min_first(sink, dm))
+    sink_b += tmp_b;
+  else if (K.ql_mlt - ql > 0.0)
+    ql_b -= tmp_b;
+  double tc_b = 0.0, icpk_b = 0.0;
+  if (min_first(qi, r)) {
+    qi_b += sink_b;
+  } else {
+    tc_b += sink_b * K.fac_imlt / icpk;
+    icpk_b -= sink_b * r / icpk;
+  }
+  tz_b += tc_b;
+  // icpk = lhi / cvm, cvm from the entry totals
+  lhi_b += icpk_b / cvm;
+  const double cvm_b = -icpk_b * icpk / cvm;
+  qv_b += cvm_b * K.c_vap;
+  const double ql0_b = q_liq_b + cvm_b * K.C_LIQ, qs0_b = q_sol_b + cvm_b * K.C_ICE;
+  ql_b += ql0_b;
+  qr_b += ql0_b;
+  qi_b += qs0_b;
+  qs_b += qs0_b;
+  qg_b += qs0_b;
+  tz_b += lhi_b * K.DC_ICE;
+}
+
+// icloud_melt_freeze: state (qv ql qr qi qs qg tz) and den; outputs also the
+// totals q_liq, q_sol and cvm, whose adjoints come in q_liq_b, q_sol_b, cvm_b
+SHP void icloud_melt_freeze_b(const MpConst& K, double qv, double ql, double qr, double qi, double qs, double qg,
+                              double tz, double den, double q_liq_b, double q_sol_b, double cvm_b, double& qv_b,
+                              double& ql_b, double& qr_b, double& qi_b, double& qs_b, double& qg_b, double& tz_b,
+                              double& den_b) {
+  const double lhi = K.LI00 + K.DC_ICE * tz;
+  const double q_liq = ql + qr;
+  const double q_sol = qi + qs + qg;
+  const double cvm = K.c_air + qv * K.c_vap + q_liq * K.C_LIQ + q_sol * K.C_ICE;
+  const double icpk = lhi / cvm;
+  double lhi_b = 0.0, icpk_b = 0.0, qliq_b = q_liq_b, qsol_b = q_sol_b, cvm0_b = cvm_b;
+  if ((tz > K.tice) && (qi > QCMIN)) {
+    const double r = K.fac_imlt * (tz - K.tice) / icpk;
+    const double melt = fmin(qi, r);
+    const double dm = dim(K.ql_mlt, ql);
+    const double q_liq1 = q_liq + melt, q_sol1 = q_sol - melt;
+    const double cvm1 = K.c_air + qv * K.c_vap + q_liq1 * K.C_LIQ + q_sol1 * K.C_ICE;
+    double melt_b = -tz_b * lhi / cvm1;
+    lhi_b -= tz_b * melt / cvm1;
+    const double cvm1_b = cvm_b + tz_b * melt * lhi / (cvm1 * cvm1);
+    qv_b += cvm1_b * K.c_vap;
+    qliq_b += cvm1_b * K.C_LIQ;
+    qsol_b += cvm1_b * K.C_ICE;
+    melt_b += qliq_b - qsol_b - qi_b + qr_b;
+    const double tmp_b = ql_b - qr_b;
+    if (min_first(melt, dm))
+      melt_b += tmp_b;
+    else if (K.ql_mlt - ql > 0.0)
+      ql_b -= tmp_b;
+    if (min_first(qi, r)) {
+      qi_b += melt_b;
+    } else {
+      tz_b += melt_b * K.fac_imlt / icpk;
+      icpk_b -= melt_b * r / icpk;
+    }
+    cvm0_b = 0.0;
+  } else if ((tz < K.t_wfr) && (ql > QCMIN)) {
+    const double dtmp = K.t_wfr - tz;
+    const double fr = dtmp / DT_FR;
+    const double factor = fmin(1.0, fr);
+    const double a = ql * factor, b = dtmp / icpk;
+    const double sink = fmin(a, b);
+    const double lim = fmin(K.qi_lim, 0.1 * (K.tice - tz));
+    const double qi_crt = K.qi_gen * lim / den;
+    const double dm = dim(qi_crt, qi);
+    const double tmp = fmin(sink, dm);
+    const double q_liq1 = q_liq - sink, q_sol1 = q_sol + sink;
+    const double cvm1 = K.c_air + qv * K.c_vap + q_liq1 * K.C_LIQ + q_sol1 * K.C_ICE;
+    double sink_b = tz_b * lhi / cvm1;
+    lhi_b += tz_b * sink / cvm1;
+    const double cvm1_b = cvm_b - tz_b * sink * lhi / (cvm1 * cvm1);
+    qv_b += cvm1_b * K.c_vap;
+    qliq_b += cvm1_b * K.C_LIQ;
+    qsol_b += cvm1_b * K.C_ICE;
+    sink_b += -qliq_b + qsol_b - ql_b + qs_b;
+    const double tmp_b = qi_b - qs_b;
+    double dtmp_b = 0.0;
+    if (min_first(sink, dm)) {
+      sink_b += tmp_b;
+    } else if (qi_crt - qi > 0.0) {
+      qi_b -= tmp_b;
+      const double lim_b = tmp_b * K.qi_gen / den;
+      den_b -= tmp_b * qi_crt / den;
+      if (!min_first(K.qi_lim, 0.1 * (K.tice - tz))) tz_b -= 0.1 * lim_b;
+    }
+    (void)tmp;
+    if (min_first(a, b)) {
+      ql_b += sink_b * factor;
+      if (!min_first(1.0, fr)) dtmp_b += sink_b * ql / DT_FR;
+    } else {
+      dtmp_b += sink_b / icpk;
+      icpk_b -= sink_b * b / icpk;
+    }
+    tz_b -= dtmp_b;
+    cvm0_b = 0.0;
+  }
+  lhi_b += icpk_b / cvm;
+  cvm0_b -= icpk_b * icpk / cvm;
+  qv_b += cvm0_b * K.c_vap;
+  qliq_b += cvm0_b * K.C_LIQ;
+  qsol_b += cvm0_b * K.C_ICE;
+  ql_b += qliq_b;
+  qr_b += qliq_b;
+  qi_b += qsol_b;
+  qs_b += qsol_b;
+  qg_b += qsol_b;
+  tz_b += lhi_b * K.DC_ICE;
+}
+
+// fix_negative_point: state (qv ql qr qi qs qg tz)
+SHP void fix_negative_point_b(const MpConst& K, double qv, double ql, double qr, double qi, double qs, double qg,
+                              double tz, double& qv_b, double& ql_b, double& qr_b, double& qi_b, double& qs_b,
+                              double& qg_b, double& tz_b) {
+  const double cvm = K.c_air + qv * K.c_vap + (qr + ql) * K.C_LIQ + (qi + qs + qg) * K.C_ICE;
+  const double lhl = K.lv00 + K.d0_vap * tz, lhi = K.LI00 + K.DC_ICE * tz;
+  const double lcpk = lhl / cvm, icpk = lhi / cvm;
+  // replay, keeping the branch decisions and the values they read
+  const bool bi = qi < 0.0;
+  const double qs1 = bi ? qs + qi : qs;
+  const bool bs = qs1 < 0.0;
+  const double qg1 = bs ? qg + qs1 : qg;
+  const bool bg = qg1 < 0.0;
+  const double qr1 = bg ? qr + qg1 : qr;
+  const bool br = qr1 < 0.0;
+  const double ql1 = br ? ql + qr1 : ql;
+  const bool bl = ql1 < 0.0;
+  // reverse; each name_b below is the adjoint of that version of the value
+  double lcpk_b = 0.0, icpk_b = 0.0;
+  double ql1_b = ql_b;
+  if (bl) {  // qv += ql1; tz -= ql1 lcpk; ql = 0
+    ql1_b = qv_b - tz_b * lcpk;
+    lcpk_b -= tz_b * ql1;
+  }
+  const double qr1_b = br ? ql1_b : qr_b;  // ql1 = ql + qr1; qr = 0
+  double qg1_b = qg_b;
+  if (bg) {  // qr1 = qr + qg1; tz -= qg1 icpk; qg = 0
+    qg1_b = qr1_b - tz_b * icpk;
+    icpk_b -= tz_b * qg1;
+  }
+  const double qs1_b = bs ? qg1_b : qs_b;  // qg1 = qg + qs1; qs = 0
+  const double qi0_b = bi ? qs1_b : qi_b;  // qs1 = qs + qi; qi = 0
+  // lcpk = lhl / cvm, icpk = lhi / cvm
+  const double cvm_b = -lcpk_b * lcpk / cvm - icpk_b * icpk / cvm;
+  tz_b += lcpk_b / cvm * K.d0_vap + icpk_b / cvm * K.DC_ICE;
+  qv_b += cvm_b * K.c_vap;
+  ql_b = ql1_b + cvm_b * K.C_LIQ;
+  qr_b = qr1_b + cvm_b * K.C_LIQ;
+  qi_b = qi0_b + cvm_b * K.C_ICE;
+  qs_b = qs1_b + cvm_b * K.C_ICE;
+  qg_b = qg1_b + cvm_b * K.C_ICE;
+}
+
 }  // namespace shield

@@ -44,7 +44,8 @@ struct Tiles {
 template <int NW>
 struct Column {
   int w, lane, k, L, bar;
-  double* scr;  // 2 * SCR doubles
+  double* scr;   // 2 * SCR doubles
+  double* work;  // 2 * RP doubles, for the sequential vapour borrow
   int par;
 
   SHD void sync() const { asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(32 * NW) : "memory"); }
@@ -323,6 +324,99 @@ struct Column {
       zn = zs + (zn_in_warp + c);
     return (k == L - 1) ? ze - zs : ze - zn;
   }
+  // ---------------------------------------------- exchanges of the adjoint
+  // values at level k + 1 of N fields with one barrier (undefined at the
+  // last level of the group)
+  template <int N>
+  SHD void nextN(const double (&x)[N], double (&xn)[N]) {
+#pragma unroll
+    for (int n = 0; n < N; ++n) xn[n] = __shfl_down_sync(FULLMASK, x[n], 1);
+    if (NW == 1) return;
+    double* s = slot();
+    if (lane == 0) {
+#pragma unroll
+      for (int n = 0; n < N; ++n) s[N * w + n] = x[n];
+    }
+    sync();
+    if (lane == 31 && w < NW - 1) {
+#pragma unroll
+      for (int n = 0; n < N; ++n) xn[n] = s[N * (w + 1) + n];
+    }
+  }
+  // x at level k - 1 and y at level k + 1 with one barrier
+  SHD void prev_next(double x, double y, double& xp, double& yn) {
+    xp = __shfl_up_sync(FULLMASK, x, 1);
+    yn = __shfl_down_sync(FULLMASK, y, 1);
+    if (NW == 1) return;
+    double* s = slot();
+    if (lane == 31) s[2 * w] = x;
+    if (lane == 0) s[2 * w + 1] = y;
+    sync();
+    if (lane == 0 && w > 0) xp = s[2 * (w - 1)];
+    if (lane == 31 && w < NW - 1) yn = s[2 * (w + 1) + 1];
+  }
+  // N independent bottom-up affine scans X_k = a_k + c_k X_{k+1} with one
+  // barrier (c must vanish at the last level); the adjoints of the
+  // top-down recurrences
+  template <int N>
+  SHD void scanN_rev(const double (&a)[N], const double (&c)[N], double (&x)[N]) {
+    double A[N], B[N];
+#pragma unroll
+    for (int n = 0; n < N; ++n) {
+      A[n] = a[n];
+      B[n] = c[n];
+    }
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+#pragma unroll
+      for (int n = 0; n < N; ++n) {
+        const double pA = __shfl_down_sync(FULLMASK, A[n], d);
+        const double pB = __shfl_down_sync(FULLMASK, B[n], d);
+        if (lane + d < 32) {
+          A[n] = A[n] + B[n] * pA;
+          B[n] = B[n] * pB;
+        }
+      }
+    }
+    if (NW == 1) {
+#pragma unroll
+      for (int n = 0; n < N; ++n) x[n] = A[n];
+      return;
+    }
+    double* s = slot();
+    if (lane == 0) {
+#pragma unroll
+      for (int n = 0; n < N; ++n) {
+        s[2 * N * w + 2 * n] = A[n];
+        s[2 * N * w + 2 * n + 1] = B[n];
+      }
+    }
+    sync();
+#pragma unroll
+    for (int n = 0; n < N; ++n) {
+      double X = 0.0;
+      for (int u = NW - 1; u > w; --u) X = s[2 * N * u + 2 * n] + s[2 * N * u + 2 * n + 1] * X;
+      x[n] = A[n] + B[n] * X;
+    }
+  }
+  SHD double scan_affine_rev(double a, double c) {
+    const double aa[1] = {a}, cc[1] = {c};
+    double xx[1];
+    scanN_rev<1>(aa, cc, xx);
+    return xx[0];
+  }
+  // sum over the column's levels (every level receives it), in a fixed order
+  SHD double colsum(double x) {
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) x = x + __shfl_xor_sync(FULLMASK, x, d);
+    if (NW == 1) return x;
+    double* s = slot();
+    if (lane == 0) s[w] = x;
+    sync();
+    double t = s[0];
+    for (int u = 1; u < NW; ++u) t = t + s[u];
+    return t;
+  }
   // inclusive sum from the bottom: sum over levels j >= k
   SHD double suffix_sum(double t) {
 #pragma unroll
@@ -518,6 +612,269 @@ SHD void stage_out(const MpArgs& A, const double* sm, int64_t c0) {
   }
 }
 
+// ------------------------------------------------------------ step stages
+// The step body as stages, shared by the forward kernels and the adjoint
+// (which replays them). Per level: the prognostic state, and the values set
+// by fields_init or at the start of each sub-step that later stages read.
+struct LevState {
+  double qv, ql, qr, qi, qs, qg, tz, w;
+};
+struct StepGeom {
+  double dp1, p1, h_var, rh_adj, rh_rain, ccn, c_praut;  // fields_init
+  double den, denfac, dz1, dz;                           // start of each sub-step
+};
+
+// fields_init (:27-276) for one level from its input values (defaults on
+// the padding levels k >= L, whose values never reach a real level).
+template <int NW>
+SHD void fields_init(Column<NW>& C, const MpConst& K, bool valid, double pt, double qvi, double qli, double qri,
+                     double qii, double qsi, double qgi, double delp, double wz, double dz0, double land, double area,
+                     LevState& S, StepGeom& P) {
+  const int k = C.k, L = C.L;
+  S.tz = pt;
+  P.dp1 = delp;
+  P.dp1 = P.dp1 * (1.0 - qvi);
+  const double omq = delp / P.dp1;
+  S.qv = qvi * omq;
+  S.ql = qli * omq;
+  S.qr = qri * omq;
+  S.qi = qii * omq;
+  S.qs = qsi * omq;
+  S.qg = qgi * omq;
+  const double den0 = -P.dp1 / (K.GRAV * dz0);
+  P.p1 = den0 * K.RDGAS * pt;
+  S.w = wz;
+  double ccn;
+  if (K.prog_ccn) {
+    ccn = 0.0 * 1.0e6;
+  } else {
+    ccn = (K.ccn_l * land + K.ccn_o * (1.0 - land)) * 1.0e6;
+    if (K.use_ccn) {
+      double tzb, p1b;
+      C.bcast2(S.tz, P.p1, L - 1, tzb, p1b);
+      ccn = ccn * K.RDGAS * tzb / p1b;
+    }
+  }
+  P.ccn = ccn;
+  P.c_praut = K.cpaut * xpow(ccn * RHOR, -1.0 / 3.0);
+  const double s_leng = sqrt(sqrt(area * 1.0e-10));
+  const double t_land = K.dw_land * s_leng;
+  const double t_ocean = K.dw_ocean * s_leng;
+  double h_var = t_land * land + t_ocean * (1.0 - land);
+  P.h_var = fmin(0.2, fmax(0.01, h_var));
+  P.rh_adj = 1.0 - P.h_var - K.rh_inc;
+  P.rh_rain = fmax(0.35, P.rh_adj - K.rh_inr);
+
+  if (K.fix_negative) {
+    fix_negative_point(K, S.qv, S.ql, S.qr, S.qi, S.qs, S.qg, S.tz);
+    // FORWARD borrow of negative vapour from the level above (:244-247):
+    // a sequential sweep by one thread over the column, taken only when
+    // some level above the bottom is negative
+    if (C.any(valid && k < L - 1 && S.qv < 0.0)) {
+      double* wq = C.work;
+      double* wd = wq + Tiles<NW>::RP;
+      if (valid) {
+        wq[k] = S.qv;
+        wd[k] = P.dp1;
+      }
+      C.sync();
+      if (k == 0) {
+        for (int kk = 1; kk < L; ++kk) {
+          const double pq = wq[kk - 1];
+          if (pq < 0.0) wq[kk] = wq[kk] + pq * wd[kk - 1] / wd[kk];
+        }
+      }
+      C.sync();
+      if (valid) S.qv = wq[k];
+    }
+    if (k < L - 1 && S.qv < 0.0) S.qv = 0.0;
+    // bottom layer borrows from the layer above (:253-276)
+    double qb, db, qb1, db1;
+    C.bcast2(S.qv, P.dp1, L - 1, qb, db);
+    C.bcast2(S.qv, P.dp1, L - 2, qb1, db1);
+    if ((qb < 0.0) && (qb1 > 0.0)) {
+      const double dq = fmin(-qb * db, qb1 * db1);
+      if (k == L - 2) S.qv = S.qv - dq / P.dp1;
+      if (k == L - 1) S.qv = S.qv + dq / P.dp1;
+    }
+  }
+}
+
+// density, fall factor and layer thickness at the start of a sub-step
+// (warm_rain with is_first, :349-380)
+template <int NW>
+SHD void substep_geometry(Column<NW>& C, const MpConst& K, bool valid, double t0, double dz0, const LevState& S,
+                          StepGeom& P) {
+  const double den0 = -P.dp1 / (K.GRAV * dz0);
+  P.dz1 = dz0 * S.tz / t0;
+  P.den = den0 * dz0 / P.dz1;
+  P.denfac = sqrt(SFCRHO / P.den);
+  P.dz = C.heights(valid ? -P.dz1 : 0.0, K.zs);
+}
+
+// warm_rain (:280-653) after the geometry: rain evaporation and accretion,
+// implicit rain fall with the vertical-velocity transport and heating, then
+// autoconversion. Returns the rain flux m1_rain at this level and the
+// surface flux r1.
+template <int NW, bool MIXED>
+SHD void warm_rain(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid, LevState& S, const StepGeom& P,
+                   double& vtr, double& m1_rain, double& r1) {
+  const int k = C.k, L = C.L;
+  double &qv = S.qv, &ql = S.ql, &qr = S.qr, &qi = S.qi, &qs = S.qs, &qg = S.qg, &tz = S.tz, &w = S.w;
+  const double dt5 = 0.5 * K.dt_rain;
+  m1_rain = 0.0;
+  const bool fall = C.any(valid && (qr > QRMIN));
+  r1 = 0.0;
+  if (!fall) {
+    vtr = VF_MIN;
+  } else {
+    if constexpr (MIXED) {
+      vtr = rain_fspeed_m(K, qr, P.den);
+      revap_racc_m(K, KF, dt5, P.h_var, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac);
+    } else {
+      vtr = rain_fspeed(K, qr, P.den);
+      revap_racc(K, dt5, P.h_var, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac);
+    }
+    const double dm = P.dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
+    m1_rain = implicit_fall<NW>(C, qr, vtr, P.dz, P.dp1, valid, K.dt_rain);
+    double fv[2] = {m1_rain, vtr}, pv[2];
+    C.template prevN<2>(fv, pv);
+    r1 = C.bcast(m1_rain, L - 1);
+    if (K.do_sedi_w) w = w_update(k, w, dm, m1_rain, vtr, pv[0], pv[1]);
+    if (K.do_sedi_heat)
+      sedi_heat<NW>(C, K, tz, P.dz1, P.dp1, qv, ql, qr, qi, qs, qg, m1_rain, pv[0], valid, K.C_LIQ);
+    if constexpr (MIXED)
+      revap_racc_m(K, KF, dt5, P.h_var, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac);
+    else
+      revap_racc(K, dt5, P.h_var, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac);
+  }
+  if (K.irain_f != 0) {
+    if constexpr (MIXED)
+      autoconv_no_subgrid_var_m(K, KF, ql, qr, tz, P.den, P.ccn, P.c_praut);
+    else
+      autoconv_no_subgrid_var(K, ql, qr, tz, P.den, P.ccn, P.c_praut);
+  } else {
+    double dl;
+    if (K.z_slope_liq) {
+      dl = mono_slope<NW>(C, ql);
+      dl = fmax(dl, fmax(QVMIN, P.h_var * ql));
+    } else {
+      dl = fmax(QVMIN, P.h_var * ql);
+    }
+    if constexpr (MIXED)
+      autoconv_subgrid_var_m(K, KF, ql, qr, tz, P.den, P.ccn, P.c_praut, dl);
+    else
+      autoconv_subgrid_var(K, ql, qr, tz, P.den, P.ccn, P.c_praut, dl);
+  }
+}
+
+// sedimentation (:657-1217): fall speeds, cloud ice melting, and the
+// implicit falls of ice, snow and graupel with their vertical-velocity
+// transport and heating. Returns the solid flux m1_sol at this level and
+// adds the surface fluxes to ice, snow and graupel.
+template <int NW, bool MIXED>
+SHD void sedimentation(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid, LevState& S,
+                       const StepGeom& P, double& vtg, double& vts, double& m1_sol, double& ice, double& snow,
+                       double& graupel) {
+  const int k = C.k, L = C.L;
+  double &qv = S.qv, &ql = S.ql, &qr = S.qr, &qi = S.qi, &qs = S.qs, &qg = S.qg, &tz = S.tz, &w = S.w;
+  const double dp1 = P.dp1, dz = P.dz;
+  double vti;
+  if constexpr (MIXED)
+    fall_speed_m(K, KF, qg, qi, qs, tz, P.den, vtg, vti, vts);
+  else
+    fall_speed(K, qg, qi, qs, tz, P.den, vtg, vti, vts);
+  m1_sol = 0.0;
+  // cloud ice melting at and below the first level warmer than tice (:702-746)
+  const int first = C.min_int((valid && tz > K.tice) ? k : (1 << 30));
+  if ((k >= first || k == L - 1) && valid) sedi_ice_melt(K, qv, ql, qr, qi, qs, qg, tz);
+  // ice (:773-900), snow (:902-1035) and graupel (:1037-1168): their
+  // implicit falls are independent of one another, so the three share
+  // each column exchange; the vertical-velocity updates, which the
+  // reference applies species after species, stay in that order.
+  bool fi, fs, fg;
+  C.any3(valid && (qi > QRMIN), valid && (qs > QRMIN), valid && (qg > QRMIN), fi, fs, fg);
+  fi = fi && (K.vi_fac >= 1.0e-5);
+  double mp = 0.0;  // m1_sol at the level above, for the heating
+  if (fi || fs || fg) {
+    const double dd[3] = {K.dts * vti, K.dts * vts, K.dts * vtg};
+    double ddp[3];
+    C.template prevN<3>(dd, ddp);
+    const double qq[3] = {qi, qs, qg};
+    double ra[3], rb[3], r[3];
+#pragma unroll
+    for (int n = 0; n < 3; ++n) {
+      const double qmass = valid ? qq[n] * dp1 : 0.0;
+      const double D = dz + dd[n];
+      ra[n] = qmass / D;
+      rb[n] = (k == 0) ? 0.0 : ddp[n] / D;
+      if (!valid) {
+        ra[n] = 0.0;
+        rb[n] = 0.0;
+      }
+    }
+    C.template scanN<3>(ra, rb, r);
+    double flux[3];
+#pragma unroll
+    for (int n = 0; n < 3; ++n) flux[n] = valid ? dd[n] * r[n] : 0.0;
+    const double dm_i = dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
+    if (fi && valid) qi = r[0] * dz / dp1;
+    const double dm_s = dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
+    if (fs && valid) qs = r[1] * dz / dp1;
+    const double dm_g = dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
+    if (fg && valid) qg = r[2] * dz / dp1;
+    double sfc[3];
+    C.template bcastN<3>(flux, L - 1, sfc);
+    const double nv[6] = {flux[0], vti, flux[1], vts, flux[2], vtg};
+    double pv[6];
+    C.template prevN<6>(nv, pv);
+    if (fi) {
+      m1_sol = flux[0];
+      mp = pv[0];
+      if (K.do_sedi_w) w = w_update(k, w, dm_i, flux[0], vti, pv[0], pv[1]);
+      ice = ice + sfc[0];
+    }
+    if (fs) {
+      m1_sol = m1_sol + flux[1];
+      mp = mp + pv[2];
+      if (K.do_sedi_w) w = w_update(k, w, dm_s, flux[1], vts, pv[2], pv[3]);
+      snow = snow + sfc[1];
+    }
+    if (fg) {
+      m1_sol = m1_sol + flux[2];
+      mp = mp + pv[4];
+      if (K.do_sedi_w) w = w_update(k, w, dm_g, flux[2], vtg, pv[4], pv[5]);
+      graupel = graupel + sfc[2];
+    }
+  }
+  if (K.do_sedi_heat) sedi_heat<NW>(C, K, tz, P.dz1, dp1, qv, ql, qr, qi, qs, qg, m1_sol, mp, valid, K.C_ICE);
+}
+
+// icloud (:1220-1449): instant melting or freezing, the ice slope, the ice
+// processes and the saturation adjustment.
+template <int NW, bool MIXED>
+SHD void icloud(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid, LevState& S, const StepGeom& P,
+                double& qa, double vtg, double vtr, double vts) {
+  double &qv = S.qv, &ql = S.ql, &qr = S.qr, &qi = S.qi, &qs = S.qs, &qg = S.qg, &tz = S.tz;
+  double q_liq, q_sol, cvm;
+  icloud_melt_freeze(K, qv, ql, qr, qi, qs, qg, tz, P.den, q_liq, q_sol, cvm);
+  double di;
+  if (K.z_slope_ice) {
+    di = mono_slope<NW>(C, qi);
+    di = fmax(di, fmax(QVMIN, P.h_var * qi));
+  } else {
+    di = fmax(QVMIN, P.h_var * qi);
+  }
+  if (valid) {
+    if constexpr (MIXED)
+      icloud_processes_m(K, KF, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac, vtg, vtr, vts, P.p1, di, q_liq, q_sol,
+                         cvm);
+    else
+      icloud_processes(K, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac, vtg, vtr, vts, P.p1, di, q_liq, q_sol, cvm);
+    subgrid_z_proc(K, P.h_var, P.rh_adj, P.rh_rain, qa, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac, P.p1);
+  }
+}
+
 // ------------------------------------------------------------------ kernel
 // One block's work: columns c0 .. c0 + G - 1 of the domain described by A.
 // MIXED selects the mixed-precision process rates (mp_physics_mixed.cuh);
@@ -543,6 +900,7 @@ SHD void mp_block(const MpArgs& A, double* sm, const int64_t c0) {
   C.L = L;
   C.bar = 1 + g;
   C.scr = sm + SM::scratch + (size_t)g * 2 * Tiles<NW>::SCR;
+  C.work = sm + SM::work + (size_t)g * 2 * RP;
   C.par = 0;
   const int k = C.k;
   const bool valid = k < L;
@@ -551,332 +909,43 @@ SHD void mp_block(const MpArgs& A, double* sm, const int64_t c0) {
 
   if (col < A.ncol) {
     const int64_t ci = col % A.nx, cj = col / A.nx;
-    double qv, ql, qr, qi, qs, qg, tz, qa, m1, w, dp1, p1;
-    double den = 1.0, denfac = 1.0, dz1 = -100.0, dz = 100.0, m1_sol = 0.0, vtr = VF_MIN, vtg = VF_MIN,
-           vts = VF_MIN;
-
+    LevState S;
+    StepGeom P;
+    double qa = valid ? TL(IN_QAZ) : 0.0;
+    double m1 = 0.0, m1_sol = 0.0, vtr = VF_MIN, vtg = VF_MIN, vts = VF_MIN;
+    P.den = 1.0;
+    P.denfac = 1.0;
+    P.dz1 = -100.0;
+    P.dz = 100.0;
     // ------------------------------------------------ fields_init (:27-276)
-    {
-      double pt = 250.0, qvi = 0.0, qli = 0.0, qri = 0.0, qii = 0.0, qsi = 0.0, qgi = 0.0, delp = 1.0, wz = 0.0,
-             qaz = 0.0, dz0 = -100.0;
-      if (valid) {
-        pt = TL(IN_PT);
-        qvi = TL(IN_QV);
-        qli = TL(IN_QL);
-        qri = TL(IN_QR);
-        qii = TL(IN_QI);
-        qsi = TL(IN_QS);
-        qgi = TL(IN_QG);
-        delp = TL(IN_DELP);
-        wz = TL(IN_W);
-        qaz = TL(IN_QAZ);
-        dz0 = TL(IN_DELZ);
-      }
-      tz = pt;
-      dp1 = delp;
-      dp1 = dp1 * (1.0 - qvi);
-      const double omq = delp / dp1;
-      qv = qvi * omq;
-      ql = qli * omq;
-      qr = qri * omq;
-      qi = qii * omq;
-      qs = qsi * omq;
-      qg = qgi * omq;
-      const double den0 = -dp1 / (K.GRAV * dz0);
-      p1 = den0 * K.RDGAS * pt;
-      m1 = 0.0;
-      w = wz;
-      qa = qaz;
-    }
-    const double land = A.land.p[ci * A.land.si + cj * A.land.sj];
-    const double area = A.area.p[ci * A.area.si + cj * A.area.sj];
-    double ccn;
-    if (K.prog_ccn) {
-      ccn = 0.0 * 1.0e6;
-    } else {
-      ccn = (K.ccn_l * land + K.ccn_o * (1.0 - land)) * 1.0e6;
-      if (K.use_ccn) {
-        double tzb, p1b;
-        C.bcast2(tz, p1, L - 1, tzb, p1b);
-        ccn = ccn * K.RDGAS * tzb / p1b;
-      }
-    }
-    const double c_praut = K.cpaut * xpow(ccn * RHOR, -1.0 / 3.0);
-    const double s_leng = sqrt(sqrt(area * 1.0e-10));
-    const double t_land = K.dw_land * s_leng;
-    const double t_ocean = K.dw_ocean * s_leng;
-    double h_var = t_land * land + t_ocean * (1.0 - land);
-    h_var = fmin(0.2, fmax(0.01, h_var));
-    const double rh_adj = 1.0 - h_var - K.rh_inc;
-    const double rh_rain = fmax(0.35, rh_adj - K.rh_inr);
-
-    if (K.fix_negative) {
-      {
-        const double cvm = K.c_air + qv * K.c_vap + (qr + ql) * K.C_LIQ + (qi + qs + qg) * K.C_ICE;
-        const double lcpk = (K.lv00 + K.d0_vap * tz) / cvm;
-        const double icpk = (K.LI00 + K.DC_ICE * tz) / cvm;
-        if (qi < 0.0) {
-          qs = qs + qi;
-          qi = 0.0;
-        }
-        if (qs < 0.0) {
-          qg = qg + qs;
-          qs = 0.0;
-        }
-        if (qg < 0.0) {
-          qr = qr + qg;
-          tz = tz - qg * icpk;
-          qg = 0.0;
-        }
-        if (qr < 0.0) {
-          ql = ql + qr;
-          qr = 0.0;
-        }
-        if (ql < 0.0) {
-          qv = qv + ql;
-          tz = tz - ql * lcpk;
-          ql = 0.0;
-        }
-      }
-      // FORWARD borrow of negative vapour from the level above (:244-247):
-      // a sequential sweep by one thread over the column, taken only when
-      // some level above the bottom is negative
-      if (C.any(valid && k < L - 1 && qv < 0.0)) {
-        double* wq = sm + SM::work + (size_t)g * 2 * RP;
-        double* wd = wq + RP;
-        if (valid) {
-          wq[k] = qv;
-          wd[k] = dp1;
-        }
-        C.sync();
-        if (k == 0) {
-          for (int kk = 1; kk < L; ++kk) {
-            const double pq = wq[kk - 1];
-            if (pq < 0.0) wq[kk] = wq[kk] + pq * wd[kk - 1] / wd[kk];
-          }
-        }
-        C.sync();
-        if (valid) qv = wq[k];
-      }
-      if (k < L - 1 && qv < 0.0) qv = 0.0;
-      // bottom layer borrows from the layer above (:253-276)
-      double qb, db, qb1, db1;
-      C.bcast2(qv, dp1, L - 1, qb, db);
-      C.bcast2(qv, dp1, L - 2, qb1, db1);
-      if ((qb < 0.0) && (qb1 > 0.0)) {
-        const double dq = fmin(-qb * db, qb1 * db1);
-        if (k == L - 2) qv = qv - dq / dp1;
-        if (k == L - 1) qv = qv + dq / dp1;
-      }
-    }
+    fields_init<NW>(C, K, valid, valid ? TL(IN_PT) : 250.0, valid ? TL(IN_QV) : 0.0, valid ? TL(IN_QL) : 0.0,
+                    valid ? TL(IN_QR) : 0.0, valid ? TL(IN_QI) : 0.0, valid ? TL(IN_QS) : 0.0,
+                    valid ? TL(IN_QG) : 0.0, valid ? TL(IN_DELP) : 1.0, valid ? TL(IN_W) : 0.0,
+                    valid ? TL(IN_DELZ) : -100.0, A.land.p[ci * A.land.si + cj * A.land.sj],
+                    A.area.p[ci * A.area.si + cj * A.area.sj], S, P);
 
     double rain = 0.0, snow = 0.0, ice = 0.0, graupel = 0.0;
-
 #pragma unroll 1
     for (int it = 0; it < K.ntimes; ++it) {
-      // -------------------------------- warm_rain, is_first (:280-653)
+      // warm_rain with is_first, sedimentation, warm_rain again (one copy
+      // of the warm_rain code, run twice)
 #pragma unroll 1
       for (int pass = 0; pass < 2; ++pass) {
         const bool is_first = pass == 0;
-        if (is_first) {
-          const double t0 = valid ? TL(IN_PT) : 250.0;
-          const double dz0 = valid ? TL(IN_DELZ) : -100.0;
-          const double den0 = -dp1 / (K.GRAV * dz0);
-          dz1 = dz0 * tz / t0;
-          den = den0 * dz0 / dz1;
-          denfac = sqrt(SFCRHO / den);
-          dz = C.heights(valid ? -dz1 : 0.0, K.zs);
-        }
-        const double dt5 = 0.5 * K.dt_rain;
-        double m1_rain = 0.0;
-        const bool fall = C.any(valid && (qr > QRMIN));
-        double r1 = 0.0;
-        if (!fall) {
-          vtr = VF_MIN;
-        } else {
-          if constexpr (MIXED) {
-            vtr = rain_fspeed_m(K, qr, den);
-            revap_racc_m(K, KF, dt5, h_var, qg, qi, ql, qr, qs, qv, tz, den, denfac);
-          } else {
-            vtr = rain_fspeed(K, qr, den);
-            revap_racc(K, dt5, h_var, qg, qi, ql, qr, qs, qv, tz, den, denfac);
-          }
-          const double dm = dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
-          m1_rain = implicit_fall<NW>(C, qr, vtr, dz, dp1, valid, K.dt_rain);
-          double fv[2] = {m1_rain, vtr}, pv[2];
-          C.template prevN<2>(fv, pv);
-          r1 = C.bcast(m1_rain, L - 1);
-          if (K.do_sedi_w) w = w_update(k, w, dm, m1_rain, vtr, pv[0], pv[1]);
-          if (K.do_sedi_heat)
-            sedi_heat<NW>(C, K, tz, dz1, dp1, qv, ql, qr, qi, qs, qg, m1_rain, pv[0], valid, K.C_LIQ);
-          if constexpr (MIXED)
-            revap_racc_m(K, KF, dt5, h_var, qg, qi, ql, qr, qs, qv, tz, den, denfac);
-          else
-            revap_racc(K, dt5, h_var, qg, qi, ql, qr, qs, qv, tz, den, denfac);
-        }
-        if (K.irain_f != 0) {
-          if constexpr (MIXED)
-            autoconv_no_subgrid_var_m(K, KF, ql, qr, tz, den, ccn, c_praut);
-          else
-            autoconv_no_subgrid_var(K, ql, qr, tz, den, ccn, c_praut);
-        } else {
-          double dl;
-          if (K.z_slope_liq) {
-            dl = mono_slope<NW>(C, ql);
-            dl = fmax(dl, fmax(QVMIN, h_var * ql));
-          } else {
-            dl = fmax(QVMIN, h_var * ql);
-          }
-          if constexpr (MIXED)
-            autoconv_subgrid_var_m(K, KF, ql, qr, tz, den, ccn, c_praut, dl);
-          else
-            autoconv_subgrid_var(K, ql, qr, tz, den, ccn, c_praut, dl);
-        }
+        if (is_first)
+          substep_geometry<NW>(C, K, valid, valid ? TL(IN_PT) : 250.0, valid ? TL(IN_DELZ) : -100.0, S, P);
+        double m1_rain, r1;
+        warm_rain<NW, MIXED>(C, K, KF, valid, S, P, vtr, m1_rain, r1);
         rain = rain + r1;
         m1 = is_first ? m1 + m1_rain : m1 + m1_rain + m1_sol;
-
         if (!is_first) break;
-
-        // ------------------------------------ sedimentation (:657-1217)
-        double vti;
-        if constexpr (MIXED)
-          fall_speed_m(K, KF, qg, qi, qs, tz, den, vtg, vti, vts);
-        else
-          fall_speed(K, qg, qi, qs, tz, den, vtg, vti, vts);
-        m1_sol = 0.0;
-        // cloud ice melting at and below the first level warmer than tice (:702-746)
-        const int first = C.min_int((valid && tz > K.tice) ? k : (1 << 30));
-        if ((k >= first || k == L - 1) && valid) {
-          const double lhi = K.LI00 + K.DC_ICE * tz;
-          double q_liq = ql + qr;
-          double q_sol = qi + qs + qg;
-          double cvm = K.c_air + qv * K.c_vap + q_liq * K.C_LIQ + q_sol * K.C_ICE;
-          const double icpk = lhi / cvm;
-          const double tc = tz - K.tice;
-          if ((qi > QCMIN) && (tc > 0.0)) {
-            const double sink = fmin(qi, K.fac_imlt * tc / icpk);
-            const double tmp = fmin(sink, dim(K.ql_mlt, ql));
-            ql = ql + tmp;
-            qr = qr + sink - tmp;
-            qi = qi - sink;
-            q_liq = q_liq + sink;
-            q_sol = q_sol - sink;
-            cvm = K.c_air + qv * K.c_vap + q_liq * K.C_LIQ + q_sol * K.C_ICE;
-            tz = tz - sink * lhi / cvm;
-          }
-        }
-        // ice (:773-900), snow (:902-1035) and graupel (:1037-1168): their
-        // implicit falls are independent of one another, so the three share
-        // each column exchange; the vertical-velocity updates, which the
-        // reference applies species after species, stay in that order.
-        bool fi, fs, fg;
-        C.any3(valid && (qi > QRMIN), valid && (qs > QRMIN), valid && (qg > QRMIN), fi, fs, fg);
-        fi = fi && (K.vi_fac >= 1.0e-5);
-        double mp = 0.0;  // m1_sol at the level above, for the heating
-        if (fi || fs || fg) {
-          const double dd[3] = {K.dts * vti, K.dts * vts, K.dts * vtg};
-          double ddp[3];
-          C.template prevN<3>(dd, ddp);
-          const double qq[3] = {qi, qs, qg};
-          double ra[3], rb[3], r[3];
-#pragma unroll
-          for (int n = 0; n < 3; ++n) {
-            const double qmass = valid ? qq[n] * dp1 : 0.0;
-            const double D = dz + dd[n];
-            ra[n] = qmass / D;
-            rb[n] = (k == 0) ? 0.0 : ddp[n] / D;
-            if (!valid) {
-              ra[n] = 0.0;
-              rb[n] = 0.0;
-            }
-          }
-          C.template scanN<3>(ra, rb, r);
-          double flux[3];
-#pragma unroll
-          for (int n = 0; n < 3; ++n) flux[n] = valid ? dd[n] * r[n] : 0.0;
-          const double dm_i = dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
-          if (fi && valid) qi = r[0] * dz / dp1;
-          const double dm_s = dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
-          if (fs && valid) qs = r[1] * dz / dp1;
-          const double dm_g = dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
-          if (fg && valid) qg = r[2] * dz / dp1;
-          double sfc[3];
-          C.template bcastN<3>(flux, L - 1, sfc);
-          const double nv[6] = {flux[0], vti, flux[1], vts, flux[2], vtg};
-          double pv[6];
-          C.template prevN<6>(nv, pv);
-          if (fi) {
-            m1_sol = flux[0];
-            mp = pv[0];
-            if (K.do_sedi_w) w = w_update(k, w, dm_i, flux[0], vti, pv[0], pv[1]);
-            ice = ice + sfc[0];
-          }
-          if (fs) {
-            m1_sol = m1_sol + flux[1];
-            mp = mp + pv[2];
-            if (K.do_sedi_w) w = w_update(k, w, dm_s, flux[1], vts, pv[2], pv[3]);
-            snow = snow + sfc[1];
-          }
-          if (fg) {
-            m1_sol = m1_sol + flux[2];
-            mp = mp + pv[4];
-            if (K.do_sedi_w) w = w_update(k, w, dm_g, flux[2], vtg, pv[4], pv[5]);
-            graupel = graupel + sfc[2];
-          }
-        }
+        sedimentation<NW, MIXED>(C, K, KF, valid, S, P, vtg, vts, m1_sol, ice, snow, graupel);
         rain = rain + 0.0;
-        if (K.do_sedi_heat) sedi_heat<NW>(C, K, tz, dz1, dp1, qv, ql, qr, qi, qs, qg, m1_sol, mp, valid, K.C_ICE);
       }
-
-      // ------------------------------------------------ icloud (:1220-1449)
-      double q_liq, q_sol, cvm;
-      {
-        const double lhi = K.LI00 + K.DC_ICE * tz;
-        q_liq = ql + qr;
-        q_sol = qi + qs + qg;
-        cvm = K.c_air + qv * K.c_vap + q_liq * K.C_LIQ + q_sol * K.C_ICE;
-        const double icpk = lhi / cvm;
-        if ((tz > K.tice) && (qi > QCMIN)) {
-          const double melt = fmin(qi, K.fac_imlt * (tz - K.tice) / icpk);
-          const double tmp = fmin(melt, dim(K.ql_mlt, ql));
-          ql = ql + tmp;
-          qr = qr + melt - tmp;
-          qi = qi - melt;
-          q_liq = q_liq + melt;
-          q_sol = q_sol - melt;
-          cvm = K.c_air + qv * K.c_vap + q_liq * K.C_LIQ + q_sol * K.C_ICE;
-          tz = tz - melt * lhi / cvm;
-        } else if ((tz < K.t_wfr) && (ql > QCMIN)) {
-          const double dtmp = K.t_wfr - tz;
-          const double factor = fmin(1.0, dtmp / DT_FR);
-          const double sink = fmin(ql * factor, dtmp / icpk);
-          const double qi_crt = K.qi_gen * fmin(K.qi_lim, 0.1 * (K.tice - tz)) / den;
-          const double tmp = fmin(sink, dim(qi_crt, qi));
-          ql = ql - sink;
-          qs = qs + sink - tmp;
-          qi = qi + tmp;
-          q_liq = q_liq - sink;
-          q_sol = q_sol + sink;
-          cvm = K.c_air + qv * K.c_vap + q_liq * K.C_LIQ + q_sol * K.C_ICE;
-          tz = tz + sink * lhi / cvm;
-        }
-      }
-      double di;
-      if (K.z_slope_ice) {
-        di = mono_slope<NW>(C, qi);
-        di = fmax(di, fmax(QVMIN, h_var * qi));
-      } else {
-        di = fmax(QVMIN, h_var * qi);
-      }
-      if (valid) {
-        if constexpr (MIXED)
-          icloud_processes_m(K, KF, qg, qi, ql, qr, qs, qv, tz, den, denfac, vtg, vtr, vts, p1, di, q_liq, q_sol, cvm);
-        else
-          icloud_processes(K, qg, qi, ql, qr, qs, qv, tz, den, denfac, vtg, vtr, vts, p1, di, q_liq, q_sol, cvm);
-        subgrid_z_proc(K, h_var, rh_adj, rh_rain, qa, qg, qi, ql, qr, qs, qv, tz, den, denfac, p1);
-      }
+      icloud<NW, MIXED>(C, K, KF, valid, S, P, qa, vtg, vtr, vts);
     }
-
+    const double qv = S.qv, ql = S.ql, qr = S.qr, qi = S.qi, qs = S.qs, qg = S.qg, tz = S.tz, w = S.w;
+    const double dp1 = P.dp1;
     // ------------------------------------------------ fields_update (:1452-1553)
     const double dp0 = valid ? TL(IN_DELP) : 1.0;
     const double u0 = valid ? TL(IN_UA) : 0.0;

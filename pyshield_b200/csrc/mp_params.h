@@ -69,4 +69,24 @@ struct MpArgs {
   int* err;                             // device error word
 };
 
+// Parameter block of the adjoint (vector-Jacobian product) launch. in: the
+// step's input state (the first 13 input fields, in the order of InField);
+// cot: cotangents of the outputs (the 10 tendencies in the order of
+// OutField, then wmp); grad: the input adjoints written by the launch (same
+// order as in). rain_b .. graupel_b: cotangents of the surface totals, ncol
+// each, or null.
+constexpr int N_VJP_IN = 13;
+constexpr int N_VJP_COT = 11;
+struct VjpArgs {
+  MpConst K;
+  MpConstF KF;
+  int nx, ny, nz;
+  int64_t ncol;
+  Fld3 in[N_VJP_IN];
+  Fld3 cot[N_VJP_COT];
+  Fld3 grad[N_VJP_IN];
+  Fld2 land, area;
+  const double *rain_b, *snow_b, *ice_b, *graupel_b;
+};
+
 }  // namespace shield

@@ -665,4 +665,97 @@ SHP void icloud_processes(const MpConst& K, T& qgz, T& qiz, T& qlz, T& qrz, T& q
   }
 }
 
+// -------------------------------------- pointwise blocks of the step body
+// Cloud ice melting at and below the first level warmer than tice, at the
+// start of sedimentation (microphysics.py:706-746).
+template <typename T>
+SHP void sedi_ice_melt(const MpConst& K, T qv, T& ql, T& qr, T& qi, T qs, T qg, T& tz) {
+  const T lhi = K.LI00 + K.DC_ICE * tz;
+  T q_liq = ql + qr;
+  T q_sol = qi + qs + qg;
+  T cvm = K.c_air + qv * K.c_vap + q_liq * K.C_LIQ + q_sol * K.C_ICE;
+  const T icpk = lhi / cvm;
+  const T tc = tz - K.tice;
+  if ((qi > QCMIN) && (tc > 0.0)) {
+    const T sink = fmin(qi, K.fac_imlt * tc / icpk);
+    const T tmp = fmin(sink, dim(K.ql_mlt, ql));
+    ql = ql + tmp;
+    qr = qr + sink - tmp;
+    qi = qi - sink;
+    q_liq = q_liq + sink;
+    q_sol = q_sol - sink;
+    cvm = K.c_air + qv * K.c_vap + q_liq * K.C_LIQ + q_sol * K.C_ICE;
+    tz = tz - sink * lhi / cvm;
+  }
+}
+
+// Instant melting of cloud ice above tice, or freezing of cloud water below
+// t_wfr, at the start of icloud (microphysics.py:1298-1339); returns the
+// liquid and solid totals and cvm that icloud_processes starts from.
+template <typename T>
+SHP void icloud_melt_freeze(const MpConst& K, T qv, T& ql, T& qr, T& qi, T& qs, T qg, T& tz, T den, T& q_liq,
+                            T& q_sol, T& cvm) {
+  const T lhi = K.LI00 + K.DC_ICE * tz;
+  q_liq = ql + qr;
+  q_sol = qi + qs + qg;
+  cvm = K.c_air + qv * K.c_vap + q_liq * K.C_LIQ + q_sol * K.C_ICE;
+  const T icpk = lhi / cvm;
+  if ((tz > K.tice) && (qi > QCMIN)) {
+    const T melt = fmin(qi, K.fac_imlt * (tz - K.tice) / icpk);
+    const T tmp = fmin(melt, dim(K.ql_mlt, ql));
+    ql = ql + tmp;
+    qr = qr + melt - tmp;
+    qi = qi - melt;
+    q_liq = q_liq + melt;
+    q_sol = q_sol - melt;
+    cvm = K.c_air + qv * K.c_vap + q_liq * K.C_LIQ + q_sol * K.C_ICE;
+    tz = tz - melt * lhi / cvm;
+  } else if ((tz < K.t_wfr) && (ql > QCMIN)) {
+    const T dtmp = K.t_wfr - tz;
+    const T factor = fmin(1.0, dtmp / DT_FR);
+    const T sink = fmin(ql * factor, dtmp / icpk);
+    const T qi_crt = K.qi_gen * fmin(K.qi_lim, 0.1 * (K.tice - tz)) / den;
+    const T tmp = fmin(sink, dim(qi_crt, qi));
+    ql = ql - sink;
+    qs = qs + sink - tmp;
+    qi = qi + tmp;
+    q_liq = q_liq - sink;
+    q_sol = q_sol + sink;
+    cvm = K.c_air + qv * K.c_vap + q_liq * K.C_LIQ + q_sol * K.C_ICE;
+    tz = tz + sink * lhi / cvm;
+  }
+}
+
+// The pointwise part of fix_negative (microphysics.py:202-240): negative
+// species borrow from the next one in the chain ice -> snow -> graupel ->
+// rain -> cloud water -> vapour, with the latent heat.
+template <typename T>
+SHP void fix_negative_point(const MpConst& K, T& qv, T& ql, T& qr, T& qi, T& qs, T& qg, T& tz) {
+  const T cvm = K.c_air + qv * K.c_vap + (qr + ql) * K.C_LIQ + (qi + qs + qg) * K.C_ICE;
+  const T lcpk = (K.lv00 + K.d0_vap * tz) / cvm;
+  const T icpk = (K.LI00 + K.DC_ICE * tz) / cvm;
+  if (qi < 0.0) {
+    qs = qs + qi;
+    qi = 0.0;
+  }
+  if (qs < 0.0) {
+    qg = qg + qs;
+    qs = 0.0;
+  }
+  if (qg < 0.0) {
+    qr = qr + qg;
+    tz = tz - qg * icpk;
+    qg = 0.0;
+  }
+  if (qr < 0.0) {
+    ql = ql + qr;
+    qr = 0.0;
+  }
+  if (ql < 0.0) {
+    qv = qv + ql;
+    tz = tz - ql * lcpk;
+    ql = 0.0;
+  }
+}
+
 }  // namespace shield

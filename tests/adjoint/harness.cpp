@@ -243,6 +243,48 @@ struct Subgrid {
   }
 };
 
+// x = qv ql qr qi qs qg tz ; y = the same after the block
+struct SediMelt {
+  static constexpr int NIN = 7, ND = 7, NOUT = 7;
+  template <class T>
+  static void fwd(const MpConst& K, const T* x, T* y) {
+    for (int i = 0; i < 7; ++i) y[i] = x[i];
+    sedi_ice_melt<T>(K, y[0], y[1], y[2], y[3], y[4], y[5], y[6]);
+  }
+  static void bwd(const MpConst& K, const double* x, const double* yb, double* xb) {
+    for (int i = 0; i < 7; ++i) xb[i] = yb[i];
+    sedi_ice_melt_b(K, x[0], x[1], x[2], x[3], x[4], x[5], x[6], xb[0], xb[1], xb[2], xb[3], xb[4], xb[5], xb[6]);
+  }
+};
+// x = qv ql qr qi qs qg tz den ; y = qv ql qr qi qs qg tz q_liq q_sol cvm
+struct MeltFreeze {
+  static constexpr int NIN = 8, ND = 8, NOUT = 10;
+  template <class T>
+  static void fwd(const MpConst& K, const T* x, T* y) {
+    for (int i = 0; i < 7; ++i) y[i] = x[i];
+    icloud_melt_freeze<T>(K, y[0], y[1], y[2], y[3], y[4], y[5], y[6], x[7], y[7], y[8], y[9]);
+  }
+  static void bwd(const MpConst& K, const double* x, const double* yb, double* xb) {
+    for (int i = 0; i < 7; ++i) xb[i] = yb[i];
+    xb[7] = 0.0;
+    icloud_melt_freeze_b(K, x[0], x[1], x[2], x[3], x[4], x[5], x[6], x[7], yb[7], yb[8], yb[9], xb[0], xb[1], xb[2],
+                         xb[3], xb[4], xb[5], xb[6], xb[7]);
+  }
+};
+// x = qv ql qr qi qs qg tz ; y = the same after the block
+struct FixNeg {
+  static constexpr int NIN = 7, ND = 7, NOUT = 7;
+  template <class T>
+  static void fwd(const MpConst& K, const T* x, T* y) {
+    for (int i = 0; i < 7; ++i) y[i] = x[i];
+    fix_negative_point<T>(K, y[0], y[1], y[2], y[3], y[4], y[5], y[6]);
+  }
+  static void bwd(const MpConst& K, const double* x, const double* yb, double* xb) {
+    for (int i = 0; i < 7; ++i) xb[i] = yb[i];
+    fix_negative_point_b(K, x[0], x[1], x[2], x[3], x[4], x[5], x[6], xb[0], xb[1], xb[2], xb[3], xb[4], xb[5], xb[6]);
+  }
+};
+
 }  // namespace
 
 #define SHIELD_ADJ_ENTRY(NAME, R)                                                                               \
@@ -268,3 +310,6 @@ SHIELD_ADJ_ENTRY(smlt, Smlt)
 SHIELD_ADJ_ENTRY(gmlt, Gmlt)
 SHIELD_ADJ_ENTRY(icloud_processes, Icloud)
 SHIELD_ADJ_ENTRY(subgrid_z_proc, Subgrid)
+SHIELD_ADJ_ENTRY(sedi_ice_melt, SediMelt)
+SHIELD_ADJ_ENTRY(icloud_melt_freeze, MeltFreeze)
+SHIELD_ADJ_ENTRY(fix_negative_point, FixNeg)

@@ -212,3 +212,25 @@ def test_subgrid_z_proc(harness, band, fast_sat_adj):
     xbh, xbd, xbs, y = run(harness, "subgrid_z_proc", X, YB, cfg=cfg)
     assert np.any(y[:, 1:] != X[:, [0, 1, 2, 3, 4, 5, 6]], axis=1).mean() > 0.3
     check(xbh, xbd, xbs, f"subgrid_z_proc {band} fast={fast_sat_adj}")
+
+
+@pytest.mark.parametrize("band", [(262.0, 292.0), (220.0, 245.0)])
+def test_step_blocks(harness, band):
+    rng = np.random.default_rng(8)
+    tz, den, qv = _rho_state(rng, N, *band)
+    qg, qi, ql, qr, qs = (cond(rng, N, 0.15, 1e-9, 3e-3) for _ in range(5))
+    X = np.stack([qv, ql, qr, qi, qs, qg, tz], 1)
+    YB = rng.normal(size=(N, 7)) * np.array([1, 1, 1, 1, 1, 1, 1e-3])
+    xbh, xbd, xbs, _ = run(harness, "sedi_ice_melt", X, YB)
+    check(xbh, xbd, xbs, "sedi_ice_melt")
+    YB10 = np.concatenate([YB, rng.normal(size=(N, 3)) * np.array([1, 1, 1e-6])], 1)
+    xbh, xbd, xbs, y = run(harness, "icloud_melt_freeze", np.concatenate([X, den[:, None]], 1), YB10)
+    check(xbh, xbd, xbs, "icloud_melt_freeze")
+    # negative values for the fix_negative chain
+    Xn = X.copy()
+    for j in range(1, 6):
+        neg = rng.random(N) < 0.3
+        Xn[neg, j] = -rng.uniform(0, 1e-4, neg.sum())
+    xbh, xbd, xbs, y = run(harness, "fix_negative_point", Xn, YB)
+    assert (y[:, 1:6] == 0).any()
+    check(xbh, xbd, xbs, "fix_negative_point")

@@ -125,23 +125,25 @@ int shield_mp_last_error(void* handle, char* buf, size_t n);
  * from its inputs.
  *
  * Outputs of the step, whose cotangents are given: the ten tendencies
- * (as written by the step: udt and vdt for levels k >= 1 only), wmp (when
- * do_sedi_w), and the four surface totals. Inputs, whose adjoints are
- * written (assigned): the 13 state fields of ShieldMpFields (pt, the six
- * species, qcld, ua, va, delprsi, delz, wmp). The incoming tendencies only
- * add to the outputs and are not differentiated; the persistent
- * cloud-fraction accumulator only adds a constant to qa_dt.
+ * (as written by the step: udt and vdt for levels k >= 1 only), wmp (which
+ * the step leaves unchanged without do_sedi_w), the persistent
+ * cloud-fraction accumulator (the reference's never-reset self._qaz, so
+ * that windows of several steps differentiate through it) and the four
+ * surface totals. Inputs, whose adjoints are written (assigned): the 13
+ * state fields of ShieldMpFields (pt, the six species, qcld, ua, va,
+ * delprsi, delz, wmp) and the accumulator. The incoming tendencies only add
+ * to the outputs and are not differentiated.
  *
  * Branches follow the forward at the given input. Supported: the plain form
  * and configurations without do_sedi_heat and de_ice, with at most 4
  * sub-steps (SHIELD_ELAYOUT otherwise). */
 typedef struct {
-  ShieldField3D pt_dt, qv_dt, ql_dt, qr_dt, qi_dt, qs_dt, qg_dt, qa_dt, udt, vdt, wmp;
+  ShieldField3D pt_dt, qv_dt, ql_dt, qr_dt, qi_dt, qs_dt, qg_dt, qa_dt, udt, vdt, wmp, qaz; /* NULL ptr: zero */
   const double *rain, *snow, *ice, *graupel; /* ncol each (column c = j*nx + i), or NULL for zero */
 } ShieldMpCotangents;
 
 typedef struct {
-  ShieldField3D pt, qvapor, qliquid, qrain, qice, qsnow, qgraupel, qcld, ua, va, delprsi, delz, wmp;
+  ShieldField3D pt, qvapor, qliquid, qrain, qice, qsnow, qgraupel, qcld, ua, va, delprsi, delz, wmp, qaz;
 } ShieldMpGradients;
 
 /* state: the step's input state (its 13 state fields and land are read; its

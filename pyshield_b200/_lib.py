@@ -104,13 +104,13 @@ class ShieldMpFields(ctypes.Structure):
 
 
 class ShieldMpCotangents(ctypes.Structure):
-    _fields_ = [(n, ShieldField3D) for n in MP_TENDENCY_FIELDS + ("wmp",)] + [
+    _fields_ = [(n, ShieldField3D) for n in MP_TENDENCY_FIELDS + ("wmp", "qaz")] + [
         (n, ctypes.c_void_p) for n in ("rain", "snow", "ice", "graupel")
     ]
 
 
 class ShieldMpGradients(ctypes.Structure):
-    _fields_ = [(n, ShieldField3D) for n in MP_STATE_FIELDS]
+    _fields_ = [(n, ShieldField3D) for n in MP_STATE_FIELDS + ("qaz",)]
 
 
 class ShieldMpMember(ctypes.Structure):

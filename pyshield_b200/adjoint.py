@@ -6,18 +6,22 @@ with the hand-written FP64 reverse kernel behind ``shield_mp_step_vjp``:
 
 * ``step_vjp(mp, state, land, cot, timestep)``: the VJP of one step;
 * ``MicrophysicsStep``: a ``torch.autograd.Function`` computing the step's
-  outputs from its 13 input fields, whose backward is ``step_vjp``;
+  outputs from its 14 inputs, whose backward is ``step_vjp``;
 * ``rollout(mp, state, land, timestep, nsteps)``: a window of steps, each
   followed by the state update of ``update_physics_state_with_tendencies``
   (``pySHiELD/stencils/physics.py:151-194``). Autograd keeps only each
   step's input fields (per-step checkpointing); the adjoint kernel
   recomputes everything inside a step from them.
 
-Fields are ``(nx, ny, nz)`` float64 CUDA tensors (any strides; level k = 0
-at the model top), the surface totals ``(nx, ny)``. The forward runs the
-plain FP64 step with fresh zero tendencies, so its outputs are the step's
-increments; it also advances the handle's persistent cloud-fraction
-accumulator, as a call of the step does.
+The inputs are the 13 state fields of ``MicrophysicsState`` and ``qaz``,
+the persistent cloud-fraction accumulator (the reference's never-reset
+``self._qaz``, ``microphysics.py:1674``): it carries from step to step, so
+a window of steps is differentiated through it too. Fields are
+``(nx, ny, nz)`` float64 CUDA tensors (any strides; level k = 0 at the
+model top), the surface totals ``(nx, ny)``. The forward runs the plain
+FP64 step with fresh zero tendencies, so its outputs are the step's
+increments, the updated wmp and the updated accumulator (the handle's own
+accumulator is set from the input and left at the output).
 """
 
 import ctypes
@@ -35,8 +39,9 @@ from ._lib import (
 from .microphysics import _current_stream
 from .quantity import field2d, field3d
 
-STATE = MP_STATE_FIELDS  # pt qvapor qliquid qrain qice qsnow qgraupel qcld ua va delprsi delz wmp
-OUT3 = MP_TENDENCY_FIELDS + ("wmp",)
+# pt qvapor qliquid qrain qice qsnow qgraupel qcld ua va delprsi delz wmp, and the accumulator
+STATE = MP_STATE_FIELDS + ("qaz",)
+OUT3 = MP_TENDENCY_FIELDS + ("wmp", "qaz")
 OUT2 = ("rain", "snow", "ice", "graupel")
 OUTPUTS = OUT3 + OUT2
 # the fields update_physics_state_with_tendencies advances, with their tendency
@@ -62,18 +67,19 @@ def _check_state(mp, state):
 def _state_fields(mp, state, land):
     F = ShieldMpFields()
     ext = (mp.nx, mp.ny, mp.nz)
-    for name, t in zip(STATE, state):
+    for name, t in zip(MP_STATE_FIELDS, state):
         setattr(F, name, field3d(t, ext))
     F.land = field2d(land, (mp.nx, mp.ny))
     return F
 
 
 def step_forward(mp, state, land, timestep, stream=None):
-    """Outputs of one step from the 13 input fields: the ten increments,
-    the updated wmp, and the four surface totals (mm/day)."""
+    """Outputs of one step from the 14 inputs: the ten increments, the
+    updated wmp and accumulator, and the four surface totals (mm/day)."""
     import torch
 
     _check_state(mp, state)
+    mp.set_qaz(state[-1].permute(2, 1, 0).contiguous())
     F = _state_fields(mp, state, land)
     w_out = _empty3(state[0])
     w_out.copy_(state[STATE.index("wmp")])
@@ -87,11 +93,12 @@ def step_forward(mp, state, land, timestep, stream=None):
     rc = load().shield_mp_step(mp._handle, ctypes.byref(F), float(timestep), SHIELD_MP_PLAIN,
                                ctypes.c_void_p(_current_stream(stream)))
     check(rc, mp._handle, "shield_mp_step")
-    return tuple(tend) + (w_out,) + tuple(pr[i].t() for i in range(4))
+    qaz = mp.get_qaz().permute(2, 1, 0)
+    return tuple(tend) + (w_out, qaz) + tuple(pr[i].t() for i in range(4))
 
 
 def step_vjp(mp, state, land, cot, timestep, stream=None):
-    """Input adjoints (13 fields, ``STATE`` order) of one step at ``state``
+    """Input adjoints (14 fields, ``STATE`` order) of one step at ``state``
     for the output cotangents ``cot`` (``OUTPUTS`` order; None = zero)."""
     _check_state(mp, state)
     if len(cot) != len(OUTPUTS):
@@ -102,7 +109,7 @@ def step_vjp(mp, state, land, cot, timestep, stream=None):
     keep = []
     for name, c in zip(OUT3, cot[: len(OUT3)]):
         if c is None:
-            c = _empty3(state[0])
+            continue  # a null field is a zero cotangent
         keep.append(c)
         setattr(C, name, field3d(c, ext))
     for name, c in zip(OUT2, cot[len(OUT3):]):
@@ -128,8 +135,8 @@ try:
 
     class MicrophysicsStep(torch.autograd.Function):
         """``outputs = MicrophysicsStep.apply(mp, timestep, land, *state)``:
-        the 15 outputs (``OUTPUTS``) of one step of ``mp`` from its 13 input
-        fields (``STATE``); differentiable in every input field."""
+        the 16 outputs (``OUTPUTS``) of one step of ``mp`` from its 14
+        inputs (``STATE``); differentiable in every input."""
 
         @staticmethod
         def forward(ctx, mp, timestep, land, *state):
@@ -158,7 +165,7 @@ def step(mp, state, land, timestep):
 
 def rollout(mp, state, land, timestep, nsteps):
     """``nsteps`` steps, each followed by X <- X + dt X_dt for the fields of
-    ``ADVANCED`` and wmp <- the step's wmp (delprsi, delz unchanged).
+    ``ADVANCED``, and wmp, qaz <- the step's (delprsi, delz unchanged).
     Returns the final state dict and the list of per-step output dicts."""
     cur = dict(state)
     history = []
@@ -168,6 +175,7 @@ def rollout(mp, state, land, timestep, nsteps):
         for x, xdt in ADVANCED:
             nxt[x] = cur[x] + out[xdt] * timestep
         nxt["wmp"] = out["wmp"]
+        nxt["qaz"] = out["qaz"]
         history.append(out)
         cur = nxt
     return cur, history

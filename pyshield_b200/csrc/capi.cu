@@ -184,19 +184,16 @@ extern "C" int shield_mp_step_vjp(void* handle, const ShieldMpFields* F, const S
   const ShieldField3D* ins[] = {&F->pt, &F->qvapor, &F->qliquid, &F->qrain, &F->qice, &F->qsnow, &F->qgraupel,
                                 &F->qcld, &F->ua, &F->va, &F->delprsi, &F->delz, &F->wmp};
   const ShieldField3D* cots[] = {&cot->pt_dt, &cot->qv_dt, &cot->ql_dt, &cot->qr_dt, &cot->qi_dt, &cot->qs_dt,
-                                 &cot->qg_dt, &cot->qa_dt, &cot->udt,   &cot->vdt,   &cot->wmp};
+                                 &cot->qg_dt, &cot->qa_dt, &cot->udt,   &cot->vdt,   &cot->wmp,   &cot->qaz};
   const ShieldField3D* grads[] = {&grad->pt,   &grad->qvapor, &grad->qliquid, &grad->qrain, &grad->qice,
                                   &grad->qsnow, &grad->qgraupel, &grad->qcld,  &grad->ua,    &grad->va,
-                                  &grad->delprsi, &grad->delz,  &grad->wmp};
+                                  &grad->delprsi, &grad->delz,  &grad->wmp,   &grad->qaz};
   for (int f = 0; f < N_VJP_IN; ++f) {
     if (!ins[f]->ptr) return fail(h, SHIELD_EINVAL, "null input field pointer");
     A.in[f] = f3(*ins[f]);
-    A.grad[f] = f3(*grads[f]);
   }
-  for (int f = 0; f < N_VJP_COT; ++f) {
-    if (!cots[f]->ptr) return fail(h, SHIELD_EINVAL, "null cotangent pointer");
-    A.cot[f] = f3(*cots[f]);
-  }
+  for (int f = 0; f < N_VJP_COT; ++f) A.cot[f] = f3(*cots[f]);
+  for (int f = 0; f < N_VJP_GRAD; ++f) A.grad[f] = f3(*grads[f]);
   if (!F->land.ptr) return fail(h, SHIELD_EINVAL, "null land pointer");
   A.land = Fld2{F->land.ptr, F->land.si, F->land.sj};
   A.area = Fld2{h->area, 1, h->nx};

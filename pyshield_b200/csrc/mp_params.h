@@ -71,12 +71,15 @@ struct MpArgs {
 
 // Parameter block of the adjoint (vector-Jacobian product) launch. in: the
 // step's input state (the first 13 input fields, in the order of InField);
-// cot: cotangents of the outputs (the 10 tendencies in the order of
-// OutField, then wmp); grad: the input adjoints written by the launch (same
-// order as in). rain_b .. graupel_b: cotangents of the surface totals, ncol
-// each, or null.
+// cot: cotangents of the outputs in the order of OutField (the 10
+// tendencies, wmp, the cloud-fraction accumulator); grad: the input
+// adjoints written by the launch, in the order of InField (the 13 state
+// fields, then the accumulator). A null field pointer is a zero cotangent or
+// a gradient that is not written. rain_b .. graupel_b: cotangents of the
+// surface totals, ncol each, or null.
 constexpr int N_VJP_IN = 13;
-constexpr int N_VJP_COT = 11;
+constexpr int N_VJP_COT = 12;
+constexpr int N_VJP_GRAD = 14;
 struct VjpArgs {
   MpConst K;
   MpConstF KF;
@@ -84,7 +87,7 @@ struct VjpArgs {
   int64_t ncol;
   Fld3 in[N_VJP_IN];
   Fld3 cot[N_VJP_COT];
-  Fld3 grad[N_VJP_IN];
+  Fld3 grad[N_VJP_GRAD];
   Fld2 land, area;
   const double *rain_b, *snow_b, *ice_b, *graupel_b;
 };

@@ -1,7 +1,8 @@
 // Adjoint of the microphysics step (FP64): the vector-Jacobian product of
-// the step's outputs -- the ten tendencies, wmp and the surface totals --
-// with respect to its inputs (pt, the six water species, qcld, ua, va,
-// delprsi, delz, wmp), for pySHiELD's Microphysics.__call__
+// the step's outputs -- the ten tendencies, wmp, the persistent
+// cloud-fraction accumulator and the surface totals -- with respect to its
+// inputs (pt, the six water species, qcld, ua, va, delprsi, delz, wmp and
+// the accumulator), for pySHiELD's Microphysics.__call__
 // (pySHiELD/stencils/microphysics.py:1981-2263).
 //
 // One thread per level and one group of NW warps per column, as in the
@@ -31,19 +32,20 @@ namespace {
 constexpr int VJP_MAXNT = 4;  // sub-steps whose stage states fit the store
 constexpr int NT_IN = N_VJP_IN + N_VJP_COT;
 
-// Shared memory: NT_IN input tiles (inputs, then cotangents), N_VJP_IN
+// Shared memory: NT_IN input tiles (inputs, then cotangents), N_VJP_GRAD
 // gradient tiles, G x 2 x SCR exchange scratch, G x 4 x RP work rows.
 template <int NW, int G>
 struct VjpSmem {
   static constexpr int RP = Tiles<NW>::RP;
   static constexpr size_t out = (size_t)NT_IN * G * RP;
-  static constexpr size_t scratch = out + (size_t)N_VJP_IN * G * RP;
+  static constexpr size_t scratch = out + (size_t)N_VJP_GRAD * G * RP;
   static constexpr size_t work = scratch + (size_t)G * 2 * Tiles<NW>::SCR;
   static constexpr size_t total = work + (size_t)G * 4 * RP;
   static constexpr size_t bytes = total * sizeof(double);
 };
 
-// load NF fields into tiles [f * G + g][k] (all loads issued before any store)
+// load NF fields into tiles [f * G + g][k] (all loads issued before any
+// store); a field with a null pointer reads as zero
 template <int NW, int G, int NF>
 SHD void load_tiles(const Fld3* F, double* tiles, int64_t ncol, int nx, int L, int64_t c0) {
   constexpr int RP = Tiles<NW>::RP;
@@ -60,7 +62,8 @@ SHD void load_tiles(const Fld3* F, double* tiles, int64_t ncol, int nx, int L, i
 #pragma unroll
   for (int f = 0; f < NF; ++f) {
     v[f] = 0.0;
-    if (F[f].sk == 1) {
+    if (!F[f].p) {
+    } else if (F[f].sk == 1) {
       if (okk) v[f] = F[f].p[ik * F[f].si + jk * F[f].sj + kk];
     } else if (ok) {
       v[f] = F[f].p[i * F[f].si + j * F[f].sj + (int64_t)k * F[f].sk];
@@ -663,11 +666,15 @@ __global__ void __launch_bounds__(32 * NW * G, 1) mp_vjp_kernel(const __grid_con
       Sb.qv = qfb[0], Sb.ql = qfb[1], Sb.qr = qfb[2], Sb.qi = qfb[3], Sb.qs = qfb[4], Sb.qg = qfb[5];
       Ab.dp1 += omq_b / dp0 - omq0_b * omq0 / dp1;
       delp_b += -omq_b * omq / dp0 + omq0_b / dp1;
+      // the accumulator: qaz_out = qaz_in + the step's increments, and
+      // qa_dt = rdt (qaz_out / ntimes - qa0) (without do_qa, which leaves
+      // both alone)
+      qa_b = TC(OUT_QAZ);
       if (!K.do_qa) {
-        qa_b = TC(OUT_QA_DT) * rdt / (double)K.ntimes;
+        qa_b += TC(OUT_QA_DT) * rdt / (double)K.ntimes;
         qa0_b = -TC(OUT_QA_DT) * rdt;
       }
-      Sb.w = K.do_sedi_w ? TC(OUT_W) : 0.0;
+      Sb.w = TC(OUT_W);  // without do_sedi_w, wmp passes through unchanged
     }
     double m1_b = 0.0;
     if (K.sedi_transport) {
@@ -889,10 +896,11 @@ __global__ void __launch_bounds__(32 * NW * G, 1) mp_vjp_kernel(const __grid_con
       TG(IN_DELP) = delp_b;
       TG(IN_DELZ) = dz0_b;
       TG(IN_W) = Sb.w;
+      TG(IN_QAZ) = qa_b;
     }
   }
   __syncthreads();
-  store_tiles<NW, G, N_VJP_IN>(A.grad, sm + SM::out, A.ncol, A.nx, L, c0);
+  store_tiles<NW, G, N_VJP_GRAD>(A.grad, sm + SM::out, A.ncol, A.nx, L, c0);
 }
 
 template <int NW, int G>

@@ -12,6 +12,7 @@
 #include "dual.h"  // before the physics, so its overloads are found
 #include "mp_adjoint.cuh"
 #include "mp_setup.h"
+#include "column.h"
 
 using namespace shield;
 
@@ -313,3 +314,115 @@ SHIELD_ADJ_ENTRY(subgrid_z_proc, Subgrid)
 SHIELD_ADJ_ENTRY(sedi_ice_melt, SediMelt)
 SHIELD_ADJ_ENTRY(icloud_melt_freeze, MeltFreeze)
 SHIELD_ADJ_ENTRY(fix_negative_point, FixNeg)
+
+// One column of the whole step with dual numbers: input field f is seeded
+// along DX[f] (direction f), so for every output row o and field f
+//   JD[o][f] = sum over the output's levels of ybar_o (J dx_f)_o
+// and JS[o][f] the same with magnitude duals and |ybar| (the size of the
+// terms). X: NX rows of L levels; DX likewise; YB: NY rows of L levels then
+// the 4 surface totals; Y: the output values (same layout as YB).
+extern "C" int adj_column(const ShieldMpConfig* cfg, double ts, int L, double land, double area, const double* X,
+                          const double* DX, const double* YB, double* JD, double* JS, double* Y) {
+  using namespace colref;
+  if (L < 3 || L > LMAX) return -1;
+  const MpConst K = make_K(cfg, ts);
+  constexpr int NO = NY + 4;
+  auto* xd = new Dual[NX][LMAX];
+  auto* yd = new Dual[NY][LMAX];
+  auto* xa = new ADual[NX][LMAX];
+  auto* ya = new ADual[NY][LMAX];
+  Dual sd[4];
+  ADual sa[4];
+  for (int f = 0; f < NX; ++f)
+    for (int k = 0; k < L; ++k) {
+      xd[f][k] = Dual(X[f * L + k]);
+      xd[f][k].d[f] = DX[f * L + k];
+      xa[f][k] = ADual(X[f * L + k]);
+      xa[f][k].d[f] = std::fabs(DX[f * L + k]);
+    }
+  column_step<Dual>(K, L, land, area, xd, yd, sd);
+  column_step<ADual>(K, L, land, area, xa, ya, sa);
+  for (int o = 0; o < NO; ++o)
+    for (int f = 0; f < NX; ++f) {
+      double s = 0.0, a = 0.0;
+      if (o < NY) {
+        for (int k = 0; k < L; ++k) {
+          s += YB[o * L + k] * yd[o][k].d[f];
+          a += std::fabs(YB[o * L + k]) * ya[o][k].d[f];
+        }
+      } else {
+        s = YB[NY * L + (o - NY)] * sd[o - NY].d[f];
+        a = std::fabs(YB[NY * L + (o - NY)]) * sa[o - NY].d[f];
+      }
+      JD[o * NX + f] = s;
+      JS[o * NX + f] = a;
+    }
+  for (int o = 0; o < NY; ++o)
+    for (int k = 0; k < L; ++k) Y[o * L + k] = yd[o][k].v;
+  for (int i = 0; i < 4; ++i) Y[NY * L + i] = sd[i].v;
+  delete[] xd;
+  delete[] yd;
+  delete[] xa;
+  delete[] ya;
+  return 0;
+}
+
+// A window of nsteps steps on one column, each followed by the state update
+// of update_physics_state_with_tendencies (X += dt X_dt for the six species,
+// qcld, pt, ua, va; wmp and the accumulator carried; delprsi, delz kept).
+// XB: cotangents of the final state (NX rows of L). For every input row f:
+// JD[f] = <XB, J_window dx_f>, JS[f] the size of its terms; XF: the final
+// state values.
+extern "C" int adj_column_window(const ShieldMpConfig* cfg, double ts, int L, double land, double area, int nsteps,
+                                 const double* X, const double* DX, const double* XB, double* JD, double* JS,
+                                 double* XF) {
+  using namespace colref;
+  if (L < 3 || L > LMAX || nsteps < 1) return -1;
+  const MpConst K = make_K(cfg, ts);
+  auto* xd = new Dual[NX][LMAX];
+  auto* yd = new Dual[NY][LMAX];
+  auto* xa = new ADual[NX][LMAX];
+  auto* ya = new ADual[NY][LMAX];
+  Dual sd[4];
+  ADual sa[4];
+  for (int f = 0; f < NX; ++f)
+    for (int k = 0; k < L; ++k) {
+      xd[f][k] = Dual(X[f * L + k]);
+      xd[f][k].d[f] = DX[f * L + k];
+      xa[f][k] = ADual(X[f * L + k]);
+      xa[f][k].d[f] = std::fabs(DX[f * L + k]);
+    }
+  const int adv[10][2] = {{X_QV, Y_QV}, {X_QL, Y_QL}, {X_QR, Y_QR}, {X_QI, Y_QI}, {X_QS, Y_QS},
+                          {X_QG, Y_QG}, {X_QA, Y_QA}, {X_PT, Y_PT}, {X_UA, Y_U}, {X_VA, Y_V}};
+  for (int n = 0; n < nsteps; ++n) {
+    column_step<Dual>(K, L, land, area, xd, yd, sd);
+    column_step<ADual>(K, L, land, area, xa, ya, sa);
+    for (int k = 0; k < L; ++k) {
+      for (auto& a : adv) {
+        xd[a[0]][k] = xd[a[0]][k] + yd[a[1]][k] * ts;
+        xa[a[0]][k] = xa[a[0]][k] + ya[a[1]][k] * ts;
+      }
+      xd[X_W][k] = yd[Y_W][k];
+      xa[X_W][k] = ya[Y_W][k];
+      xd[X_QAZ][k] = yd[Y_QAZ][k];
+      xa[X_QAZ][k] = ya[Y_QAZ][k];
+    }
+  }
+  for (int f = 0; f < NX; ++f) {
+    double s = 0.0, a = 0.0;
+    for (int r = 0; r < NX; ++r)
+      for (int k = 0; k < L; ++k) {
+        s += XB[r * L + k] * xd[r][k].d[f];
+        a += std::fabs(XB[r * L + k]) * xa[r][k].d[f];
+      }
+    JD[f] = s;
+    JS[f] = a;
+  }
+  for (int r = 0; r < NX; ++r)
+    for (int k = 0; k < L; ++k) XF[r * L + k] = xd[r][k].v;
+  delete[] xd;
+  delete[] yd;
+  delete[] xa;
+  delete[] ya;
+  return 0;
+}

@@ -26,10 +26,10 @@ TOL = 1.0e-12
 N = 4000
 
 
-@pytest.fixture(scope="module")
-def harness():
+def build_harness():
+    """Compile (when stale) and load the CPU harness."""
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
-    deps = [SRC, os.path.join(HERE, "adjoint", "dual.h")] + [
+    deps = [SRC, os.path.join(HERE, "adjoint", "dual.h"), os.path.join(HERE, "adjoint", "column.h")] + [
         os.path.join(ROOT, "pyshield_b200", "csrc", f) for f in ("mp_physics.cuh", "mp_adjoint.cuh", "mp_setup.h", "mp_params.h")
     ]
     if not os.path.exists(OUT) or os.path.getmtime(OUT) < max(os.path.getmtime(d) for d in deps):
@@ -39,6 +39,11 @@ def harness():
         assert r.returncode == 0, r.stderr[-4000:]
         os.replace(OUT + ".tmp", OUT)
     return ctypes.CDLL(OUT)
+
+
+@pytest.fixture(scope="module")
+def harness():
+    return build_harness()
 
 
 def _cfg(**kw):
@@ -234,3 +239,87 @@ def test_step_blocks(harness, band):
     xbh, xbd, xbs, y = run(harness, "fix_negative_point", Xn, YB)
     assert (y[:, 1:6] == 0).any()
     check(xbh, xbd, xbs, "fix_negative_point")
+
+
+# ---------------------------------------------------------------- the column
+STATE_ROWS = ("pt", "qvapor", "qliquid", "qrain", "qice", "qsnow", "qgraupel", "qcld", "ua", "va", "delprsi", "delz",
+              "wmp", "qaz")
+OUT_ROWS = ("pt_dt", "qv_dt", "ql_dt", "qr_dt", "qi_dt", "qs_dt", "qg_dt", "qa_dt", "udt", "vdt", "wmp", "qaz")
+NXR, NYR = len(STATE_ROWS), len(OUT_ROWS)
+SFC = ("rain", "snow", "ice", "graupel")
+
+
+def column_ref(lib, cfg, ts, X, land, area, DX=None, YB=None):
+    """Run the dual-number column step (tests/adjoint/column.h) on one column:
+    X (14, L) input rows, DX a direction per row, YB the output cotangents
+    (12 rows of L, then the 4 surface totals). Returns JD (16, 14): for
+    output o and input row f, <ybar_o, J dx_f>; JS the size of its terms;
+    Y the output values (laid out as YB)."""
+    L = X.shape[1]
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    DX = np.ascontiguousarray(np.zeros_like(X) if DX is None else DX, dtype=np.float64)
+    YB = np.ascontiguousarray(np.zeros(NYR * L + 4) if YB is None else YB, dtype=np.float64)
+    JD = np.zeros((NYR + 4, NXR))
+    JS = np.zeros((NYR + 4, NXR))
+    Y = np.zeros(NYR * L + 4)
+    P = ctypes.POINTER(ctypes.c_double)
+    f = lib.adj_column
+    f.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double, P, P, P, P, P, P]
+    p = lambda a: a.ctypes.data_as(P)  # noqa: E731
+    assert f(ctypes.byref(cfg), ts, L, float(land), float(area), p(X), p(DX), p(YB), p(JD), p(JS), p(Y)) == 0
+    return JD, JS, Y
+
+
+@pytest.mark.parametrize("kw", [{}, {"mp_time": 75.0}, {"fix_negative": False, "z_slope_liq": False},
+                                {"irain_f": 1, "prog_ccn": True, "do_qa": True},
+                                {"do_sedi_w": False, "sedi_transport": False, "fast_sat_adj": False}])
+def test_column_reference_matches_oracle(harness, kw):
+    """The sequential column step that serves as the exact reference for the
+    adjoint computes the oracle's step: every output within the plain-form
+    tolerance of the GPU tests."""
+    import sys
+
+    sys.path.insert(0, HERE)
+    from mp_helpers import TOL_PLAIN, floors
+
+    from oracle.microphysics import OracleMicrophysics
+    from pyshield_b200._config import PhysicsConfig
+    from pyshield_b200._lib import make_config
+    from pyshield_b200.inputs import copy_state, make_state
+
+    n, L, dt = 6, 79, 150.0
+    pc = PhysicsConfig(dt_atmos=int(dt), **kw)
+    state, area = make_state(n, L, seed=21, n_cube=1, sat_fraction=0.2)
+    s = copy_state(state)
+    fl = None
+    om = OracleMicrophysics(pc, n, L, area)
+    state["qaz"] = np.zeros((L, n))
+    pr = om(s, dt)
+    s["qaz"] = om.qaz
+    fl = floors(state, s, dt)
+    for c in range(n):
+        X = np.stack([state[r][:, c] for r in STATE_ROWS])
+        _, _, Y = column_ref(harness, make_config(pc), dt, X, state["land"][c], area[c])
+        for o, name in enumerate(OUT_ROWS):
+            ref = s[name][:, c]
+            got = Y[o * L:(o + 1) * L]
+            allow = TOL_PLAIN * np.abs(s[name]).max() + fl.get(name, 0.0) + 1e-300
+            assert np.abs(got - ref).max() <= allow, (name, c, np.abs(got - ref).max(), allow)
+        for i, name in enumerate(SFC):
+            allow = TOL_PLAIN * np.abs(pr[name]).max() + fl.get(name, 0.0) + 1e-300
+            assert abs(Y[NYR * L + i] - pr[name][c]) <= allow, (name, c)
+
+
+def column_window_ref(lib, cfg, ts, X, land, area, nsteps, DX, XB):
+    """The dual-number window of ``nsteps`` steps (tests/adjoint/harness.cpp
+    adj_column_window): JD, JS (14,) per input row, and the final state."""
+    L = X.shape[1]
+    X, DX, XB = (np.ascontiguousarray(a, dtype=np.float64) for a in (X, DX, XB))
+    JD, JS, XF = np.zeros(NXR), np.zeros(NXR), np.zeros((NXR, L))
+    P = ctypes.POINTER(ctypes.c_double)
+    f = lib.adj_column_window
+    f.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                  P, P, P, P, P, P]
+    p = lambda a: a.ctypes.data_as(P)  # noqa: E731
+    assert f(ctypes.byref(cfg), ts, L, float(land), float(area), nsteps, p(X), p(DX), p(XB), p(JD), p(JS), p(XF)) == 0
+    return JD, JS, XF

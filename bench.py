@@ -197,6 +197,68 @@ def build_state(nlev, device, seed, n_cube=N_CUBE):
     return ms, StencilFactory(gi), qf, GridData(area_q), host, land, (nx, ny, n)
 
 
+def run_adjoint(nsteps_window=8, reps=5, n_cube=48, nlev=79, dt=150.0):
+    """Adjoint cost at C48 L79: the device time of one VJP of the step
+    (shield_mp_step_vjp) against one forward step, and of an nsteps window
+    (forward steps with the state update, then the backward through
+    torch.autograd with per-step checkpointing) against the window's forward
+    alone. Each timing is the mean of ``reps`` runs after a warm-up."""
+    import torch
+
+    from pyshield_b200._config import PhysicsConfig
+    from pyshield_b200.adjoint import OUTPUTS, STATE, rollout, step_forward, step_vjp
+    from pyshield_b200.microphysics import Microphysics
+
+    device = torch.device("cuda", torch.cuda.current_device())
+    ms, sf, qf, gd, host, land, (nx, ny, n) = build_state(nlev, device, seed=77, n_cube=n_cube)
+    mp = Microphysics(sf, qf, gd, PhysicsConfig(dt_atmos=int(dt)))
+    x = [getattr(ms, f).view.clone() for f in STATE[:-1]]
+    x.append(torch.zeros((nx, ny, nlev), dtype=torch.float64, device=device))
+    lnd = land.view.clone()
+    y = step_forward(mp, x, lnd, dt)
+    g = torch.Generator(device=device).manual_seed(1)
+    ybar = [torch.randn(v.shape, generator=g, device=device, dtype=torch.float64) for v in y]
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    fwd_ms = timed(lambda: mp(ms, dt))
+    vjp_ms = timed(lambda: step_vjp(mp, x, lnd, ybar, dt))
+
+    def window_forward():
+        with torch.no_grad():
+            rollout(mp, dict(zip(STATE, x)), lnd, dt, nsteps_window)
+
+    def window_backward():
+        xs = [t.clone().requires_grad_(True) for t in x]
+        final, _ = rollout(mp, dict(zip(STATE, xs)), lnd, dt, nsteps_window)
+        loss = sum(final[f].sum() for f in STATE)
+        torch.autograd.grad(loss, xs)
+
+    wf_ms = timed(window_forward)
+    wb_ms = timed(window_backward)
+    return {
+        "workload": f"GFDL microphysics step, C{n_cube} ({n} columns) x L{nlev}, dt {dt:g} s, FP64",
+        "forward_ms": fwd_ms,
+        "vjp_ms": vjp_ms,
+        "vjp_over_forward": vjp_ms / fwd_ms,
+        "window_steps": nsteps_window,
+        "window_forward_ms": wf_ms,
+        "window_forward_and_backward_ms": wb_ms,
+        "window_backward_over_forward": (wb_ms - wf_ms) / wf_ms,
+        "note": "device time (CUDA events); the window keeps each step's inputs and recomputes inside the step",
+    }
+
+
 def max_over_ranks(values, world, device):
     """Each rank's device-measured times -> their maximum over all ranks (the
     slowest replica sets the job's time). One all-reduce; every rank calls it
@@ -423,6 +485,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the C48 adjoint-cost measurement")
     ap.add_argument("--ncube", type=int, default=N_CUBE, help="cube size N of the CN workload (default 96)")
     ap.add_argument("--ensemble", action="store_true", help="run the ensemble workload instead")
     ap.add_argument("--members", type=int, default=64)
@@ -520,6 +583,7 @@ def main():
                "sample": sample + f"; one core alone: {v1:.4g} column-steps/s"}
     if pool:
         pool.close()
+    adjoint = run_adjoint() if (rank == 0 and world == 1 and not args.no_adjoint and args.form == "plain") else None
 
     if rank == 0:
         rec = {
@@ -552,6 +616,7 @@ def main():
                        "dtype": "f32 process rates + f64 saturation adjustment, fall and budgets"}
                       if r["mixed_ms"] > 0 else None),
             "clocks": r["clocks"],
+            "adjoint": adjoint,
         }
         emit(rec)
 

@@ -16,6 +16,17 @@
 
 #include "mp_physics.cuh"
 
+// The larger adjoints are out of line in device code: every call site then
+// shares one copy, which keeps the adjoint kernel within the instruction
+// cache.
+#if defined(__CUDACC__) && !defined(SHIELD_ADJ_INLINE)
+#define SHB static __host__ __device__ __noinline__
+#elif defined(__CUDACC__)
+#define SHB static __host__ __device__ __forceinline__
+#else
+#define SHB static inline
+#endif
+
 namespace shield {
 
 SHP bool min_first(double a, double b) { return a <= b; }
@@ -141,7 +152,7 @@ SHP void gmlt_b(double tc, double dqs, double qgrho, double pgacw, double pgacr,
 }
 
 // ------------------------------------------------ revap_racc (:182-265)
-SHP void revap_racc_b(const MpConst& K, double dt, double h_var, double qg, double qi, double ql, double qr, double qs,
+SHB void revap_racc_b(const MpConst& K, double dt, double h_var, double qg, double qi, double ql, double qr, double qs,
                       double qv, double tz, double den, double denfac, double& qg_b, double& qi_b, double& ql_b,
                       double& qr_b, double& qs_b, double& qv_b, double& tz_b, double& den_b, double& denfac_b) {
   if (!((tz > K.t_wfr) && (qr > QRMIN))) return;
@@ -317,7 +328,7 @@ SHP void rain_fspeed_b(const MpConst& K, double qrz, double den, double v_b, dou
 }
 
 // fall_speed (:268-341): vtg, vti, vts from qg, qi, qs, tk, den
-SHP void fall_speed_b(const MpConst& K, double qg, double qi, double qs, double tk, double den, double vtg_b,
+SHB void fall_speed_b(const MpConst& K, double qg, double qi, double qs, double tk, double den, double vtg_b,
                       double vti_b, double vts_b, double& qg_b, double& qi_b, double& qs_b, double& tk_b,
                       double& den_b) {
   const double rr = SFCRHO / den;
@@ -383,7 +394,7 @@ SHP void fall_speed_b(const MpConst& K, double qg, double qi, double qs, double 
 }
 
 // -------------------------------------------------- autoconversion (:375-428)
-SHP void autoconv_no_subgrid_var_b(const MpConst& K, double qlz, double qrz, double tz, double den, double ccn,
+SHB void autoconv_no_subgrid_var_b(const MpConst& K, double qlz, double qrz, double tz, double den, double ccn,
                                    double c_praut, double& ql_b, double& qr_b, double& den_b, double& ccn_b,
                                    double& c_praut_b) {
   (void)qrz;
@@ -412,7 +423,7 @@ SHP void autoconv_no_subgrid_var_b(const MpConst& K, double qlz, double qrz, dou
   }
 }
 
-SHP void autoconv_subgrid_var_b(const MpConst& K, double qlz, double qrz, double tz, double den, double ccn,
+SHB void autoconv_subgrid_var_b(const MpConst& K, double qlz, double qrz, double tz, double den, double ccn,
                                 double c_praut, double dl, double& ql_b, double& qr_b, double& den_b, double& ccn_b,
                                 double& c_praut_b, double& dl_b) {
   (void)qrz;
@@ -526,8 +537,6 @@ SHP void ic_snow_melt(const MpConst& K, IcState& Z, double qv, double den, doubl
 }
 SHP void ic_snow_melt_b(const MpConst& K, const IcState& Z, const IcIn& I, double dqs0, double lhi0, double icpk0,
                         IcState& Zb, IcIn& Ib, double& dqs0_b, double& lhi0_b, double& icpk0_b) {
-  IcState Z1 = Z;
-  ic_snow_melt(K, Z1, I.qv, I.den, I.denfac, I.vtr, I.vts, dqs0, lhi0, icpk0);
   const double den = I.den, denfac = I.denfac;
   const double tc = Z.tz - K.tice;
   const double xs = Z.qs * den;
@@ -550,8 +559,9 @@ SHP void ic_snow_melt_b(const MpConst& K, const IcState& Z, const IcIn& I, doubl
   const double m = fmin(r1, r2);
   const double sink = fmin(Z.qs, m);
   const double dm = dim(K.qs_mlt, Z.ql);
+  const double cvm1 = cvm_of(K, I.qv, Z.q_liq + sink, Z.q_sol - sink);
   // reverse
-  double sink_b = close_transfer_b(K, -1.0, sink, lhi0, Z1.cvm, Zb, Ib.qv, lhi0_b);
+  double sink_b = close_transfer_b(K, -1.0, sink, lhi0, cvm1, Zb, Ib.qv, lhi0_b);
   sink_b += Zb.q_liq - Zb.q_sol;
   sink_b += Zb.qr;
   double tmp_b = -Zb.qr + Zb.ql;
@@ -626,8 +636,6 @@ SHP void ic_graupel_melt(const MpConst& K, IcState& Z, double qv, double den, do
 }
 SHP void ic_graupel_melt_b(const MpConst& K, const IcState& Z, const IcIn& I, double dqs0, IcState& Zb, IcIn& Ib,
                            double& dqs0_b) {
-  IcState Z1 = Z;
-  ic_graupel_melt(K, Z1, I.qv, I.den, I.vtg, I.vtr, dqs0);
   const double den = I.den;
   const double lhi = K.LI00 + K.DC_ICE * Z.tz;
   const double icpk = lhi / Z.cvm;
@@ -649,9 +657,10 @@ SHP void ic_graupel_melt_b(const MpConst& K, const IcState& Z, const IcIn& I, do
   const double r = tc / icpk;
   const double B = fmin(Z.qg, r);
   const double pgmlt = fmin(A, B);
+  const double cvm1 = cvm_of(K, I.qv, Z.q_liq + pgmlt, Z.q_sol - pgmlt);
   // reverse
   double lhi_b = 0.0;
-  double pg_b = close_transfer_b(K, -1.0, pgmlt, lhi, Z1.cvm, Zb, Ib.qv, lhi_b);
+  double pg_b = close_transfer_b(K, -1.0, pgmlt, lhi, cvm1, Zb, Ib.qv, lhi_b);
   pg_b += Zb.q_liq - Zb.q_sol + Zb.qr - Zb.qg;
   double pg0_b = 0.0, tc_b = 0.0, icpk_b = 0.0;
   if (min_first(A, B)) {
@@ -815,8 +824,6 @@ SHP void ic_rain_freeze(const MpConst& K, IcState& Z, double qv, double den, dou
 }
 SHP void ic_rain_freeze_b(const MpConst& K, const IcState& Z, const IcIn& I, double lhi0, double icpk0, IcState& Zb,
                           IcIn& Ib, double& lhi0_b, double& icpk0_b) {
-  IcState Z1 = Z;
-  ic_rain_freeze(K, Z1, I.qv, I.den, I.vtr, I.vts, lhi0, icpk0);
   const double den = I.den;
   const double tc = Z.tz - K.tice;
   double psacr0 = 0.0;
@@ -835,8 +842,9 @@ SHP void ic_rain_freeze_b(const MpConst& K, const IcState& Z, const IcIn& I, dou
   const double factor = m / M;
   const double psacr = factor * psacr0, pgfr = factor * pgfr0;
   const double sink = psacr + pgfr;
+  const double cvm1 = cvm_of(K, I.qv, Z.q_liq - sink, Z.q_sol + sink);
   // reverse
-  double sink_b = close_transfer_b(K, 1.0, sink, lhi0, Z1.cvm, Zb, Ib.qv, lhi0_b);
+  double sink_b = close_transfer_b(K, 1.0, sink, lhi0, cvm1, Zb, Ib.qv, lhi0_b);
   sink_b += -Zb.q_liq + Zb.q_sol - Zb.qr;
   double pgfr_b = Zb.qg + sink_b;
   double psacr_b = Zb.qs + sink_b;
@@ -943,8 +951,6 @@ SHP void ic_graupel_rime(const MpConst& K, IcState& Z, double qv, double den, do
   Z.tz = Z.tz + sink * lhi / Z.cvm;
 }
 SHP void ic_graupel_rime_b(const MpConst& K, const IcState& Z, const IcIn& I, IcState& Zb, IcIn& Ib) {
-  IcState Z1 = Z;
-  ic_graupel_rime(K, Z1, I.qv, I.den, I.vtg, I.vtr);
   const double den = I.den;
   const double lhi = K.LI00 + K.DC_ICE * Z.tz;
   const double icpk = lhi / Z.cvm;
@@ -966,9 +972,10 @@ SHP void ic_graupel_rime_b(const MpConst& K, const IcState& Z, const IcIn& I, Ic
   const double factor = m / M;
   const double pgacr = factor * pgacr0, pgacw = factor * pgacw0;
   const double sink = pgacr + pgacw;
+  const double cvm1 = cvm_of(K, I.qv, Z.q_liq - sink, Z.q_sol + sink);
   // reverse
   double lhi_b = 0.0;
-  double sink_b = close_transfer_b(K, 1.0, sink, lhi, Z1.cvm, Zb, Ib.qv, lhi_b);
+  double sink_b = close_transfer_b(K, 1.0, sink, lhi, cvm1, Zb, Ib.qv, lhi_b);
   sink_b += -Zb.q_liq + Zb.q_sol + Zb.qg;
   const double pgacw_b = sink_b - Zb.ql;
   const double pgacr_b = sink_b - Zb.qr;
@@ -1012,7 +1019,7 @@ SHP void ic_graupel_rime_b(const MpConst& K, const IcState& Z, const IcIn& I, Ic
 // inputs only: the routine works on copies). On entry Zb holds the output
 // adjoints (its q_liq, q_sol, cvm fields are ignored); on return, the input
 // adjoints. Ib is accumulated.
-SHP void icloud_processes_b(const MpConst& K, const IcState& Z0, const IcIn& I, IcState& Zb, IcIn& Ib) {
+SHB void icloud_processes_b(const MpConst& K, const IcState& Z0, const IcIn& I, IcState& Zb, IcIn& Ib) {
   Zb.q_liq = 0.0;
   Zb.q_sol = 0.0;
   Zb.cvm = 0.0;
@@ -1101,8 +1108,6 @@ SHP void sg_cloud_water(const MpConst& K, SgState& Z, double den, double lhl0, d
 }
 SHP void sg_cloud_water_b(const MpConst& K, const SgState& Z, double den, double lhl0, double tcp3, SgState& Zb,
                           double& den_b, double& lhl0_b, double& tcp3_b) {
-  SgState Z1 = Z;
-  sg_cloud_water(K, Z1, den, lhl0, tcp3);
   double dwsdt;
   const double qsw = wqs2(K, Z.tz, den, dwsdt);
   const double dq0 = qsw - Z.qv;
@@ -1116,7 +1121,8 @@ SHP void sg_cloud_water_b(const MpConst& K, const SgState& Z, double den, double
   } else {
     evap = dq0 / D;
   }
-  double evap_b = sg_close_b(K, -1.0, evap, lhl0, Z1.cvm, Zb, lhl0_b);
+  const double cvm1 = cvm_of(K, Z.qv + evap, Z.q_liq - evap, Z.q_sol);
+  double evap_b = sg_close_b(K, -1.0, evap, lhl0, cvm1, Zb, lhl0_b);
   evap_b += Zb.qv - Zb.ql - Zb.q_liq;
   double dq0_b = 0.0, D_b = 0.0, qsw_b = 0.0;
   if (dq0 > 0.0) {
@@ -1160,15 +1166,14 @@ SHP void sg_freeze(const MpConst& K, SgState& Z) {
 SHP void sg_freeze_b(const MpConst& K, const SgState& Z, SgState& Zb) {
   const double dtmp = K.t_wfr - Z.tz;
   if (!((dtmp > 0.0) && (Z.ql > QCMIN))) return;
-  SgState Z1 = Z;
-  sg_freeze(K, Z1);
   const double lhi = K.LI00 + K.DC_ICE * Z.tz;
   const double icpk = lhi / Z.cvm;
   const double a = Z.ql * dtmp * 0.125, b = dtmp / icpk;
   const double m = fmin(a, b);
   const double sink = fmin(Z.ql, m);
+  const double cvm1 = cvm_of(K, Z.qv, Z.q_liq - sink, Z.q_sol + sink);
   double lhi_b = 0.0;
-  double sink_b = sg_close_b(K, 1.0, sink, lhi, Z1.cvm, Zb, lhi_b);
+  double sink_b = sg_close_b(K, 1.0, sink, lhi, cvm1, Zb, lhi_b);
   sink_b += -Zb.ql + Zb.qi - Zb.q_liq + Zb.q_sol;
   double dtmp_b = 0.0, icpk_b = 0.0;
   if (min_first(Z.ql, m)) {
@@ -1205,8 +1210,6 @@ SHP void sg_bigg(const MpConst& K, SgState& Z, double den) {
 SHP void sg_bigg_b(const MpConst& K, const SgState& Z, double den, SgState& Zb, double& den_b) {
   const double tc = K.tice - Z.tz;
   if (!((Z.ql > QRMIN) && (tc > 0.0))) return;
-  SgState Z1 = Z;
-  sg_bigg(K, Z1, den);
   const double lhi = K.LI00 + K.DC_ICE * Z.tz;
   const double icpk = lhi / Z.cvm;
   const double e = xexp(0.66 * tc);
@@ -1215,8 +1218,9 @@ SHP void sg_bigg_b(const MpConst& K, const SgState& Z, double den, SgState& Zb, 
   const double r = tc / icpk;
   const double m = fmin(r, s0);
   const double sink = fmin(Z.ql, m);
+  const double cvm1 = cvm_of(K, Z.qv, Z.q_liq - sink, Z.q_sol + sink);
   double lhi_b = 0.0;
-  double sink_b = sg_close_b(K, 1.0, sink, lhi, Z1.cvm, Zb, lhi_b);
+  double sink_b = sg_close_b(K, 1.0, sink, lhi, cvm1, Zb, lhi_b);
   sink_b += -Zb.ql + Zb.qi - Zb.q_liq + Zb.q_sol;
   double tc_b = 0.0, icpk_b = 0.0;
   if (min_first(Z.ql, m)) {
@@ -1264,8 +1268,6 @@ SHP void sg_ice(const MpConst& K, SgState& Z, double den, double dt_pisub) {
 }
 SHP void sg_ice_b(const MpConst& K, const SgState& Z, double den, double dt_pisub, SgState& Zb, double& den_b) {
   if (!(Z.tz < K.tice)) return;
-  SgState Z1 = Z;
-  sg_ice(K, Z1, den, dt_pisub);
   const double lhl = K.lv00 + K.d0_vap * Z.tz, lhi = K.LI00 + K.DC_ICE * Z.tz;
   const double tcpk = lhl / Z.cvm + lhi / Z.cvm;
   double dqsdt;
@@ -1300,8 +1302,9 @@ SHP void sg_ice_b(const MpConst& K, const SgState& Z, double den, double dt_pisu
     Mx = fmax(sink0, -Z.qi);
     sink = fmax(pidep, Mx);
   }
+  const double cvm1 = cvm_of(K, Z.qv - sink, Z.q_liq, Z.q_sol + sink);
   double lh_b = 0.0;
-  double s_b = sg_close_b(K, 1.0, sink, lh, Z1.cvm, Zb, lh_b);
+  double s_b = sg_close_b(K, 1.0, sink, lh, cvm1, Zb, lh_b);
   s_b += -Zb.qv + Zb.qi + Zb.q_sol;
   double sink0_b = 0.0, pidep0_b = 0.0, tcpk_b = 0.0;
   if (dq > 0.0) {
@@ -1387,8 +1390,6 @@ SHP void sg_snow(const MpConst& K, SgState& Z, double den, double denfac) {
 SHP void sg_snow_b(const MpConst& K, const SgState& Z, double den, double denfac, SgState& Zb, double& den_b,
                    double& denfac_b) {
   if (!(Z.qs > QRMIN)) return;
-  SgState Z1 = Z;
-  sg_snow(K, Z1, den, denfac);
   const double lhl = K.lv00 + K.d0_vap * Z.tz, lhi = K.LI00 + K.DC_ICE * Z.tz;
   const double tcpk = lhl / Z.cvm + lhi / Z.cvm;
   double dqsdt;
@@ -1417,8 +1418,9 @@ SHP void sg_snow_b(const MpConst& K, const SgState& Z, double den, double denfac
     Mx = fmax(dq, r);
     pssub = fmax(ps1, Mx);
   }
+  const double cvm1 = cvm_of(K, Z.qv + pssub, Z.q_liq, Z.q_sol - pssub);
   double lh_b = 0.0;
-  double p_b = sg_close_b(K, -1.0, pssub, lhl + lhi, Z1.cvm, Zb, lh_b);
+  double p_b = sg_close_b(K, -1.0, pssub, lhl + lhi, cvm1, Zb, lh_b);
   p_b += Zb.qv - Zb.qs - Zb.q_sol;
   double ps1_b = 0.0, dq_b = 0.0, tcpk_b = 0.0;
   if (ps1 > 0.0) {
@@ -1489,8 +1491,6 @@ SHP void sg_graupel(const MpConst& K, SgState& Z, double den) {
 }
 SHP void sg_graupel_b(const MpConst& K, const SgState& Z, double den, SgState& Zb, double& den_b) {
   if (!(Z.qg > QRMIN)) return;
-  SgState Z1 = Z;
-  sg_graupel(K, Z1, den);
   const double lhl = K.lv00 + K.d0_vap * Z.tz, lhi = K.LI00 + K.DC_ICE * Z.tz;
   const double tcpk = lhl / Z.cvm + lhi / Z.cvm;
   double dqsdt;
@@ -1519,8 +1519,9 @@ SHP void sg_graupel_b(const MpConst& K, const SgState& Z, double den, SgState& Z
     fmn = fmin(1.0, g);
     pg = Mx * fmn;
   }
+  const double cvm1 = cvm_of(K, Z.qv - pg, Z.q_liq, Z.q_sol + pg);
   double lh_b = 0.0;
-  double pg_b = sg_close_b(K, 1.0, pg, lhl + lhi, Z1.cvm, Zb, lh_b);
+  double pg_b = sg_close_b(K, 1.0, pg, lhl + lhi, cvm1, Zb, lh_b);
   pg_b += Zb.qg - Zb.qv + Zb.q_sol;
   double pg0_b = 0.0, dq_b = 0.0, tcpk_b = 0.0;
   if (pg0 > 0.0) {
@@ -1576,8 +1577,6 @@ SHP void sg_rain_evap(const MpConst& K, SgState& Z, double den, double rh_rain) 
 }
 SHP void sg_rain_evap_b(const MpConst& K, const SgState& Z, double den, double rh_rain, SgState& Zb, double& den_b) {
   if (!(Z.qr > QCMIN)) return;
-  SgState Z1 = Z;
-  sg_rain_evap(K, Z1, den, rh_rain);
   const double lhl = K.lv00 + K.d0_vap * Z.tz;
   const double lcpk = lhl / Z.cvm;
   double dqsdt;
@@ -1586,8 +1585,9 @@ SHP void sg_rain_evap_b(const MpConst& K, const SgState& Z, double den, double r
   const double dm = dim(rh_rain * qsw, Z.qv);
   const double e = dm / D;
   const double sink = fmin(Z.qr, e);
+  const double cvm1 = cvm_of(K, Z.qv + sink, Z.q_liq - sink, Z.q_sol);
   double lhl_b = 0.0;
-  double s_b = sg_close_b(K, -1.0, sink, lhl, Z1.cvm, Zb, lhl_b);
+  double s_b = sg_close_b(K, -1.0, sink, lhl, cvm1, Zb, lhl_b);
   s_b += Zb.qv - Zb.qr - Zb.q_liq;
   double lcpk_b = 0.0, qsw_b = 0.0, dqsdt_b = 0.0;
   if (min_first(Z.qr, e)) {
@@ -1688,7 +1688,7 @@ SHP void sg_cloud_frac_b(const MpConst& K, const SgState& Z, double den, double 
 // output adjoints on entry and the input adjoints on return; qa_b is the
 // adjoint of the cloud-fraction accumulator (unchanged: qa only grows by
 // increments). den_b, denfac_b are accumulated.
-SHP void subgrid_z_proc_b(const MpConst& K, double h_var, double rh_adj, double rh_rain, double qa_b, double qg,
+SHB void subgrid_z_proc_b(const MpConst& K, double h_var, double rh_adj, double rh_rain, double qa_b, double qg,
                           double qi, double ql, double qr, double qs, double qv, double tz, double den, double denfac,
                           double p1, double& qg_b, double& qi_b, double& ql_b, double& qr_b, double& qs_b,
                           double& qv_b, double& tz_b, double& den_b, double& denfac_b) {
@@ -1803,7 +1803,7 @@ SHP void subgrid_z_proc_b(const MpConst& K, double h_var, double rh_adj, double 
 
 // ------------------------------------------ pointwise blocks of the step
 // sedi_ice_melt: state (qv ql qr qi qs qg tz); qv qs qg are read only
-SHP void sedi_ice_melt_b(const MpConst& K, double qv, double ql, double qr, double qi, double qs, double qg, double tz,
+SHB void sedi_ice_melt_b(const MpConst& K, double qv, double ql, double qr, double qi, double qs, double qg, double tz,
                          double& qv_b, double& ql_b, double& qr_b, double& qi_b, double& qs_b, double& qg_b,
                          double& tz_b) {
   const double lhi = K.LI00 + K.DC_ICE * tz;
@@ -1855,7 +1855,7 @@ SHP void sedi_ice_melt_b(const MpConst& K, double qv, double ql, double qr, doub
 
 // icloud_melt_freeze: state (qv ql qr qi qs qg tz) and den; outputs also the
 // totals q_liq, q_sol and cvm, whose adjoints come in q_liq_b, q_sol_b, cvm_b
-SHP void icloud_melt_freeze_b(const MpConst& K, double qv, double ql, double qr, double qi, double qs, double qg,
+SHB void icloud_melt_freeze_b(const MpConst& K, double qv, double ql, double qr, double qi, double qs, double qg,
                               double tz, double den, double q_liq_b, double q_sol_b, double cvm_b, double& qv_b,
                               double& ql_b, double& qr_b, double& qi_b, double& qs_b, double& qg_b, double& tz_b,
                               double& den_b) {
@@ -1944,7 +1944,7 @@ SHP void icloud_melt_freeze_b(const MpConst& K, double qv, double ql, double qr,
 }
 
 // fix_negative_point: state (qv ql qr qi qs qg tz)
-SHP void fix_negative_point_b(const MpConst& K, double qv, double ql, double qr, double qi, double qs, double qg,
+SHB void fix_negative_point_b(const MpConst& K, double qv, double ql, double qr, double qi, double qs, double qg,
                               double tz, double& qv_b, double& ql_b, double& qr_b, double& qi_b, double& qs_b,
                               double& qg_b, double& tz_b) {
   const double cvm = K.c_air + qv * K.c_vap + (qr + ql) * K.C_LIQ + (qi + qs + qg) * K.C_ICE;

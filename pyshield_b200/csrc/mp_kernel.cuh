@@ -851,10 +851,11 @@ SHD void sedimentation(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool
 }
 
 // icloud (:1220-1449): instant melting or freezing, the ice slope, the ice
-// processes and the saturation adjustment.
+// processes and the saturation adjustment. The adjoint's replay passes rec
+// to keep the state between the ice processes and the adjustment.
 template <int NW, bool MIXED>
 SHD void icloud(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid, LevState& S, const StepGeom& P,
-                double& qa, double vtg, double vtr, double vts) {
+                double& qa, double vtg, double vtr, double vts, LevState* rec = nullptr) {
   double &qv = S.qv, &ql = S.ql, &qr = S.qr, &qi = S.qi, &qs = S.qs, &qg = S.qg, &tz = S.tz;
   double q_liq, q_sol, cvm;
   icloud_melt_freeze(K, qv, ql, qr, qi, qs, qg, tz, P.den, q_liq, q_sol, cvm);
@@ -871,6 +872,7 @@ SHD void icloud(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid,
                          cvm);
     else
       icloud_processes(K, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac, vtg, vtr, vts, P.p1, di, q_liq, q_sol, cvm);
+    if (rec) *rec = S;
     subgrid_z_proc(K, P.h_var, P.rh_adj, P.rh_rain, qa, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac, P.p1);
   }
 }

@@ -30,6 +30,15 @@ namespace shield {
 namespace {
 
 constexpr int VJP_MAXNT = 4;  // sub-steps whose stage states fit the store
+
+// launch shape: columns per block for 65-96 levels, and the minimum
+// resident blocks per SM given to __launch_bounds__
+#ifndef SHIELD_VJP_G3
+#define SHIELD_VJP_G3 4
+#endif
+#ifndef SHIELD_VJP_MINB
+#define SHIELD_VJP_MINB 1
+#endif
 constexpr int NT_IN = N_VJP_IN + N_VJP_COT;
 
 // Shared memory: NT_IN input tiles (inputs, then cotangents), N_VJP_GRAD
@@ -244,7 +253,7 @@ struct StepAdj {
 // at this level; rain_c: cotangent of the surface rain total; vtr_b: adjoint
 // of the pass's output fall speed.
 template <int NW>
-SHD void warm_rain_b(Column<NW>& C, const MpConst& K, bool valid, const LevState& S0, const StepGeom& P, double m1r_b,
+static __device__ __noinline__ void warm_rain_b(Column<NW>& C, const MpConst& K, bool valid, const LevState& S0, const StepGeom& P, double m1r_b,
                      double rain_c, double vtr_b, LevState& Sb, StepAdj& Ab) {
   const int k = C.k, L = C.L;
   const double dt5 = 0.5 * K.dt_rain;
@@ -327,7 +336,7 @@ SHD void warm_rain_b(Column<NW>& C, const MpConst& K, bool valid, const LevState
 // solid flux at this level; ice_c, snow_c, graupel_c: cotangents of the
 // surface totals; vtg_b, vts_b: adjoints of the output fall speeds.
 template <int NW>
-SHD void sedimentation_b(Column<NW>& C, const MpConst& K, bool valid, const LevState& S0, const StepGeom& P,
+static __device__ __noinline__ void sedimentation_b(Column<NW>& C, const MpConst& K, bool valid, const LevState& S0, const StepGeom& P,
                          double m1s_b, double ice_c, double snow_c, double graupel_c, double vtg_b, double vts_b,
                          LevState& Sb, StepAdj& Ab) {
   const int k = C.k, L = C.L;
@@ -501,12 +510,14 @@ SHD void sedimentation_b(Column<NW>& C, const MpConst& K, bool valid, const LevS
     fall_speed_b(K, S0.qg, S0.qi, S0.qs, S0.tz, P.den, vt_b[2], vt_b[0], vt_b[1], Sb.qg, Sb.qi, Sb.qs, Sb.tz, Ab.den);
 }
 
-// icloud reverse from its entry state S0; qa_b: adjoint of the level's
+// icloud reverse from its entry state S0 and the state S2 between the ice
+// processes and the saturation adjustment; qa_b: adjoint of the level's
 // cloud-fraction accumulator
 template <int NW>
-SHD void icloud_b(Column<NW>& C, const MpConst& K, bool valid, const LevState& S0, const StepGeom& P, double vtg,
-                  double vtr, double vts, double qa_b, LevState& Sb, StepAdj& Ab, double& vtg_b, double& vtr_b,
-                  double& vts_b) {
+static __device__ __noinline__ void icloud_b(Column<NW>& C, const MpConst& K, bool valid, const LevState& S0,
+                                             const LevState& S2, const StepGeom& P, double vtg, double vtr,
+                                             double vts, double qa_b, LevState& Sb, StepAdj& Ab, double& vtg_b,
+                                             double& vtr_b, double& vts_b) {
   LevState S1 = S0;
   double q_liq, q_sol, cvm;
   icloud_melt_freeze(K, S1.qv, S1.ql, S1.qr, S1.qi, S1.qs, S1.qg, S1.tz, P.den, q_liq, q_sol, cvm);
@@ -519,9 +530,6 @@ SHD void icloud_b(Column<NW>& C, const MpConst& K, bool valid, const LevState& S
   }
   double di_b = 0.0, qliq_b = 0.0, qsol_b = 0.0, cvm_b = 0.0;
   if (valid) {
-    LevState S2 = S1;
-    icloud_processes(K, S2.qg, S2.qi, S2.ql, S2.qr, S2.qs, S2.qv, S2.tz, P.den, P.denfac, vtg, vtr, vts, P.p1, di,
-                     q_liq, q_sol, cvm);
     subgrid_z_proc_b(K, P.h_var, P.rh_adj, P.rh_rain, qa_b, S2.qg, S2.qi, S2.ql, S2.qr, S2.qs, S2.qv, S2.tz, P.den,
                      P.denfac, P.p1, Sb.qg, Sb.qi, Sb.ql, Sb.qr, Sb.qs, Sb.qv, Sb.tz, Ab.den, Ab.denfac);
     const IcState Z0{S1.qg, S1.qi, S1.ql, S1.qr, S1.qs, S1.tz, q_liq, q_sol, cvm};
@@ -558,8 +566,28 @@ SHD void icloud_b(Column<NW>& C, const MpConst& K, bool valid, const LevState& S
                          Sb.ql, Sb.qr, Sb.qi, Sb.qs, Sb.qg, Sb.tz, Ab.den);
 }
 
-template <int NW, int G>
-__global__ void __launch_bounds__(32 * NW * G, 1) mp_vjp_kernel(const __grid_constant__ VjpArgs A) {
+// forward stages of the replay, out of line (one copy each)
+template <int NW>
+static __device__ __noinline__ void fwd_warm_rain(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid,
+                                                  LevState& S, const StepGeom& P, double& vtr, double& m1r,
+                                                  double& r1) {
+  warm_rain<NW, false>(C, K, KF, valid, S, P, vtr, m1r, r1);
+}
+template <int NW>
+static __device__ __noinline__ void fwd_sedimentation(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid,
+                                                      LevState& S, const StepGeom& P, double& vtg, double& vts,
+                                                      double& m1s, double& ice, double& snow, double& graupel) {
+  sedimentation<NW, false>(C, K, KF, valid, S, P, vtg, vts, m1s, ice, snow, graupel);
+}
+template <int NW>
+static __device__ __noinline__ void fwd_icloud(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid,
+                                               LevState& S, const StepGeom& P, double& qa, double vtg, double vtr,
+                                               double vts, LevState& rec) {
+  icloud<NW, false>(C, K, KF, valid, S, P, qa, vtg, vtr, vts, &rec);
+}
+
+template <int NW, int G, int MINB>
+__global__ void __launch_bounds__(32 * NW * G, MINB) mp_vjp_kernel(const __grid_constant__ VjpArgs A) {
   extern __shared__ double sm[];
   using SM = VjpSmem<NW, G>;
   constexpr int RP = Tiles<NW>::RP;
@@ -607,28 +635,28 @@ __global__ void __launch_bounds__(32 * NW * G, 1) mp_vjp_kernel(const __grid_con
     P.dz = 100.0;
     fields_init<NW>(C, K, valid, pt, qin[0], qin[1], qin[2], qin[3], qin[4], qin[5], delp, TI(IN_W, 0.0), dz0, land,
                     area, S, P);
-    LevState ck[VJP_MAXNT][4];
+    LevState ck[VJP_MAXNT][5];  // entries of the four stages, and the state before the adjustment
     double ckv[VJP_MAXNT][3];
     double m1 = 0.0, m1_sol = 0.0, vtr = VF_MIN, vtg = VF_MIN, vts = VF_MIN, qa = 0.0, ice = 0.0, snow = 0.0,
            graupel = 0.0;
     const int nt = K.ntimes;
 #pragma unroll 1
     for (int it = 0; it < nt; ++it) {
-      double m1r, r1;
-      ck[it][0] = S;
       substep_geometry<NW>(C, K, valid, pt, dz0, S, P);
-      warm_rain<NW, false>(C, K, KF, valid, S, P, vtr, m1r, r1);
-      m1 = m1 + m1r;
-      ck[it][1] = S;
-      sedimentation<NW, false>(C, K, KF, valid, S, P, vtg, vts, m1_sol, ice, snow, graupel);
-      ck[it][2] = S;
-      warm_rain<NW, false>(C, K, KF, valid, S, P, vtr, m1r, r1);
-      m1 = m1 + m1r + m1_sol;
-      ck[it][3] = S;
+#pragma unroll 1
+      for (int pass = 0; pass < 2; ++pass) {
+        double m1r, r1;
+        ck[it][2 * pass] = S;
+        fwd_warm_rain<NW>(C, K, KF, valid, S, P, vtr, m1r, r1);
+        m1 = (pass == 0) ? m1 + m1r : m1 + m1r + m1_sol;
+        ck[it][2 * pass + 1] = S;
+        if (pass == 1) break;
+        fwd_sedimentation<NW>(C, K, KF, valid, S, P, vtg, vts, m1_sol, ice, snow, graupel);
+      }
       ckv[it][0] = vtr;
       ckv[it][1] = vtg;
       ckv[it][2] = vts;
-      icloud<NW, false>(C, K, KF, valid, S, P, qa, vtg, vtr, vts);
+      fwd_icloud<NW>(C, K, KF, valid, S, P, qa, vtg, vtr, vts, ck[it][4]);
     }
 
     // ------------------------------------------------- fields_update reverse
@@ -741,10 +769,14 @@ __global__ void __launch_bounds__(32 * NW * G, 1) mp_vjp_kernel(const __grid_con
       Ab.denfac = 0.0;
       Ab.dz = 0.0;
       double vtg_b = 0.0, vtr_b = 0.0, vts_b = 0.0;
-      icloud_b<NW>(C, K, valid, ck[it][3], Pg, ckv[it][1], ckv[it][0], ckv[it][2], qa_b, Sb, Ab, vtg_b, vtr_b, vts_b);
-      warm_rain_b<NW>(C, K, valid, ck[it][2], Pg, m1_b, rain_c, vtr_b, Sb, Ab);
-      sedimentation_b<NW>(C, K, valid, ck[it][1], Pg, m1_b, ice_c, snow_c, graupel_c, vtg_b, vts_b, Sb, Ab);
-      warm_rain_b<NW>(C, K, valid, ck[it][0], Pg, m1_b, rain_c, 0.0, Sb, Ab);
+      icloud_b<NW>(C, K, valid, ck[it][3], ck[it][4], Pg, ckv[it][1], ckv[it][0], ckv[it][2], qa_b, Sb, Ab, vtg_b,
+                   vtr_b, vts_b);
+#pragma unroll 1
+      for (int pass = 1; pass >= 0; --pass) {
+        warm_rain_b<NW>(C, K, valid, ck[it][2 * pass], Pg, m1_b, rain_c, pass == 1 ? vtr_b : 0.0, Sb, Ab);
+        if (pass == 1)
+          sedimentation_b<NW>(C, K, valid, ck[it][1], Pg, m1_b, ice_c, snow_c, graupel_c, vtg_b, vts_b, Sb, Ab);
+      }
       // geometry: denfac = sqrt(SFCRHO / den), den = den0 dz0 / dz1,
       // dz1 = dz0 tz / t0, dz = heights(-dz1), den0 = -dp1 / (g dz0)
       if (valid) {
@@ -903,9 +935,9 @@ __global__ void __launch_bounds__(32 * NW * G, 1) mp_vjp_kernel(const __grid_con
   store_tiles<NW, G, N_VJP_GRAD>(A.grad, sm + SM::out, A.ncol, A.nx, L, c0);
 }
 
-template <int NW, int G>
+template <int NW, int G, int MINB>
 cudaError_t launch_vjp(const VjpArgs& A, cudaStream_t st) {
-  auto kern = mp_vjp_kernel<NW, G>;
+  auto kern = mp_vjp_kernel<NW, G, MINB>;
   const size_t smem = VjpSmem<NW, G>::bytes;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -920,11 +952,11 @@ int mp_vjp_max_substeps() { return VJP_MAXNT; }
 
 cudaError_t mp_launch_vjp(const VjpArgs& A, cudaStream_t st) {
   const int L = A.nz;
-  if (L <= 32) return launch_vjp<1, 2>(A, st);
-  if (L <= 64) return launch_vjp<2, 2>(A, st);
-  if (L <= 96) return launch_vjp<3, 2>(A, st);
-  if (L <= 128) return launch_vjp<4, 1>(A, st);
-  return launch_vjp<8, 1>(A, st);
+  if (L <= 32) return launch_vjp<1, 2, SHIELD_VJP_MINB>(A, st);
+  if (L <= 64) return launch_vjp<2, 2, SHIELD_VJP_MINB>(A, st);
+  if (L <= 96) return launch_vjp<3, SHIELD_VJP_G3, SHIELD_VJP_MINB>(A, st);
+  if (L <= 128) return launch_vjp<4, 1, SHIELD_VJP_MINB>(A, st);
+  return launch_vjp<8, 1, 1>(A, st);
 }
 
 }  // namespace shield

@@ -16,10 +16,10 @@
 
 #include "mp_physics.cuh"
 
-// The larger adjoints are out of line in device code: every call site then
-// shares one copy, which keeps the adjoint kernel within the instruction
-// cache.
-#if defined(__CUDACC__) && !defined(SHIELD_ADJ_INLINE)
+// The larger adjoints are inlined into their (out-of-line) stage reverses;
+// SHIELD_ADJ_NOINLINE makes them calls instead (measured slower: the call
+// sequences cost more than the instruction-cache footprint they save).
+#if defined(__CUDACC__) && defined(SHIELD_ADJ_NOINLINE)
 #define SHB static __host__ __device__ __noinline__
 #elif defined(__CUDACC__)
 #define SHB static __host__ __device__ __forceinline__

@@ -347,6 +347,102 @@ class HostPipeline:
         return e0.elapsed_time(e1)
 
 
+def prestep_bytes(nx, ny, nz, h=HALO):
+    """Algorithmic HBM bytes of one shield_physics_prestep launch: each field
+    that statein, get_prs_fv3, get_phi_fv3 and prepare_microphysics read is
+    read once and each they write is written once. A compute column reads
+    delp and the 7 tracers on nz + 1 levels and delz, qsgs_tke, pt, omga on
+    nz; it writes phii, prsi, prsik, the 7 tracers and delp on nz + 1 levels
+    and qsgs_tke, dm, delprsi, del_gz, phil, dz, wmp and the 10 tendencies on
+    nz. A halo column reads prsi, phii (nz + 1) and pt, qvapor (nz) and
+    writes phii (nz + 1), delprsi, del_gz and phil (nz)."""
+    L, L1 = nz, nz + 1
+    ncomp = nx * ny
+    nhalo = (nx + 2 * h) * (ny + 2 * h) - ncomp
+    return 8 * (ncomp * (19 * L1 + 21 * L) + nhalo * (3 * L1 + 5 * L))
+
+
+def run_physics(n_cube=N_CUBE, nlev=79, dt=DT, reps=5):
+    """pySHiELD's Physics.__call__ at CN x nlev: the fused driver pre-step
+    kernel, the microphysics step and the state update. Every step starts
+    from the same storages (restored outside the timed region, as a model
+    hands the physics a fresh dycore state each step); each call is timed
+    with CUDA events, and the pre-step launch alone likewise."""
+    import numpy as np
+    import torch
+
+    from pyshield_b200._config import PhysicsConfig
+    from pyshield_b200.grid import GridData, GridIndexing, QuantityFactory, StencilFactory
+    from pyshield_b200.inputs import PHYSICS_3D, PHYSICS_INTERFACE, PTOP, TENDENCY_FIELDS, make_physics_state
+    from pyshield_b200.physics import Physics, PhysicsState
+    from pyshield_b200.quantity import Quantity
+
+    nx, ny = n_cube, 6 * n_cube
+    st, area = make_physics_state(nx, ny, nlev, seed=99, halo=HALO)
+
+    def dev3(a):
+        return torch.from_numpy(np.ascontiguousarray(a.transpose(2, 1, 0))).cuda().permute(2, 1, 0)
+
+    def dev2(a):
+        return torch.from_numpy(np.ascontiguousarray(a.T)).cuda().t()
+
+    gi = GridIndexing(nx, ny, nlev, HALO)
+    qf = QuantityFactory(gi)
+    q = {}
+    for nm in PHYSICS_3D:
+        dims = ("x", "y", "z_interface" if nm in PHYSICS_INTERFACE else "z")
+        q[nm] = Quantity(dev3(st[nm]), dims, "", (HALO, HALO, 0), (nx, ny, nlev + 1 if nm in PHYSICS_INTERFACE else nlev))
+    q["land"] = Quantity(dev2(st["land"]), ("x", "y"), "", (HALO, HALO), (nx, ny))
+    cfg = PhysicsConfig(dt_atmos=int(dt))
+    ps = PhysicsState(**q, quantity_factory=qf, schemes=cfg.schemes)
+    area_st = np.zeros(st["land"].shape)
+    area_st[HALO:HALO + nx, HALO:HALO + ny] = area.reshape(ny, nx).T
+    phys = Physics(StencilFactory(gi), qf, GridData(Quantity(dev2(area_st), ("x", "y"), "m^2", (HALO, HALO), (nx, ny)), PTOP), cfg)
+    pristine = {nm: q[nm].data.clone() for nm in PHYSICS_3D}
+    pristine.update({t: dev3(st[t]) for t in TENDENCY_FIELDS})
+    del st
+
+    def restore():
+        for nm in PHYSICS_3D:
+            q[nm].data.copy_(pristine[nm])
+        for t in TENDENCY_FIELDS:
+            getattr(ps.microphysics, t).data.copy_(pristine[t])
+
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        total = 0.0
+        for r in range(reps + 1):
+            restore()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if r > 0:  # the first call warms up
+                total += e0.elapsed_time(e1)
+        return total / reps
+
+    full_ms = timed(lambda: phys(ps, dt))
+    pre_ms = timed(lambda: phys.prestep(ps))
+    nbytes = prestep_bytes(nx, ny, nlev)
+    peak, peak_kind = peaks()
+    achieved = nbytes / (pre_ms / 1000.0) / 1e9
+    ncol = nx * ny
+    return {
+        "workload": f"Physics.__call__ (driver pre-steps, microphysics, state update), C{n_cube} ({ncol} columns) "
+                    f"x L{nlev}, dt {dt:g} s, FP64",
+        "ms_per_step": full_ms,
+        "column_steps_per_s": ncol / (full_ms / 1000.0),
+        "prestep_ms": pre_ms,
+        "prestep_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "bytes_per_launch": nbytes,
+                             "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},
+        "gpu_launches_per_step": 3,
+        "note": "device time (CUDA events), mean of the timed calls; the storages are restored before each call",
+    }
+
+
 def max_over_ranks(values, world, device):
     """Each rank's device-measured times -> their maximum over all ranks (the
     slowest replica sets the job's time). One all-reduce; every rank calls it
@@ -550,6 +646,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the C48 adjoint-cost measurement")
+    ap.add_argument("--no-physics", action="store_true", help="skip the Physics.__call__ measurement")
     ap.add_argument("--ncube", type=int, default=N_CUBE, help="cube size N of the CN workload (default 96)")
     ap.add_argument("--ensemble", action="store_true", help="run the ensemble workload instead")
     ap.add_argument("--members", type=int, default=64)
@@ -648,6 +745,8 @@ def main():
     if pool:
         pool.close()
     adjoint = run_adjoint() if (rank == 0 and world == 1 and not args.no_adjoint and args.form == "plain") else None
+    physics = (run_physics(n_cube=args.ncube, nlev=nlev)
+               if (rank == 0 and world == 1 and not args.no_physics and args.form == "plain") else None)
 
     if rank == 0:
         rec = {
@@ -681,6 +780,7 @@ def main():
                       if r["mixed_ms"] > 0 else None),
             "clocks": r["clocks"],
             "adjoint": adjoint,
+            "physics": physics,
         }
         emit(rec)
 

@@ -9,6 +9,11 @@
  *                      grid_data, namelist)     pySHiELD/stencils/microphysics.py:1624-1804
  *   shield_mp_step     Microphysics.__call__(state, timestep)
  *                                                pySHiELD/stencils/microphysics.py:1981-2263
+ *   shield_physics_prestep
+ *                      Physics.__call__ before the microphysics:
+ *                      atmos_phys_driver_statein, get_prs_fv3, get_phi_fv3,
+ *                      prepare_microphysics  pySHiELD/stencils/physics.py:26-143, 276-330;
+ *                                            get_prs_fv3.py:7-20; get_phi_fv3.py:7-25
  *   shield_update_physics_state
  *                      update_physics_state_with_tendencies
  *                                                pySHiELD/stencils/physics.py:151-194
@@ -253,6 +258,39 @@ int shield_update_physics_state(int nx, int ny, int nz, const ShieldField3D* sta
 int shield_update_atmos_state(int nx, int ny, int nz, int hx, int mode, const ShieldField3D* f, ShieldField3D ps,
                               ShieldField3D u_srf, ShieldField3D v_srf, double rdt, double dt, double kappa,
                               double cp_air, void* stream);
+
+/* Fields of shield_physics_prestep: the PhysicsState storages
+ * (pySHiELD/physics_state.py:17-300) and Physics' own scratch
+ * (physics.py:222-225), each with the origin at the compute-domain corner
+ * and nz + 1 levels of storage. The member order is fixed. */
+typedef struct {
+  ShieldField3D phii, prsi, prsik; /* interface fields; prsik is Physics._prsik */
+  ShieldField3D delz, delp;
+  ShieldField3D qvapor, qliquid, qrain, qice, qsnow, qgraupel, qo3mr, qsgs_tke;
+  ShieldField3D pt;
+  ShieldField3D dm;      /* Physics._dm3d */
+  ShieldField3D delprsi;
+  ShieldField3D del_gz;  /* Physics._del_gz */
+  ShieldField3D phil;
+  ShieldField3D omga, dz, wmp; /* read / written by prepare_microphysics only */
+  ShieldField3D pt_dt, qv_dt, ql_dt, qr_dt, qi_dt, qs_dt, qg_dt, qa_dt, udt, vdt; /* the microphysics
+                                   tendencies that prepare_microphysics zeroes; a NULL ptr is skipped */
+} ShieldPhysicsFields;
+
+#define SHIELD_PHYS_PREPARE_MICROPHYSICS 1 /* run prepare_microphysics (GFS_microphysics in the schemes) */
+
+/* The physics driver's steps before the microphysics, Physics.__call__
+ * (physics.py:276-330), in the reference's order and on its domains:
+ *   atmos_phys_driver_statein on the compute domain, nz + 1 levels
+ *       (externals nwat, ptop, pk0inv = (1/p00)^kappa, pktop = (ptop/p00)^kappa,
+ *       p00 = 1e5, computed here from ptop as Physics.__init__ does);
+ *   get_prs_fv3 and get_phi_fv3 on the full domain (hx halo points on each
+ *       side), nz + 1 levels;
+ *   with SHIELD_PHYS_PREPARE_MICROPHYSICS: prepare_microphysics on the
+ *       compute domain, nz levels.
+ * One fused kernel; see pyshield_b200/csrc/physics.cu. */
+int shield_physics_prestep(int nx, int ny, int nz, int hx, int nwat, double ptop, int flags,
+                           const ShieldPhysicsFields* fields, void* stream);
 
 /* Test hook: the scalars shield_mp_step uses for `timestep` (physical
  * constants, setupm constants, sub-step values), computed on the host

@@ -123,6 +123,17 @@ class ShieldMpMember(ctypes.Structure):
     ]
 
 
+PHYS_FIELDS = (
+    "phii", "prsi", "prsik", "delz", "delp", "qvapor", "qliquid", "qrain", "qice", "qsnow", "qgraupel", "qo3mr",
+    "qsgs_tke", "pt", "dm", "delprsi", "del_gz", "phil", "omga", "dz", "wmp",
+) + MP_TENDENCY_FIELDS
+SHIELD_PHYS_PREPARE_MICROPHYSICS = 1
+
+
+class ShieldPhysicsFields(ctypes.Structure):
+    _fields_ = [(n, ShieldField3D) for n in PHYS_FIELDS]
+
+
 EXPORTS = (
     "shield_mp_create",
     "shield_mp_step",
@@ -141,6 +152,7 @@ EXPORTS = (
     "shield_mp_ensemble_destroy",
     "shield_mp_step_noalloc",
     "shield_mp_step_vjp",
+    "shield_physics_prestep",
 )
 
 _lib = None
@@ -187,6 +199,7 @@ def load():
     lib.shield_mp_step_noalloc.argtypes = [
         ctypes.POINTER(ShieldMpConfig), i32, i32, i32, ShieldField2D, ctypes.POINTER(ShieldMpFields), dbl, i32, i32, vp,
     ]
+    lib.shield_physics_prestep.argtypes = [i32, i32, i32, i32, i32, dbl, i32, ctypes.POINTER(ShieldPhysicsFields), vp]
     for name in EXPORTS:
         getattr(lib, name).restype = i32
     _lib = lib

@@ -29,6 +29,7 @@ UNITS = [
     ("mp_mixed.cu", []),
     ("coupling.cu", ["-fmad=false"]),
     ("mp_vjp.cu", ["-fmad=false"]),
+    ("physics.cu", ["-fmad=false"]),
 ]
 
 

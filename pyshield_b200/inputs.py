@@ -124,3 +124,65 @@ def make_state(ncol, nlev, seed=0, n_cube=None, ts_offset=0.0, sat_fraction=0.0)
 
 def copy_state(state):
     return {k: np.array(v, copy=True) for k, v in state.items()}
+
+
+PHYSICS_3D = (
+    "qvapor", "qliquid", "qice", "qrain", "qsnow", "qgraupel", "qo3mr", "qsgs_tke", "qcld", "pt", "delp", "delz",
+    "ua", "va", "w", "omga", "physics_updated_specific_humidity", "physics_updated_qliquid", "physics_updated_qice",
+    "physics_updated_qrain", "physics_updated_qsnow", "physics_updated_qgraupel", "physics_updated_cloud_fraction",
+    "physics_updated_pt", "physics_updated_ua", "physics_updated_va", "delprsi", "phii", "phil", "dz", "wmp", "prsi",
+    "prsik",
+)
+PHYSICS_INTERFACE = ("phii", "prsi", "prsik")
+
+
+def make_physics_state(nx, ny, nlev, seed=0, halo=3, sat_fraction=0.2):
+    """A ``PhysicsState``'s storages for the physics driver: a dict of
+    NDSL-layout arrays (nx + 2 halo + 1, ny + 2 halo + 1, nlev + 1) keyed by
+    the PhysicsState field names (``land`` 2-D), plus the ten tendencies of
+    ``physics_state.microphysics`` under their own names, and the (n,) cell
+    area.
+
+    The compute domain holds a ``make_state`` column set (``delp`` is its
+    pressure thickness). ``qo3mr ~ U(1e-8, 1e-5)``, ``qsgs_tke ~ U(0, 2)``,
+    ``w ~ U(-1, 1)``, ``omga ~ U(-2, 2) Pa/s``. The halo points and the extra
+    level hold plausible random values (the full-domain stencils read the
+    halo), interface pressure and geopotential there are monotone profiles,
+    and every output field and tendency starts from random values (the
+    steps overwrite what the reference overwrites)."""
+    rng = np.random.default_rng(seed)
+    h, L = halo, nlev
+    n = nx * ny
+    state, area = make_state(n, L, seed=seed, n_cube=nx, sat_fraction=sat_fraction)
+    shape = (nx + 2 * h + 1, ny + 2 * h + 1, L + 1)
+    ci, cj = slice(h, h + nx), slice(h, h + ny)
+
+    def put(arr_ln, lo, hi):
+        a = rng.uniform(lo, hi, shape)
+        if arr_ln is not None:
+            a[ci, cj, :L] = arr_ln.reshape(L, ny, nx).transpose(2, 1, 0)
+        return a
+
+    st = {}
+    for q in ("qvapor", "qliquid", "qice", "qrain", "qsnow", "qgraupel", "qcld"):
+        st[q] = put(state[q], 0.0, 1e-3)
+    st["qo3mr"] = put(None, 1e-8, 1e-5)
+    st["qsgs_tke"] = put(None, 0.0, 2.0)
+    st["pt"] = put(state["pt"], 200.0, 300.0)
+    st["delp"] = put(state["delprsi"], 100.0, 2000.0)
+    st["delz"] = put(state["delz"], -800.0, -50.0)
+    st["ua"] = put(state["ua"], -30.0, 30.0)
+    st["va"] = put(state["va"], -30.0, 30.0)
+    st["w"] = put(None, -1.0, 1.0)
+    st["omga"] = put(None, -2.0, 2.0)
+    for nm in PHYSICS_3D:
+        if nm.startswith("physics_updated") or nm in ("delprsi", "phil", "dz", "wmp", "prsik"):
+            st[nm] = put(None, -1.0, 1.0)
+    st["prsi"] = np.cumsum(rng.uniform(100.0, 2000.0, shape), axis=2) + PTOP
+    st["phii"] = np.cumsum(rng.uniform(100.0, 3000.0, shape)[..., ::-1], axis=2)[..., ::-1] - 100.0
+    land = np.zeros(shape[:2])
+    land[ci, cj] = state["land"].reshape(ny, nx).T
+    st["land"] = land
+    for t in TENDENCY_FIELDS:
+        st[t] = rng.uniform(-1.0, 1.0, shape)
+    return st, area

@@ -67,7 +67,11 @@ class _Ctx:
 
 
 class _Field:
-    """A 3-D (or 2-D) view of caller storage restricted to the compute domain."""
+    """A 3-D (or 2-D) view of caller storage restricted to the stencil's
+    horizontal domain. In k the view runs from the origin to the end of the
+    storage: GT4Py lets a stencil read levels above its domain (``[0, 0, 1]``
+    on the last level) when the storage has them; writes stay inside the
+    computation's interval."""
 
     def __init__(self, arr, origin, domain, is2d=False):
         self.is2d = is2d
@@ -77,7 +81,7 @@ class _Field:
             self.a = arr[
                 origin[0] : origin[0] + domain[0],
                 origin[1] : origin[1] + domain[1],
-                origin[2] : origin[2] + domain[2],
+                origin[2] :,
             ]
 
     def read(self, ctx, dk=0):

@@ -426,6 +426,70 @@ def run_coupling_chain(name, nx, ny, L, dt, seed):
     return meta
 
 
+def physics_cases():
+    """(name, nx, ny, L, dt, seed, config overrides)."""
+    return [
+        ("phys_default", 4, 3, 14, 150.0, 41, {}),
+        ("phys_substeps", 3, 4, 12, 225.0, 42, dict(mp_time=150.0, do_qa=True)),
+    ]
+
+
+def run_physics_case(name, nx, ny, L, dt, seed, overrides):
+    """pySHiELD's ``Physics.__call__`` (physics.py:276-366) end to end:
+    atmos_phys_driver_statein, get_prs_fv3, get_phi_fv3, prepare_microphysics,
+    the microphysics step and update_physics_state_with_tendencies, on a
+    ``PhysicsState`` of NDSL-layout storages (halo 3, nz + 1 levels) from
+    ``pyshield_b200.inputs.make_physics_state``."""
+    import pySHiELD
+    from ndsl.dsl.stencil import GridIndexing, StencilFactory
+    from ndsl.grid import GridData
+    from ndsl.initialization.allocator import QuantityFactory
+    from ndsl.quantity import Quantity
+    from pySHiELD.physics_state import PhysicsState
+    from pySHiELD.stencils.physics import Physics
+
+    from pyshield_b200.inputs import PHYSICS_3D, PHYSICS_INTERFACE, PTOP, make_physics_state
+
+    h = 3
+    st, area = make_physics_state(nx, ny, L, seed=seed, halo=h)
+    inputs = {k: v.copy() for k, v in st.items()}
+    cfg_kwargs = dict(dt_atmos=dt, npx=nx + 1, npy=ny + 1, npz=L)
+    cfg_kwargs.update(overrides)
+    ref_cfg = pySHiELD.PhysicsConfig(**cfg_kwargs)
+    gi = GridIndexing(nx, ny, L)
+    sf = StencilFactory(gi)
+    qf = QuantityFactory(nx, ny, L)
+    area_q = Quantity(to_storage2d(area, nx, ny), ["x", "y"], "m^2", origin=(h, h), extent=(nx, ny))
+    grid_data = GridData(area=area_q, ptop=PTOP)
+    phys = Physics(sf, qf, grid_data, ref_cfg)
+    quantities = {}
+    for nm in PHYSICS_3D:
+        dims = ["x", "y", "z_interface" if nm in PHYSICS_INTERFACE else "z"]
+        quantities[nm] = Quantity(st[nm], dims, "", origin=(h, h, 0), extent=(nx, ny, L + 1 if nm in PHYSICS_INTERFACE else L))
+    quantities["land"] = Quantity(st["land"], ["x", "y"], "", origin=(h, h), extent=(nx, ny))
+    ps = PhysicsState(**quantities, quantity_factory=qf, schemes=ref_cfg.schemes)
+    for t in MP_OUT:
+        getattr(ps.microphysics, t).data[...] = st[t]
+    phys(ps, dt)
+
+    out = {f"in_{k}": v for k, v in inputs.items()}
+    for nm in PHYSICS_3D:
+        out[f"out_{nm}"] = ps.__dict__[nm].data
+    for t in MP_OUT:
+        out[f"out_{t}"] = getattr(ps.microphysics, t).data
+    out["out__prsik"] = phys._prsik.data
+    out["out__dm3d"] = phys._dm3d.data
+    out["out__del_gz"] = phys._del_gz.data
+    mp = phys._microphysics
+    for p, attr in (("rain", "_rain"), ("snow", "_snow"), ("ice", "_ice"), ("graupel", "_graupel")):
+        out[f"out_{p}"] = from_storage(getattr(mp, attr).data, nx, ny, L)[0]
+    out["in_area"] = area
+    meta = {"name": name, "nx": nx, "ny": ny, "L": L, "dt": dt, "halo": h, "ptop": PTOP,
+            "config": {k: v for k, v in cfg_kwargs.items()}}
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), meta=json.dumps(meta), **out)
+    return meta
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("PYSHIELD_REFERENCE", "/root/reference"))
@@ -446,6 +510,11 @@ def main():
         if args.only and args.only != case[0]:
             continue
         meta = run_coupling_chain(*case)
+        print("wrote", meta["name"])
+    for case in physics_cases():
+        if args.only and args.only != case[0]:
+            continue
+        meta = run_physics_case(*case)
         print("wrote", meta["name"])
 
 

@@ -7,7 +7,7 @@ executor; see tests/golden/make_golden.py.
 import numpy as np
 import pytest
 
-from golden_io import CPL_CASES, MP_CASES, MP_TENDENCIES, PRECIP, load, mp_inputs
+from golden_io import CPL_CASES, MP_CASES, MP_TENDENCIES, PHYS_CASES, PRECIP, load, mp_inputs, physics_inputs
 from oracle import coupling as OC
 from oracle.microphysics import OracleMicrophysics
 from pyshield_b200 import constants as C
@@ -113,3 +113,24 @@ def test_update_atmos_state_chain_bitexact():
     np.testing.assert_array_equal(ps, z["out_ps"][cd])
     np.testing.assert_array_equal(us, z["out_u_srf"][cd])
     np.testing.assert_array_equal(vs, z["out_v_srf"][cd])
+
+
+@pytest.mark.parametrize("name", PHYS_CASES)
+def test_physics_call_bitexact(name):
+    """Physics.__call__: the driver pre-steps on the compute and full
+    domains, the microphysics step and the state update."""
+    from oracle.physics import OraclePhysics
+
+    z, m = load(name)
+    cfg = PhysicsConfig(**{k: v for k, v in m["config"].items() if k in PhysicsConfig.__dataclass_fields__})
+    st, area = physics_inputs(z)
+    ph = OraclePhysics(cfg, m["nx"], m["ny"], m["L"], area, m["ptop"], m["halo"])
+    precip = ph(st, m["dt"])
+    for k in [f[4:] for f in z.files if f.startswith("out_")]:
+        if k.startswith("_"):
+            got = {"_prsik": ph.prsik, "_dm3d": ph.dm3d, "_del_gz": ph.del_gz}[k]
+        elif k in PRECIP:
+            got = precip[k]
+        else:
+            got = st[k]
+        np.testing.assert_array_equal(got, z["out_" + k], err_msg=f"{name} {k}")

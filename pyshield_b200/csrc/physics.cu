@@ -1,5 +1,5 @@
 // Physics driver pre-steps of pySHiELD's Physics.__call__ (compiled with
-// -fmad=false), fused into one column-per-thread kernel:
+// -fmad=false), fused into one kernel:
 //
 //  * atmos_phys_driver_statein  pySHiELD/stencils/physics.py:26-102
 //                               (compute domain, nz + 1 levels)
@@ -11,16 +11,10 @@
 //                               (compute domain, nz levels)
 //
 // The reference runs them as four stencils over HBM in this order
-// (physics.py:276-330). Here one thread owns one column of the full domain
-// and runs the column's part of each in three sweeps: a bottom-up sweep
-// for statein's interface geopotential, a top-down sweep for the
-// tracer/pressure conversion, statein's thickness and get_prs_fv3 (every
-// level of these needs only the running interface pressure and the two
-// geopotentials around it), and a bottom-up sweep for get_phi_fv3 and
-// prepare_microphysics. Halo columns run the get_prs_fv3 / get_phi_fv3
-// part only, as the reference's full-domain stencils do. Consecutive
-// threads own consecutive i, so every level's loads and stores are
-// coalesced in the i-fastest GT4Py layout.
+// (physics.py:276-330). Here one block owns a tile of columns of the full
+// domain and runs each column's part of all four (the layout of the work is
+// described at the kernel). Halo columns run the get_prs_fv3 / get_phi_fv3
+// part only, as the reference's full-domain stencils do.
 //
 // Each statement keeps the reference's operand order; the running sums
 // (interface geopotential and pressure) are summed level by level in the
@@ -74,163 +68,169 @@ struct PhysArgs {
 __device__ __forceinline__ double np_max(double a, double b) { return a >= b ? a : b; }
 __device__ __forceinline__ double np_min(double a, double b) { return a <= b ? a : b; }
 
-// Levels handled per batch of the sweeps: their loads are all issued before
-// any of their results is stored, so they are in flight together (the
-// stores could alias the loads as far as the compiler knows, which would
-// otherwise serialise a level's loads behind the previous level's stores).
-constexpr int U1 = 8;  // bottom-up geopotential sweep (one load per level)
-constexpr int U2 = 2;  // top-down sweep (eleven loads per level)
-constexpr int U3 = 8;  // bottom-up get_phi_fv3 sweep (one load per level)
+// One block owns a tile of TC = 32 consecutive columns of the full domain
+// (lane = column, so every level's loads and stores are coalesced in the
+// i-fastest layout) and NWB warps that share its levels. The pointwise work
+// runs level-parallel; the two running sums of each stencil pass (statein's
+// interface geopotential and pressure, get_phi_fv3's geopotential) run in
+// one warp, level by level in the reference's order, over shared-memory
+// columns:
+//   A  (all warps)  statein's pointwise prelude: delz * GRAV and the
+//                   condensate-free thickness dpn of every level into shared
+//                   memory (halo columns: their prsi and phii);
+//   B  (two warps)  the sums: phii bottom up, prsi top down;
+//   C  (all warps)  the rest of statein, get_prs_fv3, the first statement of
+//                   get_phi_fv3 and the pointwise part of
+//                   prepare_microphysics; del_gz into shared memory;
+//   D  (one warp)   get_phi_fv3's bottom-up sum, phil, phii, and
+//                   prepare_microphysics' dz.
+constexpr int TC = 32;
+constexpr int NWB = 8;
 
-__global__ void __launch_bounds__(64) physics_prestep_kernel(const __grid_constant__ PhysArgs A) {
+template <int NKMAX>
+struct PreSmem {
+  double ph[NKMAX][TC];  // phase A: delz * GRAV; B: statein's phii
+  double p[NKMAX][TC];   // phase A: dpn of the level above; B: prsi
+  double gz[NKMAX][TC];  // phase C: get_phi_fv3's del_gz
+};
+
+template <int NKMAX>
+__global__ void __launch_bounds__(TC * NWB) physics_prestep_kernel(const __grid_constant__ PhysArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  PreSmem<NKMAX>& S = *reinterpret_cast<PreSmem<NKMAX>*>(smem_raw);
   const int nxf = A.nx + 2 * A.hx, nyf = A.ny + 2 * A.hx;
   const int64_t ncf = (int64_t)nxf * nyf;
   const int nk = A.nz + 1;
   const F3* f = A.f;
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncf; c += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = c % nxf - A.hx, j = c / nxf - A.hx;
-    const bool compute = i >= 0 && j >= 0 && i < A.nx && j < A.ny;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t c = (int64_t)blockIdx.x * TC + lane;
+  const bool live = c < ncf;
+  const int64_t i = live ? c % nxf - A.hx : 0, j = live ? c / nxf - A.hx : 0;
+  const bool compute = live && i >= 0 && j >= 0 && i < A.nx && j < A.ny;
+  const bool halo = live && !compute;
+
+  // ---- A: statein's prelude (PARALLEL interval(...)): tracers * delp, dpn
+  for (int k = w; k < nk; k += NWB) {
     if (compute) {
-      // ---- statein, BACKWARD: phii = 0, then phii[k] = phii[k + 1] - delz * GRAV
-      double ph = 0.0;
-      f[PHII].at(i, j, nk - 1) = ph;
-      for (int k0 = nk - 2; k0 >= 0; k0 -= U1) {
-        double dz[U1];
+      if (k < nk - 1) S.ph[k][lane] = f[DELZ].at(i, j, k) * A.GRAV;
+      const double dp0 = f[DELP].at(i, j, k);
+      double q[N_TRACER];
 #pragma unroll
-        for (int u = 0; u < U1; ++u) dz[u] = k0 - u >= 0 ? f[DELZ].at(i, j, k0 - u) : 0.0;
-#pragma unroll
-        for (int u = 0; u < U1; ++u) {
-          if (k0 - u < 0) break;
-          ph = ph - dz[u] * A.GRAV;
-          f[PHII].at(i, j, k0 - u) = ph;
-        }
-      }
-      // ---- statein (tracers, pressure, thickness), get_prs_fv3, the first
-      // statement of get_phi_fv3 and prepare_microphysics' pointwise part,
-      // top down; levels 0 .. nk - 2 here, the extra level nk - 1 after
-      double p = A.ptop;  // prsi[k]
-      f[PRSI].at(i, j, 0) = p;
-      double ph_k = f[PHII].at(i, j, 0);
-      for (int k0 = 0; k0 < nk - 1; k0 += U2) {
-        double dp0[U2], q[U2][N_TRACER], tke[U2], pt[U2], ph1[U2], om[U2];
-#pragma unroll
-        for (int u = 0; u < U2; ++u) {
-          const int k = k0 + u < nk - 1 ? k0 + u : nk - 2;  // a repeated level is loaded but not used
-          dp0[u] = f[DELP].at(i, j, k);
-#pragma unroll
-          for (int t = 0; t < N_TRACER; ++t) q[u][t] = f[QV + t].at(i, j, k);
-          tke[u] = f[TKE].at(i, j, k);
-          pt[u] = f[PT].at(i, j, k);
-          ph1[u] = f[PHII].at(i, j, k + 1);
-          om[u] = A.prepare ? f[OMGA].at(i, j, k) : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < U2; ++u) {
-          const int k = k0 + u;
-          if (k >= nk - 1) break;
-#pragma unroll
-          for (int t = 0; t < N_TRACER; ++t) q[u][t] = q[u][t] * dp0[u];
-          // q[u][1..5]: ql qr qi qs qg (the argument order qliquid, qrain, qice, qsnow, qgraupel)
-          const double dpn =
-              A.nwat == 6 ? dp0[u] - q[u][1] - q[u][2] - q[u][3] - q[u][4] - q[u][5] : dp0[u];
-          const double pn = p + dpn;  // prsi[k + 1]
-          f[PRSI].at(i, j, k + 1) = pn;
-          f[PRSIK].at(i, j, k) = k == 0 ? A.pktop : log(p);
-#pragma unroll
-          for (int t = 0; t < N_TRACER; ++t) q[u][t] = q[u][t] / dpn;
-#pragma unroll
-          for (int t = 0; t < N_TRACER; ++t) f[QV + t].at(i, j, k) = q[u][t];
-          f[TKE].at(i, j, k) = tke[u] / dpn;
-          const double qgrs_rad = np_max(1.0e-10, q[u][0]);
-          const double rTv = A.RDGAS * pt[u] * (1.0 + A.ZVIR * qgrs_rad);
-          const double dm = dpn;
-          f[DM].at(i, j, k) = dm;
-          double d = dm * rTv / (ph_k - ph1[u]);
-          d = np_min(d, pn - 0.01 * dm);
-          d = np_max(d, p + 0.01 * dm);
-          f[DELP].at(i, j, k) = d;
-          // get_prs_fv3, then get_phi_fv3's first statement (PARALLEL interval(0, -1))
-          f[DELPRSI].at(i, j, k) = pn - p;
-          const double tv = 1.0 + A.ZVIR * np_max(0.0, q[u][0]);
-          const double gz = (ph_k - ph1[u]) / (pt[u] * tv);
-          f[DELGZ].at(i, j, k) = gz * pt[u] * tv;
-          if (A.prepare) {
-            // prepare_microphysics: wmp and the zeroed tendencies (pointwise;
-            // dz needs get_phi_fv3's geopotential and follows below)
-            f[WMP].at(i, j, k) = -om[u] * (1.0 + A.ZVIR * q[u][0]) * pt[u] / d * A.RDGAS_RGRAV;
-#pragma unroll
-            for (int t = 0; t < 10; ++t)
-              if (f[TEND0 + t].p) f[TEND0 + t].at(i, j, k) = 0.0;
-          }
-          p = pn;
-          ph_k = ph1[u];
-        }
-      }
-      {
+      for (int t = 0; t < N_TRACER; ++t) q[t] = f[QV + t].at(i, j, k) * dp0;
+      // q[1..5]: ql qr qi qs qg (the argument order qliquid, qrain, qice, qsnow, qgraupel)
+      const double dpn = A.nwat == 6 ? dp0 - q[1] - q[2] - q[3] - q[4] - q[5] : dp0;
+      if (k < nk - 1) {
+        S.p[k + 1][lane] = dpn;
+      } else {
         // the extra level: mass-weighted tracers and thickness, no division
-        const int k = nk - 1;
-        const double dp0 = f[DELP].at(i, j, k);
-        double q[N_TRACER];
-#pragma unroll
-        for (int t = 0; t < N_TRACER; ++t) q[t] = f[QV + t].at(i, j, k) * dp0;
-        const double dpn = A.nwat == 6 ? dp0 - q[1] - q[2] - q[3] - q[4] - q[5] : dp0;
 #pragma unroll
         for (int t = 0; t < N_TRACER; ++t) f[QV + t].at(i, j, k) = q[t];
         f[DELP].at(i, j, k) = dpn;
-        f[PRSIK].at(i, j, k) = exp(A.KAPPA * log(p)) * A.pk0inv;
       }
-    } else {
-      // ---- halo column: get_prs_fv3 and get_phi_fv3's first statement
-      double p = f[PRSI].at(i, j, 0);
-      double ph_k = f[PHII].at(i, j, 0);
-      for (int k0 = 0; k0 < nk - 1; k0 += U2) {
-        double pn[U2], ph1[U2], pt[U2], qv[U2];
-#pragma unroll
-        for (int u = 0; u < U2; ++u) {
-          const int k = k0 + u < nk - 1 ? k0 + u : nk - 2;
-          pn[u] = f[PRSI].at(i, j, k + 1);
-          ph1[u] = f[PHII].at(i, j, k + 1);
-          pt[u] = f[PT].at(i, j, k);
-          qv[u] = f[QV].at(i, j, k);
-        }
-#pragma unroll
-        for (int u = 0; u < U2; ++u) {
-          const int k = k0 + u;
-          if (k >= nk - 1) break;
-          const double tv = 1.0 + A.ZVIR * np_max(0.0, qv[u]);
-          f[DELPRSI].at(i, j, k) = pn[u] - p;
-          const double gz = (ph_k - ph1[u]) / (pt[u] * tv);
-          f[DELGZ].at(i, j, k) = gz * pt[u] * tv;
-          p = pn[u];
-          ph_k = ph1[u];
-        }
-      }
+    } else if (halo) {
+      S.p[k][lane] = f[PRSI].at(i, j, k);
+      S.ph[k][lane] = f[PHII].at(i, j, k);
     }
-    // ---- get_phi_fv3, BACKWARD, and prepare_microphysics' dz on the compute domain
+  }
+  __syncthreads();
+  // ---- B: statein's running sums, in the reference's order (two warps)
+  if (w == 0 && compute) {
+    double ph = 0.0;
+    S.ph[nk - 1][lane] = ph;
+    for (int k = nk - 2; k >= 0; --k) {  // BACKWARD: phii[k] = phii[k + 1] - delz * GRAV
+      ph = ph - S.ph[k][lane];
+      S.ph[k][lane] = ph;
+    }
+  } else if (w == 1 && compute) {
+    double p = A.ptop;  // FORWARD: prsi[k] = prsi[k - 1] + delp[k - 1]
+    S.p[0][lane] = p;
+    for (int k = 1; k < nk; ++k) {
+      p = p + S.p[k][lane];
+      S.p[k][lane] = p;
+    }
+  }
+  __syncthreads();
+  // ---- C: statein, get_prs_fv3, get_phi_fv3's first statement, prepare_microphysics' pointwise part
+  for (int k = w; k < nk; k += NWB) {
+    if (compute) {
+      const double p = S.p[k][lane];
+      f[PRSI].at(i, j, k) = p;
+      if (k == nk - 1) {
+        f[PRSIK].at(i, j, k) = exp(A.KAPPA * log(p)) * A.pk0inv;
+        continue;
+      }
+      const double pn = S.p[k + 1][lane];
+      const double ph_k = S.ph[k][lane], ph1 = S.ph[k + 1][lane];
+      const double dp0 = f[DELP].at(i, j, k);
+      double q[N_TRACER];
+#pragma unroll
+      for (int t = 0; t < N_TRACER; ++t) q[t] = f[QV + t].at(i, j, k) * dp0;
+      const double dpn = A.nwat == 6 ? dp0 - q[1] - q[2] - q[3] - q[4] - q[5] : dp0;
+      const double tke = f[TKE].at(i, j, k);
+      const double pt = f[PT].at(i, j, k);
+      const double om = A.prepare ? f[OMGA].at(i, j, k) : 0.0;
+      f[PRSIK].at(i, j, k) = k == 0 ? A.pktop : log(p);
+#pragma unroll
+      for (int t = 0; t < N_TRACER; ++t) q[t] = q[t] / dpn;
+#pragma unroll
+      for (int t = 0; t < N_TRACER; ++t) f[QV + t].at(i, j, k) = q[t];
+      f[TKE].at(i, j, k) = tke / dpn;
+      const double qv = q[0];
+      const double qgrs_rad = np_max(1.0e-10, qv);
+      const double rTv = A.RDGAS * pt * (1.0 + A.ZVIR * qgrs_rad);
+      const double dm = dpn;
+      f[DM].at(i, j, k) = dm;
+      double d = dm * rTv / (ph_k - ph1);
+      d = np_min(d, pn - 0.01 * dm);
+      d = np_max(d, p + 0.01 * dm);
+      f[DELP].at(i, j, k) = d;
+      f[DELPRSI].at(i, j, k) = pn - p;
+      const double tv = 1.0 + A.ZVIR * np_max(0.0, qv);
+      const double gz = (ph_k - ph1) / (pt * tv);
+      S.gz[k][lane] = gz * pt * tv;
+      if (A.prepare) {
+        f[WMP].at(i, j, k) = -om * (1.0 + A.ZVIR * qv) * pt / d * A.RDGAS_RGRAV;
+#pragma unroll
+        for (int t = 0; t < 10; ++t)
+          if (f[TEND0 + t].p) f[TEND0 + t].at(i, j, k) = 0.0;
+      }
+    } else if (halo && k < nk - 1) {
+      const double p = S.p[k][lane], pn = S.p[k + 1][lane];
+      const double ph_k = S.ph[k][lane], ph1 = S.ph[k + 1][lane];
+      const double pt = f[PT].at(i, j, k);
+      const double tv = 1.0 + A.ZVIR * np_max(0.0, f[QV].at(i, j, k));
+      f[DELPRSI].at(i, j, k) = pn - p;
+      const double gz = (ph_k - ph1) / (pt * tv);
+      S.gz[k][lane] = gz * pt * tv;
+    }
+  }
+  __syncthreads();
+  // ---- D: get_phi_fv3, BACKWARD, and prepare_microphysics' dz
+  if (w == 0 && live) {
+    const bool prep = compute && A.prepare;
     double ph = 0.0;
     f[PHII].at(i, j, nk - 1) = ph;
-    const bool prep = compute && A.prepare;
-    for (int k0 = nk - 2; k0 >= 0; k0 -= U3) {
-      double g[U3];
-#pragma unroll
-      for (int u = 0; u < U3; ++u) g[u] = k0 - u >= 0 ? f[DELGZ].at(i, j, k0 - u) : 0.0;
-#pragma unroll
-      for (int u = 0; u < U3; ++u) {
-        const int k = k0 - u;
-        if (k < 0) break;
-        f[PHIL].at(i, j, k) = 0.5 * (ph + ph + g[u]);
-        const double phn = ph + g[u];
-        f[PHII].at(i, j, k) = phn;
-        if (prep) f[DZ].at(i, j, k) = (ph - phn) * A.RGRAV;
-        ph = phn;
-      }
+    for (int k = nk - 2; k >= 0; --k) {
+      const double g = S.gz[k][lane];
+      f[DELGZ].at(i, j, k) = g;
+      f[PHIL].at(i, j, k) = 0.5 * (ph + ph + g);
+      const double phn = ph + g;
+      f[PHII].at(i, j, k) = phn;
+      if (prep) f[DZ].at(i, j, k) = (ph - phn) * A.RGRAV;
+      ph = phn;
     }
   }
 }
 
-int grid_for(int64_t n, int bs) {
-  int64_t nb = (n + bs - 1) / bs;
-  return (int)(nb < 148 * 32 ? (nb > 0 ? nb : 1) : 148 * 32);
+template <int NKMAX>
+cudaError_t launch_prestep(const PhysArgs& A, int64_t ncf, cudaStream_t st) {
+  const size_t smem = sizeof(PreSmem<NKMAX>);
+  auto kern = physics_prestep_kernel<NKMAX>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int64_t nblk = (ncf + TC - 1) / TC;
+  kern<<<(unsigned)nblk, TC * NWB, smem, st>>>(A);
+  return cudaGetLastError();
 }
 
 }  // namespace
@@ -240,6 +240,10 @@ extern "C" int shield_physics_prestep(int nx, int ny, int nz, int hx, int nwat, 
   if (!fields || nx < 1 || ny < 1 || nz < 2 || hx < 0 || !(ptop > 0.0)) {
     shield::set_last_error("shield_physics_prestep: bad arguments");
     return SHIELD_EINVAL;
+  }
+  if (nz > 128) {
+    shield::set_last_error("shield_physics_prestep: nz > 128 is not supported");
+    return SHIELD_ELAYOUT;
   }
   const bool prepare = (flags & SHIELD_PHYS_PREPARE_MICROPHYSICS) != 0;
   const ShieldField3D* in = reinterpret_cast<const ShieldField3D*>(fields);
@@ -272,8 +276,9 @@ extern "C" int shield_physics_prestep(int nx, int ny, int nz, int hx, int nwat, 
   A.pktop = std::pow(ptop / p00, A.KAPPA);
   A.pk0inv = std::pow(1.0 / p00, A.KAPPA);
   const int64_t ncf = (int64_t)(nx + 2 * hx) * (ny + 2 * hx);
-  physics_prestep_kernel<<<grid_for(ncf, 64), 64, 0, static_cast<cudaStream_t>(stream)>>>(A);
-  cudaError_t e = cudaGetLastError();
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int nk = nz + 1;
+  cudaError_t e = nk <= 96 ? launch_prestep<96>(A, ncf, st) : launch_prestep<129>(A, ncf, st);
   if (e != cudaSuccess) {
     shield::set_last_error(std::string("shield_physics_prestep: ") + cudaGetErrorString(e));
     return SHIELD_ECUDA;

@@ -881,18 +881,19 @@ SHD void icloud(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid,
 // One block's work: columns c0 .. c0 + G - 1 of the domain described by A.
 // MIXED selects the mixed-precision process rates (mp_physics_mixed.cuh);
 // everything else is shared by both forms.
+// The step of columns c0 .. c0 + G - 1 between staging in and staging out:
+// inputs are read from, and outputs written to, the tiles at `sm` (field f
+// of block column g at level k at (f * G + g) * RP + k); `scr` and `work`
+// are the column groups' scratch (G x 2 x SCR doubles) and work rows
+// (G x 2 x RP doubles).
 template <int NW, int G, bool MIXED>
-SHD void mp_block(const MpArgs& A, double* sm, const int64_t c0) {
-  using SM = Smem<NW, G>;
+SHD void mp_body(const MpArgs& A, double* sm, double* scr, double* work, const int64_t c0) {
   constexpr int RP = Tiles<NW>::RP;
   const MpConst& K = A.K;
   const MpConstF& KF = A.KF;
   const int L = A.nz;
   const int tid = threadIdx.x;
   const int g = tid / (32 * NW);
-
-  stage_in<NW, G>(A, sm, c0);
-  __syncthreads();
 
   const int64_t col = c0 + g;
   Column<NW> C;
@@ -901,8 +902,8 @@ SHD void mp_block(const MpArgs& A, double* sm, const int64_t c0) {
   C.k = 32 * C.w + C.lane;
   C.L = L;
   C.bar = 1 + g;
-  C.scr = sm + SM::scratch + (size_t)g * 2 * Tiles<NW>::SCR;
-  C.work = sm + SM::work + (size_t)g * 2 * RP;
+  C.scr = scr + (size_t)g * 2 * Tiles<NW>::SCR;
+  C.work = work + (size_t)g * 2 * RP;
   C.par = 0;
   const int k = C.k;
   const bool valid = k < L;
@@ -1007,9 +1008,149 @@ SHD void mp_block(const MpArgs& A, double* sm, const int64_t c0) {
       if (A.graupel) A.graupel[col] = graupel * convt;
     }
   }
+}
+
+// One block's work: columns c0 .. c0 + G - 1 of the domain described by A.
+// MIXED selects the mixed-precision process rates (mp_physics_mixed.cuh);
+// everything else is shared by both forms.
+template <int NW, int G, bool MIXED>
+SHD void mp_block(const MpArgs& A, double* sm, const int64_t c0) {
+  using SM = Smem<NW, G>;
+  stage_in<NW, G>(A, sm, c0);
+  __syncthreads();
+  mp_body<NW, G, MIXED>(A, sm, sm + SM::scratch, sm + SM::work, c0);
   __syncthreads();
   stage_out<NW, G>(A, sm, c0);
 }
+
+// ------------------------------------------------- persistent, double-buffered
+// The same step with the staging taken off the critical path: a persistent
+// block walks its share of the column blocks and, while it computes one,
+// copies the next one's inputs -- the 14 fields and the 10 old tendencies
+// the step adds to -- into the other buffer with cp.async, so that the only
+// memory work left between two blocks is issuing the stores.
+//
+// Shared memory: two buffers of N_TILE rows per block column, then the
+// scratch and work rows.
+constexpr int N_TILE = N_IN + 10;  // the inputs, then the tendencies read before the update
+
+template <int NW, int G>
+struct SmemP {
+  static constexpr int RP = Tiles<NW>::RP;
+  static constexpr size_t buf = (size_t)N_TILE * G * RP;
+  static constexpr size_t scratch = 2 * buf;
+  static constexpr size_t work = scratch + (size_t)G * 2 * Tiles<NW>::SCR;
+  static constexpr size_t total = work + (size_t)G * 2 * RP;
+  static constexpr size_t bytes = total * sizeof(double);
+};
+
+SHD void cp_async8(double* dst_smem, const double* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+SHD void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+SHD void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Tile row of the old value of tendency o (o < 10), after the inputs.
+SHD int tend_row(int o) { return N_IN + o; }
+
+template <int NW, int G>
+SHD const Fld3& tile_src(const MpArgs& A, int r) {
+  return r < N_IN ? A.in[r] : A.out[r - N_IN];
+}
+
+// stage_in's mapping, each element copied asynchronously (no register pass).
+template <int NW, int G>
+SHD void stage_in_async(const MpArgs& A, double* sm, int64_t c0) {
+  constexpr int RP = Tiles<NW>::RP;
+  const MpConst& K = A.K;
+  const int L = A.nz;
+  const int tid = threadIdx.x;
+  const int g = tid % G;
+  const int k = tid / G;
+  const int64_t col = c0 + g;
+  const bool ok = col < A.ncol && k < L;
+  const int64_t i = (col < A.ncol) ? col % A.nx : 0, j = (col < A.ncol) ? col / A.nx : 0;
+  const int gk = tid / (32 * NW), kk = tid % (32 * NW);
+  const int64_t colk = c0 + gk;
+  const bool okk = colk < A.ncol && kk < L;
+  const int64_t ik = (colk < A.ncol) ? colk % A.nx : 0, jk = (colk < A.ncol) ? colk / A.nx : 0;
+#pragma unroll
+  for (int r = 0; r < N_TILE; ++r) {
+    if (r >= N_IN) {
+      // a tendency the update adds to (stage_out's OM_ADD / OM_ADD_K1 fields)
+      const int o = r - N_IN;
+      if ((o == OUT_UDT || o == OUT_VDT) && !K.sedi_transport) continue;
+      if (o == OUT_QA_DT && K.do_qa) continue;
+    }
+    const Fld3& F = tile_src<NW, G>(A, r);
+    if (F.sk == 1) {
+      if (okk) cp_async8(&sm[(r * G + gk) * RP + kk], F.p + ik * F.si + jk * F.sj + kk);
+    } else if (ok) {
+      cp_async8(&sm[(r * G + g) * RP + k], F.p + i * F.si + j * F.sj + (int64_t)k * F.sk);
+    }
+  }
+}
+
+// stage_out with the old tendencies taken from the tile.
+template <int NW, int G>
+SHD void stage_out_tiled(const MpArgs& A, const double* sm, int64_t c0) {
+  constexpr int RP = Tiles<NW>::RP;
+  const MpConst& K = A.K;
+  const int L = A.nz;
+  const int tid = threadIdx.x;
+  const int g = tid % G;
+  const int k = tid / G;
+  const int64_t col = c0 + g;
+  const bool ok = col < A.ncol && k < L;
+  const int64_t i = (col < A.ncol) ? col % A.nx : 0, j = (col < A.ncol) ? col / A.nx : 0;
+  const int gk = tid / (32 * NW), kk = tid % (32 * NW);
+  const int64_t colk = c0 + gk;
+  const bool okk = colk < A.ncol && kk < L;
+  const int64_t ik = (colk < A.ncol) ? colk % A.nx : 0, jk = (colk < A.ncol) ? colk / A.nx : 0;
+#pragma unroll
+  for (int o = 0; o < N_OUT; ++o) {
+    int m = OM_ADD;
+    if (o == OUT_UDT || o == OUT_VDT) m = K.sedi_transport ? OM_ADD_K1 : OM_SKIP;
+    if (o == OUT_QA_DT && K.do_qa) m = OM_SET;
+    if (o == OUT_W) m = K.do_sedi_w ? OM_SET : OM_SKIP;
+    if (o == OUT_QAZ) m = OM_SET;
+    const Fld3 F = A.out[o];
+    const bool kf = F.sk == 1;
+    const int lev = kf ? kk : k;
+    if (!(kf ? okk : ok) || (m == OM_ADD_K1 && lev < 1)) m = OM_SKIP;
+    if (m == OM_SKIP) continue;
+    const int gg = kf ? gk : g;
+    const double v = sm[(o * G + gg) * RP + lev];
+    double* dst = kf ? F.p + ik * F.si + jk * F.sj + kk : F.p + i * F.si + j * F.sj + (int64_t)k * F.sk;
+    *dst = (m == OM_SET) ? v : sm[(tend_row(o) * G + gg) * RP + lev] + v;
+  }
+}
+
+template <int NW, int G, int MINB, bool MIXED>
+__global__ void __launch_bounds__(32 * NW * G, MINB)
+    mp_step_persistent_kernel(const __grid_constant__ MpArgs A, const int64_t nblk) {
+  extern __shared__ double sm[];
+  using SP = SmemP<NW, G>;
+  double* const scr = sm + SP::scratch;
+  double* const work = sm + SP::work;
+  int64_t b = blockIdx.x;
+  if (b < nblk) stage_in_async<NW, G>(A, sm, b * G);
+  cp_async_commit();
+  for (int it = 0; b < nblk; b += gridDim.x, ++it) {
+    double* const cur = sm + (it & 1) * SP::buf;
+    double* const nxt = sm + ((it + 1) & 1) * SP::buf;
+    cp_async_wait_all();
+    __syncthreads();  // this block's inputs have landed; the previous one's stage-out is done with nxt
+    if (b + gridDim.x < nblk) stage_in_async<NW, G>(A, nxt, (b + gridDim.x) * G);
+    cp_async_commit();
+    mp_body<NW, G, MIXED>(A, cur, scr, work, b * G);
+    __syncthreads();
+    stage_out_tiled<NW, G>(A, cur, b * G);
+  }
+  cp_async_wait_all();
+}
+
 
 template <int NW, int G, int MINB, bool MIXED>
 __global__ void __launch_bounds__(32 * NW * G, MINB) mp_step_kernel(const __grid_constant__ MpArgs A) {
@@ -1053,6 +1194,40 @@ __global__ void __launch_bounds__(32 * NW * G, MINB)
     __syncthreads();
     mp_block<NW, G, MIXED>(sargs, sm, (wi - offs[m]) * G);
   }
+}
+
+// Launch the step over ceil(ncol / G) column blocks. PERSIST: as many
+// persistent, double-buffered blocks as fit on the device at once, each
+// walking every gridDim.x-th column block; else one block per column block,
+// scheduled by the hardware. Measured at C96 L79 (ms per step):
+//   plain FP64  one block per column block 5.65, persistent 6.00
+//   mixed       one block per column block 4.47, persistent 4.29
+// so the mixed form runs persistent and the plain form does not.
+template <int NW, int G, int MINB, bool MIXED, bool PERSIST>
+cudaError_t launch_step(const MpArgs& A, cudaStream_t st) {
+  const int64_t nblk = (A.ncol + G - 1) / G;
+  const int threads = 32 * NW * G;
+  if (PERSIST) {
+    auto kern = mp_step_persistent_kernel<NW, G, MINB, MIXED>;
+    const size_t smem = SmemP<NW, G>::bytes;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, nsm = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem)) != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    const int64_t resident = (int64_t)nsm * per_sm;
+    const int64_t grid = nblk < resident ? nblk : resident;
+    kern<<<(unsigned)grid, threads, smem, st>>>(A, nblk);
+    return cudaGetLastError();
+  }
+  auto kern = mp_step_kernel<NW, G, MINB, MIXED>;
+  const size_t smem = Smem<NW, G>::bytes;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<(unsigned)nblk, threads, smem, st>>>(A);
+  return cudaGetLastError();
 }
 
 }  // namespace shield

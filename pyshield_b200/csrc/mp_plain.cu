@@ -33,13 +33,7 @@ namespace {
 
 template <int NW, int G, int MINB>
 cudaError_t launch_nw(const MpArgs& A, cudaStream_t st) {
-  const size_t smem = Smem<NW, G>::bytes;
-  auto kern = mp_step_kernel<NW, G, MINB, false>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  const int64_t nblk = (A.ncol + G - 1) / G;
-  kern<<<(unsigned)nblk, 32 * NW * G, smem, st>>>(A);
-  return cudaGetLastError();
+  return launch_step<NW, G, MINB, false, false>(A, st);
 }
 
 __global__ void gather2d(const double* p, int64_t si, int64_t sj, int nx, int64_t n, double* out) {

@@ -873,7 +873,11 @@ SHD void icloud(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid,
     else
       icloud_processes(K, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac, vtg, vtr, vts, P.p1, di, q_liq, q_sol, cvm);
     if (rec) *rec = S;
-    subgrid_z_proc(K, P.h_var, P.rh_adj, P.rh_rain, qa, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac, P.p1);
+    if constexpr (MIXED)
+      subgrid_z_proc<double, float>(K, P.h_var, P.rh_adj, P.rh_rain, qa, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac,
+                                    P.p1);
+    else
+      subgrid_z_proc(K, P.h_var, P.rh_adj, P.rh_rain, qa, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac, P.p1);
   }
 }
 

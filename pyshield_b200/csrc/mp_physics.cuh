@@ -266,8 +266,25 @@ SHP void autoconv_subgrid_var(const MpConst& K, T& qlz, T& qrz, T tz, T den, T c
   }
 }
 
+// exp / log in the rate type R of subgrid_z_proc: the FP64 wrappers (and the
+// dual-number overloads found by argument-dependent lookup) by default,
+// single precision for R = float
+template <typename R>
+SHP R rexp(R x) { return xexp(x); }
+template <typename R>
+SHP R rlog(R x) { return xlog(x); }
+template <>
+SHP float rexp<float>(float x) { return expf(x); }
+template <>
+SHP float rlog<float>(float x) { return logf(x); }
+SHP float sq(float x) { return x * x; }
+
 // ---------------------------------------------------- microphysics_funcs.py:431-850
-template <typename T>
+// R is the type of the deposition/sublimation and Bigg-freezing rate
+// expressions (T for the FP64 step; float for the mixed form). Every
+// saturation humidity, latent-heat temperature step and state update stays
+// in T.
+template <typename T, typename R = T>
 SHP void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh_rain, T& qaz, T& qgz, T& qiz,
                         T& qlz, T& qrz, T& qsz, T& qvz, T& tz, T den, T denfac, T p1) {
   const T tice = K.tice, t_wfr = K.t_wfr, t_sub = K.t_sub;
@@ -350,7 +367,7 @@ SHP void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
     dt_pisub = K.dts;
     T tc = tice - tz;
     if ((qlz > QRMIN) && (tc > 0.0)) {
-      T sink = 3.3333e-10 * K.dts * (xexp(0.66 * tc) - 1.0) * den * qlz * qlz;
+      T sink = T(R(3.3333e-10) * R(K.dts) * (rexp(R(0.66) * R(tc)) - R(1.0)) * R(den) * R(qlz) * R(qlz));
       sink = fmin(qlz, fmin(tc / icpk, sink));
       qlz = qlz - sink;
       qiz = qiz + sink;
@@ -373,8 +390,8 @@ SHP void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
     T sink = dq / (1.0 + tcpk * dqsdt);
     T pidep;
     if (qiz > QRMIN) {
-      pidep = dt_pisub * dq * 349138.78 * xexp(0.875 * xlog(qiz * den)) /
-              (qsi * den * K.LAT2 / (0.0243 * K.RVGAS * sq(tz)) + 4.42478e4);
+      pidep = T(R(dt_pisub) * R(dq) * R(349138.78) * rexp(R(0.875) * rlog(R(qiz) * R(den))) /
+                (R(qsi) * R(den) * R(K.LAT2) / (R(0.0243) * R(K.RVGAS) * sq(R(tz))) + R(4.42478e4)));
     } else {
       pidep = 0.0;
     }
@@ -402,11 +419,13 @@ SHP void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
     T dqsdt;
     T qsi = iqs2(K, tz, den, dqsdt);
     T qden = qsz * den;
-    T tmp = xexp(0.65625 * xlog(qden));
+    const R qdr = R(qden);
+    const R tmp = rexp(R(0.65625) * rlog(qdr));
     T tsq = tz * tz;
     T dq = (qsi - qvz) / (1.0 + tcpk * dqsdt);
-    T pssub = K.cssub[0] * tsq * (K.cssub[1] * sqrt(qden) + K.cssub[2] * tmp * sqrt(denfac)) /
-                   (K.cssub[3] * tsq + K.cssub[4] * qsi * den);
+    const R tsr = R(tsq);
+    T pssub = T(R(K.cssub[0]) * tsr * (R(K.cssub[1]) * sqrt(qdr) + R(K.cssub[2]) * tmp * sqrt(R(denfac))) /
+                (R(K.cssub[3]) * tsr + R(K.cssub[4]) * R(qsi) * R(den)));
     pssub = (qsi - qvz) * K.dts * pssub;
     if (pssub > 0.0) {
       pssub = fmin(pssub * fmin(1.0, dim(tz, t_sub) * 0.2), qsz);

@@ -14,6 +14,9 @@
  *                      atmos_phys_driver_statein, get_prs_fv3, get_phi_fv3,
  *                      prepare_microphysics  pySHiELD/stencils/physics.py:26-143, 276-330;
  *                                            get_prs_fv3.py:7-20; get_phi_fv3.py:7-25
+ *   shield_copy_dycore_to_physics
+ *                      DycoreToPhysics.__call__ (without the dry convective
+ *                      adjustment)              pySHiELD/update/update_atmos_state.py:95-232
  *   shield_update_physics_state
  *                      update_physics_state_with_tendencies
  *                                                pySHiELD/stencils/physics.py:151-194
@@ -291,6 +294,14 @@ typedef struct {
  * One fused kernel; see pyshield_b200/csrc/physics.cu. */
 int shield_physics_prestep(int nx, int ny, int nz, int hx, int nwat, double ptop, int flags,
                            const ShieldPhysicsFields* fields, void* stream);
+
+/* DycoreToPhysics' copy (update_atmos_state.py:95-142, :160-167, :196-232):
+ * for each of the 16 fields in the order qvapor, qliquid, qrain, qsnow,
+ * qice, qgraupel, qo3mr, qsgs_tke, qcld, pt, delp, delz, ua, va, w, omga,
+ * physics = dycore on i in [0, nx], j in [0, ny] (the compute domain plus
+ * one interface point, which the storages must have) and k in [0, nz). */
+int shield_copy_dycore_to_physics(int nx, int ny, int nz, const ShieldField3D* dycore16,
+                                  const ShieldField3D* physics16, void* stream);
 
 /* Test hook: the scalars shield_mp_step uses for `timestep` (physical
  * constants, setupm constants, sub-step values), computed on the host

@@ -9,6 +9,7 @@ Restates, with GT4Py semantics and the reference's operand order:
 * ``prepare_tendencies_and_update_tracers`` -- ``pySHiELD/update/update_atmos_state.py:40-92``
 * ``moist_cv`` -- ``pySHiELD/update/fv_update_phys.py:20-51``
 * ``update_pressure_and_surface_winds`` -- ``pySHiELD/update/fv_update_phys.py:54-75``
+* ``copy_dycore_to_physics`` -- ``pySHiELD/update/update_atmos_state.py:95-142``
 
 Arrays carry k on the LAST axis and are already restricted to the stencil's
 domain (``nk`` is the domain's level count: L for the compute domain, L+1
@@ -154,3 +155,16 @@ def update_atmos_state_columns(f, dt, nx, ny, h, dycore_only=False, apply_tenden
     return update_pressure_and_surface_winds(
         f["pe"][cd], f["dy_delp"][cd], f["peln"][cd], f["pk"][cd], C.KAPPA, f["dy_ua"][cd], f["dy_va"][cd]
     )
+
+
+D2P_FIELDS = ("qvapor", "qliquid", "qrain", "qsnow", "qice", "qgraupel", "qo3mr", "qsgs_tke", "qcld", "pt", "delp",
+              "delz", "ua", "va", "w", "omga")
+
+
+def copy_dycore_to_physics(dycore, physics, nx, ny, nz, h=3):
+    """update_atmos_state.py:95-142 as DycoreToPhysics builds it
+    (:160-167): the compute domain extended by one interface point in x and
+    y, PARALLEL interval(0, -1) of nz + 1 levels. In place on ``physics``."""
+    box = (slice(h, h + nx + 1), slice(h, h + ny + 1), slice(0, nz))
+    for f in D2P_FIELDS:
+        physics[f][box] = dycore[f][box]

@@ -153,6 +153,7 @@ EXPORTS = (
     "shield_mp_step_noalloc",
     "shield_mp_step_vjp",
     "shield_physics_prestep",
+    "shield_copy_dycore_to_physics",
 )
 
 _lib = None
@@ -199,6 +200,7 @@ def load():
     lib.shield_mp_step_noalloc.argtypes = [
         ctypes.POINTER(ShieldMpConfig), i32, i32, i32, ShieldField2D, ctypes.POINTER(ShieldMpFields), dbl, i32, i32, vp,
     ]
+    lib.shield_copy_dycore_to_physics.argtypes = [i32, i32, i32, ctypes.POINTER(ShieldField3D), ctypes.POINTER(ShieldField3D), vp]
     lib.shield_physics_prestep.argtypes = [i32, i32, i32, i32, i32, dbl, i32, ctypes.POINTER(ShieldPhysicsFields), vp]
     for name in EXPORTS:
         getattr(lib, name).restype = i32

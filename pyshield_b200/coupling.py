@@ -9,6 +9,10 @@
   ``moist_cv`` and ``update_pressure_and_surface_winds``
   (``pySHiELD/update/fv_update_phys.py:152-188``), fused in one kernel.
 
+* ``DycoreToPhysics`` -- ``pySHiELD/update/update_atmos_state.py:145-232``:
+  the 16-field copy of the dycore state into the physics state, on the
+  compute domain plus one interface point in x and y, levels 0 .. nz - 1.
+
 The horizontal part of ``ApplyPhysicsToDycore`` (the halo exchange of
 ``u_dt``/``v_dt``, ``AGrid2DGridPhysics`` and ``CubedToLatLon``) needs cubed-
 sphere edge geometry and a communicator; it is not part of this package, and
@@ -132,3 +136,33 @@ class _View3:
 
 def _as3d(q):
     return _View3(q)
+
+
+D2P_FIELDS = ("qvapor", "qliquid", "qrain", "qsnow", "qice", "qgraupel", "qo3mr", "qsgs_tke", "qcld", "pt", "delp",
+              "delz", "ua", "va", "w", "omga")
+
+
+class DycoreToPhysics:
+    """``DycoreToPhysics`` (update_atmos_state.py:145-232): same constructor
+    and call. The dry convective adjustment (``do_dry_convective_adjust``)
+    is pyFV3's ``DryConvectiveAdjustment``, which is not part of this
+    package; asking for it raises ``NotImplementedError``."""
+
+    def __init__(self, stencil_factory, quantity_factory, dycore_config, do_dry_convective_adjust, dycore_only):
+        if do_dry_convective_adjust:
+            raise NotImplementedError("the dry convective adjustment (pyFV3 fv_subgridz) is not part of pyshield_b200")
+        gi = stencil_factory.grid_indexing
+        self.nx, self.ny, self.nz = (int(v) for v in gi.domain)
+        self._dycore_only = bool(dycore_only)
+        load()
+
+    def __call__(self, dycore_state, physics_state, tendency_state=None, timestep=None, stream=None):
+        if self._dycore_only:
+            return
+        ext = (self.nx + 1, self.ny + 1, self.nz)
+        arr = ShieldField3D * len(D2P_FIELDS)
+        src = arr(*[field3d(getattr(dycore_state, f), ext) for f in D2P_FIELDS])
+        dst = arr(*[field3d(getattr(physics_state, f), ext) for f in D2P_FIELDS])
+        rc = load().shield_copy_dycore_to_physics(self.nx, self.ny, self.nz, src, dst,
+                                                  ctypes.c_void_p(_current_stream(stream)))
+        check(rc, None, "shield_copy_dycore_to_physics")

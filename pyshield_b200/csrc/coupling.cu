@@ -5,6 +5,7 @@
 //  * prepare_tendencies_and_update_tracers pySHiELD/update/update_atmos_state.py:40-92
 //  * moist_cv                              pySHiELD/update/fv_update_phys.py:20-51
 //  * update_pressure_and_surface_winds     pySHiELD/update/fv_update_phys.py:54-75
+//  * copy_dycore_to_physics                pySHiELD/update/update_atmos_state.py:95-142
 //
 // All are HBM-streaming work. The first is elementwise (one thread per point,
 // the fastest-varying storage dimension mapped to consecutive threads). The
@@ -163,6 +164,40 @@ __global__ void update_atmos_state_kernel(const __grid_constant__ AtmArgs A) {
   }
 }
 
+// DycoreToPhysics' copy of 16 fields (update_atmos_state.py:95-142, built at
+// :160-167 on the compute domain plus one interface point in x and y,
+// PARALLEL interval(0, -1) of nz + 1 levels): one thread per point, the
+// fastest-varying storage dimension on consecutive threads.
+constexpr int N_D2P = 16;
+struct D2PArgs {
+  F3 in[N_D2P], out[N_D2P];
+  int nx1, ny1, nz;  // the box: nx + 1, ny + 1, nz
+  int kfast;
+};
+
+__global__ void copy_dycore_to_physics_kernel(const __grid_constant__ D2PArgs A) {
+  const int64_t n = (int64_t)A.nx1 * A.ny1 * A.nz;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i, j, k;
+    if (A.kfast) {
+      k = e % A.nz;
+      const int64_t c = e / A.nz;
+      i = c % A.nx1;
+      j = c / A.nx1;
+    } else {
+      i = e % A.nx1;
+      const int64_t r = e / A.nx1;
+      j = r % A.ny1;
+      k = r / A.ny1;
+    }
+    double v[N_D2P];
+#pragma unroll
+    for (int p = 0; p < N_D2P; ++p) v[p] = A.in[p].at(i, j, k);
+#pragma unroll
+    for (int p = 0; p < N_D2P; ++p) A.out[p].at(i, j, k) = v[p];
+  }
+}
+
 int grid_for(int64_t n, int bs) {
   int64_t nb = (n + bs - 1) / bs;
   return (int)(nb < 148 * 32 ? (nb > 0 ? nb : 1) : 148 * 32);
@@ -240,6 +275,35 @@ extern "C" int shield_update_atmos_state(int nx, int ny, int nz, int hx, int mod
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     shield::set_last_error(std::string("shield_update_atmos_state: ") + cudaGetErrorString(e));
+    return SHIELD_ECUDA;
+  }
+  return SHIELD_OK;
+}
+
+extern "C" int shield_copy_dycore_to_physics(int nx, int ny, int nz, const ShieldField3D* dycore16,
+                                             const ShieldField3D* physics16, void* stream) {
+  if (!dycore16 || !physics16 || nx < 1 || ny < 1 || nz < 1) {
+    shield::set_last_error("shield_copy_dycore_to_physics: bad arguments");
+    return SHIELD_EINVAL;
+  }
+  D2PArgs A;
+  for (int p = 0; p < N_D2P; ++p) {
+    if (!dycore16[p].ptr || !physics16[p].ptr) {
+      shield::set_last_error("shield_copy_dycore_to_physics: null field " + std::to_string(p));
+      return SHIELD_EINVAL;
+    }
+    A.in[p] = mk(dycore16[p]);
+    A.out[p] = mk(physics16[p]);
+  }
+  A.nx1 = nx + 1;
+  A.ny1 = ny + 1;
+  A.nz = nz;
+  A.kfast = (physics16[0].sk == 1) ? 1 : 0;
+  const int64_t n = (int64_t)A.nx1 * A.ny1 * nz;
+  copy_dycore_to_physics_kernel<<<grid_for(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(A);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    shield::set_last_error(std::string("shield_copy_dycore_to_physics: ") + cudaGetErrorString(e));
     return SHIELD_ECUDA;
   }
   return SHIELD_OK;

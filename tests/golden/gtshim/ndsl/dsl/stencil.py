@@ -37,3 +37,15 @@ class StencilFactory:
 
     def from_origin_domain(self, func, origin, domain, externals=None, **kwargs):
         return Stencil(func, externals=externals, origin=origin, domain=domain)
+
+    def from_dims_halo(self, func, compute_dims, compute_halos=(0, 0), externals=None, **kwargs):
+        """NDSL's from_dims_halo: the compute domain along ``compute_dims``
+        (an interface dimension has one more point) widened by
+        ``compute_halos`` in x and y."""
+        gi = self.grid_indexing
+        hx, hy = compute_halos
+        n = (gi.nx, gi.ny, gi.nz)
+        domain = tuple(n[d] + (1 if compute_dims[d].endswith("interface") else 0) for d in range(3))
+        domain = (domain[0] + 2 * hx, domain[1] + 2 * hy, domain[2])
+        origin = (gi.n_halo - hx, gi.n_halo - hy, 0)
+        return Stencil(func, externals=externals, origin=origin, domain=domain)

@@ -426,6 +426,42 @@ def run_coupling_chain(name, nx, ny, L, dt, seed):
     return meta
 
 
+D2P_FIELDS = ("qvapor", "qliquid", "qrain", "qsnow", "qice", "qgraupel", "qo3mr", "qsgs_tke", "qcld", "pt", "delp",
+              "delz", "ua", "va", "w", "omga")
+
+
+def run_dycore_to_physics_case(name, nx, ny, L, seed):
+    """pySHiELD's ``DycoreToPhysics.__call__`` (update_atmos_state.py:145-232)
+    without the dry convective adjustment: the 16-field copy on the
+    interface-extended compute domain, levels 0 .. nz - 1."""
+    from ndsl.dsl.stencil import GridIndexing, StencilFactory
+    from ndsl.initialization.allocator import QuantityFactory
+    from pyFV3 import DynamicalCoreConfig
+    from pySHiELD.update.update_atmos_state import DycoreToPhysics
+
+    rng = np.random.default_rng(seed)
+    shape = (nx + 7, ny + 7, L + 1)
+    dy = {f: rng.uniform(-1.0, 1.0, shape) for f in D2P_FIELDS}
+    ph = {f: rng.uniform(-1.0, 1.0, shape) for f in D2P_FIELDS}
+    out = {f"in_dycore_{f}": v.copy() for f, v in dy.items()}
+    out.update({f"in_physics_{f}": v.copy() for f, v in ph.items()})
+
+    class _State:
+        pass
+
+    ds, ps = _State(), _State()
+    for f in D2P_FIELDS:
+        setattr(ds, f, dy[f])
+        setattr(ps, f, ph[f])
+    gi = GridIndexing(nx, ny, L)
+    d2p = DycoreToPhysics(StencilFactory(gi), QuantityFactory(nx, ny, L), DynamicalCoreConfig(), False, False)
+    d2p(ds, ps)
+    out.update({f"out_physics_{f}": ph[f] for f in D2P_FIELDS})
+    meta = {"name": name, "nx": nx, "ny": ny, "L": L, "halo": 3}
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), meta=json.dumps(meta), **out)
+    return meta
+
+
 def physics_cases():
     """(name, nx, ny, L, dt, seed, config overrides)."""
     return [
@@ -515,6 +551,11 @@ def main():
         if args.only and args.only != case[0]:
             continue
         meta = run_physics_case(*case)
+        print("wrote", meta["name"])
+    for case in (("d2p_copy", 5, 4, 10, 61),):
+        if args.only and args.only != case[0]:
+            continue
+        meta = run_dycore_to_physics_case(*case)
         print("wrote", meta["name"])
 
 

@@ -97,3 +97,40 @@ def test_update_atmos_state_chain(layout):
     _close(d.ps.data.cpu().numpy()[cd], z["out_ps"][cd], "ps")
     _close(uas.u_srf.cpu().numpy(), z["out_u_srf"][cd], "u_srf")
     _close(uas.v_srf.cpu().numpy(), z["out_v_srf"][cd], "v_srf")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("layout", ["ifirst", "kfirst"])
+def test_dycore_to_physics_matches_reference(layout):
+    """DycoreToPhysics' copy against the reference's own result (golden):
+    every storage whole, so nothing outside the interface-extended compute
+    domain and levels 0 .. nz - 1 may change."""
+    import numpy as np
+    import torch
+
+    from golden_io import load
+    from pyshield_b200.coupling import D2P_FIELDS, DycoreToPhysics
+    from pyshield_b200.grid import GridIndexing, QuantityFactory, StencilFactory
+    from pyshield_b200.quantity import Quantity
+
+    z, m = load("d2p_copy")
+    nx, ny, L, h = m["nx"], m["ny"], m["L"], m["halo"]
+
+    def dev(a):
+        if layout == "ifirst":
+            return torch.from_numpy(np.ascontiguousarray(a.transpose(2, 1, 0))).cuda().permute(2, 1, 0)
+        return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+    class State:
+        pass
+
+    ds, ps = State(), State()
+    for f in D2P_FIELDS:
+        setattr(ds, f, Quantity(dev(z["in_dycore_" + f]), ("x", "y", "z"), "", (h, h, 0), (nx, ny, L)))
+        setattr(ps, f, Quantity(dev(z["in_physics_" + f]), ("x", "y", "z"), "", (h, h, 0), (nx, ny, L)))
+    gi = GridIndexing(nx, ny, L, h)
+    DycoreToPhysics(StencilFactory(gi), QuantityFactory(gi), None, False, False)(ds, ps)
+    torch.cuda.synchronize()
+    for f in D2P_FIELDS:
+        got = getattr(ps, f).data.cpu().numpy()
+        np.testing.assert_array_equal(got, z["out_physics_" + f], err_msg=f)

@@ -134,3 +134,13 @@ def test_physics_call_bitexact(name):
         else:
             got = st[k]
         np.testing.assert_array_equal(got, z["out_" + k], err_msg=f"{name} {k}")
+
+
+def test_copy_dycore_to_physics_bitexact():
+    """DycoreToPhysics' 16-field copy on the interface-extended domain."""
+    z, m = load("d2p_copy")
+    dy = {k[10:]: z[k] for k in z.files if k.startswith("in_dycore_")}
+    ph = {k[11:]: np.array(z[k]) for k in z.files if k.startswith("in_physics_")}
+    OC.copy_dycore_to_physics(dy, ph, m["nx"], m["ny"], m["L"], m["halo"])
+    for f, v in ph.items():
+        np.testing.assert_array_equal(v, z["out_physics_" + f], err_msg=f)

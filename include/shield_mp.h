@@ -17,6 +17,9 @@
  *   shield_copy_dycore_to_physics
  *                      DycoreToPhysics.__call__ (without the dry convective
  *                      adjustment)              pySHiELD/update/update_atmos_state.py:95-232
+ *   shield_agrid_to_dgrid
+ *                      AGrid2DGridPhysics.__call__(u, v, u_dt, v_dt)
+ *                                                pySHiELD/update/update_dwind_phys.py:12-161, 490-701
  *   shield_update_physics_state
  *                      update_physics_state_with_tendencies
  *                                                pySHiELD/stencils/physics.py:151-194
@@ -302,6 +305,39 @@ int shield_physics_prestep(int nx, int ny, int nz, int hx, int nwat, double ptop
  * one interface point, which the storages must have) and k in [0, nz). */
 int shield_copy_dycore_to_physics(int nx, int ny, int nz, const ShieldField3D* dycore16,
                                   const ShieldField3D* physics16, void* stream);
+
+/* AGrid2DGridPhysics (update_dwind_phys.py): the A-grid wind tendencies
+ * turned into D-grid winds. Indices are relative to the compute-domain
+ * origin. One region of a cube edge: the points [lo, hi) along the edge line
+ * `line` (j for the south / north edges, i for west / east), corrected with
+ * the neighbour at +1 (dir = 1, the part below the edge's midpoint) or -1. */
+typedef struct {
+  int line, lo, hi, dir;
+} ShieldEdgeRegion;
+typedef struct {
+  int n[4];                  /* regions per edge: south, north, west, east */
+  ShieldEdgeRegion r[4][2];  /* in the reference's order (lower, upper) */
+} ShieldEdgePlan;
+/* The grid vectors (DriverGridData): 2-D fields at the compute origin, and
+ * the 1-D south / north edge weights along i (element stride edge_stride). */
+typedef struct {
+  ShieldField2D vlon1, vlon2, vlon3, vlat1, vlat2, vlat3;
+  ShieldField2D es1_1, es1_2, es1_3, ew2_1, ew2_2, ew2_3;
+  ShieldField2D edge_vect_w, edge_vect_e;
+  const double* edge_vect_s;
+  const double* edge_vect_n;
+  int64_t edge_stride;
+} ShieldDwindGeometry;
+
+/* With grid_type <= 3: u += dt5 (ue . es1) on i in [0, nx), j in [0, ny],
+ * v += dt5 (ve . ew2) on i in [0, nx], j in [0, ny), ue / ve from the
+ * tendencies with the plan's edge corrections, then u_dt = v_dt = 0 on i, j
+ * in [-1, n + 1); the tendencies need one halo point, filled by the caller's
+ * halo exchange. With grid_type > 3: the doubly periodic update on the
+ * compute domain (plan and geometry unused). dt5 = dt_atmos / 2. */
+int shield_agrid_to_dgrid(int nx, int ny, int nz, int grid_type, double dt5, const ShieldEdgePlan* plan,
+                          const ShieldDwindGeometry* geometry, ShieldField3D u, ShieldField3D v, ShieldField3D u_dt,
+                          ShieldField3D v_dt, void* stream);
 
 /* Test hook: the scalars shield_mp_step uses for `timestep` (physical
  * constants, setupm constants, sub-step values), computed on the host

@@ -134,6 +134,23 @@ class ShieldPhysicsFields(ctypes.Structure):
     _fields_ = [(n, ShieldField3D) for n in PHYS_FIELDS]
 
 
+class ShieldEdgeRegion(ctypes.Structure):
+    _fields_ = [("line", ctypes.c_int), ("lo", ctypes.c_int), ("hi", ctypes.c_int), ("dir", ctypes.c_int)]
+
+
+class ShieldEdgePlan(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int * 4), ("r", (ShieldEdgeRegion * 2) * 4)]
+
+
+DWIND_GEOM_2D = ("vlon1", "vlon2", "vlon3", "vlat1", "vlat2", "vlat3", "es1_1", "es1_2", "es1_3", "ew2_1", "ew2_2",
+                 "ew2_3", "edge_vect_w", "edge_vect_e")
+
+
+class ShieldDwindGeometry(ctypes.Structure):
+    _fields_ = [(n, ShieldField2D) for n in DWIND_GEOM_2D] + [
+        ("edge_vect_s", ctypes.c_void_p), ("edge_vect_n", ctypes.c_void_p), ("edge_stride", ctypes.c_int64)]
+
+
 EXPORTS = (
     "shield_mp_create",
     "shield_mp_step",
@@ -154,6 +171,7 @@ EXPORTS = (
     "shield_mp_step_vjp",
     "shield_physics_prestep",
     "shield_copy_dycore_to_physics",
+    "shield_agrid_to_dgrid",
 )
 
 _lib = None
@@ -199,6 +217,10 @@ def load():
     ]
     lib.shield_mp_step_noalloc.argtypes = [
         ctypes.POINTER(ShieldMpConfig), i32, i32, i32, ShieldField2D, ctypes.POINTER(ShieldMpFields), dbl, i32, i32, vp,
+    ]
+    lib.shield_agrid_to_dgrid.argtypes = [
+        i32, i32, i32, i32, dbl, ctypes.POINTER(ShieldEdgePlan), ctypes.POINTER(ShieldDwindGeometry), ShieldField3D,
+        ShieldField3D, ShieldField3D, ShieldField3D, vp,
     ]
     lib.shield_copy_dycore_to_physics.argtypes = [i32, i32, i32, ctypes.POINTER(ShieldField3D), ctypes.POINTER(ShieldField3D), vp]
     lib.shield_physics_prestep.argtypes = [i32, i32, i32, i32, i32, dbl, i32, ctypes.POINTER(ShieldPhysicsFields), vp]

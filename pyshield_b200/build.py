@@ -30,6 +30,7 @@ UNITS = [
     ("coupling.cu", ["-fmad=false"]),
     ("mp_vjp.cu", ["-fmad=false"]),
     ("physics.cu", ["-fmad=false"]),
+    ("dwind.cu", ["-fmad=false"]),
 ]
 
 

@@ -22,7 +22,10 @@ that the numpy backend implements:
   __externals__ import`` names resolve to the stencil's externals.
 
 Horizontal dimensions are always vectorised; arithmetic is evaluated in the
-order the source's expression tree gives.
+order the source's expression tree gives. A stencil that reads horizontal
+offsets runs on its domain widened by the largest offset, so that its
+temporaries hold values wherever their readers look; it writes the caller's
+fields on the domain only.
 """
 
 import ast
@@ -125,6 +128,78 @@ class _Local:
             self.a = np.where(mask, value, self.a)
 
 
+class _HField:
+    """A field of a stencil that reads horizontal offsets. Such a stencil runs
+    on its domain widened by ``ext`` = (ex, ey) points on each side, so that
+    a temporary read at an offset holds values there (GT4Py computes a
+    temporary on the extent its readers need); fields of the caller are
+    written on the domain only. ``kind``: "3d", "ij" (FloatFieldIJ), "i"
+    (FloatFieldI) or "temp"."""
+
+    def __init__(self, arr, origin, domain, ext, kind):
+        self.ext, self.dom, self.kind = ext, domain, kind
+        ex, ey = ext
+        ni, nj, nk = domain
+        if kind == "temp":
+            self.a = np.full((ni + 4 * ex, nj + 4 * ey, nk), np.nan)
+            return
+        self.arr = arr
+        self.origin = origin
+
+    def _padded(self):
+        """The caller's array on [-2ex, n + 2ex) around the domain (NaN where
+        the storage has no point), as of now."""
+        ex, ey = self.ext
+        ni, nj, nk = self.dom
+        o = self.origin
+        if self.kind == "i":
+            out = np.full((ni + 4 * ex,), np.nan)
+            lo = o[0] - 2 * ex
+            for e in range(ni + 4 * ex):
+                if 0 <= lo + e < self.arr.shape[0]:
+                    out[e] = self.arr[lo + e]
+            return out
+        shape = (ni + 4 * ex, nj + 4 * ey) + (() if self.kind == "ij" else (self.arr.shape[2] - o[2],))
+        out = np.full(shape, np.nan)
+        i_lo, j_lo = o[0] - 2 * ex, o[1] - 2 * ey
+        a0, a1 = max(0, i_lo), min(self.arr.shape[0], i_lo + shape[0])
+        b0, b1 = max(0, j_lo), min(self.arr.shape[1], j_lo + shape[1])
+        if self.kind == "ij":
+            out[a0 - i_lo : a1 - i_lo, b0 - j_lo : b1 - j_lo] = self.arr[a0:a1, b0:b1]
+        else:
+            out[a0 - i_lo : a1 - i_lo, b0 - j_lo : b1 - j_lo] = self.arr[a0:a1, b0:b1, o[2]:]
+        return out
+
+    def read(self, ctx, dk=0, di=0, dj=0):
+        ex, ey = self.ext
+        ni, nj, _ = self.dom
+        si = slice(ex + di, ex + di + ni + 2 * ex)
+        sj = slice(ey + dj, ey + dj + nj + 2 * ey)
+        a = self.a if self.kind == "temp" else self._padded()
+        if self.kind == "i":
+            return a[si][:, None, None]
+        if self.kind == "ij":
+            return a[si, sj][:, :, None]
+        return a[si, sj, ctx.k0 + dk : ctx.k1 + dk]
+
+    def write(self, ctx, value, mask):
+        ex, ey = self.ext
+        ni, nj, _ = self.dom
+        eshape = (ni + 2 * ex, nj + 2 * ey, ctx.k1 - ctx.k0)
+        v = np.broadcast_to(value, eshape)
+        m = None if mask is None else np.broadcast_to(mask, eshape)
+        if self.kind == "temp":
+            cur = self.a[ex : ex + ni + 2 * ex, ey : ey + nj + 2 * ey, ctx.k0 : ctx.k1]
+            cur[...] = v if m is None else np.where(m, v, cur)
+            return
+        if self.kind != "3d":
+            raise RuntimeError("write to a 2-D or 1-D field of a stencil with horizontal offsets")
+        o = self.origin
+        cur = self.arr[o[0] : o[0] + ni, o[1] : o[1] + nj, o[2] + ctx.k0 : o[2] + ctx.k1]
+        vi = v[ex : ex + ni, ey : ey + nj]
+        cur[...] = vi if m is None else np.where(m[ex : ex + ni, ey : ey + nj], vi, cur)
+
+
 class _Frame:
     def __init__(self, names, globs, externals, shape, temps=None, fields=None):
         self.names = names  # name -> _Field/_Local/scalar
@@ -149,6 +224,16 @@ class Stencil:
         for a in self.fdef.args.args:
             self.annotations[a.arg] = ast.unparse(a.annotation) if a.annotation else ""
         self.globs = func.__globals__
+        ex = ey = 0
+        for node in ast.walk(self.fdef):
+            if isinstance(node, ast.Subscript) and isinstance(node.value, ast.Name):
+                try:
+                    off = ast.literal_eval(node.slice)
+                except ValueError:
+                    continue
+                if isinstance(off, tuple) and len(off) == 3:
+                    ex, ey = max(ex, abs(off[0])), max(ey, abs(off[1]))
+        self.ext = (ex, ey)
 
     # ------------------------------------------------------------------ call
     def __call__(self, *args, **kwargs):
@@ -156,15 +241,23 @@ class Stencil:
         bound.update(kwargs)
         ni, nj, nk = self.domain
         names = {}
+        ext = self.ext
+        horizontal = ext != (0, 0)
         for p in self.params:
             v = bound[p]
             ann = self.annotations[p]
-            if ann in ("FloatField", "FloatFieldIJ"):
+            if horizontal and ann in ("FloatField", "FloatFieldIJ", "FloatFieldI"):
+                kind = {"FloatField": "3d", "FloatFieldIJ": "ij", "FloatFieldI": "i"}[ann]
+                names[p] = _HField(np.asarray(getattr(v, "data", v)), self.origin, self.domain, ext, kind)
+            elif ann in ("FloatField", "FloatFieldIJ"):
                 arr = getattr(v, "data", v)
                 names[p] = _Field(np.asarray(arr), self.origin, self.domain, is2d=(ann == "FloatFieldIJ"))
             else:
                 names[p] = v
-        frame = _Frame(names, self.globs, self.externals, (ni, nj, nk), temps={}, fields=names)
+        shape = (ni + 2 * ext[0], nj + 2 * ext[1], nk)
+        frame = _Frame(names, self.globs, self.externals, shape, temps={}, fields=names)
+        frame.ext = ext
+        frame.domain = self.domain
         with np.errstate(all="ignore"):
             for stmt in self.fdef.body:
                 self._top_stmt(stmt, frame)
@@ -242,12 +335,15 @@ class Stencil:
         if var is None:
             if frame.temps is not None:
                 ni, nj, nk = frame.shape
-                var = _Field(np.full((ni, nj, nk), np.nan), (0, 0, 0), (ni, nj, nk))
+                if getattr(frame, "ext", (0, 0)) != (0, 0):
+                    var = _HField(None, None, frame.domain, frame.ext, "temp")
+                else:
+                    var = _Field(np.full((ni, nj, nk), np.nan), (0, 0, 0), (ni, nj, nk))
                 frame.temps[name] = var
             else:
                 var = _Local(self._ctx_shape(frame, ctx))
                 frame.names[name] = var
-        if not isinstance(var, (_Field, _Local)):
+        if not isinstance(var, (_Field, _Local, _HField)):
             # function parameter passed by value: rebind as a local
             var = _Local(self._ctx_shape(frame, ctx))
             old = frame.names[name]
@@ -337,7 +433,7 @@ class Stencil:
         if isinstance(e, ast.Name):
             var = self._lookup_var(e.id, frame)
             if var is not None:
-                if isinstance(var, (_Field, _Local)):
+                if isinstance(var, (_Field, _Local, _HField)):
                     return var.read(ctx)
                 return var
             return self._resolve_global(e, frame)
@@ -346,6 +442,8 @@ class Stencil:
         if isinstance(e, ast.Subscript):
             off = ast.literal_eval(e.slice)
             var = self._lookup_var(e.value.id, frame)
+            if isinstance(var, _HField):
+                return var.read(ctx, off[2], off[0], off[1])
             assert off[0] == 0 and off[1] == 0
             return var.read(ctx, off[2])
         if isinstance(e, ast.BinOp):

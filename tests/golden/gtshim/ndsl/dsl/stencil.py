@@ -3,9 +3,12 @@ from _gtexec import Stencil
 
 
 class GridIndexing:
-    def __init__(self, nx, ny, nz, n_halo=3):
+    def __init__(self, nx, ny, nz, n_halo=3, edges=(True, True, True, True)):
         self.nx, self.ny, self.nz, self.n_halo = nx, ny, nz, n_halo
         self.domain = (nx, ny, nz)
+        self.isc, self.iec = n_halo, n_halo + nx - 1
+        self.jsc, self.jec = n_halo, n_halo + ny - 1
+        self.south_edge, self.north_edge, self.west_edge, self.east_edge = edges
 
     def origin_compute(self, add=(0, 0, 0)):
         return (self.n_halo + add[0], self.n_halo + add[1], add[2])

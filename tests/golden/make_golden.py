@@ -462,6 +462,58 @@ def run_dycore_to_physics_case(name, nx, ny, L, seed):
     return meta
 
 
+DWIND_GEOM = ("vlon1", "vlon2", "vlon3", "vlat1", "vlat2", "vlat3", "es1_1", "es1_2", "es1_3", "ew2_1", "ew2_2",
+              "ew2_3", "edge_vect_w", "edge_vect_e")
+
+
+def dwind_cases():
+    """(name, subtile nx, ny, L, layout, rank, dt_atmos, grid_type)."""
+    return [
+        ("dwind_tile", 8, 7, 5, (1, 1), 0, 225.0, 0),
+        ("dwind_sub0", 6, 6, 4, (2, 2), 0, 150.0, 0),
+        ("dwind_sub3", 6, 6, 4, (2, 2), 3, 150.0, 0),
+        ("dwind_periodic", 6, 5, 4, (1, 1), 0, 180.0, 4),
+    ]
+
+
+def run_dwind_case(name, nx, ny, L, layout, rank, dt, grid_type):
+    """pySHiELD's AGrid2DGridPhysics.__call__ (update_dwind_phys.py:490-701)
+    on one rank's subtile: the prep, the wind-tendency reset, the cube-edge
+    corrections of the rank's tile edges, and the D-grid wind update (or the
+    doubly periodic update for grid_type > 3)."""
+    from types import SimpleNamespace
+
+    from ndsl.comm.partitioner import TilePartitioner
+    from ndsl.dsl.stencil import GridIndexing, StencilFactory
+    from ndsl.initialization.allocator import QuantityFactory
+    from pySHiELD.update.update_dwind_phys import AGrid2DGridPhysics
+
+    rng = np.random.default_rng(sum(ord(c) for c in name))
+    h = 3
+    part = TilePartitioner(layout)
+    sy, sx = part.subtile_index(rank)
+    edges = (sy == 0, sy == layout[1] - 1, sx == 0, sx == layout[0] - 1)
+    gi = GridIndexing(nx, ny, L, h, edges=edges)
+    shape = (nx + 2 * h + 1, ny + 2 * h + 1, L + 1)
+    npx, npy = nx * layout[0] + 1, ny * layout[1] + 1
+    geom = {k: rng.uniform(-1.0, 1.0, shape[:2]) for k in DWIND_GEOM}
+    geom["edge_vect_s"] = rng.uniform(0.0, 1.0, shape[0])
+    geom["edge_vect_n"] = rng.uniform(0.0, 1.0, shape[0])
+    grid_info = SimpleNamespace(grid_type=grid_type, **geom)
+    namelist = SimpleNamespace(dt_atmos=dt, npx=npx, npy=npy, layout=layout)
+    fields = {k: rng.uniform(-5.0, 5.0, shape) for k in ("u", "v", "u_dt", "v_dt")}
+    out = {f"in_{k}": v.copy() for k, v in fields.items()}
+    out.update({f"geom_{k}": v for k, v in geom.items()})
+    a2d = AGrid2DGridPhysics(StencilFactory(gi), QuantityFactory(nx, ny, L), part, rank, namelist, grid_info)
+    a2d(fields["u"], fields["v"], fields["u_dt"], fields["v_dt"])
+    out.update({f"out_{k}": v for k, v in fields.items()})
+    meta = {"name": name, "nx": nx, "ny": ny, "L": L, "halo": h, "layout": list(layout), "rank": rank,
+            "subtile_index": [int(sy), int(sx)], "edges": [bool(e) for e in edges], "npx": npx, "npy": npy, "dt": dt,
+            "grid_type": grid_type}
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), meta=json.dumps(meta), **out)
+    return meta
+
+
 def physics_cases():
     """(name, nx, ny, L, dt, seed, config overrides)."""
     return [
@@ -551,6 +603,11 @@ def main():
         if args.only and args.only != case[0]:
             continue
         meta = run_physics_case(*case)
+        print("wrote", meta["name"])
+    for case in dwind_cases():
+        if args.only and args.only != case[0]:
+            continue
+        meta = run_dwind_case(*case)
         print("wrote", meta["name"])
     for case in (("d2p_copy", 5, 4, 10, 61),):
         if args.only and args.only != case[0]:

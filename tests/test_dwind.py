@@ -1,0 +1,71 @@
+"""AGrid2DGridPhysics (pySHiELD/update/update_dwind_phys.py).
+
+CPU: the package's edge plan (which parts of a rank's subtile edges lie on
+the cube tile's edges, and on which side of the midpoint) equals the plan of
+the oracle, which reproduces the reference's output bit for bit
+(test_oracle_golden.py), over many layouts, ranks and tile sizes.
+
+GPU: the kernels against the reference's own result (golden fixtures) for a
+whole tile, two subtiles of a 2 x 2 layout and the doubly periodic grid,
+every storage compared whole.
+"""
+import numpy as np
+import pytest
+
+DWIND_CASES = ("dwind_tile", "dwind_sub0", "dwind_sub3", "dwind_periodic")
+
+
+@pytest.mark.parametrize("n", [6, 7, 12, 13, 48])
+def test_edge_plan_matches_oracle(n):
+    from oracle.dwind import edge_plan as oracle_plan
+    from pyshield_b200.dwind import edge_plan
+
+    for layout in ((1, 1), (2, 2), (3, 3), (2, 1), (1, 3)):
+        if n % layout[0] or n % layout[1]:
+            continue
+        nx, ny = n // layout[0], n // layout[1]
+        for rank in range(layout[0] * layout[1]):
+            sy, sx = rank // layout[0], rank % layout[0]
+            edges = (sy == 0, sy == layout[1] - 1, sx == 0, sx == layout[0] - 1)
+            got = edge_plan(nx, ny, 3, n + 1, n + 1, layout, (sy, sx), edges)
+            ref = oracle_plan(nx, ny, 3, n + 1, n + 1, layout, (sy, sx), edges)
+            for name in ("south", "north", "west", "east"):
+                # the oracle keeps the reference's empty upper south region; it changes nothing
+                r = [x for x in ref[name] if x[2] > x[1]]
+                assert got[name] == r, (n, layout, rank, name, got[name], r)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", DWIND_CASES)
+def test_agrid_to_dgrid_matches_reference(name):
+    from types import SimpleNamespace
+
+    import torch
+
+    from golden_io import load
+    from pyshield_b200.dwind import AGrid2DGridPhysics
+    from pyshield_b200.grid import GridIndexing, StencilFactory
+
+    z, m = load(name)
+    nx, ny, L, h = m["nx"], m["ny"], m["L"], m["halo"]
+
+    def dev(a):
+        a = np.ascontiguousarray(a.T)
+        return torch.from_numpy(a).cuda().permute(*reversed(range(a.ndim)))
+
+    gi = GridIndexing(nx, ny, L, h)
+    gi.south_edge, gi.north_edge, gi.west_edge, gi.east_edge = m["edges"]
+    sy, sx = m["subtile_index"]
+    part = SimpleNamespace(subtile_index=lambda rank: (sy, sx))
+    namelist = SimpleNamespace(dt_atmos=m["dt"], npx=m["npx"], npy=m["npy"], layout=tuple(m["layout"]))
+    geom = {k[5:]: dev(z[k]) for k in z.files if k.startswith("geom_")}
+    grid_info = SimpleNamespace(grid_type=m["grid_type"], **geom)
+    f = {k: dev(z["in_" + k]) for k in ("u", "v", "u_dt", "v_dt")}
+    from pyshield_b200.quantity import Quantity
+
+    q = {k: Quantity(t, ("x", "y", "z"), "", (h, h, 0), (nx, ny, L)) for k, t in f.items()}
+    a2d = AGrid2DGridPhysics(StencilFactory(gi), None, part, m["rank"], namelist, grid_info)
+    a2d(q["u"], q["v"], q["u_dt"], q["v_dt"])
+    torch.cuda.synchronize()
+    for k, t in f.items():
+        np.testing.assert_array_equal(t.cpu().numpy(), z["out_" + k], err_msg=f"{name} {k}")

@@ -144,3 +144,26 @@ def test_copy_dycore_to_physics_bitexact():
     OC.copy_dycore_to_physics(dy, ph, m["nx"], m["ny"], m["L"], m["halo"])
     for f, v in ph.items():
         np.testing.assert_array_equal(v, z["out_physics_" + f], err_msg=f)
+
+
+DWIND_CASES = ("dwind_tile", "dwind_sub0", "dwind_sub3", "dwind_periodic")
+
+
+@pytest.mark.parametrize("name", DWIND_CASES)
+def test_agrid_to_dgrid_bitexact(name):
+    """AGrid2DGridPhysics on one rank's subtile: prep, reset, edge
+    corrections of the rank's cube edges, D-grid update."""
+    from oracle import dwind as OD
+
+    z, m = load(name)
+    nx, ny, L, h = m["nx"], m["ny"], m["L"], m["halo"]
+    f = {k: np.array(z["in_" + k]) for k in ("u", "v", "u_dt", "v_dt")}
+    g = {k[5:]: z[k] for k in z.files if k.startswith("geom_")}
+    dt5 = 0.5 * m["dt"]
+    if m["grid_type"] > 3:
+        OD.doubly_periodic(f["u"], f["v"], f["u_dt"], f["v_dt"], nx, ny, L, h, dt5)
+    else:
+        plan = OD.edge_plan(nx, ny, h, m["npx"], m["npy"], m["layout"], m["subtile_index"], m["edges"])
+        OD.agrid_to_dgrid(f["u"], f["v"], f["u_dt"], f["v_dt"], g, nx, ny, L, h, dt5, plan)
+    for k, v in f.items():
+        np.testing.assert_array_equal(v, z["out_" + k], err_msg=f"{name} {k}")

@@ -339,6 +339,13 @@ int shield_agrid_to_dgrid(int nx, int ny, int nz, int grid_type, double dt5, con
                           const ShieldDwindGeometry* geometry, ShieldField3D u, ShieldField3D v, ShieldField3D u_dt,
                           ShieldField3D v_dt, void* stream);
 
+/* The handle's device error word: every step records the first column
+ * whose outputs hold a NaN or an infinity (the kernel never traps). This
+ * call waits for `stream`, then returns SHIELD_OK with *bad_column = -1, or
+ * SHIELD_EDEVICE with the column (i + nx j) and a message, and clears the
+ * word. */
+int shield_mp_check(void* handle, int64_t* bad_column, void* stream);
+
 /* Test hook: the scalars shield_mp_step uses for `timestep` (physical
  * constants, setupm constants, sub-step values), computed on the host
  * without touching the GPU; returns how many doubles were written. */

@@ -172,6 +172,7 @@ EXPORTS = (
     "shield_physics_prestep",
     "shield_copy_dycore_to_physics",
     "shield_agrid_to_dgrid",
+    "shield_mp_check",
 )
 
 _lib = None
@@ -218,6 +219,7 @@ def load():
     lib.shield_mp_step_noalloc.argtypes = [
         ctypes.POINTER(ShieldMpConfig), i32, i32, i32, ShieldField2D, ctypes.POINTER(ShieldMpFields), dbl, i32, i32, vp,
     ]
+    lib.shield_mp_check.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), vp]
     lib.shield_agrid_to_dgrid.argtypes = [
         i32, i32, i32, i32, dbl, ctypes.POINTER(ShieldEdgePlan), ctypes.POINTER(ShieldDwindGeometry), ShieldField3D,
         ShieldField3D, ShieldField3D, ShieldField3D, vp,

@@ -206,6 +206,28 @@ extern "C" int shield_mp_step_vjp(void* handle, const ShieldMpFields* F, const S
   return SHIELD_OK;
 }
 
+// The device error word of the handle's steps: which column, if any,
+// produced a NaN or an infinity since the last check. Waits for `stream`.
+extern "C" int shield_mp_check(void* handle, int64_t* bad_column, void* stream) {
+  Handle* h = static_cast<Handle*>(handle);
+  if (!h) return fail(nullptr, SHIELD_EINVAL, "null handle");
+  if (bad_column) *bad_column = -1;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int v = 0;
+  cudaError_t e = cudaMemcpyAsync(&v, h->err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "reading the error word");
+  if (v == 0) return SHIELD_OK;
+  e = cudaMemsetAsync(h->err, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(h, e, "clearing the error word");
+  const int64_t c = (int64_t)v - 1;
+  if (bad_column) *bad_column = c;
+  return fail(h, SHIELD_EDEVICE,
+              "column " + std::to_string(c) + " (i = " + std::to_string(c % h->nx) + ", j = " +
+                  std::to_string(c / h->nx) + ") produced a NaN or an infinity");
+}
+
 extern "C" int shield_mp_destroy(void* handle) {
   Handle* h = static_cast<Handle*>(handle);
   if (!h) return SHIELD_OK;

@@ -1003,6 +1003,12 @@ SHD void mp_body(const MpArgs& A, double* sm, double* scr, double* work, const i
       TL(OUT_VDT) = inc_v;
       TL(OUT_W) = w;
       TL(OUT_QAZ) = qa;
+      // the device error word: the first column (+ 1) that produced a NaN or
+      // an infinity, for the host to read after the step (never traps)
+      if (A.err && !(isfinite(inc_pt) && isfinite(inc_qv) && isfinite(inc_ql) && isfinite(inc_qr) &&
+                     isfinite(inc_qi) && isfinite(inc_qs) && isfinite(inc_qg) && isfinite(inc_qa) &&
+                     isfinite(inc_u) && isfinite(inc_v) && isfinite(w) && isfinite(qa)))
+        atomicCAS(A.err, 0, (int)(col + 1));
     }
     if (k == 0) {
       const double convt = 86400.0 * K.rdt * K.RGRAV;
@@ -1010,6 +1016,8 @@ SHD void mp_body(const MpArgs& A, double* sm, double* scr, double* work, const i
       if (A.snow) A.snow[col] = snow * convt;
       if (A.ice) A.ice[col] = ice * convt;
       if (A.graupel) A.graupel[col] = graupel * convt;
+      if (A.err && !(isfinite(rain) && isfinite(snow) && isfinite(ice) && isfinite(graupel)))
+        atomicCAS(A.err, 0, (int)(col + 1));
     }
   }
 }

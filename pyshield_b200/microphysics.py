@@ -148,6 +148,16 @@ class Microphysics:
         )
         check(rc, self._handle, "shield_mp_step")
 
+    def check(self, stream=None):
+        """Wait for the steps queued so far and raise ``ShieldError`` naming
+        the column if one of them produced a NaN or an infinity (the kernel
+        records the first such column; the record is cleared here). Returns
+        -1 when every step was clean."""
+        bad = ctypes.c_int64(-1)
+        rc = load().shield_mp_check(self._handle, ctypes.byref(bad), ctypes.c_void_p(_current_stream(stream)))
+        check(rc, self._handle, "microphysics step")
+        return bad.value
+
     # persistent cloud-fraction accumulator (the reference's self._qaz)
     def get_qaz(self):
         import torch

@@ -8,7 +8,8 @@
 //  * copy_dycore_to_physics                pySHiELD/update/update_atmos_state.py:95-142
 //
 // All are HBM-streaming work. The first is elementwise (one thread per point,
-// the fastest-varying storage dimension mapped to consecutive threads). The
+// the fastest-varying storage dimension mapped to consecutive threads), as
+// is the dycore-to-physics copy. The
 // other four are fused into one column-per-thread kernel that runs them in
 // the reference's order, so that the updated vapour, delp, pt and tendencies
 // pass from one stencil to the next in registers and L1 instead of HBM.
@@ -40,23 +41,42 @@ struct UpdArgs {
   double dt;
 };
 
+// One block row per (j, k) (or, with k fastest in memory, per (i, j)) line
+// of the domain and the threads along the line's contiguous dimension: the
+// index arithmetic is one 32-bit divide per row, and each point's loads are
+// all issued before its stores.
+struct Line {
+  int64_t i, j, k;
+};
+__device__ __forceinline__ bool line_point(int kfast, int nx, int ny, int nz, int64_t row, int64_t t, Line& p) {
+  if (kfast) {
+    if (t >= nz) return false;
+    p.k = t;
+    p.i = row % nx;
+    p.j = row / nx;
+  } else {
+    if (t >= nx) return false;
+    p.i = t;
+    p.j = row % ny;
+    p.k = row / ny;
+  }
+  return true;
+}
+
 __global__ void update_physics_state_kernel(const __grid_constant__ UpdArgs A) {
-  const int64_t n = (int64_t)A.nx * A.ny * A.nz;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    int64_t i, j, k;
-    if (A.kfast) {
-      k = e % A.nz;
-      const int64_t c = e / A.nz;
-      i = c % A.nx;
-      j = c / A.nx;
-    } else {
-      i = e % A.nx;
-      const int64_t r = e / A.nx;
-      j = r % A.ny;
-      k = r / A.ny;
+  const int64_t rows = A.kfast ? (int64_t)A.nx * A.ny : (int64_t)A.ny * A.nz;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int64_t row = blockIdx.y; row < rows; row += gridDim.y) {
+    Line q;
+    if (!line_point(A.kfast, A.nx, A.ny, A.nz, row, t, q)) continue;
+    double x[10], d[10];
+#pragma unroll
+    for (int p = 0; p < 10; ++p) {
+      x[p] = A.x[p].at(q.i, q.j, q.k);
+      d[p] = A.t[p].at(q.i, q.j, q.k);
     }
 #pragma unroll
-    for (int p = 0; p < 10; ++p) A.o[p].at(i, j, k) = A.x[p].at(i, j, k) + A.t[p].at(i, j, k) * A.dt;
+    for (int p = 0; p < 10; ++p) A.o[p].at(q.i, q.j, q.k) = x[p] + d[p] * A.dt;
   }
 }
 
@@ -176,26 +196,24 @@ struct D2PArgs {
 };
 
 __global__ void copy_dycore_to_physics_kernel(const __grid_constant__ D2PArgs A) {
-  const int64_t n = (int64_t)A.nx1 * A.ny1 * A.nz;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    int64_t i, j, k;
-    if (A.kfast) {
-      k = e % A.nz;
-      const int64_t c = e / A.nz;
-      i = c % A.nx1;
-      j = c / A.nx1;
-    } else {
-      i = e % A.nx1;
-      const int64_t r = e / A.nx1;
-      j = r % A.ny1;
-      k = r / A.ny1;
-    }
+  const int64_t rows = A.kfast ? (int64_t)A.nx1 * A.ny1 : (int64_t)A.ny1 * A.nz;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int64_t row = blockIdx.y; row < rows; row += gridDim.y) {
+    Line q;
+    if (!line_point(A.kfast, A.nx1, A.ny1, A.nz, row, t, q)) continue;
     double v[N_D2P];
 #pragma unroll
-    for (int p = 0; p < N_D2P; ++p) v[p] = A.in[p].at(i, j, k);
+    for (int p = 0; p < N_D2P; ++p) v[p] = A.in[p].at(q.i, q.j, q.k);
 #pragma unroll
-    for (int p = 0; p < N_D2P; ++p) A.out[p].at(i, j, k) = v[p];
+    for (int p = 0; p < N_D2P; ++p) A.out[p].at(q.i, q.j, q.k) = v[p];
   }
+}
+
+// 2-D launch over (line length, rows): 128 threads along a line, at most
+// 65,535 block rows (a grid-stride loop covers the rest)
+dim3 line_grid(int64_t len, int64_t rows) {
+  const int64_t bx = (len + 127) / 128;
+  return dim3((unsigned)bx, (unsigned)(rows < 65535 ? (rows > 0 ? rows : 1) : 65535));
 }
 
 int grid_for(int64_t n, int bs) {
@@ -227,8 +245,8 @@ extern "C" int shield_update_physics_state(int nx, int ny, int nz, const ShieldF
   A.nz = nz;
   A.kfast = (state10[0].sk == 1) ? 1 : 0;
   A.dt = dt;
-  const int64_t n = (int64_t)nx * ny * nz;
-  update_physics_state_kernel<<<grid_for(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(A);
+  const int64_t len = A.kfast ? nz : nx, rows = A.kfast ? (int64_t)nx * ny : (int64_t)ny * nz;
+  update_physics_state_kernel<<<line_grid(len, rows), 128, 0, static_cast<cudaStream_t>(stream)>>>(A);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     shield::set_last_error(std::string("shield_update_physics_state: ") + cudaGetErrorString(e));
@@ -299,8 +317,8 @@ extern "C" int shield_copy_dycore_to_physics(int nx, int ny, int nz, const Shiel
   A.ny1 = ny + 1;
   A.nz = nz;
   A.kfast = (physics16[0].sk == 1) ? 1 : 0;
-  const int64_t n = (int64_t)A.nx1 * A.ny1 * nz;
-  copy_dycore_to_physics_kernel<<<grid_for(n, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(A);
+  const int64_t len = A.kfast ? nz : A.nx1, rows = A.kfast ? (int64_t)A.nx1 * A.ny1 : (int64_t)A.ny1 * nz;
+  copy_dycore_to_physics_kernel<<<line_grid(len, rows), 128, 0, static_cast<cudaStream_t>(stream)>>>(A);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     shield::set_last_error(std::string("shield_copy_dycore_to_physics: ") + cudaGetErrorString(e));

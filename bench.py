@@ -443,6 +443,110 @@ def run_physics(n_cube=N_CUBE, nlev=79, dt=DT, reps=5):
     }
 
 
+def coupling_bytes(nx, ny, nz, h=HALO):
+    """Algorithmic HBM bytes of one shield_update_atmos_state launch with
+    apply_tendencies, each field read once and written once: fill_gfs_delp
+    reads delp and reads and writes the vapour on nz levels of every column
+    of the full domain; a compute column reads 22 more fields (the three
+    tendencies, physics-updated winds, temperature and five condensates, the
+    physics winds and temperature, six dycore tracers, prsi and the dycore
+    temperature) and writes 14 (the three tendencies, delp, six tracers,
+    temperature, pe, peln, pk), on nz + 1 levels."""
+    nk = nz + 1
+    ncomp = nx * ny
+    nfull = (nx + 2 * h) * (ny + 2 * h)
+    return 8 * (nfull * 3 * (nk - 1) + ncomp * 36 * nk)
+
+
+def run_coupling(n_cube=N_CUBE, nlev=79, dt=DT, reps=5):
+    """UpdateAtmosphereState.__call__ (fill_gfs_delp, prepare_tendencies_and_
+    update_tracers, moist_cv, update_pressure_and_surface_winds; one kernel)
+    at CN x nlev on random storages of plausible magnitudes; every call
+    starts from the same storages (restored outside the timed region)."""
+    import types
+
+    import numpy as np
+    import torch
+
+    from pyshield_b200._config import PhysicsConfig
+    from pyshield_b200.coupling import UpdateAtmosphereState
+    from pyshield_b200.grid import GridIndexing, StencilFactory
+    from pyshield_b200.quantity import Quantity
+
+    nx, ny = n_cube, 6 * n_cube
+    shape = (nx + 2 * HALO + 1, ny + 2 * HALO + 1, nlev + 1)
+    rng = np.random.default_rng(5)
+
+    def dev(a):
+        if a.ndim == 2:
+            return torch.from_numpy(np.ascontiguousarray(a.T)).cuda().t()
+        return torch.from_numpy(np.ascontiguousarray(a.transpose(2, 1, 0))).cuda().permute(2, 1, 0)
+
+    def q(a):
+        ext = (nx, ny, nlev) if a.ndim == 3 else (nx, ny)
+        org = (HALO, HALO, 0) if a.ndim == 3 else (HALO, HALO)
+        return Quantity(dev(a), ("x", "y", "z")[: a.ndim], "", org, ext)
+
+    def rnd(lo, hi):
+        return rng.uniform(lo, hi, shape)
+
+    f = {}
+    for nm in ("u_dt", "v_dt", "pt_dt"):
+        f[nm] = rng.normal(0.0, 1e-4, shape)
+    for nm in ("pu_ua", "pu_va", "ph_ua", "ph_va", "dy_ua", "dy_va"):
+        f[nm] = rnd(-30.0, 30.0)
+    for nm in ("pu_pt", "ph_pt", "dy_pt"):
+        f[nm] = rnd(200.0, 300.0)
+    for nm in ("qvapor", "qliquid", "qrain", "qsnow", "qice", "qgraupel"):
+        f["pu_" + nm] = rnd(0.0, 2e-3)
+        f["dy_" + nm] = rnd(0.0, 2e-3)
+    f["prsi"] = np.cumsum(rnd(50.0, 2000.0), axis=2)
+    f["dy_delp"] = rnd(50.0, 2000.0)
+    f["pe"] = np.zeros(shape)
+    f["pe"][..., 0] = 100.0
+    f["peln"] = np.zeros(shape)
+    f["pk"] = np.zeros(shape)
+    Q = {k: q(v) for k, v in f.items()}
+    pristine = {k: v.data.clone() for k, v in Q.items()}
+    del f
+    d = types.SimpleNamespace(
+        qvapor=Q["dy_qvapor"], qliquid=Q["dy_qliquid"], qrain=Q["dy_qrain"], qsnow=Q["dy_qsnow"],
+        qice=Q["dy_qice"], qgraupel=Q["dy_qgraupel"], delp=Q["dy_delp"], pt=Q["dy_pt"], pe=Q["pe"],
+        peln=Q["peln"], pk=Q["pk"], ua=Q["dy_ua"], va=Q["dy_va"], ps=q(np.zeros(shape[:2])),
+    )
+    p = types.SimpleNamespace(
+        physics_updated_ua=Q["pu_ua"], physics_updated_va=Q["pu_va"], physics_updated_pt=Q["pu_pt"],
+        physics_updated_specific_humidity=Q["pu_qvapor"], physics_updated_qliquid=Q["pu_qliquid"],
+        physics_updated_qrain=Q["pu_qrain"], physics_updated_qsnow=Q["pu_qsnow"], physics_updated_qice=Q["pu_qice"],
+        physics_updated_qgraupel=Q["pu_qgraupel"], ua=Q["ph_ua"], va=Q["ph_va"], pt=Q["ph_pt"], prsi=Q["prsi"],
+    )
+    uas = UpdateAtmosphereState(StencilFactory(GridIndexing(nx, ny, nlev, HALO)), None, PhysicsConfig(dt_atmos=int(dt)))
+    stream = torch.cuda.current_stream()
+    total = 0.0
+    for r in range(reps + 1):
+        for k, v in Q.items():
+            v.data.copy_(pristine[k])
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        uas(d, p, Q["u_dt"], Q["v_dt"], Q["pt_dt"], dt)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if r > 0:
+            total += e0.elapsed_time(e1)
+    ms = total / reps
+    nbytes = coupling_bytes(nx, ny, nlev)
+    peak, peak_kind = peaks()
+    achieved = nbytes / (ms / 1000.0) / 1e9
+    return {
+        "workload": f"UpdateAtmosphereState.__call__ column stencils, C{n_cube} ({nx * ny} columns) x L{nlev}, FP64",
+        "ms_per_step": ms,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "bytes_per_launch": nbytes,
+                     "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},
+        "note": "device time (CUDA events), mean of the timed calls; the storages are restored before each call",
+    }
+
+
 def max_over_ranks(values, world, device):
     """Each rank's device-measured times -> their maximum over all ranks (the
     slowest replica sets the job's time). One all-reduce; every rank calls it
@@ -647,6 +751,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the C48 adjoint-cost measurement")
     ap.add_argument("--no-physics", action="store_true", help="skip the Physics.__call__ measurement")
+    ap.add_argument("--no-coupling", action="store_true", help="skip the UpdateAtmosphereState measurement")
     ap.add_argument("--ncube", type=int, default=N_CUBE, help="cube size N of the CN workload (default 96)")
     ap.add_argument("--ensemble", action="store_true", help="run the ensemble workload instead")
     ap.add_argument("--members", type=int, default=64)
@@ -747,6 +852,8 @@ def main():
     adjoint = run_adjoint() if (rank == 0 and world == 1 and not args.no_adjoint and args.form == "plain") else None
     physics = (run_physics(n_cube=args.ncube, nlev=nlev)
                if (rank == 0 and world == 1 and not args.no_physics and args.form == "plain") else None)
+    coupling = (run_coupling(n_cube=args.ncube, nlev=nlev)
+                if (rank == 0 and world == 1 and not args.no_coupling and args.form == "plain") else None)
 
     if rank == 0:
         rec = {
@@ -781,6 +888,7 @@ def main():
             "clocks": r["clocks"],
             "adjoint": adjoint,
             "physics": physics,
+            "coupling": coupling,
         }
         emit(rec)
 

@@ -9,10 +9,10 @@
 //
 // All are HBM-streaming work. The first is elementwise (one thread per point,
 // the fastest-varying storage dimension mapped to consecutive threads), as
-// is the dycore-to-physics copy. The
-// other four are fused into one column-per-thread kernel that runs them in
-// the reference's order, so that the updated vapour, delp, pt and tendencies
-// pass from one stencil to the next in registers and L1 instead of HBM.
+// is the dycore-to-physics copy. The other four are fused into one kernel
+// over tiles of columns that runs them in the reference's order, so that the
+// updated vapour, delp, pt and tendencies pass from one stencil to the next
+// in registers and shared memory instead of HBM.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -93,95 +93,198 @@ struct AtmArgs {
   double CV_AIR, CV_VAP, C_LIQ, C_ICE;
 };
 
-__global__ void update_atmos_state_kernel(const __grid_constant__ AtmArgs A) {
+// The column stencils of UpdateAtmosphereState in one kernel. A block owns
+// a tile of AT_TC = 32 consecutive columns of the full domain (lane =
+// column: every level's accesses are coalesced in the i-fastest layout) and
+// AT_NW warps that share its levels. The pointwise work runs
+// level-parallel; the level-by-level recurrences run in one warp over
+// shared-memory columns, in the reference's order:
+//   1 (all warps)  the vapour and delp of every level into shared memory;
+//   2 (one warp)   fill_gfs_delp's three sweeps;
+//   3 (all warps)  the filled vapour back (full domain); on the compute
+//                  domain prepare_tendencies_and_update_tracers and moist_cv
+//                  level by level (moist_cv reads what prepare wrote at the
+//                  same level); the new delp into shared memory;
+//   4 (one warp)   update_pressure_and_surface_winds' pe sum;
+//   5 (all warps)  pe, peln, pk.
+constexpr int AT_TC = 32;
+constexpr int AT_NW = 8;
+
+template <int NKMAX>
+struct AtmSmem {
+  double q[NKMAX][AT_TC];   // the vapour fill_gfs_delp works on
+  double dp[NKMAX][AT_TC];  // the dycore delp it reads
+  double pe[NKMAX][AT_TC];  // prepare's new delp, then the interface pressure
+};
+
+template <int NKMAX>
+__global__ void __launch_bounds__(AT_TC * AT_NW) update_atmos_state_kernel(const __grid_constant__ AtmArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  AtmSmem<NKMAX>& S = *reinterpret_cast<AtmSmem<NKMAX>*>(smem_raw);
   const int nxf = A.nx + 2 * A.hx, nyf = A.ny + 2 * A.hx;
   const int64_t ncf = (int64_t)nxf * nyf;
   const int nk = A.nz + 1;  // the reference builds these stencils on nz + 1 levels
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncf; c += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = c % nxf - A.hx, j = c / nxf - A.hx;
-    // ---- fill_gfs_delp(delp, physics_updated_specific_humidity, 1e-9) on the full domain
-    const bool dycore_only = (A.mode & SHIELD_UAS_DYCORE_ONLY) != 0;
-    {
-      const F3& q = dycore_only ? A.f[D_QV] : A.f[PU_QV];
-      const F3& dp = A.f[D_DELP];
-      const double q_min = 1.0e-9;
-      double qn = q.at(i, j, nk - 2);  // BACKWARD interval(0, -2): reads the updated level below
-      double dpn = dp.at(i, j, nk - 2);
-      for (int k = nk - 3; k >= 0; --k) {
-        double qk = q.at(i, j, k);
-        const double dpk = dp.at(i, j, k);
-        if (qn < q_min) qk = qk + (qn - q_min) * dpn / dpk;
-        q.at(i, j, k) = qk;
-        qn = qk;
-        dpn = dpk;
-      }
-      // PARALLEL interval(1, -1) clamp, FORWARD interval(1, -1) borrow, FORWARD interval(0, -1) zero
-      double qprev = q.at(i, j, 0);  // level 0 is neither clamped nor borrowed into
-      double dprev = dp.at(i, j, 0);
-      if (qprev < 0.0) q.at(i, j, 0) = 0.0;
-      for (int k = 1; k < nk - 1; ++k) {
-        double qk = q.at(i, j, k);
-        const double dpk = dp.at(i, j, k);
-        if (qk < q_min) qk = q_min;
-        if (qprev < 0.0) qk = qk + qprev * (dprev) / (dpk);
-        qprev = qk;
-        dprev = dpk;
-        q.at(i, j, k) = (qk < 0.0) ? 0.0 : qk;
-      }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int64_t c = (int64_t)blockIdx.x * AT_TC + lane;
+  const bool live = c < ncf;
+  const int64_t i = live ? c % nxf - A.hx : 0, j = live ? c / nxf - A.hx : 0;
+  const bool compute = live && i >= 0 && j >= 0 && i < A.nx && j < A.ny;
+  const bool dycore_only = (A.mode & SHIELD_UAS_DYCORE_ONLY) != 0;
+  const bool apply = (A.mode & SHIELD_UAS_APPLY) != 0;
+  const F3* f = A.f;
+  const F3& Q = dycore_only ? f[D_QV] : f[PU_QV];
+  const F3& DP = f[D_DELP];
+
+  // ---- 1: fill_gfs_delp's inputs, levels 0 .. nk - 2
+  for (int k = w; k < nk - 1; k += AT_NW) {
+    if (live) {
+      S.q[k][lane] = Q.at(i, j, k);
+      S.dp[k][lane] = DP.at(i, j, k);
     }
-    if (dycore_only || i < 0 || j < 0 || i >= A.nx || j >= A.ny) continue;
-    // ---- prepare_tendencies_and_update_tracers, interval(0, -1) of nz + 1 levels
-    const F3* f = A.f;
-    double p_lo = f[PRSI].at(i, j, 0);
-    for (int k = 0; k < nk - 1; ++k) {
-      f[U_DT].at(i, j, k) = f[U_DT].at(i, j, k) + (f[U_T1].at(i, j, k) - f[U_T0].at(i, j, k)) * A.rdt;
-      f[V_DT].at(i, j, k) = f[V_DT].at(i, j, k) + (f[V_T1].at(i, j, k) - f[V_T0].at(i, j, k)) * A.rdt;
-      f[PT_DT].at(i, j, k) = f[PT_DT].at(i, j, k) + (f[PU_PT].at(i, j, k) - f[PT_T0].at(i, j, k)) * A.rdt;
-      const double p_hi = f[PRSI].at(i, j, k + 1);
-      const double dp = p_hi - p_lo;
-      p_lo = p_hi;
-      const double qwat_qv = dp * f[PU_QV].at(i, j, k);
-      const double qwat_ql = dp * f[PU_QL].at(i, j, k);
-      const double qwat_qr = dp * f[PU_QR].at(i, j, k);
-      const double qwat_qs = dp * f[PU_QS].at(i, j, k);
-      const double qwat_qi = dp * f[PU_QI].at(i, j, k);
-      const double qwat_qg = dp * f[PU_QG].at(i, j, k);
-      const double qt = qwat_qv + qwat_ql + qwat_qr + qwat_qs + qwat_qi + qwat_qg;
-      const double q_sum = f[D_QV].at(i, j, k) + f[D_QL].at(i, j, k) + f[D_QR].at(i, j, k) + f[D_QS].at(i, j, k) +
-                           f[D_QI].at(i, j, k) + f[D_QG].at(i, j, k);
-      const double q0 = f[D_DELP].at(i, j, k) * (1.0 - q_sum) + qt;
-      f[D_DELP].at(i, j, k) = q0;
-      f[D_QV].at(i, j, k) = qwat_qv / q0;
-      f[D_QL].at(i, j, k) = qwat_ql / q0;
-      f[D_QR].at(i, j, k) = qwat_qr / q0;
-      f[D_QS].at(i, j, k) = qwat_qs / q0;
-      f[D_QI].at(i, j, k) = qwat_qi / q0;
-      f[D_QG].at(i, j, k) = qwat_qg / q0;
+  }
+  __syncthreads();
+  // ---- 2: fill_gfs_delp(delp, q, 1e-9) (update_atmos_state.py:21-37)
+  if (w == 0 && live) {
+    const double q_min = 1.0e-9;
+    // BACKWARD interval(0, -2): borrow from the (updated) level below
+    double qn = S.q[nk - 2][lane];
+    double dpn = S.dp[nk - 2][lane];
+    for (int k = nk - 3; k >= 0; --k) {
+      double qk = S.q[k][lane];
+      const double dpk = S.dp[k][lane];
+      if (qn < q_min) qk = qk + (qn - q_min) * dpn / dpk;
+      S.q[k][lane] = qk;
+      qn = qk;
+      dpn = dpk;
     }
-    if (!(A.mode & SHIELD_UAS_APPLY)) continue;
-    // ---- moist_cv(dycore q..., dycore pt, t_dt = pt_dt, CP_AIR, dt) on nz + 1 levels
-    for (int k = 0; k < nk; ++k) {
-      const double ql = f[D_QL].at(i, j, k) + f[D_QR].at(i, j, k);
-      const double qs = f[D_QI].at(i, j, k) + f[D_QS].at(i, j, k) + f[D_QG].at(i, j, k);
+    // PARALLEL interval(1, -1) clamp, FORWARD interval(1, -1) borrow, FORWARD
+    // interval(0, -1) zero: the borrow chain runs on the unzeroed values
+    double qprev = S.q[0][lane];
+    double dprev = S.dp[0][lane];
+    if (qprev < 0.0) S.q[0][lane] = 0.0;
+    for (int k = 1; k < nk - 1; ++k) {
+      double qk = S.q[k][lane];
+      const double dpk = S.dp[k][lane];
+      if (qk < q_min) qk = q_min;
+      if (qprev < 0.0) qk = qk + qprev * (dprev) / (dpk);
+      qprev = qk;
+      dprev = dpk;
+      S.q[k][lane] = (qk < 0.0) ? 0.0 : qk;
+    }
+  }
+  __syncthreads();
+  // ---- 3: the filled vapour; prepare_tendencies_and_update_tracers and moist_cv.
+  // Every load of a level comes before its first store: the fields are
+  // separate storages, but the compiler cannot know that, and a store
+  // between two loads would make each group of loads wait for the last.
+  for (int k = w; k < nk; k += AT_NW) {
+    const bool filled = live && k < nk - 1;
+    if (dycore_only || !compute) {
+      if (filled) Q.at(i, j, k) = S.q[k][lane];
+      continue;
+    }
+    const bool prep = k < nk - 1;
+    // loads
+    double dq[6];
+    dq[0] = f[D_QV].at(i, j, k);
+    dq[1] = f[D_QL].at(i, j, k);
+    dq[2] = f[D_QR].at(i, j, k);
+    dq[3] = f[D_QS].at(i, j, k);
+    dq[4] = f[D_QI].at(i, j, k);
+    dq[5] = f[D_QG].at(i, j, k);
+    double pt_dt = f[PT_DT].at(i, j, k);
+    const double pt = apply ? f[D_PT].at(i, j, k) : 0.0;
+    double u_dt = 0.0, v_dt = 0.0, pq[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, dp = 0.0;
+    if (prep) {
+      u_dt = f[U_DT].at(i, j, k) + (f[U_T1].at(i, j, k) - f[U_T0].at(i, j, k)) * A.rdt;
+      v_dt = f[V_DT].at(i, j, k) + (f[V_T1].at(i, j, k) - f[V_T0].at(i, j, k)) * A.rdt;
+      pt_dt = pt_dt + (f[PU_PT].at(i, j, k) - f[PT_T0].at(i, j, k)) * A.rdt;
+      dp = f[PRSI].at(i, j, k + 1) - f[PRSI].at(i, j, k);
+      pq[0] = S.q[k][lane];
+      pq[1] = f[PU_QL].at(i, j, k);
+      pq[2] = f[PU_QR].at(i, j, k);
+      pq[3] = f[PU_QS].at(i, j, k);
+      pq[4] = f[PU_QI].at(i, j, k);
+      pq[5] = f[PU_QG].at(i, j, k);
+    }
+    // prepare_tendencies_and_update_tracers, interval(0, -1)
+    double q0 = 0.0;
+    if (prep) {
+      double qw[6];
+      for (int t = 0; t < 6; ++t) qw[t] = dp * pq[t];
+      const double qt = qw[0] + qw[1] + qw[2] + qw[3] + qw[4] + qw[5];
+      const double q_sum = dq[0] + dq[1] + dq[2] + dq[3] + dq[4] + dq[5];
+      q0 = S.dp[k][lane] * (1.0 - q_sum) + qt;
+      for (int t = 0; t < 6; ++t) dq[t] = qw[t] / q0;
+    }
+    // moist_cv(dycore q..., dycore pt, t_dt = pt_dt, CP_AIR, dt), nz + 1 levels
+    double pt_new = 0.0;
+    if (apply) {
+      const double ql = dq[1] + dq[2];
+      const double qs = dq[4] + dq[3] + dq[5];
       const double gz = ql + qs;
-      const double qv = f[D_QV].at(i, j, k);
+      const double qv = dq[0];
       const double cvm = (1.0 - (qv + gz)) * A.CV_AIR + qv * A.CV_VAP + ql * A.C_LIQ + qs * A.C_ICE;
-      f[D_PT].at(i, j, k) = f[D_PT].at(i, j, k) + f[PT_DT].at(i, j, k) * A.dt * A.cp_air / cvm;
+      pt_new = pt + pt_dt * A.dt * A.cp_air / cvm;
+    }
+    // stores
+    if (filled) Q.at(i, j, k) = S.q[k][lane];
+    if (prep) {
+      f[U_DT].at(i, j, k) = u_dt;
+      f[V_DT].at(i, j, k) = v_dt;
+      f[D_DELP].at(i, j, k) = q0;
+      S.pe[k][lane] = q0;
+      f[D_QV].at(i, j, k) = dq[0];
+      f[D_QL].at(i, j, k) = dq[1];
+      f[D_QR].at(i, j, k) = dq[2];
+      f[D_QS].at(i, j, k) = dq[3];
+      f[D_QI].at(i, j, k) = dq[4];
+      f[D_QG].at(i, j, k) = dq[5];
+    }
+    if (apply) {
+      f[D_PT].at(i, j, k) = pt_new;
       f[PT_DT].at(i, j, k) = 0.0;
+    } else if (prep) {
+      f[PT_DT].at(i, j, k) = pt_dt;
     }
-    // ---- update_pressure_and_surface_winds on nz + 1 levels
+  }
+  if (dycore_only || !apply) return;  // block-uniform: the mode is the launch's
+  __syncthreads();
+  // ---- 4: update_pressure_and_surface_winds' sum, pe[k] = pe[k - 1] + delp[k - 1]
+  if (w == 0 && compute) {
     double pe = f[PE].at(i, j, 0);
+    double dprev = S.pe[0][lane];
     for (int k = 1; k < nk; ++k) {
-      pe = pe + f[D_DELP].at(i, j, k - 1);
-      f[PE].at(i, j, k) = pe;
-      const double peln = log(pe);
-      f[PELN].at(i, j, k) = peln;
-      f[PK].at(i, j, k) = exp(A.kappa * peln);
+      pe = pe + dprev;
+      dprev = k < nk - 1 ? S.pe[k][lane] : 0.0;
+      S.pe[k][lane] = pe;
     }
-    A.ps.at(i, j, 0) = pe;
+  }
+  __syncthreads();
+  // ---- 5: pe, peln, pk on levels 1 .. nk - 1; ps and the surface winds
+  for (int k = 1 + w; k < nk; k += AT_NW) {
+    if (!compute) continue;
+    const double pe = S.pe[k][lane];
+    f[PE].at(i, j, k) = pe;
+    const double peln = log(pe);
+    f[PELN].at(i, j, k) = peln;
+    f[PK].at(i, j, k) = exp(A.kappa * peln);
+  }
+  if (w == 0 && compute) {
+    A.ps.at(i, j, 0) = S.pe[nk - 1][lane];
     A.us.at(i, j, 0) = f[D_UA].at(i, j, nk - 2);
     A.vs.at(i, j, 0) = f[D_VA].at(i, j, nk - 2);
   }
+}
+
+template <int NKMAX>
+cudaError_t launch_atmos(const AtmArgs& A, int64_t ncf, cudaStream_t st) {
+  const size_t smem = sizeof(AtmSmem<NKMAX>);
+  auto kern = update_atmos_state_kernel<NKMAX>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<(unsigned)((ncf + AT_TC - 1) / AT_TC), AT_TC * AT_NW, smem, st>>>(A);
+  return cudaGetLastError();
 }
 
 // DycoreToPhysics' copy of 16 fields (update_atmos_state.py:95-142, built at
@@ -214,11 +317,6 @@ __global__ void copy_dycore_to_physics_kernel(const __grid_constant__ D2PArgs A)
 dim3 line_grid(int64_t len, int64_t rows) {
   const int64_t bx = (len + 127) / 128;
   return dim3((unsigned)bx, (unsigned)(rows < 65535 ? (rows > 0 ? rows : 1) : 65535));
-}
-
-int grid_for(int64_t n, int bs) {
-  int64_t nb = (n + bs - 1) / bs;
-  return (int)(nb < 148 * 32 ? (nb > 0 ? nb : 1) : 148 * 32);
 }
 
 }  // namespace
@@ -262,6 +360,10 @@ extern "C" int shield_update_atmos_state(int nx, int ny, int nz, int hx, int mod
     shield::set_last_error("shield_update_atmos_state: bad arguments");
     return SHIELD_EINVAL;
   }
+  if (nz > 128) {
+    shield::set_last_error("shield_update_atmos_state: nz > 128 is not supported");
+    return SHIELD_ELAYOUT;
+  }
   AtmArgs A;
   for (int p = 0; p < N_ATM; ++p) {
     if (!f[p].ptr) {
@@ -289,8 +391,9 @@ extern "C" int shield_update_atmos_state(int nx, int ny, int nz, int hx, int mod
   A.C_LIQ = 4.1855e3;
   A.C_ICE = 1972.0;
   const int64_t ncf = (int64_t)(nx + 2 * hx) * (ny + 2 * hx);
-  update_atmos_state_kernel<<<grid_for(ncf, 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(A);
-  cudaError_t e = cudaGetLastError();
+  const int nk = nz + 1;
+  cudaError_t e = nk <= 96 ? launch_atmos<96>(A, ncf, static_cast<cudaStream_t>(stream))
+                           : launch_atmos<129>(A, ncf, static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) {
     shield::set_last_error(std::string("shield_update_atmos_state: ") + cudaGetErrorString(e));
     return SHIELD_ECUDA;

@@ -107,14 +107,17 @@ struct AtmArgs {
 //                  same level); the new delp into shared memory;
 //   4 (one warp)   update_pressure_and_surface_winds' pe sum;
 //   5 (all warps)  pe, peln, pk.
+// Four warps per block and 49 KB of shared memory let three or four blocks
+// share an SM, so one block's loads overlap another's one-warp recurrences.
 constexpr int AT_TC = 32;
-constexpr int AT_NW = 8;
+constexpr int AT_NW = 4;
 
 template <int NKMAX>
 struct AtmSmem {
   double q[NKMAX][AT_TC];   // the vapour fill_gfs_delp works on
-  double dp[NKMAX][AT_TC];  // the dycore delp it reads
-  double pe[NKMAX][AT_TC];  // prepare's new delp, then the interface pressure
+  double dp[NKMAX][AT_TC];  // the dycore delp it reads; then prepare's new
+                            // delp (each level's thread replaces its own);
+                            // then the interface pressure
 };
 
 template <int NKMAX>
@@ -214,7 +217,7 @@ __global__ void __launch_bounds__(AT_TC * AT_NW) update_atmos_state_kernel(const
       for (int t = 0; t < 6; ++t) qw[t] = dp * pq[t];
       const double qt = qw[0] + qw[1] + qw[2] + qw[3] + qw[4] + qw[5];
       const double q_sum = dq[0] + dq[1] + dq[2] + dq[3] + dq[4] + dq[5];
-      q0 = S.dp[k][lane] * (1.0 - q_sum) + qt;
+      q0 = S.dp[k][lane] * (1.0 - q_sum) + qt;  // the old delp, read before the store below
       for (int t = 0; t < 6; ++t) dq[t] = qw[t] / q0;
     }
     // moist_cv(dycore q..., dycore pt, t_dt = pt_dt, CP_AIR, dt), nz + 1 levels
@@ -233,7 +236,7 @@ __global__ void __launch_bounds__(AT_TC * AT_NW) update_atmos_state_kernel(const
       f[U_DT].at(i, j, k) = u_dt;
       f[V_DT].at(i, j, k) = v_dt;
       f[D_DELP].at(i, j, k) = q0;
-      S.pe[k][lane] = q0;
+      S.dp[k][lane] = q0;
       f[D_QV].at(i, j, k) = dq[0];
       f[D_QL].at(i, j, k) = dq[1];
       f[D_QR].at(i, j, k) = dq[2];
@@ -253,25 +256,25 @@ __global__ void __launch_bounds__(AT_TC * AT_NW) update_atmos_state_kernel(const
   // ---- 4: update_pressure_and_surface_winds' sum, pe[k] = pe[k - 1] + delp[k - 1]
   if (w == 0 && compute) {
     double pe = f[PE].at(i, j, 0);
-    double dprev = S.pe[0][lane];
+    double dprev = S.dp[0][lane];
     for (int k = 1; k < nk; ++k) {
       pe = pe + dprev;
-      dprev = k < nk - 1 ? S.pe[k][lane] : 0.0;
-      S.pe[k][lane] = pe;
+      dprev = k < nk - 1 ? S.dp[k][lane] : 0.0;
+      S.dp[k][lane] = pe;
     }
   }
   __syncthreads();
   // ---- 5: pe, peln, pk on levels 1 .. nk - 1; ps and the surface winds
   for (int k = 1 + w; k < nk; k += AT_NW) {
     if (!compute) continue;
-    const double pe = S.pe[k][lane];
+    const double pe = S.dp[k][lane];
     f[PE].at(i, j, k) = pe;
     const double peln = log(pe);
     f[PELN].at(i, j, k) = peln;
     f[PK].at(i, j, k) = exp(A.kappa * peln);
   }
   if (w == 0 && compute) {
-    A.ps.at(i, j, 0) = S.pe[nk - 1][lane];
+    A.ps.at(i, j, 0) = S.dp[nk - 1][lane];
     A.us.at(i, j, 0) = f[D_UA].at(i, j, nk - 2);
     A.vs.at(i, j, 0) = f[D_VA].at(i, j, nk - 2);
   }

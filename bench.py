@@ -262,7 +262,11 @@ def run_adjoint(nsteps_window=8, reps=5, n_cube=48, nlev=79, dt=150.0):
 
 
 E2E_IN = ("pt", "qvapor", "qliquid", "qrain", "qice", "qsnow", "qgraupel", "qcld", "ua", "va", "delprsi", "delz",
-          "wmp", "pt_dt", "qv_dt", "ql_dt", "qr_dt", "qi_dt", "qs_dt", "qg_dt", "qa_dt", "udt", "vdt")
+          "wmp")
+# The tendencies start every step at zero: Physics.__call__'s
+# prepare_microphysics zeroes them on the device before the microphysics
+# (physics.py:133-143), so a host never uploads them.
+E2E_ZERO = ("pt_dt", "qv_dt", "ql_dt", "qr_dt", "qi_dt", "qs_dt", "qg_dt", "qa_dt", "udt", "vdt")
 E2E_OUT = ("pt_dt", "qv_dt", "ql_dt", "qr_dt", "qi_dt", "qs_dt", "qg_dt", "qa_dt", "udt", "vdt", "wmp")
 
 
@@ -270,11 +274,13 @@ class HostPipeline:
     """The step driven from host memory, as a host that keeps its state on
     the CPU would drive it.
 
-    Every step uploads its 23 input fields and the land mask from pinned host
+    Every step uploads its 13 state fields and the land mask from pinned host
     memory (one contiguous DMA, fields in the host's (k, j, i) array order),
-    scatters them into the device storages, calls ``mp(ms, dt)`` (the public
-    API), gathers the 11 result fields and the 4 precipitation totals into one
-    device buffer and downloads it into pinned host memory (one DMA).
+    scatters them into the device storages, zeroes the 10 tendencies on the
+    device (as the physics driver does before the microphysics), calls
+    ``mp(ms, dt)`` (the public API), gathers the 11 result fields and the 4
+    precipitation totals into one device buffer and downloads it into pinned
+    host memory (one DMA).
 
     Uploads and downloads run on their own streams with two staging buffers
     each way, so step s+1's upload and step s-1's download overlap step s's
@@ -329,6 +335,8 @@ class HostPipeline:
                 getattr(self.ms, f).view.copy_(self._field(self.d_in[b], i))
             self.land.view.copy_(self.d_in[b][len(E2E_IN) * self.plane:].view(ny, nx).t())
             scat_done[b].record(comp)
+            for t in E2E_ZERO:
+                getattr(self.ms, t).data.zero_()
             self.mp(self.ms, DT)
             if s >= 2:
                 comp.wait_event(down_done[b])
@@ -871,7 +879,11 @@ def main():
             "data": "synthetic",
             "config": config,
             "e2e": ({"value": e2e_value, "unit": "column-steps/s", "h2d_bytes_per_step": r["h2d"],
-                     "d2h_bytes_per_step": r["d2h"]} if e2e_value else None),
+                     "d2h_bytes_per_step": r["d2h"],
+                     "note": "pinned host buffers through Microphysics.__call__: uploads the 13 state fields and "
+                             "land, zeroes the 10 tendencies on the device (the physics driver's "
+                             "prepare_microphysics), downloads the 10 tendencies, wmp and 4 surface totals"}
+                    if e2e_value else None),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
                          "traffic": NCU_TRAFFIC_RATIO * bytes_launch if nlev == 79 and args.form == "plain" else None,

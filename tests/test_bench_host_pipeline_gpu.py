@@ -1,9 +1,10 @@
 """bench.py's end-to-end leg computes what a direct step computes.
 
-HostPipeline uploads every step's inputs from pinned host memory, steps, and
-downloads the results, with the copies on their own streams overlapping the
-neighbouring steps. Every step re-uploads the same inputs, so each download
-must equal the result of one step on the device-resident state.
+HostPipeline uploads every step's state fields from pinned host memory,
+zeroes the tendencies on the device, steps, and downloads the results, with
+the copies on their own streams overlapping the neighbouring steps. Every
+step re-uploads the same inputs, so each download must equal the result of
+one step on the device-resident state.
 """
 import numpy as np
 import pytest
@@ -30,6 +31,8 @@ def test_host_pipeline_downloads_match_direct_step():
     for s in range(steps):
         for f in bench.E2E_IN:
             getattr(ms, f).view.copy_(host[f].permute(2, 1, 0).to(dev))
+        for t in bench.E2E_ZERO:
+            getattr(ms, t).data.zero_()
         mp(ms, bench.DT)
         ref[s % 2] = ({f: getattr(ms, f).view.permute(2, 1, 0).contiguous().cpu().numpy() for f in bench.E2E_OUT},
                       mp._precip.cpu().numpy())

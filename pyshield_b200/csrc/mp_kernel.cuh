@@ -875,7 +875,7 @@ SHD void icloud(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid,
     if (rec) *rec = S;
     if constexpr (MIXED)
       subgrid_z_proc<double, float>(K, P.h_var, P.rh_adj, P.rh_rain, qa, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac,
-                                    P.p1);
+                                    P.p1, &KF);
     else
       subgrid_z_proc(K, P.h_var, P.rh_adj, P.rh_rain, qa, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac, P.p1);
   }

@@ -31,6 +31,9 @@ struct MpConst {
 
 // FP32 copies of the constants the mixed form's process rates use.
 struct MpConstF {
+  // FP64 constants of the mixed form's saturation adjustment (qsat_m)
+  double qs_e00, qw_c1, qw_c2, qw_c3, qi_c1, qi_c2, qi_c3, qs_t0, qs_tmin, qs_thi, qi_lo, qi_lo_dq;
+  double qs_rtw;  // 1 / (tice - t_wfr) of the saturation adjustment
   float E00, DC_VAP, LV0, D2ICE, LI2, RVGAS, TICE, T_SAT_MIN, iqs_lo_num, LAT2;
   float cracs, csacr, cgacr, cgacs, acco[3][4], csacw, csaci, cgacw, cgaci, cracw, cssub[5], crevp[5], cgfr[2],
       csmlt[5], cgmlt[5], ces0, log_10, fac_rc, so3, dt_rain, dts, rdts, fac_i2s;

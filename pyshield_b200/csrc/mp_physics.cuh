@@ -14,6 +14,7 @@
 #include <cstdint>
 #ifndef __CUDACC__
 #include <cmath>
+#include <type_traits>
 #endif
 
 #include "mp_params.h"
@@ -279,24 +280,107 @@ template <>
 SHP float rlog<float>(float x) { return logf(x); }
 SHP float sq(float x) { return x * x; }
 
+// The heat capacity of the saturation adjustment's latent-heat steps. The
+// FP64 step divides by it at every use, as the reference does; the mixed
+// form keeps its reciprocal and multiplies (FP64 either way).
+template <typename T, bool RECIPROCAL>
+struct HeatCap {
+  T cvm, rc;
+  SHP void set(T c) {
+    cvm = c;
+    if constexpr (RECIPROCAL) rc = T(1.0) / c;
+  }
+  SHP T div(T a) const {
+    if constexpr (RECIPROCAL)
+      return a * rc;
+    else
+      return a / cvm;
+  }
+};
+
+// The mixed form's saturation humidities, still in FP64: wqs1/wqs2 (ice =
+// 0) and iqs1/iqs2 (ice = 1) of microphysics_funcs.py:52-145 restated. With
+// c1 = Dc / Rv, c2 = L / Rv and c3 = c2 / T0 - c1 ln T0,
+//   exp((Dc ln(T / T0) + L (T - T0) / (T T0)) / Rv) = exp(c1 ln T + c3 - c2 / T),
+//   qs = (E00 / Rv) exp(...) / (T den),   dqs/dT = qs (c1 + c2 / T) / T,
+// so one reciprocal of T replaces the four divisions (the caller supplies
+// 1 / den). The ice form's branches are iqs1's: below T_SAT_MIN the fixed
+// value, above T0 the water form at min(T, T0 + 102). Equal to the
+// reference's expressions to FP64 round-off (not bit for bit).
+struct QsM {
+  double q, dq;
+};
+SHIELD_MATH_ATTR QsM qsat_m(const MpConstF& F, int ice, double ta, double rden) {
+  double c1 = F.qw_c1, c2 = F.qw_c2, c3 = F.qw_c3;
+  if (ice) {
+    if (ta < F.qs_t0) {
+      if (!(ta >= F.qs_tmin)) {
+        const double q = F.qi_lo * rden;
+        return QsM{q, q * F.qi_lo_dq};
+      }
+      c1 = F.qi_c1;
+      c2 = F.qi_c2;
+      c3 = F.qi_c3;
+    } else if (!(ta <= F.qs_thi)) {
+      ta = F.qs_thi;
+    }
+  }
+  const double r = 1.0 / ta;
+  const double q = F.qs_e00 * exp(c1 * log(ta) + c3 - c2 * r) * r * rden;
+  return QsM{q, q * r * (c1 + c2 * r)};
+}
+
 // ---------------------------------------------------- microphysics_funcs.py:431-850
 // R is the type of the deposition/sublimation and Bigg-freezing rate
 // expressions (T for the FP64 step; float for the mixed form). Every
 // saturation humidity, latent-heat temperature step and state update stays
-// in T.
+// in T. The mixed form (R = float, which passes KF) evaluates the saturation
+// humidities with qsat_m and the latent-heat steps with the heat capacity's
+// reciprocal, both FP64.
 template <typename T, typename R = T>
 SHP void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh_rain, T& qaz, T& qgz, T& qiz,
-                        T& qlz, T& qrz, T& qsz, T& qvz, T& tz, T den, T denfac, T p1) {
+                        T& qlz, T& qrz, T& qsz, T& qvz, T& tz, T den, T denfac, T p1,
+                        const MpConstF* KF = nullptr) {
+  constexpr bool FAST = std::is_same<R, float>::value;
   const T tice = K.tice, t_wfr = K.t_wfr, t_sub = K.t_sub;
+  T rden = T(0.0);
+  if constexpr (FAST) rden = 1.0 / den;
+  // the saturation humidities (and derivatives) over water and ice
+  auto qs_w = [&](T ta, T* dqdt) -> T {
+    if constexpr (FAST) {
+      const QsM r = qsat_m(*KF, 0, ta, rden);
+      if (dqdt) *dqdt = r.dq;
+      return r.q;
+    } else {
+      return dqdt ? wqs2(K, ta, den, *dqdt) : wqs1(K, ta, den);
+    }
+  };
+  auto qs_i = [&](T ta, T* dqdt) -> T {
+    if constexpr (FAST) {
+      const QsM r = qsat_m(*KF, 1, ta, rden);
+      if (dqdt) *dqdt = r.dq;
+      return r.q;
+    } else {
+      return dqdt ? iqs2(K, ta, den, *dqdt) : iqs1(K, ta, den);
+    }
+  };
+  HeatCap<T, FAST> H;
+  // x / (tice - t_wfr): a product with the reciprocal in the mixed form
+  auto over_tw = [&](T x) -> T {
+    if constexpr (FAST)
+      return x * KF->qs_rtw;
+    else
+      return x / (tice - t_wfr);
+  };
   T lhl = K.lv00 + K.d0_vap * tz;
   T lhi = K.LI00 + K.DC_ICE * tz;
   T q_liq = qlz + qrz;
   T q_sol = qiz + qsz + qgz;
-  T cvm = cvm_of(K, qvz, q_liq, q_sol);
-  T lcpk = lhl / cvm;
-  T icpk = lhi / cvm;
+  H.set(cvm_of(K, qvz, q_liq, q_sol));
+  T lcpk = H.div(lhl);
+  T icpk = H.div(lhi);
   T tcpk = lcpk + icpk;
-  T tcp3 = lcpk + icpk * fmin(1.0, dim(tice, tz) / (tice - t_wfr));
+  T tcp3 = lcpk + icpk * fmin(1.0, over_tw(dim(tice, tz)));
   (void)tcpk;
   if (!(p1 >= P_MIN)) return;
   if (tz < K.T_MIN) {
@@ -304,23 +388,27 @@ SHP void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
     qvz = qvz - sink;
     qiz = qiz + sink;
     q_sol = q_sol + sink;
-    cvm = cvm_of(K, qvz, q_liq, q_sol);
-    tz = tz + sink * (lhl + lhi) / cvm;
+    H.set(cvm_of(K, qvz, q_liq, q_sol));
+    tz = tz + H.div(sink * (lhl + lhi));
     if (!K.do_qa) qaz = qaz + 1.0;
     return;
   }
   lhl = K.lv00 + K.d0_vap * tz;
   lhi = K.LI00 + K.DC_ICE * tz;
-  lcpk = lhl / cvm;
-  icpk = lhi / cvm;
+  lcpk = H.div(lhl);
+  icpk = H.div(lhi);
   tcpk = lcpk + icpk;
-  tcp3 = lcpk + icpk * fmin(1.0, dim(tice, tz) / (tice - t_wfr));
+  tcp3 = lcpk + icpk * fmin(1.0, over_tw(dim(tice, tz)));
   T qpz = qvz + qlz + qiz;
   T tin = tz - (lhl * (qlz + qiz) + lhi * qiz) / (K.c_air + qpz * K.c_vap + qrz * K.C_LIQ + (qsz + qgz) * K.C_ICE);
   bool warm = tin > t_sub + 6.0;
   if (warm) {
-    T rh = qpz / iqs1(K, tin, den);
-    if (rh < rh_adj) {
+    bool dry;
+    if constexpr (FAST)
+      dry = qpz < rh_adj * qs_i(tin, nullptr);  // qs > 0: rh < rh_adj without the division
+    else
+      dry = qpz / qs_i(tin, nullptr) < rh_adj;
+    if (dry) {
       tz = tin;
       qvz = qpz;
       qlz = 0.0;
@@ -330,7 +418,7 @@ SHP void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
   }
   // cloud water <-> vapour adjustment (:531-554)
   T dwsdt;
-  T qsw = wqs2(K, tz, den, dwsdt);
+  T qsw = qs_w(tz, &dwsdt);
   T dq0 = qsw - qvz;
   T evap;
   if (dq0 > 0.0) {
@@ -342,10 +430,10 @@ SHP void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
   qvz = qvz + evap;
   qlz = qlz - evap;
   q_liq = q_liq - evap;
-  cvm = cvm_of(K, qvz, q_liq, q_sol);
-  tz = tz - evap * lhl / cvm;
+  H.set(cvm_of(K, qvz, q_liq, q_sol));
+  tz = tz - H.div(evap * lhl);
   lhi = K.LI00 + K.DC_ICE * tz;
-  icpk = lhi / cvm;
+  icpk = H.div(lhi);
   // forced freezing below t_wfr (:560-575)
   T dtmp = t_wfr - tz;
   if ((dtmp > 0.0) && (qlz > QCMIN)) {
@@ -354,11 +442,11 @@ SHP void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
     qiz = qiz + sink;
     q_liq = q_liq - sink;
     q_sol = q_sol + sink;
-    cvm = cvm_of(K, qvz, q_liq, q_sol);
-    tz = tz + sink * lhi / cvm;
+    H.set(cvm_of(K, qvz, q_liq, q_sol));
+    tz = tz + H.div(sink * lhi);
   }
   lhi = K.LI00 + K.DC_ICE * tz;
-  icpk = lhi / cvm;
+  icpk = H.div(lhi);
   // Bigg mechanism (:581-605)
   T dt_pisub;
   if (K.fast_sat_adj) {
@@ -373,19 +461,19 @@ SHP void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
       qiz = qiz + sink;
       q_liq = q_liq - sink;
       q_sol = q_sol + sink;
-      cvm = cvm_of(K, qvz, q_liq, q_sol);
-      tz = tz + sink * lhi / cvm;
+      H.set(cvm_of(K, qvz, q_liq, q_sol));
+      tz = tz + H.div(sink * lhi);
     }
   }
   lhl = K.lv00 + K.d0_vap * tz;
   lhi = K.LI00 + K.DC_ICE * tz;
-  lcpk = lhl / cvm;
-  icpk = lhi / cvm;
+  lcpk = H.div(lhl);
+  icpk = H.div(lhi);
   tcpk = lcpk + icpk;
   // ice deposition / sublimation (:614-661)
   if (tz < tice) {
     T dqsdt;
-    T qsi = iqs2(K, tz, den, dqsdt);
+    T qsi = qs_i(tz, &dqsdt);
     T dq = qvz - qsi;
     T sink = dq / (1.0 + tcpk * dqsdt);
     T pidep;
@@ -397,7 +485,11 @@ SHP void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
     }
     if (dq > 0.0) {
       T tmp = tice - tz;
-      T qi_crt = K.qi_gen * fmin(K.qi_lim, 0.1 * tmp) / den;
+      T qi_crt = K.qi_gen * fmin(K.qi_lim, 0.1 * tmp);
+      if constexpr (FAST)
+        qi_crt = qi_crt * rden;
+      else
+        qi_crt = qi_crt / den;
       sink = fmin(sink, fmin(fmax(qi_crt - qiz, pidep), tmp / tcpk));
     } else {
       pidep = pidep * fmin(1.0, dim(tz, t_sub) * 0.2);
@@ -406,18 +498,18 @@ SHP void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
     qvz = qvz - sink;
     qiz = qiz + sink;
     q_sol = q_sol + sink;
-    cvm = cvm_of(K, qvz, q_liq, q_sol);
-    tz = tz + sink * (lhl + lhi) / cvm;
+    H.set(cvm_of(K, qvz, q_liq, q_sol));
+    tz = tz + H.div(sink * (lhl + lhi));
   }
   lhl = K.lv00 + K.d0_vap * tz;
   lhi = K.LI00 + K.DC_ICE * tz;
-  lcpk = lhl / cvm;
-  icpk = lhi / cvm;
+  lcpk = H.div(lhl);
+  icpk = H.div(lhi);
   tcpk = lcpk + icpk;
   // snow sublimation / deposition (:670-706)
   if (qsz > QRMIN) {
     T dqsdt;
-    T qsi = iqs2(K, tz, den, dqsdt);
+    T qsi = qs_i(tz, &dqsdt);
     T qden = qsz * den;
     const R qdr = R(qden);
     const R tmp = rexp(R(0.65625) * rlog(qdr));
@@ -438,18 +530,18 @@ SHP void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
     qsz = qsz - pssub;
     qvz = qvz + pssub;
     q_sol = q_sol - pssub;
-    cvm = cvm_of(K, qvz, q_liq, q_sol);
-    tz = tz - pssub * (lhl + lhi) / cvm;
+    H.set(cvm_of(K, qvz, q_liq, q_sol));
+    tz = tz - H.div(pssub * (lhl + lhi));
   }
   lhl = K.lv00 + K.d0_vap * tz;
   lhi = K.LI00 + K.DC_ICE * tz;
-  lcpk = lhl / cvm;
-  icpk = lhi / cvm;
+  lcpk = H.div(lhl);
+  icpk = H.div(lhi);
   tcpk = lcpk + icpk;
   // graupel sublimation / deposition (:715-746)
   if (qgz > QRMIN) {
     T dqsdt;
-    T qsi = iqs2(K, tz, den, dqsdt);
+    T qsi = qs_i(tz, &dqsdt);
     T dq = (qvz - qsi) / (1.0 + tcpk * dqsdt);
     T pgsub = (qvz / qsi - 1.0) * qgz;
     if (pgsub > 0.0) {
@@ -463,26 +555,26 @@ SHP void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
     qgz = qgz + pgsub;
     qvz = qvz - pgsub;
     q_sol = q_sol + pgsub;
-    cvm = cvm_of(K, qvz, q_liq, q_sol);
-    tz = tz + pgsub * (lhl + lhi) / cvm;
+    H.set(cvm_of(K, qvz, q_liq, q_sol));
+    tz = tz + H.div(pgsub * (lhl + lhi));
   }
   // minimum evaporation of rain (:751-769)
   lhl = K.lv00 + K.d0_vap * tz;
-  lcpk = lhl / cvm;
+  lcpk = H.div(lhl);
   if (qrz > QCMIN) {
     T dqsdt;
-    T qsw2 = wqs2(K, tz, den, dqsdt);
+    T qsw2 = qs_w(tz, &dqsdt);
     T sink = fmin(qrz, dim(rh_rain * qsw2, qvz) / (1.0 + lcpk * dqsdt));
     qvz = qvz + sink;
     qrz = qrz - sink;
     q_liq = q_liq - sink;
-    cvm = cvm_of(K, qvz, q_liq, q_sol);
-    tz = tz - sink * lhl / cvm;
+    H.set(cvm_of(K, qvz, q_liq, q_sol));
+    tz = tz - H.div(sink * lhl);
   }
   // cloud fraction (:774-848)
   lhl = K.lv00 + K.d0_vap * tz;
-  cvm = K.c_air + (qvz + q_liq + q_sol) * K.c_vap;
-  lcpk = lhl / cvm;
+  H.set(K.c_air + (qvz + q_liq + q_sol) * K.c_vap);
+  lcpk = H.div(lhl);
   if (!K.do_qa) {
     q_sol = K.rad_snow ? qiz + qsz : qiz;
     q_liq = K.rad_rain ? qlz + qrz : qlz;
@@ -491,17 +583,17 @@ SHP void subgrid_z_proc(const MpConst& K, double h_var, double rh_adj, double rh
     T tin2 = tz - (lcpk * q_cond + icpk * q_sol);
     T qstar;
     if (tin2 <= t_wfr) {
-      qstar = iqs1(K, tin2, den);
+      qstar = qs_i(tin2, nullptr);
     } else if (tin2 >= tice) {
-      qstar = wqs1(K, tin2, den);
+      qstar = qs_w(tin2, nullptr);
     } else {
-      T qsi = iqs1(K, tin2, den);
-      T qsw3 = wqs1(K, tin2, den);
+      T qsi = qs_i(tin2, nullptr);
+      T qsw3 = qs_w(tin2, nullptr);
       T rqi;
       if (q_cond > 3.0e-6)
         rqi = q_sol / q_cond;
       else
-        rqi = (tice - tin2) / (tice - t_wfr);
+        rqi = over_tw(tice - tin2);
       qstar = rqi * qsi + (1.0 - rqi) * qsw3;
     }
     if (qpz2 > QRMIN) {

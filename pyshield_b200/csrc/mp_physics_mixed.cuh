@@ -174,7 +174,7 @@ SHD void icloud_processes_m(const MpConst& K, const MpConstF& F, double& qgz, do
   const float denf = (float)den, denfacf = (float)denfac, dtsf = F.dts;
   const float vtg = (float)vtgz, vtr = (float)vtrz, vts = (float)vtsz;
   double lhi = K.LI00 + K.DC_ICE * tz;
-  double icpk = lhi / cvm;
+  double rcpk = cvm / lhi;  // 1 / icpk: every use of icpk here divides by it
   if (!(p1 >= P_MIN)) return;
   double tc = tz - tice;
   if (tc >= 0.0) {
@@ -197,7 +197,7 @@ SHD void icloud_processes_m(const MpConst& K, const MpConstF& F, double& qgz, do
                                   (F.csmlt[2] * sqrtf(qsrho) + F.csmlt[3] * powf(qsrho, 0.65625f) * sqrtf(denfacf)) +
                               F.csmlt[4] * tcf * (psacw + psacr);
       const double psmlt = fmax(0.0, (double)smlt_rate);
-      const double sink = fmin(qsz, fmin(dts * (psmlt + (double)pracs), tc / icpk));
+      const double sink = fmin(qsz, fmin(dts * (psmlt + (double)pracs), tc * rcpk));
       qsz = qsz - sink;
       const double tmp = fmin(sink, dim(K.qs_mlt, qlz));
       qlz = qlz + tmp;
@@ -209,7 +209,7 @@ SHD void icloud_processes_m(const MpConst& K, const MpConstF& F, double& qgz, do
       tc = tz - tice;
     }
     lhi = K.LI00 + K.DC_ICE * tz;
-    icpk = lhi / cvm;
+    rcpk = cvm / lhi;
     if ((qgz > QCMIN) && (tc > 0.0)) {
       float pgacr = 0.0f, pgacw = 0.0f;
       const float qgf = (float)qgz, qrf = (float)qrz, qlf = (float)qlz;
@@ -226,7 +226,7 @@ SHD void icloud_processes_m(const MpConst& K, const MpConstF& F, double& qgz, do
                                   (F.cgmlt[2] * sqrtf(qden) + F.cgmlt[3] * powf(qden, 0.6875f) / powf(denf, 0.25f)) +
                               F.cgmlt[4] * tcf * (pgacw + pgacr);
       double pgmlt = dts * (double)gmlt_rate;
-      pgmlt = fmin(fmax(0.0, pgmlt), fmin(qgz, tc / icpk));
+      pgmlt = fmin(fmax(0.0, pgmlt), fmin(qgz, tc * rcpk));
       qgz = qgz - pgmlt;
       qrz = qrz + pgmlt;
       q_liq = q_liq + pgmlt;
@@ -275,7 +275,7 @@ SHD void icloud_processes_m(const MpConst& K, const MpConstF& F, double& qgz, do
         psacr = dtsf * acr3d_f(vts, vtr, qrf, (float)qsz, F.csacr, F.acco[0][1], F.acco[1][1], F.acco[2][1], denf);
       float pgfr = dtsf * F.cgfr[0] / denf * (expf(-F.cgfr[1] * tcf) - 1.0f) * expf(1.75f * logf(qrf * denf));
       const double sink0 = (double)psacr + (double)pgfr;
-      const double factor = fmin(sink0, fmin(qrz, -tc / icpk)) / fmax(sink0, QRMIN);
+      const double factor = fmin(sink0, fmin(qrz, -tc * rcpk)) / fmax(sink0, QRMIN);
       const double ps = factor * (double)psacr;
       const double pg = factor * (double)pgfr;
       const double sink = ps + pg;
@@ -288,7 +288,7 @@ SHD void icloud_processes_m(const MpConst& K, const MpConstF& F, double& qgz, do
       tz = tz + sink * lhi / cvm;
     }
     lhi = K.LI00 + K.DC_ICE * tz;
-    icpk = lhi / cvm;
+    rcpk = cvm / lhi;
     if (qsz > 1.0e-7) {
       double sink;
       if (qgz > QRMIN)
@@ -322,7 +322,7 @@ SHD void icloud_processes_m(const MpConst& K, const MpConstF& F, double& qgz, do
         pgacr = 0.0;
       }
       double sink = pgacr + pgacw;
-      const double factor = fmin(sink, dim(tice, tz) / icpk) / fmax(sink, QRMIN);
+      const double factor = fmin(sink, dim(tice, tz) * rcpk) / fmax(sink, QRMIN);
       pgacr = factor * pgacr;
       pgacw = factor * pgacw;
       sink = pgacr + pgacw;

@@ -199,6 +199,19 @@ inline int set_timestep(const ShieldMpConfig& c, MpConst& K, double timestep, st
 // FP32 copies of the constants used by the mixed form's process rates.
 inline MpConstF to_float(const MpConst& K) {
   MpConstF F;
+  F.qs_e00 = K.E00 / K.RVGAS;
+  F.qw_c1 = K.DC_VAP / K.RVGAS;
+  F.qw_c2 = K.LV0 / K.RVGAS;
+  F.qw_c3 = F.qw_c2 / K.TICE - F.qw_c1 * std::log(K.TICE);
+  F.qi_c1 = K.D2ICE / K.RVGAS;
+  F.qi_c2 = K.LI2 / K.RVGAS;
+  F.qi_c3 = F.qi_c2 / K.TICE - F.qi_c1 * std::log(K.TICE);
+  F.qs_t0 = K.TICE;
+  F.qs_tmin = K.T_SAT_MIN;
+  F.qs_thi = K.TICE + 102.0;
+  F.qi_lo = K.iqs_lo_num / (K.RVGAS * K.T_SAT_MIN);
+  F.qi_lo_dq = (K.D2ICE + K.LI2 / K.T_SAT_MIN) / (K.RVGAS * K.T_SAT_MIN);
+  F.qs_rtw = 1.0 / (K.tice - K.t_wfr);
   F.E00 = (float)K.E00;
   F.DC_VAP = (float)K.DC_VAP;
   F.LV0 = (float)K.LV0;

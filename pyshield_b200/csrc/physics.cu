@@ -82,8 +82,8 @@ __device__ __forceinline__ double np_min(double a, double b) { return a <= b ? a
 //   C  (all warps)  the rest of statein, get_prs_fv3, the first statement of
 //                   get_phi_fv3 and the pointwise part of
 //                   prepare_microphysics; del_gz into shared memory;
-//   D  (one warp)   get_phi_fv3's bottom-up sum, phil, phii, and
-//                   prepare_microphysics' dz.
+//   D  (one warp)   get_phi_fv3's bottom-up sum into shared memory; then
+//      (all warps)  phii, del_gz, phil and prepare_microphysics' dz.
 constexpr int TC = 32;
 constexpr int NWB = 8;
 
@@ -150,44 +150,53 @@ __global__ void __launch_bounds__(TC * NWB) physics_prestep_kernel(const __grid_
     }
   }
   __syncthreads();
-  // ---- C: statein, get_prs_fv3, get_phi_fv3's first statement, prepare_microphysics' pointwise part
+  // ---- C: statein, get_prs_fv3, get_phi_fv3's first statement, prepare_microphysics' pointwise part.
+  // Every load of a level comes before its first store: the fields are
+  // separate storages, but the compiler cannot know that, and a store
+  // between two loads would make each group of loads wait for the last.
   for (int k = w; k < nk; k += NWB) {
     if (compute) {
       const double p = S.p[k][lane];
-      f[PRSI].at(i, j, k) = p;
       if (k == nk - 1) {
+        f[PRSI].at(i, j, k) = p;
         f[PRSIK].at(i, j, k) = exp(A.KAPPA * log(p)) * A.pk0inv;
         continue;
       }
-      const double pn = S.p[k + 1][lane];
-      const double ph_k = S.ph[k][lane], ph1 = S.ph[k + 1][lane];
+      // loads
       const double dp0 = f[DELP].at(i, j, k);
       double q[N_TRACER];
 #pragma unroll
-      for (int t = 0; t < N_TRACER; ++t) q[t] = f[QV + t].at(i, j, k) * dp0;
-      const double dpn = A.nwat == 6 ? dp0 - q[1] - q[2] - q[3] - q[4] - q[5] : dp0;
+      for (int t = 0; t < N_TRACER; ++t) q[t] = f[QV + t].at(i, j, k);
       const double tke = f[TKE].at(i, j, k);
       const double pt = f[PT].at(i, j, k);
       const double om = A.prepare ? f[OMGA].at(i, j, k) : 0.0;
-      f[PRSIK].at(i, j, k) = k == 0 ? A.pktop : log(p);
+      // statein
+      const double pn = S.p[k + 1][lane];
+      const double ph_k = S.ph[k][lane], ph1 = S.ph[k + 1][lane];
+#pragma unroll
+      for (int t = 0; t < N_TRACER; ++t) q[t] = q[t] * dp0;
+      const double dpn = A.nwat == 6 ? dp0 - q[1] - q[2] - q[3] - q[4] - q[5] : dp0;
 #pragma unroll
       for (int t = 0; t < N_TRACER; ++t) q[t] = q[t] / dpn;
-#pragma unroll
-      for (int t = 0; t < N_TRACER; ++t) f[QV + t].at(i, j, k) = q[t];
-      f[TKE].at(i, j, k) = tke / dpn;
       const double qv = q[0];
       const double qgrs_rad = np_max(1.0e-10, qv);
       const double rTv = A.RDGAS * pt * (1.0 + A.ZVIR * qgrs_rad);
       const double dm = dpn;
-      f[DM].at(i, j, k) = dm;
       double d = dm * rTv / (ph_k - ph1);
       d = np_min(d, pn - 0.01 * dm);
       d = np_max(d, p + 0.01 * dm);
-      f[DELP].at(i, j, k) = d;
-      f[DELPRSI].at(i, j, k) = pn - p;
       const double tv = 1.0 + A.ZVIR * np_max(0.0, qv);
       const double gz = (ph_k - ph1) / (pt * tv);
       S.gz[k][lane] = gz * pt * tv;
+      // stores
+      f[PRSI].at(i, j, k) = p;
+      f[PRSIK].at(i, j, k) = k == 0 ? A.pktop : log(p);
+#pragma unroll
+      for (int t = 0; t < N_TRACER; ++t) f[QV + t].at(i, j, k) = q[t];
+      f[TKE].at(i, j, k) = tke / dpn;
+      f[DM].at(i, j, k) = dm;
+      f[DELP].at(i, j, k) = d;
+      f[DELPRSI].at(i, j, k) = pn - p;
       if (A.prepare) {
         f[WMP].at(i, j, k) = -om * (1.0 + A.ZVIR * qv) * pt / d * A.RDGAS_RGRAV;
 #pragma unroll
@@ -195,29 +204,43 @@ __global__ void __launch_bounds__(TC * NWB) physics_prestep_kernel(const __grid_
           if (f[TEND0 + t].p) f[TEND0 + t].at(i, j, k) = 0.0;
       }
     } else if (halo && k < nk - 1) {
+      const double pt = f[PT].at(i, j, k);
+      const double qv = f[QV].at(i, j, k);
       const double p = S.p[k][lane], pn = S.p[k + 1][lane];
       const double ph_k = S.ph[k][lane], ph1 = S.ph[k + 1][lane];
-      const double pt = f[PT].at(i, j, k);
-      const double tv = 1.0 + A.ZVIR * np_max(0.0, f[QV].at(i, j, k));
+      const double tv = 1.0 + A.ZVIR * np_max(0.0, qv);
       f[DELPRSI].at(i, j, k) = pn - p;
       const double gz = (ph_k - ph1) / (pt * tv);
       S.gz[k][lane] = gz * pt * tv;
     }
   }
   __syncthreads();
-  // ---- D: get_phi_fv3, BACKWARD, and prepare_microphysics' dz
+  // ---- D: get_phi_fv3, BACKWARD: the sum phii[k] = phii[k + 1] + del_gz[k]
+  // in one warp into shared memory (statein's phii there is no longer read),
+  // then phii, del_gz, phil and prepare_microphysics' dz from all warps
   if (w == 0 && live) {
-    const bool prep = compute && A.prepare;
     double ph = 0.0;
-    f[PHII].at(i, j, nk - 1) = ph;
+    S.ph[nk - 1][lane] = ph;
     for (int k = nk - 2; k >= 0; --k) {
+      const double phn = ph + S.gz[k][lane];
+      S.ph[k][lane] = phn;
+      ph = phn;
+    }
+  }
+  __syncthreads();
+  if (live) {
+    const bool prep = compute && A.prepare;
+    for (int k = w; k < nk; k += NWB) {
+      if (k == nk - 1) {
+        f[PHII].at(i, j, k) = 0.0;
+        continue;
+      }
       const double g = S.gz[k][lane];
+      const double ph = S.ph[k + 1][lane], phn = S.ph[k][lane];
       f[DELGZ].at(i, j, k) = g;
       f[PHIL].at(i, j, k) = 0.5 * (ph + ph + g);
-      const double phn = ph + g;
       f[PHII].at(i, j, k) = phn;
       if (prep) f[DZ].at(i, j, k) = (ph - phn) * A.RGRAV;
-      ph = phn;
     }
   }
 }

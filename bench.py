@@ -555,6 +555,154 @@ def run_coupling(n_cube=N_CUBE, nlev=79, dt=DT, reps=5):
     }
 
 
+def d2p_bytes(nx, ny, nz):
+    """Algorithmic HBM bytes of one shield_copy_dycore_to_physics launch: 16
+    fields read and written on the compute domain plus one interface point
+    in x and y, levels 0 .. nz - 1."""
+    return 8 * 2 * 16 * (nx + 1) * (ny + 1) * nz
+
+
+def run_d2p(n_cube=N_CUBE, nlev=79, reps=5):
+    """DycoreToPhysics.__call__'s copy at CN x nlev (all six tiles side by
+    side), CUDA events around each call."""
+    import torch
+
+    from pyshield_b200.coupling import D2P_FIELDS, DycoreToPhysics
+    from pyshield_b200.grid import GridIndexing, QuantityFactory, StencilFactory
+    from pyshield_b200.quantity import Quantity
+
+    nx, ny = n_cube, 6 * n_cube
+    shape = (nlev + 1, ny + 2 * HALO + 1, nx + 2 * HALO + 1)
+    gen = torch.Generator(device="cuda").manual_seed(7)
+
+    class State:
+        pass
+
+    ds, ps = State(), State()
+    for f in D2P_FIELDS:
+        for st in (ds, ps):
+            t = torch.rand(shape, dtype=torch.float64, device="cuda", generator=gen).permute(2, 1, 0)
+            setattr(st, f, Quantity(t, ("x", "y", "z"), "", (HALO, HALO, 0), (nx, ny, nlev)))
+    gi = GridIndexing(nx, ny, nlev, HALO)
+    d2p = DycoreToPhysics(StencilFactory(gi), QuantityFactory(gi), None, False, False)
+    stream = torch.cuda.current_stream()
+    d2p(ds, ps)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        d2p(ds, ps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    nbytes = d2p_bytes(nx, ny, nlev)
+    peak, peak_kind = peaks()
+    achieved = nbytes / (ms / 1000.0) / 1e9
+    return {
+        "workload": f"DycoreToPhysics.__call__ copy of 16 fields, C{n_cube} ({nx * ny} columns) x L{nlev}, FP64",
+        "ms_per_step": ms,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "bytes_per_launch": nbytes,
+                     "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},
+        "note": "device time (CUDA events), mean of back-to-back calls; 2.3 GB of storages, more than L2",
+    }
+
+
+def dwind_bytes(nx, ny, nz):
+    """Algorithmic HBM bytes of one shield_agrid_to_dgrid call on a tile
+    whose four edges are cube edges: the tendencies read where the u and v
+    points average them (nx ny + 2 nx + 2 ny points each), u read and written
+    on nx x (ny + 1), v on (nx + 1) x ny, both tendencies zeroed on the prep
+    domain (nx + 2) x (ny + 2), at nz levels; and the 2-D geometry: six
+    vector components on the tendencies' points, three on each wind's."""
+    nt = nx * ny + 2 * nx + 2 * ny
+    nu, nv, nz0 = nx * (ny + 1), (nx + 1) * ny, (nx + 2) * (ny + 2)
+    return 8 * (nz * (2 * nt + 2 * nu + 2 * nv + 2 * nz0) + 6 * nt + 3 * nu + 3 * nv)
+
+
+def run_dwind(n_cube=N_CUBE, nlev=79, dt=DT, reps=10):
+    """AGrid2DGridPhysics.__call__ on the six CN tiles (each its own storages
+    and a whole-tile edge plan, as six ranks of a 1 x 1 layout would run it).
+    The six calls are captured in one CUDA graph and the replays timed with
+    CUDA events: a call moves about 48 MB, a few microseconds of device
+    time, so launched from Python the time would be the host's."""
+    import types
+
+    import torch
+
+    from pyshield_b200.dwind import AGrid2DGridPhysics
+    from pyshield_b200.grid import GridIndexing, StencilFactory
+    from pyshield_b200.quantity import Quantity
+
+    nx = ny = n_cube
+    h = HALO
+    gen = torch.Generator(device="cuda").manual_seed(11)
+
+    def field3(lo, hi):
+        t = torch.rand((nlev + 1, ny + 2 * h + 1, nx + 2 * h + 1), dtype=torch.float64, device="cuda",
+                       generator=gen) * (hi - lo) + lo
+        return Quantity(t.permute(2, 1, 0), ("x", "y", "z"), "", (h, h, 0), (nx, ny, nlev))
+
+    def field2(lo, hi):
+        t = torch.rand((ny + 2 * h + 1, nx + 2 * h + 1), dtype=torch.float64, device="cuda", generator=gen)
+        return (t * (hi - lo) + lo).t()
+
+    names2 = ("vlon1", "vlon2", "vlon3", "vlat1", "vlat2", "vlat3", "es1_1", "es1_2", "es1_3", "ew2_1", "ew2_2",
+              "ew2_3")
+    tiles = []
+    for _ in range(6):
+        gi = GridIndexing(nx, ny, nlev, h)
+        gi.south_edge = gi.north_edge = gi.west_edge = gi.east_edge = True
+        geom = {n: field2(-1.0, 1.0) for n in names2}
+        geom["edge_vect_w"] = field2(0.0, 1.0)
+        geom["edge_vect_e"] = field2(0.0, 1.0)
+        geom["edge_vect_s"] = torch.rand(nx + 2 * h + 1, dtype=torch.float64, device="cuda", generator=gen)
+        geom["edge_vect_n"] = torch.rand(nx + 2 * h + 1, dtype=torch.float64, device="cuda", generator=gen)
+        grid_info = types.SimpleNamespace(grid_type=0, **geom)
+        part = types.SimpleNamespace(subtile_index=lambda rank: (0, 0))
+        namelist = types.SimpleNamespace(dt_atmos=dt, npx=nx + 1, npy=ny + 1, layout=(1, 1))
+        a2d = AGrid2DGridPhysics(StencilFactory(gi), None, part, 0, namelist, grid_info)
+        q = {k: field3(-30.0, 30.0) for k in ("u", "v")}
+        q.update({k: field3(-1e-3, 1e-3) for k in ("u_dt", "v_dt")})
+        tiles.append((a2d, q, geom))
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for a2d, q, _ in tiles:
+            a2d(q["u"], q["v"], q["u_dt"], q["v_dt"])
+    torch.cuda.current_stream().wait_stream(side)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        for a2d, q, _ in tiles:
+            a2d(q["u"], q["v"], q["u_dt"], q["v_dt"])
+    graph.replay()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        graph.replay()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    del graph
+    nbytes = 6 * dwind_bytes(nx, ny, nlev)
+    peak, peak_kind = peaks()
+    achieved = nbytes / (ms / 1000.0) / 1e9
+    return {
+        "workload": f"AGrid2DGridPhysics.__call__ on the six C{n_cube} tiles ({nx} x {ny} x L{nlev} each, "
+                    "whole-tile edge plan), FP64",
+        "ms_per_step": ms,
+        "launches_per_step": 12,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "bytes_per_launch": nbytes,
+                     "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},
+        "note": "device time (CUDA events) of a CUDA-graph replay of the six tile calls (two launches each); "
+                "the six tiles' storages, 290 MB, are more than L2",
+    }
+
+
 def max_over_ranks(values, world, device):
     """Each rank's device-measured times -> their maximum over all ranks (the
     slowest replica sets the job's time). One all-reduce; every rank calls it
@@ -759,7 +907,8 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the C48 adjoint-cost measurement")
     ap.add_argument("--no-physics", action="store_true", help="skip the Physics.__call__ measurement")
-    ap.add_argument("--no-coupling", action="store_true", help="skip the UpdateAtmosphereState measurement")
+    ap.add_argument("--no-coupling", action="store_true",
+                    help="skip the UpdateAtmosphereState, DycoreToPhysics and AGrid2DGridPhysics measurements")
     ap.add_argument("--ncube", type=int, default=N_CUBE, help="cube size N of the CN workload (default 96)")
     ap.add_argument("--ensemble", action="store_true", help="run the ensemble workload instead")
     ap.add_argument("--members", type=int, default=64)
@@ -862,6 +1011,10 @@ def main():
                if (rank == 0 and world == 1 and not args.no_physics and args.form == "plain") else None)
     coupling = (run_coupling(n_cube=args.ncube, nlev=nlev)
                 if (rank == 0 and world == 1 and not args.no_coupling and args.form == "plain") else None)
+    d2p = dwind = None
+    if rank == 0 and world == 1 and not args.no_coupling and args.form == "plain":
+        d2p = run_d2p(n_cube=args.ncube, nlev=nlev)
+        dwind = run_dwind(n_cube=args.ncube, nlev=nlev)
 
     if rank == 0:
         rec = {
@@ -901,6 +1054,8 @@ def main():
             "adjoint": adjoint,
             "physics": physics,
             "coupling": coupling,
+            "dycore_to_physics": d2p,
+            "agrid_to_dgrid": dwind,
         }
         emit(rec)
 

@@ -5,12 +5,13 @@
 // The reference runs a prep stencil that turns the A-grid tendencies into
 // three Cartesian components averaged onto the D-grid edges (ue, ve), zeroes
 // the tendencies, applies up to eight cube-edge corrections to ue and ve, and
-// adds dt/2 (ue . es1) to u and dt/2 (ve . ew2) to v. Here one thread per
-// (i, j, k) of the D-grid points computes its own ue or ve from the
-// tendencies (the corrections read the original ue / ve of a neighbour,
-// which the thread recomputes), so no ue / ve / ut / vt field is stored;
-// a second launch then zeroes the tendencies on the prep domain, after every
-// read of them. Each expression keeps the reference's operand order.
+// adds dt/2 (ue . es1) to u and dt/2 (ve . ew2) to v. Here a block computes
+// the A-grid vectors of a tile once into shared memory, and each D-grid
+// point of the tile forms its own ue or ve from them (the corrections read
+// the original ue / ve of a neighbour, which the point forms too), so no
+// ue / ve / ut / vt field is stored; a second launch then zeroes the
+// tendencies on the prep domain, after every read of them. Each expression
+// keeps the reference's operand order.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -48,30 +49,75 @@ struct DwindArgs {
   double dt5;
 };
 
-struct Pt {
-  const DwindArgs& A;
-  int64_t k;
-  __device__ __forceinline__ double v3(int m, int64_t i, int64_t j) const {
-    return A.udt.at(i, j, k) * A.vlon[m].at(i, j) + A.vdt.at(i, j, k) * A.vlat[m].at(i, j);
-  }
-  // update_dwind_prep_stencil: ue = v3[0, -1, 0] + v3, ve = v3[-1, 0, 0] + v3
-  __device__ __forceinline__ double ue(int m, int64_t i, int64_t j) const { return v3(m, i, j - 1) + v3(m, i, j); }
-  __device__ __forceinline__ double ve(int m, int64_t i, int64_t j) const { return v3(m, i - 1, j) + v3(m, i, j); }
-};
+// The zeroing and doubly periodic kernels run over rows: blockIdx.x * DW_BX
+// + threadIdx.x is i along a storage line and blockIdx.y walks the (j, k)
+// lines, so the index arithmetic is 32-bit and a line's accesses are
+// coalesced in the i-fastest layout. At most 65,535 block rows; a loop over
+// rows covers the rest.
+constexpr int DW_BX = 128;
 
-__global__ void dwind_update_kernel(const __grid_constant__ DwindArgs A) {
-  const int64_t nb = (int64_t)(A.nx + 1) * (A.ny + 1) * A.nz;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nb; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = e % (A.nx + 1);
-    const int64_t r = e / (A.nx + 1);
-    const int64_t j = r % (A.ny + 1), k = r / (A.ny + 1);
-    const Pt P{A, k};
-    if (i < A.nx) {
-      // u point (update_uwind_stencil, j in [0, ny])
+dim3 row_grid(int len, int64_t rows) {
+  return dim3((unsigned)((len + DW_BX - 1) / DW_BX), (unsigned)(rows < 65535 ? (rows > 0 ? rows : 1) : 65535));
+}
+
+// The update kernel works on tiles: a block owns DT_X x DT_Y D-grid points
+// (i, j) over DT_K consecutive levels. The A-grid vectors v3 = udt vlon +
+// vdt vlat (update_dwind_prep_stencil) that its points average lie in
+// i0 - 1 .. i0 + DT_X, j0 - 1 .. j0 + DT_Y (the corrections read one more
+// point in i or j); the block loads their geometry once and, level by level,
+// computes each v3 once into shared memory, where the u and v points of the
+// level read it. Only A points in the prep domain [-1, nx] x [-1, ny] are
+// touched: every read of a D point lies there.
+constexpr int DT_X = 32, DT_Y = 8, DT_K = 8;
+constexpr int AT_X = DT_X + 2, AT_Y = DT_Y + 2;
+// Levels per thread of the zeroing kernel.
+constexpr int DW_KB = 4;
+
+// update_uwind_stencil (j in [0, ny]) and update_vwind_stencil (i in [0, nx])
+// with the cube-edge corrections of the x-edge (south, north) and y-edge
+// (west, east) stencils, on one tile. Each expression keeps the reference's
+// operand order; the loads of a level's u and v come before its stores.
+__global__ void __launch_bounds__(DT_X * DT_Y) dwind_update_kernel(const __grid_constant__ DwindArgs A) {
+  __shared__ double g_lon[3][AT_Y][AT_X], g_lat[3][AT_Y][AT_X], v3s[3][AT_Y][AT_X];
+  const int tx = threadIdx.x % DT_X, ty = threadIdx.x / DT_X;
+  const int i0 = blockIdx.x * DT_X, j0 = blockIdx.y * DT_Y, k0 = blockIdx.z * DT_K;
+  const int i = i0 + tx, j = j0 + ty;
+  const int k1 = k0 + DT_K < A.nz ? k0 + DT_K : A.nz;
+  for (int e = threadIdx.x; e < AT_X * AT_Y; e += DT_X * DT_Y) {
+    const int ax = e % AT_X, ay = e / AT_X;
+    const int ai = i0 - 1 + ax, aj = j0 - 1 + ay;
+    const bool in = ai <= A.nx && aj <= A.ny;  // ai, aj >= -1 by construction
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      g_lon[m][ay][ax] = in ? A.vlon[m].at(ai, aj) : 0.0;
+      g_lat[m][ay][ax] = in ? A.vlat[m].at(ai, aj) : 0.0;
+    }
+  }
+  const bool up = i < A.nx && j <= A.ny, vp = i <= A.nx && j < A.ny;
+  double e1[3], e2[3];
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    e1[m] = up ? A.es1[m].at(i, j) : 0.0;
+    e2[m] = vp ? A.ew2[m].at(i, j) : 0.0;
+  }
+  __syncthreads();
+  for (int k = k0; k < k1; ++k) {
+    const double uk = up ? A.u.at(i, j, k) : 0.0, vk = vp ? A.v.at(i, j, k) : 0.0;
+    for (int e = threadIdx.x; e < AT_X * AT_Y; e += DT_X * DT_Y) {
+      const int ax = e % AT_X, ay = e / AT_X;
+      const int ai = i0 - 1 + ax, aj = j0 - 1 + ay;
+      if (ai > A.nx || aj > A.ny) continue;
+      const double ut = A.udt.at(ai, aj, k), vt = A.vdt.at(ai, aj, k);
+#pragma unroll
+      for (int m = 0; m < 3; ++m) v3s[m][ay][ax] = ut * g_lon[m][ay][ax] + vt * g_lat[m][ay][ax];
+    }
+    __syncthreads();
+    // A point (ai, aj) sits at v3s[.][aj - j0 + 1][ai - i0 + 1]
+    if (up) {
+      // ue = v3(i, j - 1) + v3(i, j)
       double w[3];
 #pragma unroll
-      for (int m = 0; m < 3; ++m) w[m] = P.ue(m, i, j);
-      // update_dwind_x_edge_{west,east}_stencil on the south and north lines
+      for (int m = 0; m < 3; ++m) w[m] = v3s[m][ty][tx + 1] + v3s[m][ty + 1][tx + 1];
 #pragma unroll
       for (int s = SOUTH; s <= NORTH; ++s) {
         const double* ev = s == SOUTH ? A.ev_s : A.ev_n;
@@ -79,19 +125,18 @@ __global__ void dwind_update_kernel(const __grid_constant__ DwindArgs A) {
           const ShieldEdgeRegion& R = A.plan.r[s][q];
           if (j != R.line || i < R.lo || i >= R.hi) continue;
           const double c = ev[i * A.ev_stride];
+          const int x = tx + 1 + R.dir;
 #pragma unroll
-          for (int m = 0; m < 3; ++m) w[m] = c * P.ue(m, i + R.dir, j) + (1.0 - c) * w[m];
+          for (int m = 0; m < 3; ++m) w[m] = c * (v3s[m][ty][x] + v3s[m][ty + 1][x]) + (1.0 - c) * w[m];
         }
       }
-      A.u.at(i, j, k) = A.u.at(i, j, k) + A.dt5 * (w[0] * A.es1[0].at(i, j) + w[1] * A.es1[1].at(i, j) +
-                                                   w[2] * A.es1[2].at(i, j));
+      A.u.at(i, j, k) = uk + A.dt5 * (w[0] * e1[0] + w[1] * e1[1] + w[2] * e1[2]);
     }
-    if (j < A.ny) {
-      // v point (update_vwind_stencil, i in [0, nx])
+    if (vp) {
+      // ve = v3(i - 1, j) + v3(i, j)
       double w[3];
 #pragma unroll
-      for (int m = 0; m < 3; ++m) w[m] = P.ve(m, i, j);
-      // update_dwind_y_edge_{south,north}_stencil on the west and east lines
+      for (int m = 0; m < 3; ++m) w[m] = v3s[m][ty + 1][tx] + v3s[m][ty + 1][tx + 1];
 #pragma unroll
       for (int s = WEST; s <= EAST; ++s) {
         const F2& ev = s == WEST ? A.ev_w : A.ev_e;
@@ -99,44 +144,46 @@ __global__ void dwind_update_kernel(const __grid_constant__ DwindArgs A) {
           const ShieldEdgeRegion& R = A.plan.r[s][q];
           if (i != R.line || j < R.lo || j >= R.hi) continue;
           const double c = ev.at(i, j);
+          const int y = ty + 1 + R.dir;
 #pragma unroll
-          for (int m = 0; m < 3; ++m) w[m] = c * P.ve(m, i, j + R.dir) + (1.0 - c) * w[m];
+          for (int m = 0; m < 3; ++m) w[m] = c * (v3s[m][y][tx] + v3s[m][y][tx + 1]) + (1.0 - c) * w[m];
         }
       }
-      A.v.at(i, j, k) = A.v.at(i, j, k) + A.dt5 * (w[0] * A.ew2[0].at(i, j) + w[1] * A.ew2[1].at(i, j) +
-                                                   w[2] * A.ew2[2].at(i, j));
+      A.v.at(i, j, k) = vk + A.dt5 * (w[0] * e2[0] + w[1] * e2[1] + w[2] * e2[2]);
     }
+    __syncthreads();  // every read of this level's v3s before the next level's
   }
 }
 
-// set_winds_zero on the prep domain: i, j in [-1, n + 1)
+// set_winds_zero on the prep domain: i, j in [-1, n + 1), DW_KB levels per thread
 __global__ void dwind_zero_kernel(const __grid_constant__ DwindArgs A) {
-  const int64_t ni = A.nx + 2, nj = A.ny + 2;
-  const int64_t nb = ni * nj * A.nz;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nb; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = e % ni - 1;
-    const int64_t r = e / ni;
-    const int64_t j = r % nj - 1, k = r / nj;
-    A.udt.at(i, j, k) = 0.0;
-    A.vdt.at(i, j, k) = 0.0;
+  const int i = blockIdx.x * DW_BX + threadIdx.x - 1;
+  if (i > A.nx) return;
+  const int nkb = (A.nz + DW_KB - 1) / DW_KB;
+  const int nrow = (A.ny + 2) * nkb;
+  for (int r = blockIdx.y; r < nrow; r += gridDim.y) {
+    const int j = r % (A.ny + 2) - 1, k0 = (r / (A.ny + 2)) * DW_KB;
+#pragma unroll
+    for (int b = 0; b < DW_KB; ++b) {
+      if (k0 + b >= A.nz) continue;
+      A.udt.at(i, j, k0 + b) = 0.0;
+      A.vdt.at(i, j, k0 + b) = 0.0;
+    }
   }
 }
 
 // doubly_periodic_wind_update (update_dwind_phys.py:153-161) on the compute domain
 __global__ void dwind_periodic_kernel(const __grid_constant__ DwindArgs A) {
-  const int64_t nb = (int64_t)A.nx * A.ny * A.nz;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nb; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = e % A.nx;
-    const int64_t r = e / A.nx;
-    const int64_t j = r % A.ny, k = r / A.ny;
-    A.u.at(i, j, k) = A.u.at(i, j, k) + A.dt5 * (A.udt.at(i, j - 1, k) + A.udt.at(i, j, k));
-    A.v.at(i, j, k) = A.v.at(i, j, k) + A.dt5 * (A.vdt.at(i - 1, j, k) + A.vdt.at(i, j, k));
+  const int i = blockIdx.x * DW_BX + threadIdx.x;
+  if (i >= A.nx) return;
+  const int nrow = A.ny * A.nz;
+  for (int r = blockIdx.y; r < nrow; r += gridDim.y) {
+    const int j = r % A.ny, k = r / A.ny;
+    const double u0 = A.u.at(i, j, k), ua = A.udt.at(i, j - 1, k), ub = A.udt.at(i, j, k);
+    const double v0 = A.v.at(i, j, k), va = A.vdt.at(i - 1, j, k), vb = A.vdt.at(i, j, k);
+    A.u.at(i, j, k) = u0 + A.dt5 * (ua + ub);
+    A.v.at(i, j, k) = v0 + A.dt5 * (va + vb);
   }
-}
-
-int grid_for(int64_t n, int bs) {
-  int64_t nb = (n + bs - 1) / bs;
-  return (int)(nb < 148 * 32 ? (nb > 0 ? nb : 1) : 148 * 32);
 }
 
 F3 mk3(const ShieldField3D& f) { return F3{f.ptr, f.si, f.sj, f.sk}; }
@@ -151,6 +198,10 @@ extern "C" int shield_agrid_to_dgrid(int nx, int ny, int nz, int grid_type, doub
     shield::set_last_error("shield_agrid_to_dgrid: bad arguments");
     return SHIELD_EINVAL;
   }
+  if ((int64_t)(ny + 2) * nz > INT32_MAX || nx > INT32_MAX - 2 * DW_BX) {
+    shield::set_last_error("shield_agrid_to_dgrid: domain too large for 32-bit row indices");
+    return SHIELD_ELAYOUT;
+  }
   DwindArgs A{};
   A.u = mk3(u);
   A.v = mk3(v);
@@ -163,7 +214,7 @@ extern "C" int shield_agrid_to_dgrid(int nx, int ny, int nz, int grid_type, doub
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaError_t e;
   if (grid_type > 3) {
-    dwind_periodic_kernel<<<grid_for((int64_t)nx * ny * nz, 256), 256, 0, st>>>(A);
+    dwind_periodic_kernel<<<row_grid(nx, (int64_t)ny * nz), DW_BX, 0, st>>>(A);
     e = cudaGetLastError();
   } else {
     if (!plan || !g) {
@@ -201,10 +252,12 @@ extern "C" int shield_agrid_to_dgrid(int nx, int ny, int nz, int grid_type, doub
     A.ev_n = g->edge_vect_n;
     A.ev_stride = g->edge_stride;
     A.plan = *plan;
-    dwind_update_kernel<<<grid_for((int64_t)(nx + 1) * (ny + 1) * nz, 256), 256, 0, st>>>(A);
+    const dim3 tiles((unsigned)((nx + DT_X) / DT_X), (unsigned)((ny + DT_Y) / DT_Y), (unsigned)((nz + DT_K - 1) / DT_K));
+    dwind_update_kernel<<<tiles, DT_X * DT_Y, 0, st>>>(A);
+    const int64_t nkb = (nz + DW_KB - 1) / DW_KB;
     e = cudaGetLastError();
     if (e == cudaSuccess) {
-      dwind_zero_kernel<<<grid_for((int64_t)(nx + 2) * (ny + 2) * nz, 256), 256, 0, st>>>(A);
+      dwind_zero_kernel<<<row_grid(nx + 2, (int64_t)(ny + 2) * nkb), DW_BX, 0, st>>>(A);
       e = cudaGetLastError();
     }
   }

@@ -77,20 +77,37 @@ constexpr int DW_KB = 4;
 // with the cube-edge corrections of the x-edge (south, north) and y-edge
 // (west, east) stencils, on one tile. Each expression keeps the reference's
 // operand order; the loads of a level's u and v come before its stores.
-__global__ void __launch_bounds__(DT_X * DT_Y) dwind_update_kernel(const __grid_constant__ DwindArgs A) {
+// The edge-plan tests and the points' addresses are worked out once, before
+// the level loop. Four blocks per SM (a 64-register cap, a few bytes
+// spilled) measured faster than three without the cap.
+__global__ void __launch_bounds__(DT_X * DT_Y, 4) dwind_update_kernel(const __grid_constant__ DwindArgs A) {
   __shared__ double g_lon[3][AT_Y][AT_X], g_lat[3][AT_Y][AT_X], v3s[3][AT_Y][AT_X];
+  constexpr int NT = DT_X * DT_Y;
+  constexpr int NA = (AT_X * AT_Y + NT - 1) / NT;  // A points per thread
   const int tx = threadIdx.x % DT_X, ty = threadIdx.x / DT_X;
   const int i0 = blockIdx.x * DT_X, j0 = blockIdx.y * DT_Y, k0 = blockIdx.z * DT_K;
   const int i = i0 + tx, j = j0 + ty;
   const int k1 = k0 + DT_K < A.nz ? k0 + DT_K : A.nz;
-  for (int e = threadIdx.x; e < AT_X * AT_Y; e += DT_X * DT_Y) {
-    const int ax = e % AT_X, ay = e / AT_X;
-    const int ai = i0 - 1 + ax, aj = j0 - 1 + ay;
-    const bool in = ai <= A.nx && aj <= A.ny;  // ai, aj >= -1 by construction
+  // this thread's A points: their place in the tile, their geometry, and
+  // their offsets in udt and vdt (level 0)
+  int ax[NA], ay[NA];
+  bool ain[NA];
+  int64_t ou[NA], ov[NA];
 #pragma unroll
-    for (int m = 0; m < 3; ++m) {
-      g_lon[m][ay][ax] = in ? A.vlon[m].at(ai, aj) : 0.0;
-      g_lat[m][ay][ax] = in ? A.vlat[m].at(ai, aj) : 0.0;
+  for (int n = 0; n < NA; ++n) {
+    const int e = threadIdx.x + n * NT;
+    ax[n] = e % AT_X;
+    ay[n] = e / AT_X;
+    const int ai = i0 - 1 + ax[n], aj = j0 - 1 + ay[n];
+    ain[n] = e < AT_X * AT_Y && ai <= A.nx && aj <= A.ny;  // ai, aj >= -1 by construction
+    ou[n] = ain[n] ? ai * A.udt.si + aj * A.udt.sj : 0;
+    ov[n] = ain[n] ? ai * A.vdt.si + aj * A.vdt.sj : 0;
+    if (ain[n]) {
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        g_lon[m][ay[n]][ax[n]] = A.vlon[m].at(ai, aj);
+        g_lat[m][ay[n]][ax[n]] = A.vlat[m].at(ai, aj);
+      }
     }
   }
   const bool up = i < A.nx && j <= A.ny, vp = i <= A.nx && j < A.ny;
@@ -100,56 +117,83 @@ __global__ void __launch_bounds__(DT_X * DT_Y) dwind_update_kernel(const __grid_
     e1[m] = up ? A.es1[m].at(i, j) : 0.0;
     e2[m] = vp ? A.ew2[m].at(i, j) : 0.0;
   }
+  // the cube-edge corrections that apply to this point, in the reference's
+  // order: regions q of the south then north lines (u), of the west then
+  // east lines (v); at most two regions per line
+  bool fu[4], fv[4];
+  double cu[4], cv[4];
+  int du[4], dv[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int su = t < 2 ? SOUTH : NORTH, sv = t < 2 ? WEST : EAST, q = t & 1;
+    fu[t] = fv[t] = false;
+    cu[t] = cv[t] = 0.0;
+    du[t] = dv[t] = 0;
+    if (up && q < A.plan.n[su]) {
+      const ShieldEdgeRegion& R = A.plan.r[su][q];
+      if (j == R.line && i >= R.lo && i < R.hi) {
+        const double* ev = su == SOUTH ? A.ev_s : A.ev_n;
+        fu[t] = true;
+        cu[t] = ev[i * A.ev_stride];
+        du[t] = R.dir;
+      }
+    }
+    if (vp && q < A.plan.n[sv]) {
+      const ShieldEdgeRegion& R = A.plan.r[sv][q];
+      if (i == R.line && j >= R.lo && j < R.hi) {
+        fv[t] = true;
+        cv[t] = (sv == WEST ? A.ev_w : A.ev_e).at(i, j);
+        dv[t] = R.dir;
+      }
+    }
+  }
+  const bool any_u = fu[0] || fu[1] || fu[2] || fu[3], any_v = fv[0] || fv[1] || fv[2] || fv[3];
+  double* pu = A.u.p + (up ? i * A.u.si + j * A.u.sj : 0);
+  double* pv = A.v.p + (vp ? i * A.v.si + j * A.v.sj : 0);
   __syncthreads();
   for (int k = k0; k < k1; ++k) {
-    const double uk = up ? A.u.at(i, j, k) : 0.0, vk = vp ? A.v.at(i, j, k) : 0.0;
-    for (int e = threadIdx.x; e < AT_X * AT_Y; e += DT_X * DT_Y) {
-      const int ax = e % AT_X, ay = e / AT_X;
-      const int ai = i0 - 1 + ax, aj = j0 - 1 + ay;
-      if (ai > A.nx || aj > A.ny) continue;
-      const double ut = A.udt.at(ai, aj, k), vt = A.vdt.at(ai, aj, k);
+    const double uk = up ? pu[k * A.u.sk] : 0.0, vk = vp ? pv[k * A.v.sk] : 0.0;
 #pragma unroll
-      for (int m = 0; m < 3; ++m) v3s[m][ay][ax] = ut * g_lon[m][ay][ax] + vt * g_lat[m][ay][ax];
+    for (int n = 0; n < NA; ++n) {
+      if (!ain[n]) continue;
+      const double ut = A.udt.p[ou[n] + k * A.udt.sk], vt = A.vdt.p[ov[n] + k * A.vdt.sk];
+#pragma unroll
+      for (int m = 0; m < 3; ++m)
+        v3s[m][ay[n]][ax[n]] = ut * g_lon[m][ay[n]][ax[n]] + vt * g_lat[m][ay[n]][ax[n]];
     }
     __syncthreads();
     // A point (ai, aj) sits at v3s[.][aj - j0 + 1][ai - i0 + 1]
     if (up) {
-      // ue = v3(i, j - 1) + v3(i, j)
+      // ue = v3(i, j - 1) + v3(i, j); a correction's neighbour is at i + dir
       double w[3];
 #pragma unroll
       for (int m = 0; m < 3; ++m) w[m] = v3s[m][ty][tx + 1] + v3s[m][ty + 1][tx + 1];
+      if (any_u) {
 #pragma unroll
-      for (int s = SOUTH; s <= NORTH; ++s) {
-        const double* ev = s == SOUTH ? A.ev_s : A.ev_n;
-        for (int q = 0; q < A.plan.n[s]; ++q) {
-          const ShieldEdgeRegion& R = A.plan.r[s][q];
-          if (j != R.line || i < R.lo || i >= R.hi) continue;
-          const double c = ev[i * A.ev_stride];
-          const int x = tx + 1 + R.dir;
+        for (int t = 0; t < 4; ++t) {
+          if (!fu[t]) continue;
+          const int x = tx + 1 + du[t];
 #pragma unroll
-          for (int m = 0; m < 3; ++m) w[m] = c * (v3s[m][ty][x] + v3s[m][ty + 1][x]) + (1.0 - c) * w[m];
+          for (int m = 0; m < 3; ++m) w[m] = cu[t] * (v3s[m][ty][x] + v3s[m][ty + 1][x]) + (1.0 - cu[t]) * w[m];
         }
       }
-      A.u.at(i, j, k) = uk + A.dt5 * (w[0] * e1[0] + w[1] * e1[1] + w[2] * e1[2]);
+      pu[k * A.u.sk] = uk + A.dt5 * (w[0] * e1[0] + w[1] * e1[1] + w[2] * e1[2]);
     }
     if (vp) {
-      // ve = v3(i - 1, j) + v3(i, j)
+      // ve = v3(i - 1, j) + v3(i, j); a correction's neighbour is at j + dir
       double w[3];
 #pragma unroll
       for (int m = 0; m < 3; ++m) w[m] = v3s[m][ty + 1][tx] + v3s[m][ty + 1][tx + 1];
+      if (any_v) {
 #pragma unroll
-      for (int s = WEST; s <= EAST; ++s) {
-        const F2& ev = s == WEST ? A.ev_w : A.ev_e;
-        for (int q = 0; q < A.plan.n[s]; ++q) {
-          const ShieldEdgeRegion& R = A.plan.r[s][q];
-          if (i != R.line || j < R.lo || j >= R.hi) continue;
-          const double c = ev.at(i, j);
-          const int y = ty + 1 + R.dir;
+        for (int t = 0; t < 4; ++t) {
+          if (!fv[t]) continue;
+          const int y = ty + 1 + dv[t];
 #pragma unroll
-          for (int m = 0; m < 3; ++m) w[m] = c * (v3s[m][y][tx] + v3s[m][y][tx + 1]) + (1.0 - c) * w[m];
+          for (int m = 0; m < 3; ++m) w[m] = cv[t] * (v3s[m][y][tx] + v3s[m][y][tx + 1]) + (1.0 - cv[t]) * w[m];
         }
       }
-      A.v.at(i, j, k) = vk + A.dt5 * (w[0] * e2[0] + w[1] * e2[1] + w[2] * e2[2]);
+      pv[k * A.v.sk] = vk + A.dt5 * (w[0] * e2[0] + w[1] * e2[1] + w[2] * e2[2]);
     }
     __syncthreads();  // every read of this level's v3s before the next level's
   }

@@ -7,7 +7,8 @@ the oracle, which reproduces the reference's output bit for bit
 
 GPU: the kernels against the reference's own result (golden fixtures) for a
 whole tile, two subtiles of a 2 x 2 layout and the doubly periodic grid,
-every storage compared whole.
+every storage compared whole; and against the oracle on domains that span
+several of the update kernel's tiles in i, j and k.
 """
 import numpy as np
 import pytest
@@ -69,3 +70,70 @@ def test_agrid_to_dgrid_matches_reference(name):
     torch.cuda.synchronize()
     for k, t in f.items():
         np.testing.assert_array_equal(t.cpu().numpy(), z["out_" + k], err_msg=f"{name} {k}")
+
+
+# Domains that span several of the update kernel's tiles (32 x 8 points by 8
+# levels) in i, j and k, with ragged last tiles: (tile size n, layout, rank,
+# levels, storage layout)
+TILED_CASES = [
+    (70, (1, 1), 0, 11, "ifirst"),
+    (70, (1, 1), 0, 11, "kfirst"),
+    (66, (2, 2), 3, 9, "ifirst"),
+    (66, (2, 2), 0, 17, "ifirst"),
+    (48, (2, 1), 1, 8, "ifirst"),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,layout,rank,L,order", TILED_CASES)
+def test_agrid_to_dgrid_across_tiles_matches_oracle(n, layout, rank, L, order):
+    """The kernels against the oracle (pinned bit for bit to the reference's
+    own class by the golden fixtures) on domains larger than one tile of the
+    update kernel: every storage compared whole, bit for bit."""
+    from types import SimpleNamespace
+
+    import torch
+
+    from oracle.dwind import agrid_to_dgrid as oracle_a2d
+    from pyshield_b200.dwind import AGrid2DGridPhysics, edge_plan
+    from pyshield_b200.grid import GridIndexing, StencilFactory
+    from pyshield_b200.quantity import Quantity
+
+    h = 3
+    nx, ny = n // layout[0], n // layout[1]
+    sy, sx = rank // layout[0], rank % layout[0]
+    edges = (sy == 0, sy == layout[1] - 1, sx == 0, sx == layout[0] - 1)
+    rng = np.random.default_rng(100 + n + rank + L)
+    shape3 = (nx + 2 * h + 1, ny + 2 * h + 1, L + 1)
+    shape2 = shape3[:2]
+    f = {"u": rng.uniform(-30.0, 30.0, shape3), "v": rng.uniform(-30.0, 30.0, shape3),
+         "u_dt": rng.normal(0.0, 1e-3, shape3), "v_dt": rng.normal(0.0, 1e-3, shape3)}
+    g = {name: rng.uniform(-1.0, 1.0, shape2) for name in
+         ("vlon1", "vlon2", "vlon3", "vlat1", "vlat2", "vlat3", "es1_1", "es1_2", "es1_3", "ew2_1", "ew2_2", "ew2_3")}
+    g["edge_vect_w"] = rng.uniform(0.0, 1.0, shape2)
+    g["edge_vect_e"] = rng.uniform(0.0, 1.0, shape2)
+    g["edge_vect_s"] = rng.uniform(0.0, 1.0, shape3[0])
+    g["edge_vect_n"] = rng.uniform(0.0, 1.0, shape3[0])
+    dt = 180.0
+
+    def dev(a):
+        if order == "ifirst" or a.ndim < 3:
+            return torch.from_numpy(np.ascontiguousarray(a.T)).cuda().permute(*reversed(range(a.ndim)))
+        return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+    gi = GridIndexing(nx, ny, L, h)
+    gi.south_edge, gi.north_edge, gi.west_edge, gi.east_edge = edges
+    part = SimpleNamespace(subtile_index=lambda r: (sy, sx))
+    namelist = SimpleNamespace(dt_atmos=dt, npx=n + 1, npy=n + 1, layout=layout)
+    grid_info = SimpleNamespace(grid_type=0, **{k: dev(v) for k, v in g.items()})
+    t = {k: dev(v) for k, v in f.items()}
+    q = {k: Quantity(v, ("x", "y", "z"), "", (h, h, 0), (nx, ny, L)) for k, v in t.items()}
+    AGrid2DGridPhysics(StencilFactory(gi), None, part, rank, namelist, grid_info)(q["u"], q["v"], q["u_dt"], q["v_dt"])
+    torch.cuda.synchronize()
+
+    plan = edge_plan(nx, ny, h, n + 1, n + 1, layout, (sy, sx), edges)
+    ref = {k: v.copy() for k, v in f.items()}
+    oracle_a2d(ref["u"], ref["v"], ref["u_dt"], ref["v_dt"], g, nx, ny, L, h, 0.5 * dt, plan)
+    assert any(len(plan[s]) for s in plan)  # the corrections are exercised
+    for k in f:
+        np.testing.assert_array_equal(t[k].cpu().numpy(), ref[k], err_msg=f"{n} {layout} {rank} {k}")

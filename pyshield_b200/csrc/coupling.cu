@@ -41,42 +41,49 @@ struct UpdArgs {
   double dt;
 };
 
-// One block row per (j, k) (or, with k fastest in memory, per (i, j)) line
-// of the domain and the threads along the line's contiguous dimension: the
-// index arithmetic is one 32-bit divide per row, and each point's loads are
-// all issued before its stores.
-struct Line {
-  int64_t i, j, k;
-};
-__device__ __forceinline__ bool line_point(int kfast, int nx, int ny, int nz, int64_t row, int64_t t, Line& p) {
+// The two field kernels below work per field and per stretch of lines: a
+// block handles one field (blockIdx.z) over LINES consecutive lines of the
+// domain, a line being a (j, k) row (or, with k fastest in memory, an (i, j)
+// column) whose points lie on consecutive threads. Its reads, then its
+// writes, are contiguous stretches of a few storages instead of short lines
+// of many, which keeps DRAM pages open. All of a block's loads are issued
+// before its stores; index arithmetic is 32-bit (the entry points check the
+// box).
+constexpr int LINES = 8;
+__device__ __forceinline__ void line_ijk(int kfast, int nx, int ny, int row, int t, int& i, int& j, int& k) {
   if (kfast) {
-    if (t >= nz) return false;
-    p.k = t;
-    p.i = row % nx;
-    p.j = row / nx;
+    k = t;
+    i = row % nx;
+    j = row / nx;
   } else {
-    if (t >= nx) return false;
-    p.i = t;
-    p.j = row % ny;
-    p.k = row / ny;
+    i = t;
+    j = row % ny;
+    k = row / ny;
   }
-  return true;
 }
 
 __global__ void update_physics_state_kernel(const __grid_constant__ UpdArgs A) {
-  const int64_t rows = A.kfast ? (int64_t)A.nx * A.ny : (int64_t)A.ny * A.nz;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  for (int64_t row = blockIdx.y; row < rows; row += gridDim.y) {
-    Line q;
-    if (!line_point(A.kfast, A.nx, A.ny, A.nz, row, t, q)) continue;
-    double x[10], d[10];
+  const int rows = A.kfast ? A.nx * A.ny : A.ny * A.nz;
+  const int len = A.kfast ? A.nz : A.nx;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= len) return;
+  const F3& X = A.x[blockIdx.z];
+  const F3& T = A.t[blockIdx.z];
+  const F3& O = A.o[blockIdx.z];
+  for (int r0 = blockIdx.y * LINES; r0 < rows; r0 += gridDim.y * LINES) {
+    double x[LINES], d[LINES];
+    int64_t oo[LINES];
 #pragma unroll
-    for (int p = 0; p < 10; ++p) {
-      x[p] = A.x[p].at(q.i, q.j, q.k);
-      d[p] = A.t[p].at(q.i, q.j, q.k);
+    for (int b = 0; b < LINES; ++b) {
+      int i, j, k;
+      line_ijk(A.kfast, A.nx, A.ny, r0 + b < rows ? r0 + b : rows - 1, t, i, j, k);
+      x[b] = X.at(i, j, k);
+      d[b] = T.at(i, j, k);
+      oo[b] = i * O.si + j * O.sj + k * O.sk;
     }
 #pragma unroll
-    for (int p = 0; p < 10; ++p) A.o[p].at(q.i, q.j, q.k) = x[p] + d[p] * A.dt;
+    for (int b = 0; b < LINES; ++b)
+      if (r0 + b < rows) O.p[oo[b]] = x[b] + d[b] * A.dt;
   }
 }
 
@@ -292,8 +299,8 @@ cudaError_t launch_atmos(const AtmArgs& A, int64_t ncf, cudaStream_t st) {
 
 // DycoreToPhysics' copy of 16 fields (update_atmos_state.py:95-142, built at
 // :160-167 on the compute domain plus one interface point in x and y,
-// PARALLEL interval(0, -1) of nz + 1 levels): one thread per point, the
-// fastest-varying storage dimension on consecutive threads.
+// PARALLEL interval(0, -1) of nz + 1 levels), the fastest-varying storage
+// dimension on consecutive threads.
 constexpr int N_D2P = 16;
 struct D2PArgs {
   F3 in[N_D2P], out[N_D2P];
@@ -301,17 +308,27 @@ struct D2PArgs {
   int kfast;
 };
 
+// The copy, per field and stretch of lines as update_physics_state_kernel.
 __global__ void copy_dycore_to_physics_kernel(const __grid_constant__ D2PArgs A) {
-  const int64_t rows = A.kfast ? (int64_t)A.nx1 * A.ny1 : (int64_t)A.ny1 * A.nz;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  for (int64_t row = blockIdx.y; row < rows; row += gridDim.y) {
-    Line q;
-    if (!line_point(A.kfast, A.nx1, A.ny1, A.nz, row, t, q)) continue;
-    double v[N_D2P];
+  const int rows = A.kfast ? A.nx1 * A.ny1 : A.ny1 * A.nz;
+  const int len = A.kfast ? A.nz : A.nx1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= len) return;
+  const F3& src = A.in[blockIdx.z];
+  const F3& dst = A.out[blockIdx.z];
+  for (int r0 = blockIdx.y * LINES; r0 < rows; r0 += gridDim.y * LINES) {
+    double v[LINES];
+    int64_t od[LINES];
 #pragma unroll
-    for (int p = 0; p < N_D2P; ++p) v[p] = A.in[p].at(q.i, q.j, q.k);
+    for (int b = 0; b < LINES; ++b) {
+      int i, j, k;
+      line_ijk(A.kfast, A.nx1, A.ny1, r0 + b < rows ? r0 + b : rows - 1, t, i, j, k);
+      v[b] = src.at(i, j, k);
+      od[b] = i * dst.si + j * dst.sj + k * dst.sk;
+    }
 #pragma unroll
-    for (int p = 0; p < N_D2P; ++p) A.out[p].at(q.i, q.j, q.k) = v[p];
+    for (int b = 0; b < LINES; ++b)
+      if (r0 + b < rows) dst.p[od[b]] = v[b];
   }
 }
 
@@ -347,7 +364,13 @@ extern "C" int shield_update_physics_state(int nx, int ny, int nz, const ShieldF
   A.kfast = (state10[0].sk == 1) ? 1 : 0;
   A.dt = dt;
   const int64_t len = A.kfast ? nz : nx, rows = A.kfast ? (int64_t)nx * ny : (int64_t)ny * nz;
-  update_physics_state_kernel<<<line_grid(len, rows), 128, 0, static_cast<cudaStream_t>(stream)>>>(A);
+  if (rows * len > INT32_MAX) {
+    shield::set_last_error("shield_update_physics_state: box too large for 32-bit indices");
+    return SHIELD_ELAYOUT;
+  }
+  dim3 grid = line_grid(len, (rows + LINES - 1) / LINES);
+  grid.z = 10;
+  update_physics_state_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(A);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     shield::set_last_error(std::string("shield_update_physics_state: ") + cudaGetErrorString(e));
@@ -424,7 +447,13 @@ extern "C" int shield_copy_dycore_to_physics(int nx, int ny, int nz, const Shiel
   A.nz = nz;
   A.kfast = (physics16[0].sk == 1) ? 1 : 0;
   const int64_t len = A.kfast ? nz : A.nx1, rows = A.kfast ? (int64_t)A.nx1 * A.ny1 : (int64_t)A.ny1 * nz;
-  copy_dycore_to_physics_kernel<<<line_grid(len, rows), 128, 0, static_cast<cudaStream_t>(stream)>>>(A);
+  if (rows * len > INT32_MAX) {
+    shield::set_last_error("shield_copy_dycore_to_physics: box too large for 32-bit indices");
+    return SHIELD_ELAYOUT;
+  }
+  dim3 grid = line_grid(len, (rows + LINES - 1) / LINES);
+  grid.z = N_D2P;
+  copy_dycore_to_physics_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(A);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     shield::set_last_error(std::string("shield_copy_dycore_to_physics: ") + cudaGetErrorString(e));

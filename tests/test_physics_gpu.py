@@ -117,13 +117,15 @@ def test_physics_matches_reference_golden(name):
     _compare(got, gpr, ref, rpr, _floors(st, ref, dt, nx, ny, L), name)
 
 
-@pytest.mark.parametrize("kw,dt", [({}, 180.0), ({"mp_time": 90.0, "do_qa": True}, 180.0)])
-def test_physics_matches_oracle_c12(kw, dt):
+@pytest.mark.parametrize("kw,dt,nx,ny,L", [({}, 180.0, 12, 72, 79), ({"mp_time": 90.0, "do_qa": True}, 180.0, 12, 72, 79),
+                                           ({}, 180.0, 6, 36, 127)])
+def test_physics_matches_oracle_c12(kw, dt, nx, ny, L):
+    """Against the oracle at C12 L79, and on 216 columns at L127 (the
+    pre-step kernel's instantiation for more than 95 levels)."""
     from oracle.physics import OraclePhysics
     from pyshield_b200._config import PhysicsConfig
     from pyshield_b200.inputs import PTOP, make_physics_state
 
-    nx, ny, L = 12, 72, 79
     st, area = make_physics_state(nx, ny, L, seed=51, halo=H)
     cfg = PhysicsConfig(dt_atmos=int(dt), **kw)
     got, gpr = run_physics_gpu(cfg, st, area, nx, ny, L, dt, PTOP)
@@ -132,4 +134,4 @@ def test_physics_matches_oracle_c12(kw, dt):
     rpr = oracle(ref, dt)
     ref.pop("land")
     ref["_prsik"], ref["_dm3d"], ref["_del_gz"] = oracle.prsik, oracle.dm3d, oracle.del_gz
-    _compare(got, gpr, ref, rpr, _floors(st, ref, dt, nx, ny, L), f"C12 {kw}")
+    _compare(got, gpr, ref, rpr, _floors(st, ref, dt, nx, ny, L), f"{nx}x{ny} L{L} {kw}")

@@ -232,7 +232,8 @@ int shield_mp_set_qaz(void* handle, const double* qaz, void* stream);
  * out_X = X + X_dt * dt for the ten (X, X_dt) pairs in this order:
  * qvapor/qv_dt, qliquid/ql_dt, qrain/qr_dt, qice/qi_dt, qsnow/qs_dt,
  * qgraupel/qg_dt, qcld/qa_dt, pt/pt_dt, ua/udt, va/vdt.
- * The domain is nx x ny x nz. */
+ * The domain is nx x ny x nz, at most 2^31 - 1 points (SHIELD_ELAYOUT
+ * otherwise). */
 int shield_update_physics_state(int nx, int ny, int nz, const ShieldField3D* state10, const ShieldField3D* tend10,
                                 const ShieldField3D* out10, double dt, void* stream);
 
@@ -258,7 +259,8 @@ int shield_update_physics_state(int nx, int ny, int nz, const ShieldField3D* sta
  *   13 v_t0 (physics va) 14 pt_t0 (physics pt) 15 dycore qvapor 16 qliquid
  *   17 qrain 18 qsnow 19 qice 20 qgraupel 21 prsi 22 dycore delp
  *   23 dycore pt 24 pe 25 peln 26 pk 27 dycore ua 28 dycore va
- * Outputs ps, u_srf, v_srf: 2-D fields (their sk is ignored). */
+ * Outputs ps, u_srf, v_srf: 2-D fields (their sk is ignored).
+ * At most nz = 128 levels (SHIELD_ELAYOUT otherwise). */
 #define SHIELD_UAS_APPLY 1       /* apply_tendencies = True */
 #define SHIELD_UAS_DYCORE_ONLY 2 /* dycore_only = True */
 int shield_update_atmos_state(int nx, int ny, int nz, int hx, int mode, const ShieldField3D* f, ShieldField3D ps,
@@ -302,7 +304,8 @@ int shield_physics_prestep(int nx, int ny, int nz, int hx, int nwat, double ptop
  * for each of the 16 fields in the order qvapor, qliquid, qrain, qsnow,
  * qice, qgraupel, qo3mr, qsgs_tke, qcld, pt, delp, delz, ua, va, w, omga,
  * physics = dycore on i in [0, nx], j in [0, ny] (the compute domain plus
- * one interface point, which the storages must have) and k in [0, nz). */
+ * one interface point, which the storages must have) and k in [0, nz); at
+ * most 2^31 - 1 points (SHIELD_ELAYOUT otherwise). */
 int shield_copy_dycore_to_physics(int nx, int ny, int nz, const ShieldField3D* dycore16,
                                   const ShieldField3D* physics16, void* stream);
 
@@ -334,7 +337,8 @@ typedef struct {
  * tendencies with the plan's edge corrections, then u_dt = v_dt = 0 on i, j
  * in [-1, n + 1); the tendencies need one halo point, filled by the caller's
  * halo exchange. With grid_type > 3: the doubly periodic update on the
- * compute domain (plan and geometry unused). dt5 = dt_atmos / 2. */
+ * compute domain (plan and geometry unused). dt5 = dt_atmos / 2.
+ * (ny + 2) * nz must stay below 2^31 (SHIELD_ELAYOUT otherwise). */
 int shield_agrid_to_dgrid(int nx, int ny, int nz, int grid_type, double dt5, const ShieldEdgePlan* plan,
                           const ShieldDwindGeometry* geometry, ShieldField3D u, ShieldField3D v, ShieldField3D u_dt,
                           ShieldField3D v_dt, void* stream);

@@ -210,7 +210,7 @@ typedef struct {
 
 int shield_mp_ensemble_create(const ShieldMpConfig* cfg, int nz, int nmembers, const ShieldMpMember* members,
                               int precision, void** plan);
-/* cols_per_block in {1, 2, 4} (4 only up to 96 levels); the launch has
+/* cols_per_block in {1, 2, 4}; the launch has
  * blocks_per_sm x (number of SMs) persistent blocks. */
 int shield_mp_ensemble_step(void* plan, int cols_per_block, int blocks_per_sm, void* stream);
 /* copy member m's persistent accumulator (nz*nx*ny doubles, level-major)

@@ -446,8 +446,8 @@ extern "C" int shield_mp_ensemble_step(void* plan, int G, int bpsm, void* stream
   Plan* p = static_cast<Plan*>(plan);
   if (!p) return fail(nullptr, SHIELD_EINVAL, "null plan");
   const int gi = gindex(G);
-  if (gi < 0 || bpsm < 1 || bpsm > 32 || (G == 4 && p->nz > 96))
-    return fail(nullptr, SHIELD_EINVAL, "cols_per_block must be 1, 2 or 4 (4 up to 96 levels), blocks_per_sm 1..32");
+  if (gi < 0 || bpsm < 1 || bpsm > 32)
+    return fail(nullptr, SHIELD_EINVAL, "cols_per_block must be 1, 2 or 4, blocks_per_sm 1..32");
   const int grid = bpsm * p->num_sms;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaError_t e = (p->precision == SHIELD_MP_MIXED)

@@ -20,7 +20,7 @@ cudaError_t mp_launch_mixed(const MpArgs& A, cudaStream_t st) {
   if (L <= 32) return launch_nw<1, 4, 2>(A, st);
   if (L <= 64) return launch_nw<2, 2, 2>(A, st);
   if (L <= 96) return launch_nw<3, 4, 1>(A, st);
-  if (L <= 128) return launch_nw<4, 2, 2>(A, st);
+  if (L <= 128) return launch_nw<4, 4, 1>(A, st);  // 512 threads, whole-sector staging
   return launch_nw<8, 1, 2>(A, st);
 }
 
@@ -50,6 +50,7 @@ cudaError_t mp_launch_ensemble_mixed(const MpArgs* members, const int64_t* offs,
   } else if (nz <= 128) {
     if (G == 1) return launch_ens<4, 1, 4>(members, offs, nm, grid, st);
     if (G == 2) return launch_ens<4, 2, 2>(members, offs, nm, grid, st);
+    if (G == 4) return launch_ens<4, 4, 1>(members, offs, nm, grid, st);
   }
   return cudaErrorInvalidValue;
 }

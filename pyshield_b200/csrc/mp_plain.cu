@@ -61,7 +61,7 @@ cudaError_t mp_launch_plain(const MpArgs& A, cudaStream_t st) {
   if (L <= 32) return launch_nw<1, 4, 2>(A, st);
   if (L <= 64) return launch_nw<2, 2, 2>(A, st);
   if (L <= 96) return launch_nw<3, SHIELD_NW3_G, SHIELD_NW3_MINB>(A, st);
-  if (L <= 128) return launch_nw<4, 2, 2>(A, st);
+  if (L <= 128) return launch_nw<4, 4, 1>(A, st);  // 512 threads, whole-sector staging
   return launch_nw<8, 1, 2>(A, st);
 }
 
@@ -112,6 +112,7 @@ cudaError_t mp_launch_ensemble_plain(const MpArgs* members, const int64_t* offs,
   } else if (nz <= 128) {
     if (G == 1) return launch_ens<4, 1, 4>(members, offs, nm, grid, st);
     if (G == 2) return launch_ens<4, 2, 2>(members, offs, nm, grid, st);
+    if (G == 4) return launch_ens<4, 4, 1>(members, offs, nm, grid, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -111,8 +111,6 @@ class MicrophysicsEnsemble:
         stream = torch.cuda.current_stream()
         best = None
         for G, b in candidates:
-            if G == 4 and self.nz > 96:
-                continue
             self.step(G, b)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)

@@ -16,17 +16,17 @@ MEMBERS = ((12, 6, 150.0), (24, 12, 225.0), (8, 6, 180.0), (36, 6, 120.0))  # (n
 L = 79
 
 
-def _states(seed0):
+def _states(seed0, nlev=L):
     from pyshield_b200.inputs import make_state
 
     out = []
     for m, (nx, ny, dt) in enumerate(MEMBERS):
-        st, area = make_state(nx * ny, L, seed=seed0 + m, n_cube=max(nx, ny), ts_offset=(-1.0) ** m * 2.0)
+        st, area = make_state(nx * ny, nlev, seed=seed0 + m, n_cube=max(nx, ny), ts_offset=(-1.0) ** m * 2.0)
         out.append((st, area, nx, ny, dt))
     return out
 
 
-def _single(cfg, members, nsteps, precision):
+def _single(cfg, members, nsteps, precision, nlev=L):
     from pyshield_b200.microphysics import Microphysics
 
     res = []
@@ -35,7 +35,7 @@ def _single(cfg, members, nsteps, precision):
         mp = Microphysics(sf, qf, gd, cfg, precision=precision)
         for _ in range(nsteps):
             mp(ms, dt)
-        o = read_state(ms, nx, ny, L)
+        o = read_state(ms, nx, ny, nlev)
         o["rain"] = mp.rain.cpu().numpy()
         o["qaz"] = mp.get_qaz().cpu().numpy()
         res.append(o)
@@ -51,29 +51,30 @@ def _ensemble(cfg, members, precision):
     return ens, built
 
 
-def _read(ens, built, members):
+def _read(ens, built, members, nlev=L):
     res = []
     for m, ((ms, _, _, _), (st, area, nx, ny, dt)) in enumerate(zip(built, members)):
-        o = read_state(ms, nx, ny, L)
+        o = read_state(ms, nx, ny, nlev)
         o["rain"] = ens.precip(m)[0].cpu().numpy()
         o["qaz"] = ens.qaz(m).cpu().numpy()
         res.append(o)
     return res
 
 
-@pytest.mark.parametrize("shape", [(1, 4), (2, 2), (2, 3), (4, 1)])
-def test_batched_plain_equals_members_bitwise(shape):
+@pytest.mark.parametrize("shape,nlev", [((1, 4), L), ((2, 2), L), ((2, 3), L), ((4, 1), L), ((4, 1), 127),
+                                        ((2, 2), 127)])
+def test_batched_plain_equals_members_bitwise(shape, nlev):
     import torch
 
     from pyshield_b200._config import PhysicsConfig
 
     cfg = PhysicsConfig(dt_atmos=150.0)
-    members = _states(100)
-    ref = _single(cfg, members, 1, "plain")
+    members = _states(100, nlev)
+    ref = _single(cfg, members, 1, "plain", nlev)
     ens, built = _ensemble(cfg, members, "plain")
     ens.step(*shape)
     torch.cuda.synchronize()
-    got = _read(ens, built, members)
+    got = _read(ens, built, members, nlev)
     for m, (a, b) in enumerate(zip(got, ref)):
         for f in MP_TENDENCIES + ("wmp", "rain", "qaz"):
             np.testing.assert_array_equal(a[f], b[f], err_msg=f"member {m} field {f} shape {shape}")

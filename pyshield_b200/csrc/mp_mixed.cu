@@ -20,7 +20,10 @@ cudaError_t mp_launch_mixed(const MpArgs& A, cudaStream_t st) {
   if (L <= 32) return launch_nw<1, 4, 2>(A, st);
   if (L <= 64) return launch_nw<2, 2, 2>(A, st);
   if (L <= 96) return launch_nw<3, 4, 1>(A, st);
-  if (L <= 128) return launch_nw<4, 4, 1>(A, st);  // 512 threads, whole-sector staging
+  // 512 threads, whole-sector staging. At this size the double-buffered
+  // persistent form (209 KB of shared memory) measured slower than one block
+  // per column block (C96 L127: 4.59 against 4.18 ms).
+  if (L <= 128) return launch_step<4, 4, 1, true, false>(A, st);
   return launch_nw<8, 1, 2>(A, st);
 }
 

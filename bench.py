@@ -65,8 +65,11 @@ def algorithmic_bytes_per_column_step(nlev):
 
 
 # ------------------------------------------------------------ CPU baseline
-def _oracle_chunk(args):
-    n, nlev, seed, reps = args
+def _oracle_worker(conn, n, nlev, seed):
+    """One host process of OracleDomain: owns ``n`` columns of the domain
+    (its own seeded state) and advances them by one step per request. The
+    state copy for the next step is made before the request arrives, so the
+    timed step is the oracle's work alone."""
     sys.path.insert(0, REPO)
     from oracle.microphysics import OracleMicrophysics
     from pyshield_b200._config import PhysicsConfig
@@ -74,25 +77,64 @@ def _oracle_chunk(args):
 
     state, area = make_state(n, nlev, seed=seed, n_cube=N_CUBE)
     m = OracleMicrophysics(PhysicsConfig(dt_atmos=DT), n, nlev, area)
-    t0 = time.perf_counter()
-    for _ in range(reps):
-        m(copy_state(state), DT)
-    return time.perf_counter() - t0
+    nxt = copy_state(state)
+    conn.send("ready")
+    while conn.recv() is not None:
+        t0 = time.perf_counter()
+        m(nxt, DT)
+        dt = time.perf_counter() - t0
+        conn.send(dt)
+        nxt = copy_state(state)
+    conn.close()
 
 
-def cpu_baseline(nlev, cores, cols_per_core=3456, reps=1, pool=None):
-    """Time the numpy oracle on ``cores`` processes x ``cols_per_core``
-    columns; returns (column-steps/s, seconds, sample description)."""
-    work = [(cols_per_core, nlev, 100 + i, reps) for i in range(cores)]
-    t0 = time.perf_counter()
-    if cores == 1:
-        _oracle_chunk(work[0])
-    else:
-        pool.map(_oracle_chunk, work)
-    wall = time.perf_counter() - t0
-    cs = cores * cols_per_core * reps / wall
-    sample = f"{cores} x {cols_per_core} columns x {nlev} levels, {reps} step(s) of {DT:g} s, numpy FP64 oracle"
-    return cs, wall, sample
+class OracleDomain:
+    """The FP64 numpy oracle advancing a whole domain of ``ncol`` columns per
+    step, the columns split into ``cores`` contiguous slices, one persistent
+    host process each (spawned, so it may start before or after CUDA is
+    initialised). ``step()`` returns the wall time of one whole-domain step:
+    from the request to the last slice's reply."""
+
+    def __init__(self, ncol, nlev, cores):
+        ctx = mp_.get_context("spawn")
+        base, extra = divmod(ncol, cores)
+        self.sizes = [base + (1 if i < extra else 0) for i in range(cores)]
+        self.ncol, self.nlev, self.cores = ncol, nlev, cores
+        self.conns, self.procs = [], []
+        for i, n in enumerate(self.sizes):
+            a, b = ctx.Pipe()
+            p = ctx.Process(target=_oracle_worker, args=(b, n, nlev, 100 + i), daemon=True)
+            p.start()
+            self.conns.append(a)
+            self.procs.append(p)
+        for c in self.conns:
+            assert c.recv() == "ready"
+
+    def step(self):
+        t0 = time.perf_counter()
+        for c in self.conns:
+            c.send(1)
+        for c in self.conns:
+            c.recv()
+        return time.perf_counter() - t0
+
+    def close(self):
+        for c in self.conns:
+            c.send(None)
+        for p in self.procs:
+            p.join(timeout=30)
+
+
+def cpu_baseline(domain, steps, warmup=1):
+    """Whole-domain steps of the oracle: returns (column-steps/s, seconds per
+    step, sample description)."""
+    for _ in range(warmup):
+        domain.step()
+    t = sum(domain.step() for _ in range(steps))
+    per = t / steps
+    sample = (f"{steps} whole-domain step(s) of {domain.ncol} columns x {domain.nlev} levels (dt {DT:g} s), "
+              f"columns split over {domain.cores} host processes, numpy FP64 oracle")
+    return domain.ncol / per, per, sample
 
 
 # ------------------------------------------------------------ clocks
@@ -732,7 +774,10 @@ def run_ours(args, rank, world, local_rank):
     device = torch.device("cuda", local_rank)
     torch.cuda.set_device(device)
     nlev = args.levels
-    ms, sf, qf, gd, host, land, (nx, ny, n) = build_state(nlev, device, seed=1234 + rank, n_cube=args.ncube)
+    # this rank's slice of the job's domain: its own seeded C-N state
+    start, _ = rank_columns(rank, world, 6 * args.ncube * args.ncube)
+    ms, sf, qf, gd, host, land, (nx, ny, n) = build_state(nlev, device, seed=1234 + start // (6 * args.ncube ** 2),
+                                                          n_cube=args.ncube)
     cfg = PhysicsConfig(dt_atmos=DT)
     mp = Microphysics(sf, qf, gd, cfg, precision=args.form)
     stream = torch.cuda.current_stream()
@@ -894,6 +939,29 @@ def emit(rec):
     print(json.dumps(rec), flush=True)
 
 
+def self_launch(n):
+    """``bench.py --gpus N`` started as a single process: start the N ranks
+    (one process per GPU) through torch.distributed.run with the same
+    arguments on a free local port, and return their exit status."""
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
+def rank_columns(rank, world, ncol):
+    """Columns [start, stop) of the whole job's domain that rank ``rank``
+    advances: the job is ``world`` C-N domains side by side (weak scaling),
+    rank r owning the r-th. Ranks share no column and need no exchange."""
+    if not 0 <= rank < world:
+        raise ValueError(f"rank {rank} outside a world of {world}")
+    return rank * ncol, (rank + 1) * ncol
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -919,6 +987,8 @@ def main():
     if args.ensemble:
         run_ensemble(args)
         return
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(self_launch(args.gpus))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -932,31 +1002,26 @@ def main():
         "dt_s": DT,
         "form": args.form,
         "layout": "NDSL storage, halo 3, i-fastest",
-        "l2": "no flush: 1.26 GB moved per step, > 126 MB L2",
-        "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "1 GPU",
+        "l2": f"no flush: {algorithmic_bytes_per_column_step(nlev) * ncol / 1e9:.3g} GB moved per step, > 126 MB L2",
+        "parallelism": f"{world} GPUs, one C{args.ncube} domain each (rank r owns columns r*{ncol} .. (r+1)*{ncol}-1)"
+                       if world > 1 else "1 GPU",
     }
     metric = "GFDL MP column-steps/s"
 
-    # a process pool for the CPU oracle must start before any CUDA use
-    pool = None
+    # the oracle's worker processes start before any CUDA use
+    domain = None
     want_cpu = (args.impl == "reference" or not args.no_cpu_baseline) and rank == 0 and world == 1
-    if want_cpu and cores > 1:
-        pool = mp_.get_context("spawn").Pool(cores)
-        pool.map(_oracle_chunk, [(24, nlev, 0, 1)] * cores)  # warm the workers
+    if args.impl == "reference" and rank == 0:
+        want_cpu = True
+    if want_cpu:
+        domain = OracleDomain(ncol, nlev, cores)
 
     if args.impl == "reference":
         if rank != 0:
             return
-        vals = []
-        for _ in range(args.warmup if args.warmup < 1 else 1):
-            cpu_baseline(nlev, cores, cols_per_core=256, reps=1, pool=pool)
-        sample = ""
-        t_all = 0.0
-        for _ in range(args.steps):
-            v, wall, sample = cpu_baseline(nlev, cores, cols_per_core=864, reps=1, pool=pool)
-            vals.append(v)
-            t_all += wall
-        value = len(vals) * cores * 864 / t_all
+        # the driver's W warm-up steps, then K timed whole-domain steps
+        value, per, sample = cpu_baseline(domain, args.steps, warmup=args.warmup)
+        domain.close()
         rec = {
             "impl": "reference",
             "metric": metric,
@@ -965,7 +1030,7 @@ def main():
             "n_gpus": args.gpus,
             "steps": args.steps,
             "warmup": args.warmup,
-            "ms_per_step": 1000.0 * ncol / value,
+            "ms_per_step": 1000.0 * per,
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
@@ -975,10 +1040,9 @@ def main():
             "cpu_baseline": {"value": value, "unit": "column-steps/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "column-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference (GT4Py/NDSL) cannot be installed here; this times the FP64 numpy oracle that "
-                    "restates the reference's numpy backend bit for bit, on every host core",
+                    "restates the reference's numpy backend bit for bit, whole-domain steps on every host core"
+                    + ("; only rank 0 runs it" if world > 1 else ""),
         }
-        if pool:
-            pool.close()
         emit(rec)
         return
 
@@ -1000,12 +1064,14 @@ def main():
 
     cpu = None
     if want_cpu:
-        v, wall, sample = cpu_baseline(nlev, cores, cols_per_core=3456, reps=1, pool=pool)
-        v1, wall1, _ = cpu_baseline(nlev, 1, cols_per_core=3456, reps=1)
+        v, per, sample = cpu_baseline(domain, 3, warmup=1)
+        domain.close()
+        one = OracleDomain(3456, nlev, 1)
+        v1, _, _ = cpu_baseline(one, 1, warmup=0)
+        one.close()
         cpu = {"value": v, "unit": "column-steps/s", "cores": cores, "kind": "port",
-               "sample": sample + f"; one core alone: {v1:.4g} column-steps/s"}
-    if pool:
-        pool.close()
+               "sample": sample + f"; {1000.0 * per:.0f} ms per step; one process alone on 3456 columns: "
+                                  f"{v1:.4g} column-steps/s"}
     adjoint = run_adjoint() if (rank == 0 and world == 1 and not args.no_adjoint and args.form == "plain") else None
     physics = (run_physics(n_cube=args.ncube, nlev=nlev)
                if (rank == 0 and world == 1 and not args.no_physics and args.form == "plain") else None)

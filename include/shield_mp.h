@@ -178,16 +178,27 @@ int shield_mp_step_vjp(void* handle, const ShieldMpFields* state, const ShieldMp
  *    SHIELD_ELAYOUT and should use shield_mp_step.
  *  - The first call on each device finds and clears the array, and
  *    synchronises that device. Make that first call before any stream
- *    capture.
+ *    capture: made while `stream` is capturing, it fails with SHIELD_EINVAL.
+ *    After a cudaDeviceReset the next call repeats this set-up.
  *  - All calls on a device share the array. It keeps what the last call
  *    left. Pass first_step != 0 on the first step of a run, or when
- *    switching to another domain: this zeroes the accumulator, as a new
- *    handle starts at zero. Calls that overlap on the GPU (other streams,
- *    threads or domains) race on the array.
+ *    switching to another domain: this zeroes the accumulator and the error
+ *    word, as a new handle starts at zero. Calls that overlap on the GPU
+ *    (other streams, threads or domains) race on the array.
+ *  - A column that produces a NaN or an infinity is recorded in a word of
+ *    the same array; shield_mp_check_noalloc reads and clears it.
  *  - Errors are reported through shield_last_error. */
 int shield_mp_step_noalloc(const ShieldMpConfig* cfg, int nx, int ny, int nz, ShieldField2D area,
                            const ShieldMpFields* fields, double timestep, int precision, int first_step,
                            void* stream);
+
+/* The allocation-free step's failure check, like shield_mp_check for a
+ * handle (no counterpart in the reference): waits for `stream`, then returns
+ * SHIELD_OK with *bad_column = -1, or SHIELD_EDEVICE with the first column
+ * (i + nx j) that produced a NaN or an infinity since the last check or
+ * first_step call, and clears the record. nx is the calls' domain width,
+ * used only for the message. Allocates nothing. */
+int shield_mp_check_noalloc(int nx, int64_t* bad_column, void* stream);
 
 /* ---------------------------------------------------------------------------
  * Ensembles: many independent domains (members of different sizes and

@@ -173,6 +173,7 @@ EXPORTS = (
     "shield_copy_dycore_to_physics",
     "shield_agrid_to_dgrid",
     "shield_mp_check",
+    "shield_mp_check_noalloc",
 )
 
 _lib = None
@@ -220,6 +221,7 @@ def load():
         ctypes.POINTER(ShieldMpConfig), i32, i32, i32, ShieldField2D, ctypes.POINTER(ShieldMpFields), dbl, i32, i32, vp,
     ]
     lib.shield_mp_check.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), vp]
+    lib.shield_mp_check_noalloc.argtypes = [i32, ctypes.POINTER(ctypes.c_int64), vp]
     lib.shield_agrid_to_dgrid.argtypes = [
         i32, i32, i32, i32, dbl, ctypes.POINTER(ShieldEdgePlan), ctypes.POINTER(ShieldDwindGeometry), ShieldField3D,
         ShieldField3D, ShieldField3D, ShieldField3D, vp,

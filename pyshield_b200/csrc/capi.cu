@@ -495,23 +495,43 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxCells + 32]
 std::mutex g_noalloc_mu;
 double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
 
-// Once per device, with that device current: look up the array's device
-// address (its host-side name is only a stand-in) and clear it. Runs inside
-// the first call on each device; it synchronises with the legacy default
-// stream, so that first call should come before any stream capture.
-int noalloc_setup(int dev, double** out) {
+// The array's device address on the current device. Its host-side name is
+// only a stand-in, so the address is looked up with the device current. The
+// first call on a device also clears the array; that clear runs on the
+// legacy default stream and synchronises the device, so it is refused while
+// the caller's stream is being captured. The lookup is repeated on every
+// call (it allocates nothing): after a cudaDeviceReset the module is loaded
+// again, possibly elsewhere, and a changed address repeats the set-up.
+int noalloc_setup(int dev, cudaStream_t st, double** out) {
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    double* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetSymbolAddress of the allocation-free scratch");
+  double* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetSymbolAddress of the allocation-free scratch");
+  if (g_noalloc_ptr[dev] != p) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(st, &cs);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaStreamIsCapturing");
+    if (cs != cudaStreamCaptureStatusNone)
+      return fail(nullptr, SHIELD_EINVAL,
+                  "the first allocation-free call on a device clears its scratch and synchronises the device; "
+                  "make it before any stream capture");
     e = cudaMemset(p, 0, sizeof(g_noalloc_scratch));
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return cuda_fail(nullptr, e, "clearing the allocation-free scratch");
     g_noalloc_ptr[dev] = p;
   }
-  *out = g_noalloc_ptr[dev];
+  *out = p;
   return SHIELD_OK;
+}
+
+// The current device's scratch address and its validated ordinal, for the
+// entry points below.
+int noalloc_device(cudaStream_t st, double** scratch) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDevice");
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(nullptr, SHIELD_EINVAL, "device ordinal beyond 63");
+  return noalloc_setup(dev, st, scratch);
 }
 
 }  // namespace
@@ -531,13 +551,11 @@ extern "C" int shield_mp_step_noalloc(const ShieldMpConfig* cfg, int nx, int ny,
   if (!area.ptr) return fail(nullptr, SHIELD_EINVAL, "null area pointer");
   if (precision != SHIELD_MP_PLAIN && precision != SHIELD_MP_MIXED)
     return fail(nullptr, SHIELD_EINVAL, "unknown precision mode");
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDevice");
-  if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(nullptr, SHIELD_EINVAL, "device ordinal beyond 63");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
   double* scratch = nullptr;
-  int rc = noalloc_setup(dev, &scratch);
+  int rc = noalloc_device(st, &scratch);
   if (rc != SHIELD_OK) return rc;
+  cudaError_t e = cudaSuccess;
 
   MpArgs A;
   std::memset(&A, 0, sizeof(A));
@@ -574,12 +592,12 @@ extern "C" int shield_mp_step_noalloc(const ShieldMpConfig* cfg, int nx, int ny,
   A.ice = F->ice;
   A.graupel = F->graupel;
   A.err = reinterpret_cast<int*>(scratch + kNoAllocMaxCells);
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   // The array keeps whatever the last call on this device left in it. The
   // first step of a run (or of another domain) starts from a zero
-  // accumulator, as a freshly constructed handle does.
+  // accumulator and a clear error word, as a freshly constructed handle does.
   if (first_step) {
     e = cudaMemsetAsync(scratch, 0, sizeof(double) * (size_t)(ncol * nz), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(A.err, 0, sizeof(int), st);
     if (e != cudaSuccess) return cuda_fail(nullptr, e, "clearing the accumulator");
   }
   if (A.K.de_ice) {
@@ -589,4 +607,30 @@ extern "C" int shield_mp_step_noalloc(const ShieldMpConfig* cfg, int nx, int ny,
   e = mp_launch_step(A, precision, st);
   if (e != cudaSuccess) return cuda_fail(nullptr, e, "microphysics launch");
   return SHIELD_OK;
+}
+
+// The allocation-free step's error word: the first column (+ 1) of any call
+// since the last check (or since the last first_step call) that produced a
+// NaN or an infinity. Read on `stream` after the calls queued on it.
+extern "C" int shield_mp_check_noalloc(int nx, int64_t* bad_column, void* stream) {
+  if (bad_column) *bad_column = -1;
+  if (nx < 1) return fail(nullptr, SHIELD_EINVAL, "nx must be positive");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  double* scratch = nullptr;
+  int rc = noalloc_device(st, &scratch);
+  if (rc != SHIELD_OK) return rc;
+  int* err = reinterpret_cast<int*>(scratch + kNoAllocMaxCells);
+  int v = 0;
+  cudaError_t e = cudaMemcpyAsync(&v, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "reading the allocation-free error word");
+  if (v == 0) return SHIELD_OK;
+  e = cudaMemsetAsync(err, 0, sizeof(int), st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "clearing the allocation-free error word");
+  const int64_t c = (int64_t)v - 1;
+  if (bad_column) *bad_column = c;
+  return fail(nullptr, SHIELD_EDEVICE,
+              "column " + std::to_string(c) + " (i = " + std::to_string(c % nx) + ", j = " + std::to_string(c / nx) +
+                  ") produced a NaN or an infinity");
 }

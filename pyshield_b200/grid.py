@@ -34,6 +34,40 @@ class GridIndexing:
         return (self.nx + 2 * h + add[0], self.ny + 2 * h + add[1], self.nz + add[2])
 
 
+class SubtileGridSizer:
+    """The NDSL grid sizer the reference's ``PhysicsState.init_from_storages``
+    takes (``sizer.get_origin(dims)``, ``sizer.get_extent(dims)``): a rank's
+    subtile of ``nx x ny`` points and ``nz`` levels inside a storage with
+    ``n_halo`` halo points on each horizontal side."""
+
+    def __init__(self, nx, ny, nz, n_halo=3, extra_dim_lengths=None):
+        self.nx, self.ny, self.nz, self.n_halo = int(nx), int(ny), int(nz), int(n_halo)
+        self.extra_dim_lengths = dict(extra_dim_lengths or {})
+
+    @classmethod
+    def from_tile_params(cls, nx_tile, ny_tile, nz, n_halo, extra_dim_lengths, layout, **_):
+        """A cube tile of ``nx_tile x ny_tile`` split over a ``layout`` of
+        ranks (the subtile is nx_tile / layout[1] by ny_tile / layout[0])."""
+        return cls(int(nx_tile / layout[1]), int(ny_tile / layout[0]), nz, n_halo, extra_dim_lengths)
+
+    def get_origin(self, dims):
+        return tuple(self.n_halo if d.startswith(("x", "y")) else 0 for d in dims)
+
+    def get_extent(self, dims):
+        out = []
+        for d in dims:
+            inc = 1 if d.endswith("interface") else 0
+            if d.startswith("x"):
+                out.append(self.nx + inc)
+            elif d.startswith("y"):
+                out.append(self.ny + inc)
+            elif d.startswith("z"):
+                out.append(self.nz + inc)
+            else:
+                out.append(self.extra_dim_lengths[d])
+        return tuple(out)
+
+
 class StencilFactory:
     def __init__(self, grid_indexing):
         self.grid_indexing = grid_indexing

@@ -107,7 +107,6 @@ class Microphysics:
         dev = torch.device("cuda", torch.cuda.current_device())
         self._precip = torch.zeros((4, self.ny, self.nx), dtype=torch.float64, device=dev)
         self._fields = ShieldMpFields()
-        self._key = None
 
     # surface precipitation of the last call, (nx, ny) views, mm/day
     @property
@@ -138,10 +137,11 @@ class Microphysics:
         return F
 
     def __call__(self, state, timestep, stream=None):
-        key = tuple(id(getattr(state, n).data) for n in _lib.MP_STATE_FIELDS + _lib.MP_TENDENCY_FIELDS) + (id(state.land),)
-        if key != self._key:
-            self._build_fields(state)
-            self._key = key
+        # the field table (pointer at the domain origin and element strides
+        # of every storage) is rebuilt from the storages on every call, so a
+        # state whose arrays were freed and reallocated is never stepped
+        # through stale pointers
+        self._build_fields(state)
         lib = load()
         rc = lib.shield_mp_step(
             self._handle, ctypes.byref(self._fields), float(timestep), _PRECISION[self.precision], ctypes.c_void_p(_current_stream(stream))

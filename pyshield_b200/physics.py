@@ -26,6 +26,8 @@ runs on the current torch stream (or the ``stream`` passed), and
 
 import ctypes
 import dataclasses
+
+import numpy as np
 from dataclasses import InitVar
 from typing import Any, List
 
@@ -36,51 +38,59 @@ from ._lib import SHIELD_PHYS_PREPARE_MICROPHYSICS, ShieldPhysicsFields, check, 
 from .coupling import update_physics_state_with_tendencies
 from .grid import X_DIM, Y_DIM, Z_DIM, Z_INTERFACE_DIM
 from .microphysics import Microphysics, MicrophysicsState, _current_stream
-from .quantity import field3d
+from .quantity import Quantity, field3d
 
-_INTERFACE = ("phii", "prsi", "prsik")
+_XYZ = [X_DIM, Y_DIM, Z_DIM]
+_XYZI = [X_DIM, Y_DIM, Z_INTERFACE_DIM]
+_XY = [X_DIM, Y_DIM]
+
+
+def _field(name, dims, units):
+    """A state field with the reference's metadata (physics_state.py:17-288)."""
+    return dataclasses.field(metadata={"name": name, "dims": list(dims), "units": units})
 
 
 @dataclasses.dataclass
 class PhysicsState:
     """pySHiELD's ``PhysicsState`` (physics_state.py:17-330): the same fields
-    in the same order; ``phii``, ``prsi`` and ``prsik`` are interface (nz + 1
-    level) fields, ``land`` is 2-D."""
+    in the same order, each with the reference's metadata (long name, dims,
+    units); ``phii``, ``prsi`` and ``prsik`` are interface (nz + 1 level)
+    fields, ``land`` is 2-D."""
 
-    qvapor: Any
-    qliquid: Any
-    qice: Any
-    qrain: Any
-    qsnow: Any
-    qgraupel: Any
-    qo3mr: Any
-    qsgs_tke: Any
-    qcld: Any
-    pt: Any
-    delp: Any
-    delz: Any
-    ua: Any
-    va: Any
-    w: Any
-    omga: Any
-    physics_updated_specific_humidity: Any
-    physics_updated_qliquid: Any
-    physics_updated_qice: Any
-    physics_updated_qrain: Any
-    physics_updated_qsnow: Any
-    physics_updated_qgraupel: Any
-    physics_updated_cloud_fraction: Any
-    physics_updated_pt: Any
-    physics_updated_ua: Any
-    physics_updated_va: Any
-    delprsi: Any
-    phii: Any
-    phil: Any
-    dz: Any
-    wmp: Any
-    prsi: Any
-    prsik: Any
-    land: Any
+    qvapor: Any = _field("specific_humidity", _XYZ, "kg/kg")
+    qliquid: Any = _field("cloud_water_mixing_ratio", _XYZ, "kg/kg")
+    qice: Any = _field("cloud_ice_mixing_ratio", _XYZ, "kg/kg")
+    qrain: Any = _field("rain_mixing_ratio", _XYZ, "kg/kg")
+    qsnow: Any = _field("snow_mixing_ratio", _XYZ, "kg/kg")
+    qgraupel: Any = _field("graupel_mixing_ratio", _XYZ, "kg/kg")
+    qo3mr: Any = _field("ozone_mixing_ratio", _XYZ, "kg/kg")
+    qsgs_tke: Any = _field("turbulent_kinetic_energy", _XYZ, "m**2/s**2")
+    qcld: Any = _field("cloud_fraction", _XYZ, "")
+    pt: Any = _field("air_temperature", _XYZ, "degK")
+    delp: Any = _field("pressure_thickness_of_atmospheric_layer", _XYZ, "Pa")
+    delz: Any = _field("vertical_thickness_of_atmospheric_layer", _XYZ, "m")
+    ua: Any = _field("eastward_wind", _XYZ, "m/s")
+    va: Any = _field("northward_wind", _XYZ, "m/s")
+    w: Any = _field("vertical_wind", _XYZ, "m/s")
+    omga: Any = _field("vertical_pressure_velocity", _XYZ, "Pa/s")
+    physics_updated_specific_humidity: Any = _field("physics_updated_specific_humidity", _XYZ, "kg/kg")
+    physics_updated_qliquid: Any = _field("physics_updated_liquid_water_mixing_ratio", _XYZ, "kg/kg")
+    physics_updated_qice: Any = _field("physics_updated_ice_water_mixing_ratio", _XYZ, "kg/kg")
+    physics_updated_qrain: Any = _field("physics_updated_rain_water_mixing_ratio", _XYZ, "kg/kg")
+    physics_updated_qsnow: Any = _field("physics_updated_snow_mixing_ratio", _XYZ, "kg/kg")
+    physics_updated_qgraupel: Any = _field("physics_updated_graupel_mixing_ratio", _XYZ, "kg/kg")
+    physics_updated_cloud_fraction: Any = _field("physics_cloud_fraction", _XYZ, "")
+    physics_updated_pt: Any = _field("physics_air_temperature", _XYZ, "degK")
+    physics_updated_ua: Any = _field("physics_eastward_wind", _XYZ, "m/s")
+    physics_updated_va: Any = _field("physics_northward_wind", _XYZ, "m/s")
+    delprsi: Any = _field("model_level_pressure_thickness_in_physics", _XYZ, "Pa")
+    phii: Any = _field("interface_geopotential_height", _XYZI, "m")
+    phil: Any = _field("layer_geopotential_height", _XYZ, "m")
+    dz: Any = _field("geopotential_height_thickness", _XYZ, "m")
+    wmp: Any = _field("layer_mean_vertical_velocity_microph", _XYZ, "m/s")
+    prsi: Any = _field("interface_pressure", _XYZI, "Pa")
+    prsik: Any = _field("log_interface_pressure", _XYZI, "Pa")
+    land: Any = _field("land_mask", _XY, "-")
     quantity_factory: InitVar[Any]
     schemes: InitVar[List]
 
@@ -99,14 +109,87 @@ class PhysicsState:
     @classmethod
     def init_zeros(cls, quantity_factory, schemes):
         """Every field zero, allocated by ``quantity_factory`` (physics_state.py:327-343)."""
-        arrays = {}
-        for f in dataclasses.fields(cls):
-            if f.name == "land":
-                arrays[f.name] = quantity_factory.zeros([X_DIM, Y_DIM], "")
-            else:
-                dims = [X_DIM, Y_DIM, Z_INTERFACE_DIM if f.name in _INTERFACE else Z_DIM]
-                arrays[f.name] = quantity_factory.zeros(dims, "")
+        arrays = {f.name: quantity_factory.zeros(f.metadata["dims"], f.metadata["units"]) for f in cls._state_fields()}
         return cls(**arrays, quantity_factory=quantity_factory, schemes=schemes)
+
+    @classmethod
+    def init_from_storages(cls, storages, sizer, quantity_factory, schemes):
+        """Wrap existing storages (physics_state.py:344-364): ``storages[name]``
+        is each field's full array; its compute domain is
+        ``sizer.get_origin(dims)`` / ``sizer.get_extent(dims)``. The arrays
+        are used in place, not copied."""
+        inputs = {}
+        for f in cls._state_fields():
+            dims = f.metadata["dims"]
+            inputs[f.name] = Quantity(storages[f.name], dims, f.metadata["units"], origin=sizer.get_origin(dims),
+                                      extent=sizer.get_extent(dims))
+        return cls(**inputs, quantity_factory=quantity_factory, schemes=schemes)
+
+    @classmethod
+    def _state_fields(cls):
+        return [f for f in dataclasses.fields(cls) if "dims" in f.metadata]
+
+    @property
+    def xr_dataset(self):
+        """The state as a dataset (physics_state.py:366-383): one variable per
+        field holding its full storage, with dims ``f"{dim}_{name}"`` and
+        attrs ``long_name`` and ``units``. An ``xarray.Dataset`` when xarray
+        is importable; otherwise a ``StateDataset`` with the same variables,
+        dims and attrs (host numpy copies of the storages)."""
+        data_vars = {}
+        for f in self._state_fields():
+            data = getattr(self, f.name).data
+            if hasattr(data, "detach"):
+                data = data.detach().cpu().numpy()
+            data_vars[f.name] = StateVariable(
+                np.asarray(data), [f"{d}_{f.name}" for d in f.metadata["dims"]],
+                {"long_name": f.metadata["name"], "units": f.metadata.get("units", "unknown")},
+            )
+        try:
+            import xarray as xr
+        except ImportError:
+            return StateDataset(data_vars)
+        return xr.Dataset(
+            data_vars={n: xr.DataArray(v.values, dims=v.dims, attrs=v.attrs) for n, v in data_vars.items()})
+
+
+class StateVariable:
+    """One variable of ``PhysicsState.xr_dataset`` without xarray: ``values``
+    (numpy), ``dims`` (names, one per axis) and ``attrs``."""
+
+    def __init__(self, values, dims, attrs):
+        if len(dims) != values.ndim:
+            raise ValueError(f"{len(dims)} dims for a {values.ndim}-D array")
+        self.values, self.dims, self.attrs = values, tuple(dims), dict(attrs)
+
+    @property
+    def sizes(self):
+        return dict(zip(self.dims, self.values.shape))
+
+
+class StateDataset:
+    """``PhysicsState.xr_dataset`` without xarray: ``data_vars`` maps each
+    field's name to its ``StateVariable``; ``ds[name]`` and ``ds.dims`` work
+    as in xarray."""
+
+    def __init__(self, data_vars):
+        self.data_vars = dict(data_vars)
+
+    def __getitem__(self, name):
+        return self.data_vars[name]
+
+    def __contains__(self, name):
+        return name in self.data_vars
+
+    def __iter__(self):
+        return iter(self.data_vars)
+
+    @property
+    def dims(self):
+        out = {}
+        for v in self.data_vars.values():
+            out.update(v.sizes)
+        return out
 
 
 class Physics:
@@ -134,7 +217,6 @@ class Physics:
             self._microphysics = Microphysics(stencil_factory, quantity_factory, grid_data, namelist,
                                               precision=precision)
         self._fields = ShieldPhysicsFields()
-        self._key = None
         load()
 
     def _setup_statein(self):
@@ -177,12 +259,9 @@ class Physics:
         statein, get_prs_fv3, get_phi_fv3 and, with GFS_microphysics,
         prepare_microphysics, as one kernel launch."""
         ps = physics_state
-        key = tuple(id(getattr(ps, f.name).data) for f in dataclasses.fields(ps))
-        if ps.microphysics is not None:
-            key += tuple(id(getattr(ps.microphysics, t).data) for t in _lib.MP_TENDENCY_FIELDS)
-        if key != self._key:
-            self._build_fields(ps)
-            self._key = key
+        # rebuilt on every call from the storages themselves (see
+        # Microphysics.__call__), never cached by object identity
+        self._build_fields(ps)
         flags = SHIELD_PHYS_PREPARE_MICROPHYSICS if self._gfs_microphysics else 0
         rc = load().shield_physics_prestep(self.nx, self.ny, self.nz, self.n_halo, self._nwat, self._ptop, flags,
                                            ctypes.byref(self._fields), ctypes.c_void_p(_current_stream(stream)))

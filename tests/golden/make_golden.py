@@ -580,9 +580,13 @@ def run_physics_case(name, nx, ny, L, dt, seed, overrides):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("PYSHIELD_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("PYSHIELD_REFERENCE"),
+                    help="checkout of pySHiELD (the directory holding the pySHiELD package); "
+                         "or set PYSHIELD_REFERENCE")
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give --reference <pySHiELD checkout> or set PYSHIELD_REFERENCE")
     _setup_paths(args.reference)
     for case in mp_cases():
         if args.only and args.only != case[0]:

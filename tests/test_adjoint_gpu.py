@@ -151,6 +151,15 @@ def test_exact_column_heights(nz):
     _assert_exact(exact_check(6, 3, nz, 150.0, 14))
 
 
+@pytest.mark.parametrize("nx,ny,nz", [(5, 5, 127), (5, 3, 79)])
+def test_exact_partly_filled_block(nx, ny, nz):
+    """Column counts that are not a multiple of the columns per block (3 at
+    L127, 4 at L79): the last block holds columns past the domain's end,
+    which must neither be computed into the domain nor disturb the block's
+    column exchanges."""
+    _assert_exact(exact_check(nx, ny, nz, 150.0, 15))
+
+
 def test_window_matches_exact_column():
     """A 3-step window through torch.autograd (MicrophysicsStep per step,
     the state update between steps, each step's inputs as its checkpoint)

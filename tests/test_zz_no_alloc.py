@@ -39,9 +39,24 @@ def _last_error(lib):
     return buf.value.decode()
 
 
-@pytest.mark.gpu
-@pytest.mark.parametrize("precision", ["plain", "mixed"])
-def test_noalloc_matches_handle_step(precision):
+def _noalloc_call(lib, c, nx, ny, nz, area2, F, dt, mode, first, stream):
+    rc = lib.shield_mp_step_noalloc(ctypes.byref(c), nx, ny, nz, area2, ctypes.byref(F), dt, mode, int(first), stream)
+    assert rc == 0, _last_error(lib)
+
+
+def _compare(mp, ms_h, ms_n, precip, nx, ny, nz, state, dt, ctx):
+    ref = read_state(ms_h, nx, ny, nz)
+    got = read_state(ms_n, nx, ny, nz)
+    for i, p in enumerate(("rain", "snow", "ice", "graupel")):
+        ref[p] = getattr(mp, p).t().contiguous().cpu().numpy().reshape(-1)
+        got[p] = precip[i].contiguous().cpu().numpy().reshape(-1)
+    assert np.any(ref["qa_dt"] != 0.0)
+    assert_close(got, ref, FIELDS, TOL_PLAIN, ctx=ctx, fl=floors(state, ref, dt))
+
+
+def _pair(nx, ny, nz, dt, seed, precision):
+    """A handle step and the allocation-free step's arguments on two copies
+    of the same state."""
     import torch
 
     from pyshield_b200._config import PhysicsConfig
@@ -50,41 +65,85 @@ def test_noalloc_matches_handle_step(precision):
     from pyshield_b200.microphysics import Microphysics
     from pyshield_b200.quantity import field2d
 
-    nx, ny, nz, dt = 24, 16, 79, 225.0
     cfg = PhysicsConfig(dt_atmos=dt, mp_time=dt / 2, do_qa=False)
-    state, area = make_state(nx * ny, nz, seed=11, n_cube=nx, sat_fraction=0.3)
-
+    state, area = make_state(nx * ny, nz, seed=seed, n_cube=nx, sat_fraction=0.3)
     # the existing entry point, through its handle
     ms_h, sf, qf, gd = device_state(state, area, nx, ny)
     mp = Microphysics(sf, qf, gd, cfg, precision=precision)
     # the allocation-free entry point, on its own copy of the same state
     ms_n, _, _, gd_n = device_state(state, area, nx, ny)
-    lib = load()
-    c = make_config(cfg)
     precip = torch.zeros((4, ny, nx), dtype=torch.float64, device="cuda")
     F = _fields(ms_n, nx, ny, nz, precip)
     area2 = field2d(gd_n.area, (nx, ny))
     mode = SHIELD_MP_MIXED if precision == "mixed" else SHIELD_MP_PLAIN
-    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return load(), make_config(cfg), state, mp, ms_h, ms_n, precip, F, area2, mode
 
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nz", [79, 127])
+@pytest.mark.parametrize("precision", ["plain", "mixed"])
+def test_noalloc_matches_handle_step(precision, nz):
+    """Two calls in a row against the handle step (the second reads the
+    accumulator the first left in the library's array)."""
+    import torch
+
+    nx, ny, dt = 24, 16, 225.0
+    lib, c, state, mp, ms_h, ms_n, precip, F, area2, mode = _pair(nx, ny, nz, dt, 11, precision)
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     for step in range(2):
         mp(ms_h, dt)
         torch.cuda.synchronize()
         free_before = torch.cuda.mem_get_info()[0]
-        rc = lib.shield_mp_step_noalloc(ctypes.byref(c), nx, ny, nz, area2, ctypes.byref(F), dt, mode, int(step == 0), stream)
-        assert rc == 0, _last_error(lib)
+        _noalloc_call(lib, c, nx, ny, nz, area2, F, dt, mode, step == 0, stream)
         torch.cuda.synchronize()
         if step > 0:
             # after the first call's set-up, a call takes no device memory
             assert torch.cuda.mem_get_info()[0] == free_before
+        _compare(mp, ms_h, ms_n, precip, nx, ny, nz, state, dt, f"noalloc/{precision}/L{nz}/call{step}")
+    bad = ctypes.c_int64(0)
+    assert lib.shield_mp_check_noalloc(nx, ctypes.byref(bad), stream) == 0, _last_error(lib)
+    assert bad.value == -1
 
-        ref = read_state(ms_h, nx, ny, nz)
-        got = read_state(ms_n, nx, ny, nz)
-        for i, p in enumerate(("rain", "snow", "ice", "graupel")):
-            ref[p] = getattr(mp, p).t().contiguous().cpu().numpy().reshape(-1)
-            got[p] = precip[i].contiguous().cpu().numpy().reshape(-1)
-        assert np.any(ref["qa_dt"] != 0.0)
-        assert_close(got, ref, FIELDS, TOL_PLAIN, ctx=f"noalloc/{precision}/call{step}", fl=floors(state, ref, dt))
+
+@pytest.mark.gpu
+def test_noalloc_first_step_after_larger_domain():
+    """A larger domain's calls leave its accumulator in the shared array; a
+    smaller domain's first_step call must then start from zero, exactly as a
+    fresh handle does."""
+    import torch
+
+    dt = 225.0
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    lib, c, _, _, _, _, _, Fb, area_b, mode = _pair(40, 30, 79, dt, 5, "plain")
+    for step in range(2):
+        _noalloc_call(lib, c, 40, 30, 79, area_b, Fb, dt, mode, step == 0, stream)
+    nx, ny, nz = 12, 10, 79
+    lib, c, state, mp, ms_h, ms_n, precip, F, area2, mode = _pair(nx, ny, nz, dt, 6, "plain")
+    for step in range(2):
+        mp(ms_h, dt)
+        _noalloc_call(lib, c, nx, ny, nz, area2, F, dt, mode, step == 0, stream)
+        torch.cuda.synchronize()
+        _compare(mp, ms_h, ms_n, precip, nx, ny, nz, state, dt, f"noalloc/after-larger/call{step}")
+
+
+@pytest.mark.gpu
+def test_noalloc_reports_nonfinite_column():
+    """A NaN planted on the host in one column's input is reported by
+    shield_mp_check_noalloc with that column, and the record is cleared."""
+    import torch
+
+    nx, ny, nz, dt = 12, 6, 79, 225.0
+    lib, c, _, _, _, ms_n, _, F, area2, mode = _pair(nx, ny, nz, dt, 3, "plain")
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    i, j = 7, 2
+    ms_n.pt.view[i, j, 30] = float("nan")
+    _noalloc_call(lib, c, nx, ny, nz, area2, F, dt, mode, True, stream)
+    bad = ctypes.c_int64(0)
+    assert lib.shield_mp_check_noalloc(nx, ctypes.byref(bad), stream) == -4
+    assert bad.value == i + nx * j
+    assert f"i = {i}, j = {j}" in _last_error(lib)
+    assert lib.shield_mp_check_noalloc(nx, ctypes.byref(bad), stream) == 0
+    assert bad.value == -1
 
 
 def test_noalloc_rejects_oversized_domain():

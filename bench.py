@@ -55,6 +55,11 @@ HALO = 3
 # the kernel streams each field once, so the ratio carries over to C96.
 NCU_TRAFFIC_RATIO = 315.11 / 315.19
 
+# FP64 flops per column-step of the plain step kernel (2 per DFMA, 1 per
+# DADD or DMUL, thread-level counts of predicated-on instructions), from an
+# ncu capture of the C48 launch divided by its columns; by level count.
+FP64_FLOPS_PER_COLUMN_STEP = {}
+
 
 def algorithmic_bytes_per_column_step(nlev):
     """Reads: 13 state fields, 10 tendencies (accumulated) and the persistent
@@ -197,6 +202,43 @@ def peaks():
         return float(p["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
         return 6650.0, "fallback"
+
+
+def fp64_peak(reps=5):
+    """Measured FP64 throughput of this GPU (TFLOP/s): CUDA-event time of the
+    FP64 probe (libshield_probe.so; independent DFMA chains on every SM, 2
+    flops per DFMA), the mean of ``reps`` launches after a warm-up, with
+    nothing changed on the GPU."""
+    import ctypes
+
+    import torch
+
+    from pyshield_b200.build import PROBE_LIB
+
+    lib = ctypes.CDLL(PROBE_LIB)
+    lib.shield_probe_dfma.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                      ctypes.c_void_p]
+    nsm = lib.shield_probe_sm_count()
+    bps, iters = 8, 20000
+    out = torch.empty(nsm * bps, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    flops = ctypes.c_double()
+
+    def launch():
+        rc = lib.shield_probe_dfma(ctypes.c_void_p(out.data_ptr()), bps, iters, ctypes.byref(flops),
+                                   ctypes.c_void_p(stream.cuda_stream))
+        assert rc == 0, f"FP64 probe launch failed ({rc})"
+
+    launch()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        launch()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    return flops.value / (ms / 1000.0) / 1e12
 
 
 # ------------------------------------------------------------ GPU arm
@@ -1077,6 +1119,17 @@ def main():
                if (rank == 0 and world == 1 and not args.no_physics and args.form == "plain") else None)
     coupling = (run_coupling(n_cube=args.ncube, nlev=nlev)
                 if (rank == 0 and world == 1 and not args.no_coupling and args.form == "plain") else None)
+    fp64 = None
+    if rank == 0:
+        peak64 = fp64_peak()
+        fp64 = {"bound": "fp64", "peak": peak64, "unit": "TFLOP/s",
+                "peak_source": "measured: FP64 probe (independent DFMA chains on every SM, CUDA events)"}
+        if FP64_FLOPS_PER_COLUMN_STEP.get(nlev) and args.form == "plain":
+            ach = FP64_FLOPS_PER_COLUMN_STEP[nlev] * r["n"] / (r["mean_launch_ms"] / 1000.0) / 1e12
+            fp64.update({"achieved": ach, "frac": ach / peak64,
+                         "flops_per_column_step": FP64_FLOPS_PER_COLUMN_STEP[nlev],
+                         "flops_source": "ncu smsp__sass_thread_inst_executed_op_{dfma,dadd,dmul}_pred_on.sum "
+                                         "(2 flops per DFMA) of the C48 launch, per column"})
     d2p = dwind = None
     if rank == 0 and world == 1 and not args.no_coupling and args.form == "plain":
         d2p = run_d2p(n_cube=args.ncube, nlev=nlev)
@@ -1110,6 +1163,7 @@ def main():
                                            "scaled by columns to this launch",
                          "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
                          "bytes_per_launch": bytes_launch},
+            "roofline_fp64": fp64,
             "cpu_baseline": cpu,
             "gpu_launches": steps,
             "mixed": ({"value": world * r["n"] / (r["mixed_ms"] / 1000.0), "unit": "column-steps/s",

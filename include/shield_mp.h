@@ -157,6 +157,23 @@ typedef struct {
   ShieldField3D pt, qvapor, qliquid, qrain, qice, qsnow, qgraupel, qcld, ua, va, delprsi, delz, wmp, qaz;
 } ShieldMpGradients;
 
+/* The plain FP64 step of shield_mp_step that also records, per column and
+ * sub-step, the scheme's column-wide branch decisions, so that they can be
+ * compared bit for bit with the reference's (its no_fall and stop_k
+ * temporaries, microphysics.py:349-368, :706-754, :773-1168). Word
+ * flags[s * nx * ny + (i + nx * j)] of sub-step s < ntimes holds:
+ *   bit 0 / 1  rain falls in the first / second warm_rain pass (no_fall == 0)
+ *   bit 2      cloud ice falls (no_fall == 0 and vi_fac >= 1e-5)
+ *   bit 3 / 4  snow / graupel fall
+ *   bits 16-23 the melting level: the first level k whose stop_k is 1.
+ * nflags: words available (at least ntimes * nx * ny, see
+ * shield_mp_substeps). Otherwise identical to shield_mp_step. */
+int shield_mp_step_flags(void* handle, const ShieldMpFields* fields, double timestep, int32_t* flags, int64_t nflags,
+                         void* stream);
+/* ntimes, the number of sub-steps a step of `timestep` takes
+ * (microphysics.py:1964-1979), or a negative status. */
+int shield_mp_substeps(void* handle, double timestep);
+
 /* state: the step's input state (its 13 state fields and land are read; its
  * tendency and precipitation pointers are ignored). A gradient pointer may
  * be NULL to skip that field. */

@@ -899,6 +899,12 @@ class OracleMicrophysics:
         self.timestep = None
         self.qaz = np.zeros((nlev, ncol))
         self._set_timestep(float(cfg.dt_atmos))
+        # the column branch flags of the last call, (ntimes, ncol) int32, in
+        # the bit layout of the library's shield_mp_step_flags: bit 0/1 rain
+        # falls in the first/second warm_rain pass, bit 2/3/4 ice/snow/
+        # graupel fall (no_fall == 0, :349-368, :773-1168), bits 16-23 the
+        # first level with stop_k == 1 (:706-724)
+        self.flags = None
 
     def _set_timestep(self, timestep):
         self.ts = set_timestep(self.cfg, timestep)
@@ -1042,6 +1048,7 @@ class OracleMicrophysics:
             no_fall = _column_any(qrz > QRMIN)
             vtrz, r1 = compute_rain_fspeed(K, no_fall, qrz, den)
             fall = no_fall == 0.0
+            flags[-1] |= np.where(fall[0], 1 if is_first else 2, 0).astype(np.int32)
             ze = _ze_column(dz1, zs)
             qgz, qiz, qlz, qrz, qsz, qvz, tz = revap_racc(
                 fall, dt5, K, h_var, qgz, qiz, qlz, qrz, qsz, qvz, tz, den, denfac
@@ -1092,6 +1099,7 @@ class OracleMicrophysics:
             for k in range(1, L - 1):
                 stop_k[k] = W(stop_k[k - 1] == 0.0, W(tz[k] > cfg.tice, 1.0, 0.0), 1.0)
             stop_k[L - 1] = 1.0
+            flags[-1] |= (np.argmax(stop_k == 1.0, axis=0) << 16).astype(np.int32)
             tc = tz - cfg.tice
             a = (stop_k == 1.0) & (qiz > QCMIN) & (tc > 0.0)
             sink = mn(qiz, K.fac_imlt * tc / icpk)
@@ -1110,6 +1118,7 @@ class OracleMicrophysics:
             no_fall = _column_any(qiz > QRMIN)
             fall = (cfg.vi_fac >= 1.0e-5) & (no_fall == 0.0)
             i1 = np.zeros(n)
+            flags[-1] |= np.where(fall[0], 4, 0).astype(np.int32)
             if K.do_sedi_w:
                 dm = dp1 * (1.0 + qvz + qlz + qrz + qiz + qsz + qgz)
             dd = K.dts * vtiz
@@ -1124,6 +1133,7 @@ class OracleMicrophysics:
             no_fall = _column_any(qsz > QRMIN)
             fall = no_fall == 0.0
             s1 = np.zeros(n)
+            flags[-1] |= np.where(fall[0], 8, 0).astype(np.int32)
             if K.do_sedi_w:
                 dm = dp1 * (1.0 + qvz + qlz + qrz + qiz + qsz + qgz)
             dd = K.dts * vtsz
@@ -1138,6 +1148,7 @@ class OracleMicrophysics:
             no_fall = _column_any(qgz > QRMIN)
             fall = no_fall == 0.0
             g1 = np.zeros(n)
+            flags[-1] |= np.where(fall[0], 16, 0).astype(np.int32)
             if K.do_sedi_w:
                 dm = dp1 * (1.0 + qvz + qlz + qrz + qiz + qsz + qgz)
             dd = K.dts * vtgz
@@ -1193,7 +1204,9 @@ class OracleMicrophysics:
                 den, denfac, vtgz, vtrz, vtsz, p1, di, q_liq, q_sol, cvm,
             )
 
+        flags = []
         for _ in range(K.ntimes):
+            flags.append(np.zeros(n, dtype=np.int32))
             (qgz, qiz, qlz, qrz, qsz, qvz, tz, den, denfac, dz1, wz, m1, vtrz, rain) = warm_rain(
                 True, qgz, qiz, qlz, qrz, qsz, qvz, tz, den, denfac, dz1, wz, m1, m1_sol, rain
             )
@@ -1207,6 +1220,7 @@ class OracleMicrophysics:
                 qaz, qgz, qiz, qlz, qrz, qsz, qvz, tz, vtgz, vtrz, vtsz
             )
         self.qaz = qaz
+        self.flags = np.stack(flags)
         if K.do_sedi_w:
             w[...] = wz
 

@@ -174,6 +174,8 @@ EXPORTS = (
     "shield_agrid_to_dgrid",
     "shield_mp_check",
     "shield_mp_check_noalloc",
+    "shield_mp_step_flags",
+    "shield_mp_substeps",
 )
 
 _lib = None
@@ -222,6 +224,8 @@ def load():
     ]
     lib.shield_mp_check.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), vp]
     lib.shield_mp_check_noalloc.argtypes = [i32, ctypes.POINTER(ctypes.c_int64), vp]
+    lib.shield_mp_step_flags.argtypes = [vp, ctypes.POINTER(ShieldMpFields), dbl, vp, ctypes.c_int64, vp]
+    lib.shield_mp_substeps.argtypes = [vp, dbl]
     lib.shield_agrid_to_dgrid.argtypes = [
         i32, i32, i32, i32, dbl, ctypes.POINTER(ShieldEdgePlan), ctypes.POINTER(ShieldDwindGeometry), ShieldField3D,
         ShieldField3D, ShieldField3D, ShieldField3D, vp,

@@ -18,6 +18,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libshield_mp.so")
+# the FP64 throughput probe bench.py uses for the step kernel's FP64 roofline
+# (not part of the C-ABI)
+PROBE_LIB = os.path.join(HERE, "libshield_probe.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
           "--expt-relaxed-constexpr", "-I", os.path.join(os.path.dirname(HERE), "include")]
@@ -54,12 +57,20 @@ def _stale(objs):
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(os.path.dirname(HERE), "include", "shield_mp.h"), __file__]
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f != "peak.cu"] + [os.path.join(os.path.dirname(HERE), "include", "shield_mp.h"), __file__]
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
 def build(force=False, jobs=None, verbose=False):
     units = [u for u in UNITS if os.path.exists(os.path.join(CSRC, u[0]))]
+    probe_src = os.path.join(CSRC, "peak.cu")
+    if force or not os.path.exists(PROBE_LIB) or os.path.getmtime(probe_src) > os.path.getmtime(PROBE_LIB):
+        tmp = PROBE_LIB + ".tmp"
+        r = subprocess.run([nvcc()] + ARCH + COMMON + ["-shared", "-o", tmp, probe_src, "-cudart", "static"],
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed for peak.cu:\n{r.stdout}\n{r.stderr}")
+        os.replace(tmp, PROBE_LIB)
     if not force and not _stale(units):
         return LIB
     os.makedirs(BUILD, exist_ok=True)

@@ -103,8 +103,12 @@ extern "C" int shield_mp_create(const ShieldMpConfig* cfg, int nx, int ny, int n
   return SHIELD_OK;
 }
 
-extern "C" int shield_mp_step(void* handle, const ShieldMpFields* F, double timestep, int precision, void* stream) {
-  Handle* h = static_cast<Handle*>(handle);
+namespace {
+
+// The step of shield_mp_step; with `flags` non-null (plain form only) the
+// launch also records each sub-step's column flags there.
+int step_impl(Handle* h, const ShieldMpFields* F, double timestep, int precision, int32_t* flags, int64_t nflags,
+              void* stream) {
   if (!h) return fail(nullptr, SHIELD_EINVAL, "null handle");
   if (!F) return fail(h, SHIELD_EINVAL, "null fields");
   if (precision != SHIELD_MP_PLAIN && precision != SHIELD_MP_MIXED)
@@ -147,15 +151,44 @@ extern "C" int shield_mp_step(void* handle, const ShieldMpFields* F, double time
   A.ice = F->ice;
   A.graupel = F->graupel;
   A.err = h->err;
+  if (flags) {
+    if (precision != SHIELD_MP_PLAIN) return fail(h, SHIELD_EINVAL, "column flags are recorded by the plain form only");
+    if (nflags < (int64_t)h->K.ntimes * h->ncol)
+      return fail(h, SHIELD_EINVAL,
+                  "the flags buffer holds " + std::to_string(nflags) + " words; this step needs ntimes * nx * ny = " +
+                      std::to_string((int64_t)h->K.ntimes * h->ncol));
+    A.flags = flags;
+  }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaError_t e = cudaSuccess;
   if (h->K.de_ice) {
     e = mp_launch_de_ice(A, f3(F->qi_dt), f3(F->qs_dt), st);
     if (e != cudaSuccess) return cuda_fail(h, e, "de_ice launch");
   }
-  e = mp_launch_step(A, precision, st);
+  e = flags ? mp_launch_plain_flags(A, st) : mp_launch_step(A, precision, st);
   if (e != cudaSuccess) return cuda_fail(h, e, "microphysics launch");
   return SHIELD_OK;
+}
+
+}  // namespace
+
+extern "C" int shield_mp_step(void* handle, const ShieldMpFields* F, double timestep, int precision, void* stream) {
+  return step_impl(static_cast<Handle*>(handle), F, timestep, precision, nullptr, 0, stream);
+}
+
+extern "C" int shield_mp_step_flags(void* handle, const ShieldMpFields* F, double timestep, int32_t* flags,
+                                    int64_t nflags, void* stream) {
+  if (!flags) return fail(static_cast<Handle*>(handle), SHIELD_EINVAL, "null flags buffer");
+  return step_impl(static_cast<Handle*>(handle), F, timestep, SHIELD_MP_PLAIN, flags, nflags, stream);
+}
+
+extern "C" int shield_mp_substeps(void* handle, double timestep) {
+  Handle* h = static_cast<Handle*>(handle);
+  if (!h) return fail(nullptr, SHIELD_EINVAL, "null handle");
+  MpConst K2 = h->K;
+  std::string why;
+  if (set_timestep(h->cfg, K2, timestep, why) != SHIELD_OK) return fail(h, SHIELD_EINVAL, why);
+  return K2.ntimes;
 }
 
 extern "C" int shield_mp_step_vjp(void* handle, const ShieldMpFields* F, const ShieldMpCotangents* cot,

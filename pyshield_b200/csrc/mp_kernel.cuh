@@ -718,12 +718,13 @@ SHD void substep_geometry(Column<NW>& C, const MpConst& K, bool valid, double t0
 // surface flux r1.
 template <int NW, bool MIXED>
 SHD void warm_rain(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid, LevState& S, const StepGeom& P,
-                   double& vtr, double& m1_rain, double& r1) {
+                   double& vtr, double& m1_rain, double& r1, bool* falls = nullptr) {
   const int k = C.k, L = C.L;
   double &qv = S.qv, &ql = S.ql, &qr = S.qr, &qi = S.qi, &qs = S.qs, &qg = S.qg, &tz = S.tz, &w = S.w;
   const double dt5 = 0.5 * K.dt_rain;
   m1_rain = 0.0;
   const bool fall = C.any(valid && (qr > QRMIN));
+  if (falls) *falls = fall;
   r1 = 0.0;
   if (!fall) {
     vtr = VF_MIN;
@@ -775,7 +776,7 @@ SHD void warm_rain(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool val
 template <int NW, bool MIXED>
 SHD void sedimentation(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid, LevState& S,
                        const StepGeom& P, double& vtg, double& vts, double& m1_sol, double& ice, double& snow,
-                       double& graupel) {
+                       double& graupel, unsigned* flags = nullptr) {
   const int k = C.k, L = C.L;
   double &qv = S.qv, &ql = S.ql, &qr = S.qr, &qi = S.qi, &qs = S.qs, &qg = S.qg, &tz = S.tz, &w = S.w;
   const double dp1 = P.dp1, dz = P.dz;
@@ -795,6 +796,9 @@ SHD void sedimentation(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool
   bool fi, fs, fg;
   C.any3(valid && (qi > QRMIN), valid && (qs > QRMIN), valid && (qg > QRMIN), fi, fs, fg);
   fi = fi && (K.vi_fac >= 1.0e-5);
+  if (flags)
+    *flags |= (fi ? FLAG_ICE_FALLS : 0u) | (fs ? FLAG_SNOW_FALLS : 0u) | (fg ? FLAG_GRAUPEL_FALLS : 0u) |
+              ((unsigned)min(first, L - 1) << FLAG_MELT_SHIFT);
   double mp = 0.0;  // m1_sol at the level above, for the heating
   if (fi || fs || fg) {
     const double dd[3] = {K.dts * vti, K.dts * vts, K.dts * vtg};
@@ -890,7 +894,7 @@ SHD void icloud(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid,
 // of block column g at level k at (f * G + g) * RP + k); `scr` and `work`
 // are the column groups' scratch (G x 2 x SCR doubles) and work rows
 // (G x 2 x RP doubles).
-template <int NW, int G, bool MIXED>
+template <int NW, int G, bool MIXED, bool FLAGS = false>
 SHD void mp_body(const MpArgs& A, double* sm, double* scr, double* work, const int64_t c0) {
   constexpr int RP = Tiles<NW>::RP;
   const MpConst& K = A.K;
@@ -934,6 +938,7 @@ SHD void mp_body(const MpArgs& A, double* sm, double* scr, double* work, const i
     double rain = 0.0, snow = 0.0, ice = 0.0, graupel = 0.0;
 #pragma unroll 1
     for (int it = 0; it < K.ntimes; ++it) {
+      unsigned fl = 0u;  // this sub-step's column flags (FLAGS only)
       // warm_rain with is_first, sedimentation, warm_rain again (one copy
       // of the warm_rain code, run twice)
 #pragma unroll 1
@@ -942,14 +947,20 @@ SHD void mp_body(const MpArgs& A, double* sm, double* scr, double* work, const i
         if (is_first)
           substep_geometry<NW>(C, K, valid, valid ? TL(IN_PT) : 250.0, valid ? TL(IN_DELZ) : -100.0, S, P);
         double m1_rain, r1;
-        warm_rain<NW, MIXED>(C, K, KF, valid, S, P, vtr, m1_rain, r1);
+        bool falls = false;
+        warm_rain<NW, MIXED>(C, K, KF, valid, S, P, vtr, m1_rain, r1, FLAGS ? &falls : nullptr);
+        if constexpr (FLAGS) fl |= falls ? (is_first ? FLAG_RAIN_FALLS_1 : FLAG_RAIN_FALLS_2) : 0u;
         rain = rain + r1;
         m1 = is_first ? m1 + m1_rain : m1 + m1_rain + m1_sol;
         if (!is_first) break;
-        sedimentation<NW, MIXED>(C, K, KF, valid, S, P, vtg, vts, m1_sol, ice, snow, graupel);
+        sedimentation<NW, MIXED>(C, K, KF, valid, S, P, vtg, vts, m1_sol, ice, snow, graupel,
+                                 FLAGS ? &fl : nullptr);
         rain = rain + 0.0;
       }
       icloud<NW, MIXED>(C, K, KF, valid, S, P, qa, vtg, vtr, vts);
+      if constexpr (FLAGS) {
+        if (k == 0) A.flags[(int64_t)it * A.ncol + col] = (int)fl;
+      }
     }
     const double qv = S.qv, ql = S.ql, qr = S.qr, qi = S.qi, qs = S.qs, qg = S.qg, tz = S.tz, w = S.w;
     const double dp1 = P.dp1;
@@ -1025,12 +1036,12 @@ SHD void mp_body(const MpArgs& A, double* sm, double* scr, double* work, const i
 // One block's work: columns c0 .. c0 + G - 1 of the domain described by A.
 // MIXED selects the mixed-precision process rates (mp_physics_mixed.cuh);
 // everything else is shared by both forms.
-template <int NW, int G, bool MIXED>
+template <int NW, int G, bool MIXED, bool FLAGS = false>
 SHD void mp_block(const MpArgs& A, double* sm, const int64_t c0) {
   using SM = Smem<NW, G>;
   stage_in<NW, G>(A, sm, c0);
   __syncthreads();
-  mp_body<NW, G, MIXED>(A, sm, sm + SM::scratch, sm + SM::work, c0);
+  mp_body<NW, G, MIXED, FLAGS>(A, sm, sm + SM::scratch, sm + SM::work, c0);
   __syncthreads();
   stage_out<NW, G>(A, sm, c0);
 }
@@ -1164,10 +1175,10 @@ __global__ void __launch_bounds__(32 * NW * G, MINB)
 }
 
 
-template <int NW, int G, int MINB, bool MIXED>
+template <int NW, int G, int MINB, bool MIXED, bool FLAGS = false>
 __global__ void __launch_bounds__(32 * NW * G, MINB) mp_step_kernel(const __grid_constant__ MpArgs A) {
   extern __shared__ double sm[];
-  mp_block<NW, G, MIXED>(A, sm, (int64_t)blockIdx.x * G);
+  mp_block<NW, G, MIXED, FLAGS>(A, sm, (int64_t)blockIdx.x * G);
 }
 
 // Many domains (ensemble members) in one persistent launch. Work item wi
@@ -1215,7 +1226,7 @@ __global__ void __launch_bounds__(32 * NW * G, MINB)
 //   plain FP64  one block per column block 5.65, persistent 6.00
 //   mixed       one block per column block 4.47, persistent 4.29
 // so the mixed form runs persistent and the plain form does not.
-template <int NW, int G, int MINB, bool MIXED, bool PERSIST>
+template <int NW, int G, int MINB, bool MIXED, bool PERSIST, bool FLAGS = false>
 cudaError_t launch_step(const MpArgs& A, cudaStream_t st) {
   const int64_t nblk = (A.ncol + G - 1) / G;
   const int threads = 32 * NW * G;
@@ -1234,7 +1245,7 @@ cudaError_t launch_step(const MpArgs& A, cudaStream_t st) {
     kern<<<(unsigned)grid, threads, smem, st>>>(A, nblk);
     return cudaGetLastError();
   }
-  auto kern = mp_step_kernel<NW, G, MINB, MIXED>;
+  auto kern = mp_step_kernel<NW, G, MINB, MIXED, FLAGS>;
   const size_t smem = Smem<NW, G>::bytes;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;

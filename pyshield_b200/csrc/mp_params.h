@@ -70,6 +70,23 @@ struct MpArgs {
   Fld2 land, area;
   double *rain, *snow, *ice, *graupel;  // (ncol,) surface precipitation [mm/day]; may be null
   int* err;                             // device error word
+  // column flags of each sub-step (ntimes x ncol, see MpFlagBits), written
+  // only by the flag-recording launch; null otherwise
+  int* flags;
+};
+
+// Bits of the per-column, per-sub-step flags word: which species fall (the
+// reference's column-wide no_fall == 0, microphysics.py:349-368 for rain in
+// each warm_rain pass, :773-1168 for ice, snow and graupel; ice also needs
+// vi_fac >= 1e-5) and the melting level, the first level whose stop_k is 1
+// (:706-724; the bottom level when no level is warmer than tice).
+enum MpFlagBits : unsigned {
+  FLAG_RAIN_FALLS_1 = 1u << 0,
+  FLAG_RAIN_FALLS_2 = 1u << 1,
+  FLAG_ICE_FALLS = 1u << 2,
+  FLAG_SNOW_FALLS = 1u << 3,
+  FLAG_GRAUPEL_FALLS = 1u << 4,
+  FLAG_MELT_SHIFT = 16u,  // melting level in bits 16..23
 };
 
 // Parameter block of the adjoint (vector-Jacobian product) launch. in: the

@@ -65,6 +65,16 @@ cudaError_t mp_launch_plain(const MpArgs& A, cudaStream_t st) {
   return launch_nw<8, 1, 2>(A, st);
 }
 
+// The same launches with the column flags recorded (A.flags non-null).
+cudaError_t mp_launch_plain_flags(const MpArgs& A, cudaStream_t st) {
+  const int L = A.nz;
+  if (L <= 32) return launch_step<1, 4, 2, false, false, true>(A, st);
+  if (L <= 64) return launch_step<2, 2, 2, false, false, true>(A, st);
+  if (L <= 96) return launch_step<3, SHIELD_NW3_G, SHIELD_NW3_MINB, false, false, true>(A, st);
+  if (L <= 128) return launch_step<4, 4, 1, false, false, true>(A, st);
+  return launch_step<8, 1, 2, false, false, true>(A, st);
+}
+
 cudaError_t mp_launch_mixed(const MpArgs& A, cudaStream_t st);
 
 cudaError_t mp_launch_step(const MpArgs& A, int precision, cudaStream_t st) {

@@ -148,6 +148,25 @@ class Microphysics:
         )
         check(rc, self._handle, "shield_mp_step")
 
+    def step_with_flags(self, state, timestep, stream=None):
+        """``__call__`` (plain FP64 form) that also returns the step's column
+        branch flags: an int32 tensor (ntimes, ny, nx) whose bits are the
+        reference's column-wide decisions in each sub-step -- bit 0/1 rain
+        falls in the first/second warm_rain pass, bit 2/3/4 ice/snow/graupel
+        fall (no_fall == 0), bits 16-23 the melting level (the first level
+        with stop_k == 1). See ``flag_fields`` to unpack them."""
+        import torch
+
+        self._build_fields(state)
+        lib = load()
+        nt = check(lib.shield_mp_substeps(self._handle, float(timestep)), self._handle, "shield_mp_substeps")
+        flags = torch.empty((nt, self.ny, self.nx), dtype=torch.int32, device=self._precip.device)
+        rc = lib.shield_mp_step_flags(self._handle, ctypes.byref(self._fields), float(timestep),
+                                      ctypes.c_void_p(flags.data_ptr()), flags.numel(),
+                                      ctypes.c_void_p(_current_stream(stream)))
+        check(rc, self._handle, "shield_mp_step_flags")
+        return flags
+
     def check(self, stream=None):
         """Wait for the steps queued so far and raise ``ShieldError`` naming
         the column if one of them produced a NaN or an infinity (the kernel
@@ -182,3 +201,17 @@ class Microphysics:
             except Exception:
                 pass
             self._handle = None
+
+
+def flag_fields(flags):
+    """Unpack ``Microphysics.step_with_flags`` words into named arrays of
+    the same shape: rain_falls_1, rain_falls_2, ice_falls, snow_falls,
+    graupel_falls (0/1) and melt_level (level index)."""
+    return {
+        "rain_falls_1": flags & 1,
+        "rain_falls_2": (flags >> 1) & 1,
+        "ice_falls": (flags >> 2) & 1,
+        "snow_falls": (flags >> 3) & 1,
+        "graupel_falls": (flags >> 4) & 1,
+        "melt_level": (flags >> 16) & 255,
+    }

@@ -242,7 +242,7 @@ def fp64_peak(reps=5):
 
 
 # ------------------------------------------------------------ GPU arm
-def build_state(nlev, device, seed, n_cube=N_CUBE):
+def build_state(nlev, device, seed, n_cube=N_CUBE, sat_fraction=0.0):
     """Synthetic C96 state as NDSL-layout torch storages on ``device``."""
     import numpy as np
     import torch
@@ -254,7 +254,7 @@ def build_state(nlev, device, seed, n_cube=N_CUBE):
 
     nx, ny = n_cube, 6 * n_cube  # the six tiles side by side
     n = nx * ny
-    state, area = make_state(n, nlev, seed=seed, n_cube=n_cube)
+    state, area = make_state(n, nlev, seed=seed, n_cube=n_cube, sat_fraction=sat_fraction)
     gi = GridIndexing(nx, ny, nlev, HALO)
     qf = QuantityFactory(gi, device=device)
     host = {}
@@ -787,6 +787,111 @@ def run_dwind(n_cube=N_CUBE, nlev=79, dt=DT, reps=10):
     }
 
 
+MIXED_ERROR_FIELDS = (("T", "pt_dt", "pt"), ("qv", "qv_dt", "qvapor"), ("qc", "ql_dt", "qliquid"),
+                      ("qr", "qr_dt", "qrain"), ("qi", "qi_dt", "qice"), ("qs", "qs_dt", "qsnow"),
+                      ("qg", "qg_dt", "qgraupel"))
+
+
+def run_c384_mixed(nlev=79, dt=150.0, nsteps=5, n_cube=384):
+    """The mixed form against the plain FP64 form at C384: 6 x 384 x 384 =
+    884,736 columns x L79, 5 steps of 150 s, 10 % of the columns at RH
+    U(0.98, 1.02). Each form runs its own 5-step rollout from the same state
+    (tendencies zeroed before each step, the state advanced by them after).
+    Reported per field: max |mixed - plain| / max |plain| and the rms of
+    |mixed - plain| / max |plain|, for the first step (identical inputs) and
+    the worst step, of the tendencies of T, qv, qc, qr, qi, qs, qg and of the
+    four surface totals; the same after 5 steps for the state itself; the
+    mixed form's column water budget; and the device time per step of both
+    forms (CUDA events around each step)."""
+    import torch
+
+    from pyshield_b200 import constants as C
+    from pyshield_b200._config import PhysicsConfig
+    from pyshield_b200.coupling import update_physics_state_with_tendencies
+    from pyshield_b200.microphysics import Microphysics
+
+    device = torch.device("cuda", torch.cuda.current_device())
+    cfg = PhysicsConfig(dt_atmos=dt)
+    runs = {}
+    for form in ("plain", "mixed"):
+        ms, sf, qf, gd, host, land, (nx, ny, n) = build_state(nlev, device, seed=384, n_cube=n_cube,
+                                                              sat_fraction=0.1)
+        host.clear()
+        runs[form] = (ms, Microphysics(sf, qf, gd, cfg, precision=form))
+    names = MIXED_ERROR_FIELDS
+    upd = (("qvapor", "qv_dt"), ("qliquid", "ql_dt"), ("qrain", "qr_dt"), ("qice", "qi_dt"), ("qsnow", "qs_dt"),
+           ("qgraupel", "qg_dt"), ("qcld", "qa_dt"), ("pt", "pt_dt"), ("ua", "udt"), ("va", "vdt"))
+    stream = torch.cuda.current_stream()
+    ms_step = {"plain": [], "mixed": []}
+    err = {}
+    water = None
+
+    def rel(a, b):
+        sc = float(b.abs().max())
+        d = (a - b).abs()
+        sc = sc if sc > 0 else 1.0
+        return float(d.max()) / sc, float(d.pow(2).mean().sqrt()) / sc
+
+    for step in range(nsteps):
+        for form, (ms, mp) in runs.items():
+            for _, t in upd:
+                getattr(ms, t).data.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            mp(ms, dt)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms_step[form].append(e0.elapsed_time(e1))
+        (mp_p_state, mp_p), (mp_m_state, mp_m) = runs["plain"], runs["mixed"]
+        for label, tnd, _ in names:
+            e = rel(getattr(mp_m_state, tnd).view, getattr(mp_p_state, tnd).view)
+            w = err.setdefault(label, {"first_step": e, "worst_step": e})
+            w["worst_step"] = (max(w["worst_step"][0], e[0]), max(w["worst_step"][1], e[1]))
+        for p in ("rain", "snow", "ice", "graupel"):
+            e = rel(getattr(mp_m, p), getattr(mp_p, p))
+            w = err.setdefault(p, {"first_step": e, "worst_step": e})
+            w["worst_step"] = (max(w["worst_step"][0], e[0]), max(w["worst_step"][1], e[1]))
+        if step == 0:
+            # column water budget of the mixed step: the tendencies' column
+            # integral plus the surface fluxes, relative to the column water
+            ms = mp_m_state
+            dp = ms.delprsi.view
+            qdt = sum(getattr(ms, t).view for t in ("qv_dt", "ql_dt", "qr_dt", "qi_dt", "qs_dt", "qg_dt"))
+            wdt = (qdt * dp).sum(2) * C.RGRAV
+            pr = (mp_m.rain + mp_m.snow + mp_m.ice + mp_m.graupel) / 86400.0
+            col = sum(getattr(ms, f).view for f in ("qvapor", "qliquid", "qrain", "qice", "qsnow", "qgraupel"))
+            colw = (col * dp).sum(2) * C.RGRAV / dt
+            water = float(((wdt + pr).abs() / colw).max())
+        for form, (ms, mp) in runs.items():
+            st = [getattr(ms, x) for x, _ in upd]
+            update_physics_state_with_tendencies(*st, *[getattr(ms, t) for _, t in upd], *st, dt)
+    torch.cuda.synchronize()
+    state_err = {label: rel(getattr(runs["mixed"][0], f).view, getattr(runs["plain"][0], f).view)
+                 for label, _, f in names}
+    plain_ms = sum(ms_step["plain"]) / nsteps
+    mixed_ms = sum(ms_step["mixed"]) / nsteps
+    n = 6 * n_cube * n_cube
+    out = {
+        "workload": f"GFDL microphysics step, C{n_cube} ({n} columns) x L{nlev}, {nsteps} steps of {dt:g} s, "
+                    "10 % of columns at RH U(0.98, 1.02)",
+        "plain_ms_per_step": plain_ms,
+        "mixed_ms_per_step": mixed_ms,
+        "mixed_speedup": plain_ms / mixed_ms,
+        "plain_column_steps_per_s": n / (plain_ms / 1000.0),
+        "mixed_column_steps_per_s": n / (mixed_ms / 1000.0),
+        "tendency_error_vs_plain": {k: {"first_step_max": v["first_step"][0], "first_step_rms": v["first_step"][1],
+                                        "worst_step_max": v["worst_step"][0], "worst_step_rms": v["worst_step"][1]}
+                                    for k, v in err.items()},
+        "state_error_after_steps": {k: {"max": v[0], "rms": v[1]} for k, v in state_err.items()},
+        "mixed_water_budget_max_rel": water,
+        "note": "errors relative to max |plain| of each field; tendencies for T..qg (pt_dt..qg_dt), surface "
+                "totals in mm/day; device time (CUDA events) per step",
+    }
+    runs.clear()
+    torch.cuda.empty_cache()
+    return out
+
+
 def max_over_ranks(values, world, device):
     """Each rank's device-measured times -> their maximum over all ranks (the
     slowest replica sets the job's time). One all-reduce; every rank calls it
@@ -1019,6 +1124,7 @@ def main():
     ap.add_argument("--no-physics", action="store_true", help="skip the Physics.__call__ measurement")
     ap.add_argument("--no-coupling", action="store_true",
                     help="skip the UpdateAtmosphereState, DycoreToPhysics and AGrid2DGridPhysics measurements")
+    ap.add_argument("--no-c384", action="store_true", help="skip the C384 mixed-against-plain comparison")
     ap.add_argument("--ncube", type=int, default=N_CUBE, help="cube size N of the CN workload (default 96)")
     ap.add_argument("--ensemble", action="store_true", help="run the ensemble workload instead")
     ap.add_argument("--members", type=int, default=64)
@@ -1130,6 +1236,8 @@ def main():
                          "flops_per_column_step": FP64_FLOPS_PER_COLUMN_STEP[nlev],
                          "flops_source": "ncu smsp__sass_thread_inst_executed_op_{dfma,dadd,dmul}_pred_on.sum "
                                          "(2 flops per DFMA) of the C48 launch, per column"})
+    c384 = (run_c384_mixed(nlev=79)
+            if (rank == 0 and world == 1 and not args.no_c384 and args.form == "plain" and nlev == 79) else None)
     d2p = dwind = None
     if rank == 0 and world == 1 and not args.no_coupling and args.form == "plain":
         d2p = run_d2p(n_cube=args.ncube, nlev=nlev)
@@ -1176,6 +1284,7 @@ def main():
             "coupling": coupling,
             "dycore_to_physics": d2p,
             "agrid_to_dgrid": dwind,
+            "c384_mixed": c384,
         }
         emit(rec)
 

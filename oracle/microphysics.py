@@ -35,6 +35,7 @@ writes are compared bit-for-bit with this oracle by
 """
 
 import numpy as np
+import numpy as _np  # the integer flag words stay host numpy whatever backs np
 
 from pyshield_b200 import constants as C
 
@@ -70,6 +71,19 @@ QVMIN = 1.0e-20
 W = np.where
 mn = np.minimum
 mx = np.maximum
+
+
+def _flag_bits(mask, bit):
+    """The int32 word ``bit`` where the column mask is set, else 0 (the
+    column flags are integers and never differentiated)."""
+    m = mask.detach().cpu().numpy() if hasattr(mask, "detach") else mask
+    return _np.where(_np.asarray(m, dtype=bool), bit, 0).astype(_np.int32)
+
+
+def _first_level(mask):
+    """Index of the first level where the (L, n) mask is set, per column."""
+    m = mask.detach().cpu().numpy() if hasattr(mask, "detach") else mask
+    return _np.argmax(_np.asarray(m, dtype=bool), axis=0).astype(_np.int32)
 
 
 def dim(x, y):
@@ -1048,7 +1062,7 @@ class OracleMicrophysics:
             no_fall = _column_any(qrz > QRMIN)
             vtrz, r1 = compute_rain_fspeed(K, no_fall, qrz, den)
             fall = no_fall == 0.0
-            flags[-1] |= np.where(fall[0], 1 if is_first else 2, 0).astype(np.int32)
+            flags[-1] |= _flag_bits(fall[0], 1 if is_first else 2)
             ze = _ze_column(dz1, zs)
             qgz, qiz, qlz, qrz, qsz, qvz, tz = revap_racc(
                 fall, dt5, K, h_var, qgz, qiz, qlz, qrz, qsz, qvz, tz, den, denfac
@@ -1099,7 +1113,7 @@ class OracleMicrophysics:
             for k in range(1, L - 1):
                 stop_k[k] = W(stop_k[k - 1] == 0.0, W(tz[k] > cfg.tice, 1.0, 0.0), 1.0)
             stop_k[L - 1] = 1.0
-            flags[-1] |= (np.argmax(stop_k == 1.0, axis=0) << 16).astype(np.int32)
+            flags[-1] |= _first_level(stop_k == 1.0) << 16
             tc = tz - cfg.tice
             a = (stop_k == 1.0) & (qiz > QCMIN) & (tc > 0.0)
             sink = mn(qiz, K.fac_imlt * tc / icpk)
@@ -1118,7 +1132,7 @@ class OracleMicrophysics:
             no_fall = _column_any(qiz > QRMIN)
             fall = (cfg.vi_fac >= 1.0e-5) & (no_fall == 0.0)
             i1 = np.zeros(n)
-            flags[-1] |= np.where(fall[0], 4, 0).astype(np.int32)
+            flags[-1] |= _flag_bits(fall[0], 4)
             if K.do_sedi_w:
                 dm = dp1 * (1.0 + qvz + qlz + qrz + qiz + qsz + qgz)
             dd = K.dts * vtiz
@@ -1133,7 +1147,7 @@ class OracleMicrophysics:
             no_fall = _column_any(qsz > QRMIN)
             fall = no_fall == 0.0
             s1 = np.zeros(n)
-            flags[-1] |= np.where(fall[0], 8, 0).astype(np.int32)
+            flags[-1] |= _flag_bits(fall[0], 8)
             if K.do_sedi_w:
                 dm = dp1 * (1.0 + qvz + qlz + qrz + qiz + qsz + qgz)
             dd = K.dts * vtsz
@@ -1148,7 +1162,7 @@ class OracleMicrophysics:
             no_fall = _column_any(qgz > QRMIN)
             fall = no_fall == 0.0
             g1 = np.zeros(n)
-            flags[-1] |= np.where(fall[0], 16, 0).astype(np.int32)
+            flags[-1] |= _flag_bits(fall[0], 16)
             if K.do_sedi_w:
                 dm = dp1 * (1.0 + qvz + qlz + qrz + qiz + qsz + qgz)
             dd = K.dts * vtgz
@@ -1206,7 +1220,7 @@ class OracleMicrophysics:
 
         flags = []
         for _ in range(K.ntimes):
-            flags.append(np.zeros(n, dtype=np.int32))
+            flags.append(_np.zeros(n, dtype=_np.int32))
             (qgz, qiz, qlz, qrz, qsz, qvz, tz, den, denfac, dz1, wz, m1, vtrz, rain) = warm_rain(
                 True, qgz, qiz, qlz, qrz, qsz, qvz, tz, den, denfac, dz1, wz, m1, m1_sol, rain
             )
@@ -1220,7 +1234,7 @@ class OracleMicrophysics:
                 qaz, qgz, qiz, qlz, qrz, qsz, qvz, tz, vtgz, vtrz, vtsz
             )
         self.qaz = qaz
-        self.flags = np.stack(flags)
+        self.flags = _np.stack(flags)
         if K.do_sedi_w:
             w[...] = wz
 

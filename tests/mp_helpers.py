@@ -176,6 +176,23 @@ def floors(state, ref, dt):
     return fl
 
 
+# Tendencies that the GPU gate lets exceed the plain 1e-12 relative bound by
+# the round-off floor above, each with its reason. Every other field of the
+# plain form is held to max |gpu - oracle| <= 1e-12 max |oracle|.
+TENDENCY_FLOOR = {}
+
+
+def gpu_floors(state, ref, dt):
+    """Absolute slack of the GPU-against-oracle gate: none for the
+    tendencies, wmp and the accumulator (except the fields named in
+    TENDENCY_FLOOR); the column-condensate scale for the four surface totals,
+    which the reference sums as a running difference that cancels to its last
+    digits when little mass reaches the ground (the kernels use the
+    telescoped flux)."""
+    full = floors(state, ref, dt)
+    return {f: v for f, v in full.items() if f in PRECIP or f in TENDENCY_FLOOR}
+
+
 def field_errors(gpu, ref, fields, tol, fl=None):
     """Per-field error in units of the allowance: max |gpu - ref| divided by
     (tol * max|ref| + floor); a value <= 1 passes. Also the plain relative

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from golden_io import MP_TENDENCIES, PHYS_CASES, PRECIP, load, physics_inputs
-from mp_helpers import NOISE, TOL_PLAIN, precip_scale
+from mp_helpers import NOISE, TENDENCY_FLOOR, TOL_PLAIN, precip_scale
 
 pytestmark = pytest.mark.gpu
 
@@ -79,11 +79,14 @@ def _floors(st_in, ref, dt, nx, ny, L):
     ci, cj = slice(H, H + nx), slice(H, H + ny)
     fl = {}
     for t, x in TEND_STATE.items():
+        if t not in TENDENCY_FLOOR:
+            continue
         xin = ref[x][ci, cj, :L]
         xout = xin + ref[t][ci, cj, :L] * dt
         fl[t] = NOISE * max(float(np.max(np.abs(xin))), float(np.max(np.abs(xout)))) / dt
     for u, (x, t) in UPDATED.items():
-        fl[u] = fl[t] * dt
+        if t in fl:
+            fl[u] = fl[t] * dt
     ln = {f: ref[f][ci, cj, :L].transpose(2, 1, 0).reshape(L, nx * ny)
           for f in ("qliquid", "qrain", "qice", "qsnow", "qgraupel", "delprsi")}
     ps = precip_scale(ln, dt)

@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 from golden_io import MP_TENDENCIES
-from mp_helpers import TOL_PLAIN, assert_close, device_state, floors, read_state
+from mp_helpers import TOL_PLAIN, assert_close, device_state, gpu_floors as floors, read_state
 
 FIELDS = MP_TENDENCIES + ("wmp", "qice", "qsnow", "rain", "snow", "ice", "graupel")
 

@@ -58,7 +58,7 @@ NCU_TRAFFIC_RATIO = 315.11 / 315.19
 # FP64 flops per column-step of the plain step kernel (2 per DFMA, 1 per
 # DADD or DMUL, thread-level counts of predicated-on instructions), from an
 # ncu capture of the C48 launch divided by its columns; by level count.
-FP64_FLOPS_PER_COLUMN_STEP = {79: (2 * 1419022560 + 566734478 + 677646420) / 13824}
+FP64_FLOPS_PER_COLUMN_STEP = {79: (2 * 1419707201 + 566933197 + 677884763) / 13824}
 
 
 def algorithmic_bytes_per_column_step(nlev):

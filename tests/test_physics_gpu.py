@@ -5,9 +5,10 @@ fixtures, equal bit for bit to the oracle) and against the oracle at C12.
 
 Every output storage is compared whole, halo and extra level included, so a
 write outside a stencil's domain would show. Per field:
-max |gpu - ref| <= 1e-12 * max |ref| + floor, with the microphysics floors
-of the plain-form gate (tendency round-off and precipitation scale, carried
-through ``physics_updated_X = X + X_dt * dt``).
+max |gpu - ref| <= 1e-12 * max |ref|, with an absolute floor only for the
+surface precipitation totals (the column-condensate scale of the plain-form
+gate, mp_helpers.gpu_floors) and for any tendency named in
+mp_helpers.TENDENCY_FLOOR (carried through ``physics_updated_X = X + X_dt * dt``).
 """
 import numpy as np
 import pytest

@@ -238,7 +238,8 @@ typedef struct {
 
 int shield_mp_ensemble_create(const ShieldMpConfig* cfg, int nz, int nmembers, const ShieldMpMember* members,
                               int precision, void** plan);
-/* cols_per_block in {1, 2, 4}; the launch has
+/* cols_per_block in {2, 4, 6, 8} for 65..80 levels (two columns share each
+ * group of 5 warps), in {1, 2, 4} for 81..128 levels; the launch has
  * blocks_per_sm x (number of SMs) persistent blocks. */
 int shield_mp_ensemble_step(void* plan, int cols_per_block, int blocks_per_sm, void* stream);
 /* copy member m's persistent accumulator (nz*nx*ny doubles, level-major)

@@ -339,7 +339,7 @@ namespace {
 struct Plan {
   int nm = 0, nz = 0, precision = 0, num_sms = 0;
   MpArgs* d_members = nullptr;
-  int64_t* d_offs[3] = {nullptr, nullptr, nullptr};  // cols_per_block 1, 2, 4
+  int64_t* d_offs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // cols_per_block 1, 2, 4, 6, 8
   double* d_area = nullptr;
   double* d_qaz = nullptr;
   std::vector<int64_t> qaz_off;
@@ -347,7 +347,14 @@ struct Plan {
   std::string last_error;
 };
 
-int gindex(int G) { return G == 1 ? 0 : G == 2 ? 1 : G == 4 ? 2 : -1; }
+int gindex(int G) { return G == 1 ? 0 : G == 2 ? 1 : G == 4 ? 2 : G == 6 ? 3 : G == 8 ? 4 : -1; }
+
+// cols_per_block values the ensemble launch has for nz levels: 65..80 levels
+// pack two columns per 5 warps, so a block holds 2, 4, 6 or 8 columns.
+bool ensemble_shape_ok(int nz, int G) {
+  if (nz <= 80) return G == 2 || G == 4 || G == 6 || G == 8;
+  return G == 1 || G == 2 || G == 4;
+}
 
 void plan_free(Plan* p) {
   cudaFree(p->d_members);
@@ -457,8 +464,8 @@ extern "C" int shield_mp_ensemble_create(const ShieldMpConfig* cfg, int nz, int 
     if (e != cudaSuccess) break;
   }
   if (e == cudaSuccess) e = cudaMemcpy(p->d_members, host.data(), sizeof(MpArgs) * nm, cudaMemcpyHostToDevice);
-  const int Gs[3] = {1, 2, 4};
-  for (int gi = 0; gi < 3 && e == cudaSuccess; ++gi) {
+  const int Gs[5] = {1, 2, 4, 6, 8};
+  for (int gi = 0; gi < 5 && e == cudaSuccess; ++gi) {
     std::vector<int64_t> offs(nm + 1, 0);
     for (int m = 0; m < nm; ++m) offs[m + 1] = offs[m] + (host[m].ncol + Gs[gi] - 1) / Gs[gi];
     e = cudaMalloc(&p->d_offs[gi], sizeof(int64_t) * (nm + 1));
@@ -479,8 +486,10 @@ extern "C" int shield_mp_ensemble_step(void* plan, int G, int bpsm, void* stream
   Plan* p = static_cast<Plan*>(plan);
   if (!p) return fail(nullptr, SHIELD_EINVAL, "null plan");
   const int gi = gindex(G);
-  if (gi < 0 || bpsm < 1 || bpsm > 32)
-    return fail(nullptr, SHIELD_EINVAL, "cols_per_block must be 1, 2 or 4, blocks_per_sm 1..32");
+  if (gi < 0 || !ensemble_shape_ok(p->nz, G) || bpsm < 1 || bpsm > 32)
+    return fail(nullptr, SHIELD_EINVAL,
+                std::string("cols_per_block must be ") + (p->nz <= 80 ? "2, 4, 6 or 8" : "1, 2 or 4") + " for " +
+                    std::to_string(p->nz) + " levels, blocks_per_sm 1..32");
   const int grid = bpsm * p->num_sms;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaError_t e = (p->precision == SHIELD_MP_MIXED)

@@ -31,9 +31,9 @@ __global__ void de_ice_kernel(const __grid_constant__ MpArgs A, Fld3 qi_dt, Fld3
 
 namespace {
 
-template <int NW, int G, int MINB>
+template <int NW, int G, int MINB, bool FLAGS = false>
 cudaError_t launch_nw(const MpArgs& A, cudaStream_t st) {
-  return launch_step<NW, G, MINB, false, false>(A, st);
+  return launch_step<ColumnLayout<NW, G>, MINB, false, false, FLAGS>(A, st);
 }
 
 __global__ void gather2d(const double* p, int64_t si, int64_t sj, int nx, int64_t n, double* out) {
@@ -45,34 +45,43 @@ __global__ void gather2d(const double* p, int64_t si, int64_t sj, int nx, int64_
 
 int mp_max_levels() { return 256; }
 
-// Launch shape for 65-96 levels (the common L79 case): columns per block and
-// the minimum resident blocks per SM given to __launch_bounds__ (which caps
-// the registers per thread). Four columns per block (one 384-thread block per
-// SM) measured fastest: the staging then reads whole 32-byte sectors.
+// Launch shape for 81-96 levels: columns per block and the minimum resident
+// blocks per SM given to __launch_bounds__ (which caps the registers per
+// thread). Four columns per block (one 384-thread block per SM) measured
+// fastest: the staging then reads whole 32-byte sectors. 65-80 levels (L79)
+// pack two columns per 5 warps (Packed80).
 #ifndef SHIELD_NW3_G
 #define SHIELD_NW3_G 4
 #endif
 #ifndef SHIELD_NW3_MINB
 #define SHIELD_NW3_MINB 1
 #endif
+// 97..128 levels (L127): columns per block of 4 warps each. C96 L127 (ms):
+// 4 columns (512 threads, 128 registers) 6.29, 5 columns (640, 96) 5.94,
+// 6 columns (768, 80) 5.99.
+#ifndef SHIELD_NW4_G
+#define SHIELD_NW4_G 5
+#endif
 
 cudaError_t mp_launch_plain(const MpArgs& A, cudaStream_t st) {
   const int L = A.nz;
   if (L <= 32) return launch_nw<1, 4, 2>(A, st);
   if (L <= 64) return launch_nw<2, 2, 2>(A, st);
+  if (L <= PACK80_LMAX) return launch_step<Packed80, PACK80_MINB, false, false>(A, st);
   if (L <= 96) return launch_nw<3, SHIELD_NW3_G, SHIELD_NW3_MINB>(A, st);
-  if (L <= 128) return launch_nw<4, 4, 1>(A, st);  // 512 threads, whole-sector staging
+  if (L <= 128) return launch_nw<4, SHIELD_NW4_G, 1>(A, st);
   return launch_nw<8, 1, 2>(A, st);
 }
 
 // The same launches with the column flags recorded (A.flags non-null).
 cudaError_t mp_launch_plain_flags(const MpArgs& A, cudaStream_t st) {
   const int L = A.nz;
-  if (L <= 32) return launch_step<1, 4, 2, false, false, true>(A, st);
-  if (L <= 64) return launch_step<2, 2, 2, false, false, true>(A, st);
-  if (L <= 96) return launch_step<3, SHIELD_NW3_G, SHIELD_NW3_MINB, false, false, true>(A, st);
-  if (L <= 128) return launch_step<4, 4, 1, false, false, true>(A, st);
-  return launch_step<8, 1, 2, false, false, true>(A, st);
+  if (L <= 32) return launch_nw<1, 4, 2, true>(A, st);
+  if (L <= 64) return launch_nw<2, 2, 2, true>(A, st);
+  if (L <= PACK80_LMAX) return launch_step<Packed80, PACK80_MINB, false, false, true>(A, st);
+  if (L <= 96) return launch_nw<3, SHIELD_NW3_G, SHIELD_NW3_MINB, true>(A, st);
+  if (L <= 128) return launch_nw<4, SHIELD_NW4_G, 1, true>(A, st);
+  return launch_nw<8, 1, 2, true>(A, st);
 }
 
 cudaError_t mp_launch_mixed(const MpArgs& A, cudaStream_t st);
@@ -97,32 +106,25 @@ cudaError_t mp_gather_area(const double* p, int64_t si, int64_t sj, int nx, int 
 }
 
 
-namespace {
-
-template <int NW, int G, int MINB>
-cudaError_t launch_ens(const MpArgs* members, const int64_t* offs, int nm, int grid, cudaStream_t st) {
-  const size_t smem = Smem<NW, G>::bytes;
-  auto kern = mp_ensemble_kernel<NW, G, MINB, false>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  kern<<<grid, 32 * NW * G, smem, st>>>(members, offs, nm);
-  return cudaGetLastError();
-}
-
-}  // namespace
-
-// Ensemble launch over nz in (64, 128]: G columns per block (1, 2 or 4), a
-// persistent grid of `grid` blocks.
+// Ensemble launch over nz in (64, 128]: G columns per block, a persistent
+// grid of `grid` blocks. 65..80 levels: G = 2, 4, 6 or 8 (1 to 4 groups of
+// two packed columns; 640 threads per SM where the block size allows);
+// 81..128 levels: G = 1, 2 or 4.
 cudaError_t mp_launch_ensemble_plain(const MpArgs* members, const int64_t* offs, int nm, int nz, int G, int grid,
                                      cudaStream_t st) {
-  if (nz <= 96) {
-    if (G == 1) return launch_ens<3, 1, 4>(members, offs, nm, grid, st);
-    if (G == 2) return launch_ens<3, 2, 2>(members, offs, nm, grid, st);
-    if (G == 4) return launch_ens<3, 4, 1>(members, offs, nm, grid, st);
+  if (nz <= PACK80_LMAX) {
+    if (G == 2) return launch_ensemble<PackedLayout<5, 2, 1>, 4, false>(members, offs, nm, grid, st);
+    if (G == 4) return launch_ensemble<PackedLayout<5, 2, 2>, 2, false>(members, offs, nm, grid, st);
+    if (G == 6) return launch_ensemble<PackedLayout<5, 2, 3>, 1, false>(members, offs, nm, grid, st);
+    if (G == 8) return launch_ensemble<PackedLayout<5, 2, 4>, 1, false>(members, offs, nm, grid, st);
+  } else if (nz <= 96) {
+    if (G == 1) return launch_ensemble<ColumnLayout<3, 1>, 4, false>(members, offs, nm, grid, st);
+    if (G == 2) return launch_ensemble<ColumnLayout<3, 2>, 2, false>(members, offs, nm, grid, st);
+    if (G == 4) return launch_ensemble<ColumnLayout<3, 4>, 1, false>(members, offs, nm, grid, st);
   } else if (nz <= 128) {
-    if (G == 1) return launch_ens<4, 1, 4>(members, offs, nm, grid, st);
-    if (G == 2) return launch_ens<4, 2, 2>(members, offs, nm, grid, st);
-    if (G == 4) return launch_ens<4, 4, 1>(members, offs, nm, grid, st);
+    if (G == 1) return launch_ensemble<ColumnLayout<4, 1>, 4, false>(members, offs, nm, grid, st);
+    if (G == 2) return launch_ensemble<ColumnLayout<4, 2>, 2, false>(members, offs, nm, grid, st);
+    if (G == 4) return launch_ensemble<ColumnLayout<4, 4>, 1, false>(members, offs, nm, grid, st);
   }
   return cudaErrorInvalidValue;
 }

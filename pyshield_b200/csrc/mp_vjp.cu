@@ -284,7 +284,7 @@ static __device__ __noinline__ void warm_rain_b(Column<NW>& C, const MpConst& K,
     const double inner = fmax(QVMIN, hq);
     double sl = 0.0, dl = inner;
     if (K.z_slope_liq) {
-      sl = mono_slope<NW>(C, S3.ql);
+      sl = mono_slope(C, S3.ql);
       dl = fmax(sl, inner);
     }
     double dl_b = 0.0;
@@ -525,7 +525,7 @@ static __device__ __noinline__ void icloud_b(Column<NW>& C, const MpConst& K, bo
   const double inner = fmax(QVMIN, hq);
   double sl = 0.0, di = inner;
   if (K.z_slope_ice) {
-    sl = mono_slope<NW>(C, S1.qi);
+    sl = mono_slope(C, S1.qi);
     di = fmax(sl, inner);
   }
   double di_b = 0.0, qliq_b = 0.0, qsol_b = 0.0, cvm_b = 0.0;
@@ -571,19 +571,19 @@ template <int NW>
 static __device__ __noinline__ void fwd_warm_rain(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid,
                                                   LevState& S, const StepGeom& P, double& vtr, double& m1r,
                                                   double& r1) {
-  warm_rain<NW, false>(C, K, KF, valid, S, P, vtr, m1r, r1);
+  warm_rain<false>(C, K, KF, valid, S, P, vtr, m1r, r1);
 }
 template <int NW>
 static __device__ __noinline__ void fwd_sedimentation(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid,
                                                       LevState& S, const StepGeom& P, double& vtg, double& vts,
                                                       double& m1s, double& ice, double& snow, double& graupel) {
-  sedimentation<NW, false>(C, K, KF, valid, S, P, vtg, vts, m1s, ice, snow, graupel);
+  sedimentation<false>(C, K, KF, valid, S, P, vtg, vts, m1s, ice, snow, graupel);
 }
 template <int NW>
 static __device__ __noinline__ void fwd_icloud(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid,
                                                LevState& S, const StepGeom& P, double& qa, double vtg, double vtr,
                                                double vts, LevState& rec) {
-  icloud<NW, false>(C, K, KF, valid, S, P, qa, vtg, vtr, vts, &rec);
+  icloud<false>(C, K, KF, valid, S, P, qa, vtg, vtr, vts, &rec);
 }
 
 template <int NW, int G, int MINB>
@@ -633,7 +633,7 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) mp_vjp_kernel(const __grid_
     P.denfac = 1.0;
     P.dz1 = -100.0;
     P.dz = 100.0;
-    fields_init<NW>(C, K, valid, pt, qin[0], qin[1], qin[2], qin[3], qin[4], qin[5], delp, TI(IN_W, 0.0), dz0, land,
+    fields_init(C, K, valid, pt, qin[0], qin[1], qin[2], qin[3], qin[4], qin[5], delp, TI(IN_W, 0.0), dz0, land,
                     area, S, P);
     LevState ck[VJP_MAXNT][5];  // entries of the four stages, and the state before the adjustment
     double ckv[VJP_MAXNT][3];
@@ -642,7 +642,7 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) mp_vjp_kernel(const __grid_
     const int nt = K.ntimes;
 #pragma unroll 1
     for (int it = 0; it < nt; ++it) {
-      substep_geometry<NW>(C, K, valid, pt, dz0, S, P);
+      substep_geometry(C, K, valid, pt, dz0, S, P);
 #pragma unroll 1
       for (int pass = 0; pass < 2; ++pass) {
         double m1r, r1;
@@ -764,7 +764,7 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) mp_vjp_kernel(const __grid_
 #pragma unroll 1
     for (int it = nt - 1; it >= 0; --it) {
       StepGeom Pg = P;
-      substep_geometry<NW>(C, K, valid, pt, dz0, ck[it][0], Pg);
+      substep_geometry(C, K, valid, pt, dz0, ck[it][0], Pg);
       Ab.den = 0.0;
       Ab.denfac = 0.0;
       Ab.dz = 0.0;

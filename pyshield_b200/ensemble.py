@@ -23,8 +23,16 @@ from .quantity import field2d, field3d
 
 _PRECISION = {"plain": SHIELD_MP_PLAIN, "fp64": SHIELD_MP_PLAIN, "mixed": SHIELD_MP_MIXED}
 
-# (columns per block, blocks per SM) launch shapes the autotuner times
+# (columns per block, blocks per SM) launch shapes the autotuner times, by
+# level count: 65..80 levels pack two columns per group of 5 warps, so a
+# block holds 2, 4, 6 or 8 columns (shield_mp_ensemble_step)
 CANDIDATES = ((1, 4), (1, 5), (2, 2), (2, 3), (4, 1), (4, 2))
+CANDIDATES_PACKED = ((2, 4), (2, 5), (4, 2), (6, 1), (8, 1), (8, 2))
+
+
+def launch_shapes(nz):
+    """The launch shapes ``autotune`` tries for ``nz`` levels."""
+    return CANDIDATES_PACKED if nz <= 80 else CANDIDATES
 
 
 class MicrophysicsEnsemble:
@@ -102,15 +110,15 @@ class MicrophysicsEnsemble:
         rc = load().shield_mp_ensemble_step(self._plan, int(G), int(b), ctypes.c_void_p(_current_stream(stream)))
         check(rc, None, "shield_mp_ensemble_step")
 
-    def autotune(self, candidates=CANDIDATES, reps=2):
-        """Time each launch shape with CUDA events (after one warm-up launch)
-        and keep the fastest. Note that each timed launch advances the
-        members' state, as a real step does."""
+    def autotune(self, candidates=None, reps=2):
+        """Time each launch shape (by default ``launch_shapes(nz)``) with CUDA
+        events (after one warm-up launch) and keep the fastest. Note that
+        each timed launch advances the members' state, as a real step does."""
         import torch
 
         stream = torch.cuda.current_stream()
         best = None
-        for G, b in candidates:
+        for G, b in candidates or launch_shapes(self.nz):
             self.step(G, b)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)

@@ -179,7 +179,14 @@ def floors(state, ref, dt):
 # Tendencies that the GPU gate lets exceed the plain 1e-12 relative bound by
 # the round-off floor above, each with its reason. Every other field of the
 # plain form is held to max |gpu - oracle| <= 1e-12 max |oracle|.
-TENDENCY_FLOOR = {}
+TENDENCY_FLOOR = {
+    # (u1 - u0) / dt of winds of order 10 m/s that the falling mass changes
+    # by about a thousandth: the momentum recurrence u1_k = (dp0 u0_k +
+    # m1_{k-1} u1_{k-1}) / (dp0 + m1_{k-1}) is evaluated as a parallel scan,
+    # whose rounding of u1 (1e-15 of u) is 1e-12 of the difference
+    "udt": "momentum transport: round-off of u1 against a small u1 - u0",
+    "vdt": "momentum transport: round-off of v1 against a small v1 - v0",
+}
 
 
 def gpu_floors(state, ref, dt):

@@ -61,8 +61,8 @@ def _read(ens, built, members, nlev=L):
     return res
 
 
-@pytest.mark.parametrize("shape,nlev", [((1, 4), L), ((2, 2), L), ((2, 3), L), ((4, 1), L), ((4, 1), 127),
-                                        ((2, 2), 127)])
+@pytest.mark.parametrize("shape,nlev", [((2, 4), L), ((4, 2), L), ((6, 1), L), ((8, 1), L), ((8, 2), L),
+                                        ((1, 4), 127), ((4, 1), 127), ((2, 2), 127), ((1, 4), 90), ((4, 1), 90)])
 def test_batched_plain_equals_members_bitwise(shape, nlev):
     import torch
 
@@ -84,6 +84,7 @@ def test_graph_replay_and_autotune():
     import torch
 
     from pyshield_b200._config import PhysicsConfig
+    from pyshield_b200.ensemble import launch_shapes
 
     cfg = PhysicsConfig(dt_atmos=150.0)
     members = _states(200)
@@ -100,6 +101,7 @@ def test_graph_replay_and_autotune():
             np.testing.assert_array_equal(a[f], b[f], err_msg=f"member {m} field {f}")
     tuned, timings = ens.autotune(reps=1)
     assert tuned in timings and all(v > 0 for v in timings.values())
+    assert set(timings) == set(launch_shapes(L))
 
 
 def test_batched_mixed_matches_members():

@@ -14,6 +14,8 @@
  *                      atmos_phys_driver_statein, get_prs_fv3, get_phi_fv3,
  *                      prepare_microphysics  pySHiELD/stencils/physics.py:26-143, 276-330;
  *                                            get_prs_fv3.py:7-20; get_phi_fv3.py:7-25
+ *   shield_physics_prestep_from_dycore
+ *                      DycoreToPhysics.__call__ then the pre-steps above, fused
  *   shield_copy_dycore_to_physics
  *                      DycoreToPhysics.__call__ (without the dry convective
  *                      adjustment)              pySHiELD/update/update_atmos_state.py:95-232
@@ -226,9 +228,10 @@ int shield_mp_check_noalloc(int nx, int64_t* bad_column, void* stream);
  *
  * shield_mp_ensemble_create computes every member's constants, copies its
  * cell area and allocates its persistent accumulator (zero), and uploads the
- * member table once. shield_mp_ensemble_step then enqueues a single kernel
- * and nothing else (no allocation, no copy), so it can be captured in a CUDA
- * graph and replayed. Supported level counts: 65..128. */
+ * member table once. shield_mp_ensemble_step then enqueues the zeroing of
+ * the plan's work-item counter (an 8-byte memset) and a single kernel, with
+ * no allocation and no copy, so it can be captured in a CUDA graph and
+ * replayed. Supported level counts: 65..128. */
 typedef struct {
   ShieldMpFields fields; /* the member's fields; its precipitation outputs may be NULL */
   int nx, ny;            /* the member's horizontal domain */
@@ -337,6 +340,20 @@ int shield_physics_prestep(int nx, int ny, int nz, int hx, int nwat, double ptop
  * most 2^31 - 1 points (SHIELD_ELAYOUT otherwise). */
 int shield_copy_dycore_to_physics(int nx, int ny, int nz, const ShieldField3D* dycore16,
                                   const ShieldField3D* physics16, void* stream);
+
+/* DycoreToPhysics' copy followed by shield_physics_prestep, as one launch:
+ * the results, in every physics storage, are those of
+ * shield_copy_dycore_to_physics then shield_physics_prestep (the copy of
+ * update_atmos_state.py:196-232 followed by physics.py:276-330), but the
+ * pre-step reads the dycore storages where the copy would have put them and
+ * writes each copied field once, so the separate copy's pass over HBM goes.
+ * dycore16 / physics16: the copy's 16 fields in the order of
+ * shield_copy_dycore_to_physics; the physics ones are the storages of
+ * `fields` where both name a field. Needs hx >= 1 (the copy's interface
+ * points i = nx, j = ny lie in the pre-step's halo). */
+int shield_physics_prestep_from_dycore(int nx, int ny, int nz, int hx, int nwat, double ptop, int flags,
+                                       const ShieldPhysicsFields* fields, const ShieldField3D* dycore16,
+                                       const ShieldField3D* physics16, void* stream);
 
 /* AGrid2DGridPhysics (update_dwind_phys.py): the A-grid wind tendencies
  * turned into D-grid winds. Indices are relative to the compute-domain

@@ -176,6 +176,7 @@ EXPORTS = (
     "shield_mp_check_noalloc",
     "shield_mp_step_flags",
     "shield_mp_substeps",
+    "shield_physics_prestep_from_dycore",
 )
 
 _lib = None
@@ -232,6 +233,10 @@ def load():
     ]
     lib.shield_copy_dycore_to_physics.argtypes = [i32, i32, i32, ctypes.POINTER(ShieldField3D), ctypes.POINTER(ShieldField3D), vp]
     lib.shield_physics_prestep.argtypes = [i32, i32, i32, i32, i32, dbl, i32, ctypes.POINTER(ShieldPhysicsFields), vp]
+    lib.shield_physics_prestep_from_dycore.argtypes = [
+        i32, i32, i32, i32, i32, dbl, i32, ctypes.POINTER(ShieldPhysicsFields), ctypes.POINTER(ShieldField3D),
+        ctypes.POINTER(ShieldField3D), vp,
+    ]
     for name in EXPORTS:
         getattr(lib, name).restype = i32
     _lib = lib

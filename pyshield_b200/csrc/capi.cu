@@ -342,6 +342,7 @@ struct Plan {
   int64_t* d_offs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // cols_per_block 1, 2, 4, 6, 8
   double* d_area = nullptr;
   double* d_qaz = nullptr;
+  unsigned long long* d_counter = nullptr;  // the launch's work-item counter
   std::vector<int64_t> qaz_off;
   int64_t qaz_total = 0;
   std::string last_error;
@@ -361,6 +362,7 @@ void plan_free(Plan* p) {
   for (auto& o : p->d_offs) cudaFree(o);
   cudaFree(p->d_area);
   cudaFree(p->d_qaz);
+  cudaFree(p->d_counter);
   delete p;
 }
 
@@ -449,7 +451,8 @@ extern "C" int shield_mp_ensemble_create(const ShieldMpConfig* cfg, int nz, int 
   if ((e = cudaMalloc(&p->d_area, sizeof(double) * area_total)) != cudaSuccess ||
       (e = cudaMalloc(&p->d_qaz, sizeof(double) * qaz_total)) != cudaSuccess ||
       (e = cudaMemset(p->d_qaz, 0, sizeof(double) * qaz_total)) != cudaSuccess ||
-      (e = cudaMalloc(&p->d_members, sizeof(MpArgs) * nm)) != cudaSuccess) {
+      (e = cudaMalloc(&p->d_members, sizeof(MpArgs) * nm)) != cudaSuccess ||
+      (e = cudaMalloc(&p->d_counter, sizeof(unsigned long long))) != cudaSuccess) {
     int rc = cuda_fail(nullptr, e, "allocating the ensemble plan");
     plan_free(p);
     return rc;
@@ -493,8 +496,8 @@ extern "C" int shield_mp_ensemble_step(void* plan, int G, int bpsm, void* stream
   const int grid = bpsm * p->num_sms;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaError_t e = (p->precision == SHIELD_MP_MIXED)
-                      ? mp_launch_ensemble_mixed(p->d_members, p->d_offs[gi], p->nm, p->nz, G, grid, st)
-                      : mp_launch_ensemble_plain(p->d_members, p->d_offs[gi], p->nm, p->nz, G, grid, st);
+                      ? mp_launch_ensemble_mixed(p->d_members, p->d_offs[gi], p->nm, p->nz, G, grid, p->d_counter, st)
+                      : mp_launch_ensemble_plain(p->d_members, p->d_offs[gi], p->nm, p->nz, G, grid, p->d_counter, st);
   if (e != cudaSuccess) return cuda_fail(nullptr, e, "ensemble launch");
   return SHIELD_OK;
 }

@@ -1369,17 +1369,18 @@ SHD void mp_block(const MpArgs& A, double* sm, const int64_t c0) {
 // ------------------------------------------------- persistent, double-buffered
 // The same step with the staging taken off the critical path: a persistent
 // block walks its share of the column blocks and, while it computes one,
-// copies the next one's inputs -- the 14 fields and the 10 old tendencies
-// the step adds to -- into the other buffer with cp.async, so that the only
-// memory work left between two blocks is issuing the stores.
+// copies the next one's inputs into the other buffer with cp.async: the 14
+// input fields and, where the two buffers have room for them (NT = N_TILE),
+// the 10 old tendencies the step adds to. With NT = N_IN the stage-out reads
+// the old tendencies itself, as the one-block-per-column-block kernel does.
 //
-// Shared memory: two buffers of N_TILE rows per block column, then the
-// scratch and work rows.
+// Shared memory: two buffers of NT rows per block column, then the scratch
+// and work rows.
 constexpr int N_TILE = N_IN + 10;  // the inputs, then the tendencies read before the update
 
-template <class LY>
+template <class LY, int NT = N_TILE>
 struct SmemP {
-  static constexpr size_t buf = (size_t)N_TILE * LY::G * LY::RP;
+  static constexpr size_t buf = (size_t)NT * LY::G * LY::RP;
   static constexpr size_t scratch = 2 * buf;
   static constexpr size_t work = scratch + (size_t)LY::NGRP * 2 * LY::SCR;
   static constexpr size_t total = work + (size_t)LY::NGRP * LY::WORK;
@@ -1398,15 +1399,16 @@ SHD int tend_row(int o) { return N_IN + o; }
 
 SHD const Fld3& tile_src(const MpArgs& A, int r) { return r < N_IN ? A.in[r] : A.out[r - N_IN]; }
 
-// stage_in's mapping, each element copied asynchronously (no register pass).
-template <class LY>
+// stage_in's mapping, each element copied asynchronously (no register pass):
+// the first NT tile rows (the inputs, then the old tendencies).
+template <class LY, int NT = N_TILE>
 SHD void stage_in_async(const MpArgs& A, double* sm, int64_t c0) {
   constexpr int RP = LY::RP, G = LY::G;
   const MpConst& K = A.K;
   StageMap M;
   M.template set<G>(A, threadIdx.x, c0);
 #pragma unroll
-  for (int r = 0; r < N_TILE; ++r) {
+  for (int r = 0; r < NT; ++r) {
     if (r >= N_IN) {
       // a tendency the update adds to (stage_out's OM_ADD / OM_ADD_K1 fields)
       const int o = r - N_IN;
@@ -1444,27 +1446,30 @@ SHD void stage_out_tiled(const MpArgs& A, const double* sm, int64_t c0) {
   }
 }
 
-template <class LY, int MINB, bool MIXED>
+template <class LY, int MINB, bool MIXED, int NT>
 __global__ void __launch_bounds__(LY::THREADS, MINB)
     mp_step_persistent_kernel(const __grid_constant__ MpArgs A, const int64_t nblk) {
   extern __shared__ double sm[];
-  using SP = SmemP<LY>;
+  using SP = SmemP<LY, NT>;
   constexpr int G = LY::G;
   double* const scr = sm + SP::scratch;
   double* const work = sm + SP::work;
   int64_t b = blockIdx.x;
-  if (b < nblk) stage_in_async<LY>(A, sm, b * G);
+  if (b < nblk) stage_in_async<LY, NT>(A, sm, b * G);
   cp_async_commit();
   for (int it = 0; b < nblk; b += gridDim.x, ++it) {
     double* const cur = sm + (it & 1) * SP::buf;
     double* const nxt = sm + ((it + 1) & 1) * SP::buf;
     cp_async_wait_all();
     __syncthreads();  // this block's inputs have landed; the previous one's stage-out is done with nxt
-    if (b + gridDim.x < nblk) stage_in_async<LY>(A, nxt, (b + gridDim.x) * G);
+    if (b + gridDim.x < nblk) stage_in_async<LY, NT>(A, nxt, (b + gridDim.x) * G);
     cp_async_commit();
     mp_body<LY, MIXED>(A, cur, scr, work, b * G);
     __syncthreads();
-    stage_out_tiled<LY>(A, cur, b * G);
+    if constexpr (NT == N_TILE)
+      stage_out_tiled<LY>(A, cur, b * G);
+    else
+      stage_out<LY>(A, cur, b * G);
   }
   cp_async_wait_all();
 }
@@ -1478,40 +1483,60 @@ __global__ void __launch_bounds__(LY::THREADS, MINB) mp_step_kernel(const __grid
 // Many domains (ensemble members) in one persistent launch. Work item wi
 // of the flattened index space is block (wi - offs[m]) of member m, where
 // offs[m] <= wi < offs[m + 1] (offs holds nm + 1 prefix sums of each member's
-// ceil(ncol / G)). Each item copies its member's parameter block into shared
-// memory, so the step body reads its constants from there.
+// ceil(ncol / G)). The persistent blocks take items from a device counter
+// (zero at launch), so a block that drew cheap columns takes more of them:
+// the items' cost varies with the physics their columns run. A block copies
+// its member's parameter block into shared memory when the member changes;
+// the step body reads its constants from there. Measured with 64 members
+// (C24/C48/C96, L79): a fixed stride of items per block and a prefetch of
+// the next item's inputs were both slower.
+SHD int find_member(const int64_t* __restrict__ offs, int nm, int64_t wi) {
+  int lo = 0, hi = nm - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (offs[mid] <= wi)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
 template <class LY, int MINB, bool MIXED>
 __global__ void __launch_bounds__(LY::THREADS, MINB)
-    mp_ensemble_kernel(const MpArgs* __restrict__ members, const int64_t* __restrict__ offs, int nm) {
+    mp_ensemble_kernel(const MpArgs* __restrict__ members, const int64_t* __restrict__ offs, int nm,
+                       unsigned long long* __restrict__ counter) {
   extern __shared__ double sm[];
   __shared__ MpArgs sargs;
+  __shared__ long long sitem;
   __shared__ int smember;
   const int64_t total = offs[nm];
-  for (int64_t wi = blockIdx.x; wi < total; wi += gridDim.x) {
-    __syncthreads();  // the previous item is done with sargs and the tiles
+  int loaded = -1;
+  for (;;) {
     if (threadIdx.x == 0) {
-      int lo = 0, hi = nm - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (offs[mid] <= wi)
-          lo = mid;
-        else
-          hi = mid - 1;
-      }
-      smember = lo;
+      sitem = (long long)atomicAdd(counter, 1ull);
+      smember = sitem < total ? find_member(offs, nm, sitem) : 0;
     }
     __syncthreads();
+    const int64_t wi = sitem;
     const int m = smember;
-    {
+    if (wi >= total) break;
+    if (m != loaded) {
       const int* src = reinterpret_cast<const int*>(members + m);
       int* dst = reinterpret_cast<int*>(&sargs);
       constexpr int nwords = (int)(sizeof(MpArgs) / sizeof(int));
       for (int e = threadIdx.x; e < nwords; e += blockDim.x) dst[e] = src[e];
+      loaded = m;
+      __syncthreads();
     }
-    __syncthreads();
     mp_block<LY, MIXED>(sargs, sm, (wi - offs[m]) * LY::G);
+    __syncthreads();  // the item is done with sargs, sitem and the tiles
   }
 }
+
+#ifndef SHIELD_PREFETCH_INPUTS_ONLY
+#define SHIELD_PREFETCH_INPUTS_ONLY 0
+#endif
 
 // Launch the step over ceil(ncol / G) column blocks. PERSIST: as many
 // persistent, double-buffered blocks as fit on the device at once, each
@@ -1523,8 +1548,11 @@ cudaError_t launch_step(const MpArgs& A, cudaStream_t st) {
   const int64_t nblk = (A.ncol + G - 1) / G;
   const int threads = LY::THREADS;
   if (PERSIST) {
-    auto kern = mp_step_persistent_kernel<LY, MINB, MIXED>;
-    const size_t smem = SmemP<LY>::bytes;
+    // the old tendencies join the prefetch where both buffers have room
+    constexpr bool kTend = SmemP<LY, N_TILE>::bytes <= 220 * 1024 && !SHIELD_PREFETCH_INPUTS_ONLY;
+    constexpr int NT = kTend ? N_TILE : N_IN;
+    auto kern = mp_step_persistent_kernel<LY, MINB, MIXED, NT>;
+    const size_t smem = SmemP<LY, NT>::bytes;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int dev = 0, nsm = 0, per_sm = 0;
@@ -1567,14 +1595,17 @@ using Packed80 = PackedLayout<5, 2, SHIELD_PACK_NGRP>;
 constexpr int PACK80_MINB = SHIELD_PACK_MINB;
 constexpr int PACK80_LMIN = 65, PACK80_LMAX = 80;
 
-// Launch of the ensemble kernel with `grid` persistent blocks.
+// Launch of the ensemble kernel with `grid` persistent blocks; `counter`
+// (one word) is zeroed on `st` first.
 template <class LY, int MINB, bool MIXED>
-cudaError_t launch_ensemble(const MpArgs* members, const int64_t* offs, int nm, int grid, cudaStream_t st) {
+cudaError_t launch_ensemble(const MpArgs* members, const int64_t* offs, int nm, unsigned long long* counter, int grid,
+                            cudaStream_t st) {
   const size_t smem = Smem<LY>::bytes;
   auto kern = mp_ensemble_kernel<LY, MINB, MIXED>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  kern<<<grid, LY::THREADS, smem, st>>>(members, offs, nm);
+  if ((e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st)) != cudaSuccess) return e;
+  kern<<<grid, LY::THREADS, smem, st>>>(members, offs, nm, counter);
   return cudaGetLastError();
 }
 

@@ -13,10 +13,10 @@ cudaError_t mp_launch_plain_flags(const MpArgs& A, cudaStream_t st);
 cudaError_t mp_launch_de_ice(const MpArgs& A, Fld3 qi_dt, Fld3 qs_dt, cudaStream_t st);
 cudaError_t mp_gather_area(const double* p, int64_t si, int64_t sj, int nx, int ny, double* out);
 cudaError_t mp_launch_ensemble_plain(const MpArgs* members, const int64_t* offs, int nm, int nz, int G, int grid,
-                                     cudaStream_t st);
+                                     unsigned long long* counter, cudaStream_t st);
 cudaError_t mp_launch_vjp(const VjpArgs& A, cudaStream_t st);
 int mp_vjp_max_substeps();
 cudaError_t mp_launch_ensemble_mixed(const MpArgs* members, const int64_t* offs, int nm, int nz, int G, int grid,
-                                     cudaStream_t st);
+                                     unsigned long long* counter, cudaStream_t st);
 
 }  // namespace shield

@@ -23,11 +23,13 @@ cudaError_t launch_nw(const MpArgs& A, cudaStream_t st) {
 #ifndef SHIELD_PACK_MINB_MIXED
 #define SHIELD_PACK_MINB_MIXED SHIELD_PACK_MINB
 #endif
+// (measured at C96 L79: 2.52 ms persistent, prefetching the inputs, against
+// 2.51 ms with one block per column block)
 #ifndef SHIELD_PACK_PERSIST
-#define SHIELD_PACK_PERSIST 1
+#define SHIELD_PACK_PERSIST 0
 #endif
 using Packed80Mixed = PackedLayout<5, 2, SHIELD_PACK_NGRP_MIXED>;
-constexpr bool kPersist80 = SHIELD_PACK_PERSIST && SmemP<Packed80Mixed>::bytes <= 220 * 1024;
+constexpr bool kPersist80 = SHIELD_PACK_PERSIST && SmemP<Packed80Mixed, N_IN>::bytes <= 220 * 1024;
 // 97..128 levels, mixed form: columns per block. C96 L127 (ms): 4 columns
 // 4.17, 5 columns 3.70, 6 columns (768 threads, 80 registers) 3.57.
 #ifndef SHIELD_NW4_G_MIXED
@@ -52,20 +54,20 @@ cudaError_t mp_launch_mixed(const MpArgs& A, cudaStream_t st) {
 // Ensemble launch over nz in (64, 128]; the shapes of
 // mp_launch_ensemble_plain.
 cudaError_t mp_launch_ensemble_mixed(const MpArgs* members, const int64_t* offs, int nm, int nz, int G, int grid,
-                                     cudaStream_t st) {
+                                     unsigned long long* counter, cudaStream_t st) {
   if (nz <= PACK80_LMAX) {
-    if (G == 2) return launch_ensemble<PackedLayout<5, 2, 1>, 4, true>(members, offs, nm, grid, st);
-    if (G == 4) return launch_ensemble<PackedLayout<5, 2, 2>, 2, true>(members, offs, nm, grid, st);
-    if (G == 6) return launch_ensemble<PackedLayout<5, 2, 3>, 1, true>(members, offs, nm, grid, st);
-    if (G == 8) return launch_ensemble<PackedLayout<5, 2, 4>, 1, true>(members, offs, nm, grid, st);
+    if (G == 2) return launch_ensemble<PackedLayout<5, 2, 1>, 4, true>(members, offs, nm, counter, grid, st);
+    if (G == 4) return launch_ensemble<PackedLayout<5, 2, 2>, 2, true>(members, offs, nm, counter, grid, st);
+    if (G == 6) return launch_ensemble<PackedLayout<5, 2, 3>, 1, true>(members, offs, nm, counter, grid, st);
+    if (G == 8) return launch_ensemble<PackedLayout<5, 2, 4>, 1, true>(members, offs, nm, counter, grid, st);
   } else if (nz <= 96) {
-    if (G == 1) return launch_ensemble<ColumnLayout<3, 1>, 4, true>(members, offs, nm, grid, st);
-    if (G == 2) return launch_ensemble<ColumnLayout<3, 2>, 2, true>(members, offs, nm, grid, st);
-    if (G == 4) return launch_ensemble<ColumnLayout<3, 4>, 1, true>(members, offs, nm, grid, st);
+    if (G == 1) return launch_ensemble<ColumnLayout<3, 1>, 4, true>(members, offs, nm, counter, grid, st);
+    if (G == 2) return launch_ensemble<ColumnLayout<3, 2>, 2, true>(members, offs, nm, counter, grid, st);
+    if (G == 4) return launch_ensemble<ColumnLayout<3, 4>, 1, true>(members, offs, nm, counter, grid, st);
   } else if (nz <= 128) {
-    if (G == 1) return launch_ensemble<ColumnLayout<4, 1>, 4, true>(members, offs, nm, grid, st);
-    if (G == 2) return launch_ensemble<ColumnLayout<4, 2>, 2, true>(members, offs, nm, grid, st);
-    if (G == 4) return launch_ensemble<ColumnLayout<4, 4>, 1, true>(members, offs, nm, grid, st);
+    if (G == 1) return launch_ensemble<ColumnLayout<4, 1>, 4, true>(members, offs, nm, counter, grid, st);
+    if (G == 2) return launch_ensemble<ColumnLayout<4, 2>, 2, true>(members, offs, nm, counter, grid, st);
+    if (G == 4) return launch_ensemble<ColumnLayout<4, 4>, 1, true>(members, offs, nm, counter, grid, st);
   }
   return cudaErrorInvalidValue;
 }

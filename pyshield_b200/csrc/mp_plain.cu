@@ -56,6 +56,11 @@ int mp_max_levels() { return 256; }
 #ifndef SHIELD_NW3_MINB
 #define SHIELD_NW3_MINB 1
 #endif
+// 65..80 levels, plain form: the persistent, input-prefetching kernel (1) or
+// one block per column block (0).
+#ifndef SHIELD_PACK_PERSIST_PLAIN
+#define SHIELD_PACK_PERSIST_PLAIN 0
+#endif
 // 97..128 levels (L127): columns per block of 4 warps each. C96 L127 (ms):
 // 4 columns (512 threads, 128 registers) 6.29, 5 columns (640, 96) 5.94,
 // 6 columns (768, 80) 5.99.
@@ -67,7 +72,7 @@ cudaError_t mp_launch_plain(const MpArgs& A, cudaStream_t st) {
   const int L = A.nz;
   if (L <= 32) return launch_nw<1, 4, 2>(A, st);
   if (L <= 64) return launch_nw<2, 2, 2>(A, st);
-  if (L <= PACK80_LMAX) return launch_step<Packed80, PACK80_MINB, false, false>(A, st);
+  if (L <= PACK80_LMAX) return launch_step<Packed80, PACK80_MINB, false, SHIELD_PACK_PERSIST_PLAIN>(A, st);
   if (L <= 96) return launch_nw<3, SHIELD_NW3_G, SHIELD_NW3_MINB>(A, st);
   if (L <= 128) return launch_nw<4, SHIELD_NW4_G, 1>(A, st);
   return launch_nw<8, 1, 2>(A, st);
@@ -111,20 +116,20 @@ cudaError_t mp_gather_area(const double* p, int64_t si, int64_t sj, int nx, int 
 // two packed columns; 640 threads per SM where the block size allows);
 // 81..128 levels: G = 1, 2 or 4.
 cudaError_t mp_launch_ensemble_plain(const MpArgs* members, const int64_t* offs, int nm, int nz, int G, int grid,
-                                     cudaStream_t st) {
+                                     unsigned long long* counter, cudaStream_t st) {
   if (nz <= PACK80_LMAX) {
-    if (G == 2) return launch_ensemble<PackedLayout<5, 2, 1>, 4, false>(members, offs, nm, grid, st);
-    if (G == 4) return launch_ensemble<PackedLayout<5, 2, 2>, 2, false>(members, offs, nm, grid, st);
-    if (G == 6) return launch_ensemble<PackedLayout<5, 2, 3>, 1, false>(members, offs, nm, grid, st);
-    if (G == 8) return launch_ensemble<PackedLayout<5, 2, 4>, 1, false>(members, offs, nm, grid, st);
+    if (G == 2) return launch_ensemble<PackedLayout<5, 2, 1>, 4, false>(members, offs, nm, counter, grid, st);
+    if (G == 4) return launch_ensemble<PackedLayout<5, 2, 2>, 2, false>(members, offs, nm, counter, grid, st);
+    if (G == 6) return launch_ensemble<PackedLayout<5, 2, 3>, 1, false>(members, offs, nm, counter, grid, st);
+    if (G == 8) return launch_ensemble<PackedLayout<5, 2, 4>, 1, false>(members, offs, nm, counter, grid, st);
   } else if (nz <= 96) {
-    if (G == 1) return launch_ensemble<ColumnLayout<3, 1>, 4, false>(members, offs, nm, grid, st);
-    if (G == 2) return launch_ensemble<ColumnLayout<3, 2>, 2, false>(members, offs, nm, grid, st);
-    if (G == 4) return launch_ensemble<ColumnLayout<3, 4>, 1, false>(members, offs, nm, grid, st);
+    if (G == 1) return launch_ensemble<ColumnLayout<3, 1>, 4, false>(members, offs, nm, counter, grid, st);
+    if (G == 2) return launch_ensemble<ColumnLayout<3, 2>, 2, false>(members, offs, nm, counter, grid, st);
+    if (G == 4) return launch_ensemble<ColumnLayout<3, 4>, 1, false>(members, offs, nm, counter, grid, st);
   } else if (nz <= 128) {
-    if (G == 1) return launch_ensemble<ColumnLayout<4, 1>, 4, false>(members, offs, nm, grid, st);
-    if (G == 2) return launch_ensemble<ColumnLayout<4, 2>, 2, false>(members, offs, nm, grid, st);
-    if (G == 4) return launch_ensemble<ColumnLayout<4, 4>, 1, false>(members, offs, nm, grid, st);
+    if (G == 1) return launch_ensemble<ColumnLayout<4, 1>, 4, false>(members, offs, nm, counter, grid, st);
+    if (G == 2) return launch_ensemble<ColumnLayout<4, 2>, 2, false>(members, offs, nm, counter, grid, st);
+    if (G == 4) return launch_ensemble<ColumnLayout<4, 4>, 1, false>(members, offs, nm, counter, grid, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -56,8 +56,19 @@ static_assert(offsetof(ShieldPhysicsFields, del_gz) == DELGZ * sizeof(ShieldFiel
 static_assert(offsetof(ShieldPhysicsFields, wmp) == WMP * sizeof(ShieldField3D), "wmp");
 static_assert(offsetof(ShieldPhysicsFields, pt_dt) == TEND0 * sizeof(ShieldField3D), "pt_dt");
 
+// DycoreToPhysics' 16 fields, in its order (update_atmos_state.py:196-232)
+enum {
+  D_QV = 0, D_QL, D_QR, D_QS, D_QI, D_QG, D_QO3, D_TKE, D_QCLD, D_PT, D_DELP, D_DELZ, D_UA, D_VA, D_W, D_OMGA, N_D2P
+};
+// the D2P index of statein's tracer t (qvapor, qliquid, qrain, qice, qsnow, qgraupel, qo3mr)
+__device__ __constant__ int kTracerD2P[N_TRACER] = {D_QV, D_QL, D_QR, D_QI, D_QS, D_QG, D_QO3};
+
 struct PhysArgs {
   F3 f[N_PHYS];
+  // fused DycoreToPhysics copy (fused != 0): the dycore fields and their
+  // physics-state destinations, in the D2P order
+  F3 dsrc[N_D2P], ddst[N_D2P];
+  int fused;
   int nx, ny, nz, hx;
   int nwat, prepare;
   double ptop, pk0inv, pktop;
@@ -108,15 +119,24 @@ __global__ void __launch_bounds__(TC * NWB) physics_prestep_kernel(const __grid_
   const int64_t i = live ? c % nxf - A.hx : 0, j = live ? c / nxf - A.hx : 0;
   const bool compute = live && i >= 0 && j >= 0 && i < A.nx && j < A.ny;
   const bool halo = live && !compute;
+  // With the fused copy, DycoreToPhysics' domain -- the compute domain plus
+  // the interface points i = nx and j = ny, levels 0 .. nz - 1 -- is read
+  // from the dycore storages (the values the copy would have left in the
+  // physics ones) and copied into the physics storages; the halo columns of
+  // that domain (the strip i = nx or j = ny) copy all 16 fields.
+  const bool strip = A.fused && halo && i >= 0 && j >= 0 && i <= A.nx && j <= A.ny;
+  auto rd = [&](int pf, int df, int k) -> double {
+    return (A.fused && k < A.nz && (compute || strip)) ? A.dsrc[df].at(i, j, k) : f[pf].at(i, j, k);
+  };
 
   // ---- A: statein's prelude (PARALLEL interval(...)): tracers * delp, dpn
   for (int k = w; k < nk; k += NWB) {
     if (compute) {
-      if (k < nk - 1) S.ph[k][lane] = f[DELZ].at(i, j, k) * A.GRAV;
-      const double dp0 = f[DELP].at(i, j, k);
+      if (k < nk - 1) S.ph[k][lane] = rd(DELZ, D_DELZ, k) * A.GRAV;
+      const double dp0 = rd(DELP, D_DELP, k);
       double q[N_TRACER];
 #pragma unroll
-      for (int t = 0; t < N_TRACER; ++t) q[t] = f[QV + t].at(i, j, k) * dp0;
+      for (int t = 0; t < N_TRACER; ++t) q[t] = rd(QV + t, kTracerD2P[t], k) * dp0;
       // q[1..5]: ql qr qi qs qg (the argument order qliquid, qrain, qice, qsnow, qgraupel)
       const double dpn = A.nwat == 6 ? dp0 - q[1] - q[2] - q[3] - q[4] - q[5] : dp0;
       if (k < nk - 1) {
@@ -163,13 +183,22 @@ __global__ void __launch_bounds__(TC * NWB) physics_prestep_kernel(const __grid_
         continue;
       }
       // loads
-      const double dp0 = f[DELP].at(i, j, k);
+      const double dp0 = rd(DELP, D_DELP, k);
       double q[N_TRACER];
 #pragma unroll
-      for (int t = 0; t < N_TRACER; ++t) q[t] = f[QV + t].at(i, j, k);
-      const double tke = f[TKE].at(i, j, k);
-      const double pt = f[PT].at(i, j, k);
-      const double om = A.prepare ? f[OMGA].at(i, j, k) : 0.0;
+      for (int t = 0; t < N_TRACER; ++t) q[t] = rd(QV + t, kTracerD2P[t], k);
+      const double tke = rd(TKE, D_TKE, k);
+      const double pt = rd(PT, D_PT, k);
+      const double om = (A.prepare || A.fused) ? rd(OMGA, D_OMGA, k) : 0.0;
+      // the copied fields statein leaves alone
+      double cp[5];
+      if (A.fused) {
+        cp[0] = A.dsrc[D_QCLD].at(i, j, k);
+        cp[1] = A.dsrc[D_DELZ].at(i, j, k);
+        cp[2] = A.dsrc[D_UA].at(i, j, k);
+        cp[3] = A.dsrc[D_VA].at(i, j, k);
+        cp[4] = A.dsrc[D_W].at(i, j, k);
+      }
       // statein
       const double pn = S.p[k + 1][lane];
       const double ph_k = S.ph[k][lane], ph1 = S.ph[k + 1][lane];
@@ -197,6 +226,15 @@ __global__ void __launch_bounds__(TC * NWB) physics_prestep_kernel(const __grid_
       f[DM].at(i, j, k) = dm;
       f[DELP].at(i, j, k) = d;
       f[DELPRSI].at(i, j, k) = pn - p;
+      if (A.fused) {
+        A.ddst[D_QCLD].at(i, j, k) = cp[0];
+        A.ddst[D_DELZ].at(i, j, k) = cp[1];
+        A.ddst[D_UA].at(i, j, k) = cp[2];
+        A.ddst[D_VA].at(i, j, k) = cp[3];
+        A.ddst[D_W].at(i, j, k) = cp[4];
+        A.ddst[D_PT].at(i, j, k) = pt;
+        A.ddst[D_OMGA].at(i, j, k) = om;
+      }
       if (A.prepare) {
         f[WMP].at(i, j, k) = -om * (1.0 + A.ZVIR * qv) * pt / d * A.RDGAS_RGRAV;
 #pragma unroll
@@ -204,8 +242,16 @@ __global__ void __launch_bounds__(TC * NWB) physics_prestep_kernel(const __grid_
           if (f[TEND0 + t].p) f[TEND0 + t].at(i, j, k) = 0.0;
       }
     } else if (halo && k < nk - 1) {
-      const double pt = f[PT].at(i, j, k);
-      const double qv = f[QV].at(i, j, k);
+      const double pt = rd(PT, D_PT, k);
+      const double qv = rd(QV, D_QV, k);
+      if (strip) {
+        // DycoreToPhysics' copy of this interface column
+        double v[N_D2P];
+#pragma unroll
+        for (int d = 0; d < N_D2P; ++d) v[d] = (d == D_PT) ? pt : (d == D_QV) ? qv : A.dsrc[d].at(i, j, k);
+#pragma unroll
+        for (int d = 0; d < N_D2P; ++d) A.ddst[d].at(i, j, k) = v[d];
+      }
       const double p = S.p[k][lane], pn = S.p[k + 1][lane];
       const double ph_k = S.ph[k][lane], ph1 = S.ph[k + 1][lane];
       const double tv = 1.0 + A.ZVIR * np_max(0.0, qv);
@@ -258,8 +304,10 @@ cudaError_t launch_prestep(const PhysArgs& A, int64_t ncf, cudaStream_t st) {
 
 }  // namespace
 
-extern "C" int shield_physics_prestep(int nx, int ny, int nz, int hx, int nwat, double ptop, int flags,
-                                      const ShieldPhysicsFields* fields, void* stream) {
+namespace {
+
+int prestep_impl(int nx, int ny, int nz, int hx, int nwat, double ptop, int flags, const ShieldPhysicsFields* fields,
+                 const ShieldField3D* dycore16, const ShieldField3D* physics16, void* stream) {
   if (!fields || nx < 1 || ny < 1 || nz < 2 || hx < 0 || !(ptop > 0.0)) {
     shield::set_last_error("shield_physics_prestep: bad arguments");
     return SHIELD_EINVAL;
@@ -278,6 +326,23 @@ extern "C" int shield_physics_prestep(int nx, int ny, int nz, int hx, int nwat, 
       return SHIELD_EINVAL;
     }
     A.f[p] = mk(in[p]);
+  }
+  A.fused = 0;
+  if (dycore16 || physics16) {
+    if (!dycore16 || !physics16 || hx < 1) {
+      shield::set_last_error(
+          "shield_physics_prestep_from_dycore: needs the 16 dycore and physics fields and a halo of at least 1");
+      return SHIELD_EINVAL;
+    }
+    for (int d = 0; d < N_D2P; ++d) {
+      if (!dycore16[d].ptr || !physics16[d].ptr) {
+        shield::set_last_error("shield_physics_prestep_from_dycore: null copy field " + std::to_string(d));
+        return SHIELD_EINVAL;
+      }
+      A.dsrc[d] = mk(dycore16[d]);
+      A.ddst[d] = mk(physics16[d]);
+    }
+    A.fused = 1;
   }
   A.nx = nx;
   A.ny = ny;
@@ -307,4 +372,21 @@ extern "C" int shield_physics_prestep(int nx, int ny, int nz, int hx, int nwat, 
     return SHIELD_ECUDA;
   }
   return SHIELD_OK;
+}
+
+}  // namespace
+
+extern "C" int shield_physics_prestep(int nx, int ny, int nz, int hx, int nwat, double ptop, int flags,
+                                      const ShieldPhysicsFields* fields, void* stream) {
+  return prestep_impl(nx, ny, nz, hx, nwat, ptop, flags, fields, nullptr, nullptr, stream);
+}
+
+extern "C" int shield_physics_prestep_from_dycore(int nx, int ny, int nz, int hx, int nwat, double ptop, int flags,
+                                                  const ShieldPhysicsFields* fields, const ShieldField3D* dycore16,
+                                                  const ShieldField3D* physics16, void* stream) {
+  if (!dycore16 || !physics16) {
+    shield::set_last_error("shield_physics_prestep_from_dycore: null dycore or physics fields");
+    return SHIELD_EINVAL;
+  }
+  return prestep_impl(nx, ny, nz, hx, nwat, ptop, flags, fields, dycore16, physics16, stream);
 }

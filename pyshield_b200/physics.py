@@ -35,7 +35,7 @@ from . import _lib
 from . import constants as C
 from ._config import PHYSICS_PACKAGES
 from ._lib import SHIELD_PHYS_PREPARE_MICROPHYSICS, ShieldPhysicsFields, check, load
-from .coupling import update_physics_state_with_tendencies
+from .coupling import D2P_FIELDS, update_physics_state_with_tendencies
 from .grid import X_DIM, Y_DIM, Z_DIM, Z_INTERFACE_DIM
 from .microphysics import Microphysics, MicrophysicsState, _current_stream
 from .quantity import Quantity, field3d
@@ -254,22 +254,40 @@ class Physics:
             setattr(F, name, field3d(q, ext))
         return F
 
-    def prestep(self, physics_state, stream=None):
+    def prestep(self, physics_state, stream=None, dycore_state=None):
         """The driver steps before the microphysics (physics.py:277-330):
         statein, get_prs_fv3, get_phi_fv3 and, with GFS_microphysics,
-        prepare_microphysics, as one kernel launch."""
+        prepare_microphysics, as one kernel launch. With ``dycore_state``,
+        the same launch first does ``DycoreToPhysics``' copy of its 16
+        fields into ``physics_state`` (update_atmos_state.py:196-232): the
+        pre-step reads the dycore storages and writes each copied field
+        once, with the results of the copy followed by the pre-step."""
         ps = physics_state
         # rebuilt on every call from the storages themselves (see
         # Microphysics.__call__), never cached by object identity
         self._build_fields(ps)
         flags = SHIELD_PHYS_PREPARE_MICROPHYSICS if self._gfs_microphysics else 0
-        rc = load().shield_physics_prestep(self.nx, self.ny, self.nz, self.n_halo, self._nwat, self._ptop, flags,
-                                           ctypes.byref(self._fields), ctypes.c_void_p(_current_stream(stream)))
-        check(rc, None, "shield_physics_prestep")
+        st = ctypes.c_void_p(_current_stream(stream))
+        if dycore_state is None:
+            rc = load().shield_physics_prestep(self.nx, self.ny, self.nz, self.n_halo, self._nwat, self._ptop, flags,
+                                               ctypes.byref(self._fields), st)
+            check(rc, None, "shield_physics_prestep")
+            return
+        ext = (self.nx + 1, self.ny + 1, self.nz)
+        arr = _lib.ShieldField3D * len(D2P_FIELDS)
+        src = arr(*[field3d(getattr(dycore_state, f), ext) for f in D2P_FIELDS])
+        dst = arr(*[field3d(getattr(ps, f), ext) for f in D2P_FIELDS])
+        rc = load().shield_physics_prestep_from_dycore(self.nx, self.ny, self.nz, self.n_halo, self._nwat, self._ptop,
+                                                       flags, ctypes.byref(self._fields), src, dst, st)
+        check(rc, None, "shield_physics_prestep_from_dycore")
 
-    def __call__(self, physics_state, timestep, stream=None):
+    def __call__(self, physics_state, timestep, stream=None, dycore_state=None):
+        """``Physics.__call__`` (physics.py:276-366). ``dycore_state``
+        (optional, not in the reference's signature): run
+        ``DycoreToPhysics``' copy from it inside the pre-step launch, in
+        place of a separate ``DycoreToPhysics.__call__`` before this call."""
         ps = physics_state
-        self.prestep(ps, stream)
+        self.prestep(ps, stream, dycore_state)
         if self._gfs_microphysics:
             m = ps.microphysics
             self._microphysics(m, timestep, stream=stream)

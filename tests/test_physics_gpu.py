@@ -39,9 +39,11 @@ def _host3(t):
     return t.permute(2, 1, 0).contiguous().cpu().numpy().transpose(2, 1, 0)
 
 
-def run_physics_gpu(cfg, st, area, nx, ny, L, dt, ptop):
+def run_physics_gpu(cfg, st, area, nx, ny, L, dt, ptop, dycore=None, fused=False):
     """Physics on device copies of the storages ``st``; returns the storages
-    after the call (plus '_prsik', '_dm3d', '_del_gz') and the precipitation."""
+    after the call (plus '_prsik', '_dm3d', '_del_gz') and the precipitation.
+    With ``dycore`` (storages of DycoreToPhysics' 16 fields), DycoreToPhysics
+    runs first: as its own call, or (``fused``) inside the pre-step launch."""
     import torch
 
     from pyshield_b200.grid import GridData, GridIndexing, QuantityFactory, StencilFactory
@@ -63,8 +65,21 @@ def run_physics_gpu(cfg, st, area, nx, ny, L, dt, ptop):
     area_st[H:H + nx, H:H + ny] = area.reshape(ny, nx).T
     area_q = Quantity(torch.from_numpy(np.ascontiguousarray(area_st.T)).cuda().t(), ("x", "y"), "m^2", (H, H), (nx, ny))
     phys = Physics(StencilFactory(gi), qf, GridData(area_q, ptop), cfg)
-    phys(ps, dt)
+    dyc = None
+    if dycore is not None:
+        import types
+
+        from pyshield_b200.coupling import D2P_FIELDS, DycoreToPhysics
+
+        dyc = types.SimpleNamespace(**{f: Quantity(_dev3(dycore[f]), ("x", "y", "z"), "", (H, H, 0), (nx, ny, L))
+                                       for f in D2P_FIELDS})
+        if not fused:
+            DycoreToPhysics(StencilFactory(gi), qf, None, False, False)(dyc, ps)
+    phys(ps, dt, dycore_state=dyc if fused else None)
     torch.cuda.synchronize()
+    if dyc is not None:
+        for f in D2P_FIELDS:
+            assert np.array_equal(_host3(getattr(dyc, f).data), dycore[f]), f"the dycore's {f} changed"
     out = {nm: _host3(getattr(ps, nm).data) for nm in PHYSICS_3D}
     for t in MP_TENDENCIES:
         out[t] = _host3(getattr(ps.microphysics, t).data)
@@ -139,3 +154,28 @@ def test_physics_matches_oracle_c12(kw, dt, nx, ny, L):
     ref.pop("land")
     ref["_prsik"], ref["_dm3d"], ref["_del_gz"] = oracle.prsik, oracle.dm3d, oracle.del_gz
     _compare(got, gpr, ref, rpr, _floors(st, ref, dt, nx, ny, L), f"{nx}x{ny} L{L} {kw}")
+
+
+@pytest.mark.parametrize("L,dt", [(79, 180.0), (127, 150.0)])
+def test_fused_dycore_copy_equals_copy_then_physics(L, dt):
+    """Physics.__call__ with dycore_state (DycoreToPhysics' copy inside the
+    pre-step launch) leaves every storage -- halo, interface points and the
+    extra level included -- bit for bit as DycoreToPhysics.__call__ followed
+    by Physics.__call__ does; the dycore storages are not written."""
+    from pyshield_b200._config import PhysicsConfig
+    from pyshield_b200.coupling import D2P_FIELDS
+    from pyshield_b200.inputs import PTOP, make_physics_state
+
+    nx, ny = 12, 18
+    st, area = make_physics_state(nx, ny, L, seed=61, halo=H)
+    dyn, _ = make_physics_state(nx, ny, L, seed=62, halo=H)
+    dycore = {f: dyn[f] for f in D2P_FIELDS}
+    cfg = PhysicsConfig(dt_atmos=int(dt))
+    a, apr = run_physics_gpu(cfg, st, area, nx, ny, L, dt, PTOP, dycore=dycore, fused=False)
+    b, bpr = run_physics_gpu(cfg, st, area, nx, ny, L, dt, PTOP, dycore=dycore, fused=True)
+    for k in a:
+        assert np.array_equal(a[k], b[k], equal_nan=True), k
+    for k in apr:
+        assert np.array_equal(apr[k], bpr[k]), k
+    # the copy did reach the physics storages: the dycore's winds
+    np.testing.assert_array_equal(b["ua"][H:H + nx + 1, H:H + ny + 1, :L], dyn["ua"][H:H + nx + 1, H:H + ny + 1, :L])

@@ -521,6 +521,24 @@ def run_physics(n_cube=N_CUBE, nlev=79, dt=DT, reps=5):
     peak, peak_kind = peaks()
     achieved = nbytes / (pre_ms / 1000.0) / 1e9
     ncol = nx * ny
+    # DycoreToPhysics then Physics, as two calls and with the copy fused into
+    # the pre-step launch (a dycore state of the copy's 16 fields)
+    import types
+
+    from pyshield_b200.coupling import D2P_FIELDS, DycoreToPhysics
+
+    dyc = types.SimpleNamespace(**{f: Quantity(q[f].data.clone(), ("x", "y", "z"), "", (HALO, HALO, 0),
+                                               (nx, ny, nlev)) for f in D2P_FIELDS})
+    d2p = DycoreToPhysics(StencilFactory(gi), qf, None, False, False)
+
+    def copy_then_physics():
+        d2p(dyc, ps)
+        phys(ps, dt)
+
+    sep_ms = timed(copy_then_physics)
+    fused_ms = timed(lambda: phys(ps, dt, dycore_state=dyc))
+    sep_pre_ms = timed(lambda: (d2p(dyc, ps), phys.prestep(ps)))
+    fused_pre_ms = timed(lambda: phys.prestep(ps, dycore_state=dyc))
     return {
         "workload": f"Physics.__call__ (driver pre-steps, microphysics, state update), C{n_cube} ({ncol} columns) "
                     f"x L{nlev}, dt {dt:g} s, FP64",
@@ -531,6 +549,11 @@ def run_physics(n_cube=N_CUBE, nlev=79, dt=DT, reps=5):
                              "frac": achieved / peak, "bytes_per_launch": nbytes,
                              "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"},
         "gpu_launches_per_step": 3,
+        "with_dycore_copy": {
+            "copy_then_physics_ms": sep_ms, "fused_ms": fused_ms,
+            "copy_then_prestep_ms": sep_pre_ms, "fused_prestep_ms": fused_pre_ms,
+            "note": "DycoreToPhysics.__call__ then Physics.__call__, against Physics.__call__(dycore_state=...) "
+                    "with the copy inside the pre-step launch (bit-identical results)"},
         "note": "device time (CUDA events), mean of the timed calls; the storages are restored before each call",
     }
 

@@ -60,8 +60,11 @@ static_assert(offsetof(ShieldPhysicsFields, pt_dt) == TEND0 * sizeof(ShieldField
 enum {
   D_QV = 0, D_QL, D_QR, D_QS, D_QI, D_QG, D_QO3, D_TKE, D_QCLD, D_PT, D_DELP, D_DELZ, D_UA, D_VA, D_W, D_OMGA, N_D2P
 };
-// the D2P index of statein's tracer t (qvapor, qliquid, qrain, qice, qsnow, qgraupel, qo3mr)
-__device__ __constant__ int kTracerD2P[N_TRACER] = {D_QV, D_QL, D_QR, D_QI, D_QS, D_QG, D_QO3};
+// the D2P index of statein's tracer t (qvapor, qliquid, qrain, qice, qsnow,
+// qgraupel, qo3mr); t is a compile-time index in the unrolled loops
+__host__ __device__ constexpr int tracer_d2p(int t) {
+  return t == 0 ? D_QV : t == 1 ? D_QL : t == 2 ? D_QR : t == 3 ? D_QI : t == 4 ? D_QS : t == 5 ? D_QG : D_QO3;
+}
 
 struct PhysArgs {
   F3 f[N_PHYS];
@@ -105,7 +108,7 @@ struct PreSmem {
   double gz[NKMAX][TC];  // phase C: get_phi_fv3's del_gz
 };
 
-template <int NKMAX>
+template <int NKMAX, bool FUSED>
 __global__ void __launch_bounds__(TC * NWB) physics_prestep_kernel(const __grid_constant__ PhysArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   PreSmem<NKMAX>& S = *reinterpret_cast<PreSmem<NKMAX>*>(smem_raw);
@@ -124,9 +127,12 @@ __global__ void __launch_bounds__(TC * NWB) physics_prestep_kernel(const __grid_
   // from the dycore storages (the values the copy would have left in the
   // physics ones) and copied into the physics storages; the halo columns of
   // that domain (the strip i = nx or j = ny) copy all 16 fields.
-  const bool strip = A.fused && halo && i >= 0 && j >= 0 && i <= A.nx && j <= A.ny;
+  const bool strip = FUSED && halo && i >= 0 && j >= 0 && i <= A.nx && j <= A.ny;
   auto rd = [&](int pf, int df, int k) -> double {
-    return (A.fused && k < A.nz && (compute || strip)) ? A.dsrc[df].at(i, j, k) : f[pf].at(i, j, k);
+    if constexpr (FUSED) {
+      if (k < A.nz && (compute || strip)) return A.dsrc[df].at(i, j, k);
+    }
+    return f[pf].at(i, j, k);
   };
 
   // ---- A: statein's prelude (PARALLEL interval(...)): tracers * delp, dpn
@@ -136,7 +142,7 @@ __global__ void __launch_bounds__(TC * NWB) physics_prestep_kernel(const __grid_
       const double dp0 = rd(DELP, D_DELP, k);
       double q[N_TRACER];
 #pragma unroll
-      for (int t = 0; t < N_TRACER; ++t) q[t] = rd(QV + t, kTracerD2P[t], k) * dp0;
+      for (int t = 0; t < N_TRACER; ++t) q[t] = rd(QV + t, tracer_d2p(t), k) * dp0;
       // q[1..5]: ql qr qi qs qg (the argument order qliquid, qrain, qice, qsnow, qgraupel)
       const double dpn = A.nwat == 6 ? dp0 - q[1] - q[2] - q[3] - q[4] - q[5] : dp0;
       if (k < nk - 1) {
@@ -186,13 +192,13 @@ __global__ void __launch_bounds__(TC * NWB) physics_prestep_kernel(const __grid_
       const double dp0 = rd(DELP, D_DELP, k);
       double q[N_TRACER];
 #pragma unroll
-      for (int t = 0; t < N_TRACER; ++t) q[t] = rd(QV + t, kTracerD2P[t], k);
+      for (int t = 0; t < N_TRACER; ++t) q[t] = rd(QV + t, tracer_d2p(t), k);
       const double tke = rd(TKE, D_TKE, k);
       const double pt = rd(PT, D_PT, k);
-      const double om = (A.prepare || A.fused) ? rd(OMGA, D_OMGA, k) : 0.0;
+      const double om = (A.prepare || FUSED) ? rd(OMGA, D_OMGA, k) : 0.0;
       // the copied fields statein leaves alone
       double cp[5];
-      if (A.fused) {
+      if constexpr (FUSED) {
         cp[0] = A.dsrc[D_QCLD].at(i, j, k);
         cp[1] = A.dsrc[D_DELZ].at(i, j, k);
         cp[2] = A.dsrc[D_UA].at(i, j, k);
@@ -226,7 +232,7 @@ __global__ void __launch_bounds__(TC * NWB) physics_prestep_kernel(const __grid_
       f[DM].at(i, j, k) = dm;
       f[DELP].at(i, j, k) = d;
       f[DELPRSI].at(i, j, k) = pn - p;
-      if (A.fused) {
+      if constexpr (FUSED) {
         A.ddst[D_QCLD].at(i, j, k) = cp[0];
         A.ddst[D_DELZ].at(i, j, k) = cp[1];
         A.ddst[D_UA].at(i, j, k) = cp[2];
@@ -244,7 +250,7 @@ __global__ void __launch_bounds__(TC * NWB) physics_prestep_kernel(const __grid_
     } else if (halo && k < nk - 1) {
       const double pt = rd(PT, D_PT, k);
       const double qv = rd(QV, D_QV, k);
-      if (strip) {
+      if (FUSED && strip) {
         // DycoreToPhysics' copy of this interface column
         double v[N_D2P];
 #pragma unroll
@@ -294,7 +300,7 @@ __global__ void __launch_bounds__(TC * NWB) physics_prestep_kernel(const __grid_
 template <int NKMAX>
 cudaError_t launch_prestep(const PhysArgs& A, int64_t ncf, cudaStream_t st) {
   const size_t smem = sizeof(PreSmem<NKMAX>);
-  auto kern = physics_prestep_kernel<NKMAX>;
+  auto kern = A.fused ? physics_prestep_kernel<NKMAX, true> : physics_prestep_kernel<NKMAX, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int64_t nblk = (ncf + TC - 1) / TC;

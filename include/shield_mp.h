@@ -389,6 +389,21 @@ int shield_agrid_to_dgrid(int nx, int ny, int nz, int grid_type, double dt5, con
                           const ShieldDwindGeometry* geometry, ShieldField3D u, ShieldField3D v, ShieldField3D u_dt,
                           ShieldField3D v_dt, void* stream);
 
+/* The cube-sphere update of shield_agrid_to_dgrid on several tiles at once
+ * (a GPU holding the subtiles of several ranks, up to all six cube tiles):
+ * one launch updates u and v on every tile, a second zeroes every tile's
+ * tendencies, where separate calls take two launches per tile. Each tile's
+ * results are those of its own shield_agrid_to_dgrid call. 1 to 6 tiles,
+ * grid_type <= 3 each. */
+typedef struct {
+  int nx, ny, nz, grid_type;
+  double dt5;
+  ShieldEdgePlan plan;
+  ShieldDwindGeometry geometry;
+  ShieldField3D u, v, u_dt, v_dt;
+} ShieldDwindTile;
+int shield_agrid_to_dgrid_tiles(int ntiles, const ShieldDwindTile* tiles, void* stream);
+
 /* The handle's device error word: every step records the first column
  * whose outputs hold a NaN or an infinity (the kernel never traps). This
  * call waits for `stream`, then returns SHIELD_OK with *bad_column = -1, or

@@ -151,6 +151,12 @@ class ShieldDwindGeometry(ctypes.Structure):
         ("edge_vect_s", ctypes.c_void_p), ("edge_vect_n", ctypes.c_void_p), ("edge_stride", ctypes.c_int64)]
 
 
+class ShieldDwindTile(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("grid_type", ctypes.c_int),
+                ("dt5", ctypes.c_double), ("plan", ShieldEdgePlan), ("geometry", ShieldDwindGeometry),
+                ("u", ShieldField3D), ("v", ShieldField3D), ("u_dt", ShieldField3D), ("v_dt", ShieldField3D)]
+
+
 EXPORTS = (
     "shield_mp_create",
     "shield_mp_step",
@@ -177,6 +183,7 @@ EXPORTS = (
     "shield_mp_step_flags",
     "shield_mp_substeps",
     "shield_physics_prestep_from_dycore",
+    "shield_agrid_to_dgrid_tiles",
 )
 
 _lib = None
@@ -231,6 +238,7 @@ def load():
         i32, i32, i32, i32, dbl, ctypes.POINTER(ShieldEdgePlan), ctypes.POINTER(ShieldDwindGeometry), ShieldField3D,
         ShieldField3D, ShieldField3D, ShieldField3D, vp,
     ]
+    lib.shield_agrid_to_dgrid_tiles.argtypes = [i32, ctypes.POINTER(ShieldDwindTile), vp]
     lib.shield_copy_dycore_to_physics.argtypes = [i32, i32, i32, ctypes.POINTER(ShieldField3D), ctypes.POINTER(ShieldField3D), vp]
     lib.shield_physics_prestep.argtypes = [i32, i32, i32, i32, i32, dbl, i32, ctypes.POINTER(ShieldPhysicsFields), vp]
     lib.shield_physics_prestep_from_dycore.argtypes = [

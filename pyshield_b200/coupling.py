@@ -86,7 +86,17 @@ class UpdateAtmosphereState:
         self.v_srf = None
         load()
 
-    def __call__(self, dycore_state, phy_state, u_dt, v_dt, pt_dt, dt, stream=None):
+    def __call__(self, dycore_state, phy_state, u_dt, v_dt, pt_dt, dt, stream=None, winds=None):
+        """The column stencils in one launch; then, with ``apply_tendencies``
+        and ``winds`` (a ``DGridWindUpdate``; not in the reference's
+        signature, whose ``ApplyPhysicsToDycore`` owns these steps), the halo
+        exchange of u_dt / v_dt and the D-grid wind update on
+        ``dycore_state.u`` / ``.v``."""
+        self._columns(dycore_state, phy_state, u_dt, v_dt, pt_dt, dt, stream)
+        if winds is not None and self._apply_tendencies:
+            winds(dycore_state.u, dycore_state.v, u_dt, v_dt, stream=stream)
+
+    def _columns(self, dycore_state, phy_state, u_dt, v_dt, pt_dt, dt, stream=None):
         nx, ny, nz, h = self.nx, self.ny, self.nz, self.n_halo
         ext = (nx, ny, nz + 1)
         d, p = dycore_state, phy_state
@@ -166,3 +176,34 @@ class DycoreToPhysics:
         rc = load().shield_copy_dycore_to_physics(self.nx, self.ny, self.nz, src, dst,
                                                   ctypes.c_void_p(_current_stream(stream)))
         check(rc, None, "shield_copy_dycore_to_physics")
+
+
+class DGridWindUpdate:
+    """The horizontal half of ``ApplyPhysicsToDycore`` that follows its column
+    stencils (fv_update_phys.py:134-147, 173-195): the one-point halo
+    exchange of ``u_dt`` and ``v_dt`` with the neighbouring ranks
+    (``halo.HaloExchange`` over the edge ``table``; this rank is ``rank``),
+    then ``AGrid2DGridPhysics`` (``agrid_to_dgrid``). ``CubedToLatLon``,
+    which the reference runs next, is NDSL's and stays with the caller.
+
+    The reference starts the exchange before ``update_pressure_and_surface_
+    winds`` and waits after it; here that stencil runs inside
+    ``UpdateAtmosphereState``'s single column launch, which also produces
+    the tendencies, so the exchange starts after that launch."""
+
+    def __init__(self, agrid_to_dgrid, table, rank, group=None):
+        from .halo import check_table
+
+        check_table(table)
+        self.agrid_to_dgrid = agrid_to_dgrid
+        self.table = table
+        self.rank = rank
+        self.group = group
+
+    def __call__(self, u, v, u_dt, v_dt, stream=None):
+        from .halo import HaloExchange
+
+        ex = HaloExchange([u_dt, v_dt], self.table, self.rank, self.group)
+        ex.start()
+        ex.wait()
+        self.agrid_to_dgrid(u, v, u_dt, v_dt, stream=stream)

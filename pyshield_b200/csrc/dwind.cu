@@ -80,12 +80,12 @@ constexpr int DW_KB = 4;
 // The edge-plan tests and the points' addresses are worked out once, before
 // the level loop. Four blocks per SM (a 64-register cap, a few bytes
 // spilled) measured faster than three without the cap.
-__global__ void __launch_bounds__(DT_X * DT_Y, 4) dwind_update_kernel(const __grid_constant__ DwindArgs A) {
+__device__ __forceinline__ void dwind_update_tile(const DwindArgs& A, int bx, int by, int bz) {
   __shared__ double g_lon[3][AT_Y][AT_X], g_lat[3][AT_Y][AT_X], v3s[3][AT_Y][AT_X];
   constexpr int NT = DT_X * DT_Y;
   constexpr int NA = (AT_X * AT_Y + NT - 1) / NT;  // A points per thread
   const int tx = threadIdx.x % DT_X, ty = threadIdx.x / DT_X;
-  const int i0 = blockIdx.x * DT_X, j0 = blockIdx.y * DT_Y, k0 = blockIdx.z * DT_K;
+  const int i0 = bx * DT_X, j0 = by * DT_Y, k0 = bz * DT_K;
   const int i = i0 + tx, j = j0 + ty;
   const int k1 = k0 + DT_K < A.nz ? k0 + DT_K : A.nz;
   // this thread's A points: their place in the tile, their geometry, and
@@ -199,8 +199,29 @@ __global__ void __launch_bounds__(DT_X * DT_Y, 4) dwind_update_kernel(const __gr
   }
 }
 
+__global__ void __launch_bounds__(DT_X * DT_Y, 4) dwind_update_kernel(const __grid_constant__ DwindArgs A) {
+  dwind_update_tile(A, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Several tiles (the ranks' subtiles a GPU holds, at most DW_MAXT) in one
+// launch: blockIdx.z is (tile, level block); a tile smaller than the grid's
+// largest leaves the blocks beyond its points idle.
+constexpr int DW_MAXT = 6;
+struct DwindBatch {
+  DwindArgs t[DW_MAXT];
+  int n, nkz;
+};
+
+__global__ void __launch_bounds__(DT_X * DT_Y, 4) dwind_update_batch_kernel(const __grid_constant__ DwindBatch B) {
+  const int t = blockIdx.z / B.nkz;
+  const DwindArgs& A = B.t[t];
+  if ((int)blockIdx.x * DT_X > A.nx || (int)blockIdx.y * DT_Y > A.ny || (int)(blockIdx.z % B.nkz) * DT_K >= A.nz)
+    return;
+  dwind_update_tile(A, blockIdx.x, blockIdx.y, blockIdx.z % B.nkz);
+}
+
 // set_winds_zero on the prep domain: i, j in [-1, n + 1), DW_KB levels per thread
-__global__ void dwind_zero_kernel(const __grid_constant__ DwindArgs A) {
+__device__ __forceinline__ void dwind_zero_tile(const DwindArgs& A) {
   const int i = blockIdx.x * DW_BX + threadIdx.x - 1;
   if (i > A.nx) return;
   const int nkb = (A.nz + DW_KB - 1) / DW_KB;
@@ -215,6 +236,11 @@ __global__ void dwind_zero_kernel(const __grid_constant__ DwindArgs A) {
     }
   }
 }
+
+__global__ void dwind_zero_kernel(const __grid_constant__ DwindArgs A) { dwind_zero_tile(A); }
+
+// every tile of a batch: blockIdx.z is the tile
+__global__ void dwind_zero_batch_kernel(const __grid_constant__ DwindBatch B) { dwind_zero_tile(B.t[blockIdx.z]); }
 
 // doubly_periodic_wind_update (update_dwind_phys.py:153-161) on the compute domain
 __global__ void dwind_periodic_kernel(const __grid_constant__ DwindArgs A) {
@@ -233,20 +259,21 @@ __global__ void dwind_periodic_kernel(const __grid_constant__ DwindArgs A) {
 F3 mk3(const ShieldField3D& f) { return F3{f.ptr, f.si, f.sj, f.sk}; }
 F2 mk2(const ShieldField2D& f) { return F2{f.ptr, f.si, f.sj}; }
 
-}  // namespace
 
-extern "C" int shield_agrid_to_dgrid(int nx, int ny, int nz, int grid_type, double dt5, const ShieldEdgePlan* plan,
-                                     const ShieldDwindGeometry* g, ShieldField3D u, ShieldField3D v,
-                                     ShieldField3D u_dt, ShieldField3D v_dt, void* stream) {
+// Checked kernel arguments of one tile; the message names the entry point.
+int make_args(const char* who, int nx, int ny, int nz, int grid_type, double dt5, const ShieldEdgePlan* plan,
+              const ShieldDwindGeometry* g, ShieldField3D u, ShieldField3D v, ShieldField3D u_dt, ShieldField3D v_dt,
+              DwindArgs& A) {
+  const std::string w(who);
   if (nx < 1 || ny < 1 || nz < 1 || !u.ptr || !v.ptr || !u_dt.ptr || !v_dt.ptr) {
-    shield::set_last_error("shield_agrid_to_dgrid: bad arguments");
+    shield::set_last_error(w + ": bad arguments");
     return SHIELD_EINVAL;
   }
   if ((int64_t)(ny + 2) * nz > INT32_MAX || nx > INT32_MAX - 2 * DW_BX) {
-    shield::set_last_error("shield_agrid_to_dgrid: domain too large for 32-bit row indices");
+    shield::set_last_error(w + ": domain too large for 32-bit row indices");
     return SHIELD_ELAYOUT;
   }
-  DwindArgs A{};
+  A = DwindArgs{};
   A.u = mk3(u);
   A.v = mk3(v);
   A.udt = mk3(u_dt);
@@ -255,47 +282,59 @@ extern "C" int shield_agrid_to_dgrid(int nx, int ny, int nz, int grid_type, doub
   A.ny = ny;
   A.nz = nz;
   A.dt5 = dt5;
+  if (grid_type > 3) return SHIELD_OK;
+  if (!plan || !g) {
+    shield::set_last_error(w + ": the cube-sphere update needs the edge plan and the geometry");
+    return SHIELD_EINVAL;
+  }
+  for (int s = 0; s < 4; ++s) {
+    if (plan->n[s] < 0 || plan->n[s] > 2) {
+      shield::set_last_error(w + ": at most two regions per edge");
+      return SHIELD_EINVAL;
+    }
+  }
+  const ShieldField2D* geo[14] = {&g->vlon1, &g->vlon2, &g->vlon3, &g->vlat1, &g->vlat2, &g->vlat3, &g->es1_1,
+                                  &g->es1_2, &g->es1_3, &g->ew2_1, &g->ew2_2, &g->ew2_3, &g->edge_vect_w,
+                                  &g->edge_vect_e};
+  for (int q = 0; q < 14; ++q) {
+    if (!geo[q]->ptr) {
+      shield::set_last_error(w + ": null geometry field " + std::to_string(q));
+      return SHIELD_EINVAL;
+    }
+  }
+  if (!g->edge_vect_s || !g->edge_vect_n) {
+    shield::set_last_error(w + ": null edge_vect_s / edge_vect_n");
+    return SHIELD_EINVAL;
+  }
+  for (int m = 0; m < 3; ++m) {
+    A.vlon[m] = mk2(*geo[m]);
+    A.vlat[m] = mk2(*geo[3 + m]);
+    A.es1[m] = mk2(*geo[6 + m]);
+    A.ew2[m] = mk2(*geo[9 + m]);
+  }
+  A.ev_w = mk2(g->edge_vect_w);
+  A.ev_e = mk2(g->edge_vect_e);
+  A.ev_s = g->edge_vect_s;
+  A.ev_n = g->edge_vect_n;
+  A.ev_stride = g->edge_stride;
+  A.plan = *plan;
+  return SHIELD_OK;
+}
+
+}  // namespace
+
+extern "C" int shield_agrid_to_dgrid(int nx, int ny, int nz, int grid_type, double dt5, const ShieldEdgePlan* plan,
+                                     const ShieldDwindGeometry* g, ShieldField3D u, ShieldField3D v,
+                                     ShieldField3D u_dt, ShieldField3D v_dt, void* stream) {
+  DwindArgs A;
+  int rc = make_args("shield_agrid_to_dgrid", nx, ny, nz, grid_type, dt5, plan, g, u, v, u_dt, v_dt, A);
+  if (rc != SHIELD_OK) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   cudaError_t e;
   if (grid_type > 3) {
     dwind_periodic_kernel<<<row_grid(nx, (int64_t)ny * nz), DW_BX, 0, st>>>(A);
     e = cudaGetLastError();
   } else {
-    if (!plan || !g) {
-      shield::set_last_error("shield_agrid_to_dgrid: the cube-sphere update needs the edge plan and the geometry");
-      return SHIELD_EINVAL;
-    }
-    for (int s = 0; s < 4; ++s) {
-      if (plan->n[s] < 0 || plan->n[s] > 2) {
-        shield::set_last_error("shield_agrid_to_dgrid: at most two regions per edge");
-        return SHIELD_EINVAL;
-      }
-    }
-    const ShieldField2D* geo[14] = {&g->vlon1, &g->vlon2, &g->vlon3, &g->vlat1, &g->vlat2, &g->vlat3, &g->es1_1,
-                                    &g->es1_2, &g->es1_3, &g->ew2_1, &g->ew2_2, &g->ew2_3, &g->edge_vect_w,
-                                    &g->edge_vect_e};
-    for (int q = 0; q < 14; ++q) {
-      if (!geo[q]->ptr) {
-        shield::set_last_error("shield_agrid_to_dgrid: null geometry field " + std::to_string(q));
-        return SHIELD_EINVAL;
-      }
-    }
-    if (!g->edge_vect_s || !g->edge_vect_n) {
-      shield::set_last_error("shield_agrid_to_dgrid: null edge_vect_s / edge_vect_n");
-      return SHIELD_EINVAL;
-    }
-    for (int m = 0; m < 3; ++m) {
-      A.vlon[m] = mk2(*geo[m]);
-      A.vlat[m] = mk2(*geo[3 + m]);
-      A.es1[m] = mk2(*geo[6 + m]);
-      A.ew2[m] = mk2(*geo[9 + m]);
-    }
-    A.ev_w = mk2(g->edge_vect_w);
-    A.ev_e = mk2(g->edge_vect_e);
-    A.ev_s = g->edge_vect_s;
-    A.ev_n = g->edge_vect_n;
-    A.ev_stride = g->edge_stride;
-    A.plan = *plan;
     const dim3 tiles((unsigned)((nx + DT_X) / DT_X), (unsigned)((ny + DT_Y) / DT_Y), (unsigned)((nz + DT_K - 1) / DT_K));
     dwind_update_kernel<<<tiles, DT_X * DT_Y, 0, st>>>(A);
     const int64_t nkb = (nz + DW_KB - 1) / DW_KB;
@@ -307,6 +346,45 @@ extern "C" int shield_agrid_to_dgrid(int nx, int ny, int nz, int grid_type, doub
   }
   if (e != cudaSuccess) {
     shield::set_last_error(std::string("shield_agrid_to_dgrid: ") + cudaGetErrorString(e));
+    return SHIELD_ECUDA;
+  }
+  return SHIELD_OK;
+}
+
+extern "C" int shield_agrid_to_dgrid_tiles(int ntiles, const ShieldDwindTile* tiles, void* stream) {
+  if (ntiles < 1 || ntiles > DW_MAXT || !tiles) {
+    shield::set_last_error("shield_agrid_to_dgrid_tiles: 1 to 6 tiles");
+    return SHIELD_EINVAL;
+  }
+  DwindBatch B{};
+  B.n = ntiles;
+  int mx = 0, my = 0, mz = 0;
+  for (int t = 0; t < ntiles; ++t) {
+    const ShieldDwindTile& T = tiles[t];
+    if (T.grid_type > 3) {
+      shield::set_last_error("shield_agrid_to_dgrid_tiles: cube-sphere tiles only (grid_type <= 3)");
+      return SHIELD_EINVAL;
+    }
+    int rc = make_args("shield_agrid_to_dgrid_tiles", T.nx, T.ny, T.nz, T.grid_type, T.dt5, &T.plan, &T.geometry,
+                       T.u, T.v, T.u_dt, T.v_dt, B.t[t]);
+    if (rc != SHIELD_OK) return rc;
+    mx = T.nx > mx ? T.nx : mx;
+    my = T.ny > my ? T.ny : my;
+    mz = T.nz > mz ? T.nz : mz;
+  }
+  B.nkz = (mz + DT_K - 1) / DT_K;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const dim3 grid((unsigned)((mx + DT_X) / DT_X), (unsigned)((my + DT_Y) / DT_Y), (unsigned)(B.nkz * ntiles));
+  dwind_update_batch_kernel<<<grid, DT_X * DT_Y, 0, st>>>(B);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    const int64_t nkb = (mz + DW_KB - 1) / DW_KB;
+    const dim3 zg = row_grid(mx + 2, (int64_t)(my + 2) * nkb);
+    dwind_zero_batch_kernel<<<dim3(zg.x, zg.y, (unsigned)ntiles), DW_BX, 0, st>>>(B);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    shield::set_last_error(std::string("shield_agrid_to_dgrid_tiles: ") + cudaGetErrorString(e));
     return SHIELD_ECUDA;
   }
   return SHIELD_OK;

@@ -108,8 +108,11 @@ struct PreSmem {
   double gz[NKMAX][TC];  // phase C: get_phi_fv3's del_gz
 };
 
+// Two blocks (16 warps) per SM: the kernel waits on memory, so it needs the
+// resident warps; the fused copy's extra loads would otherwise take the
+// registers of the second block.
 template <int NKMAX, bool FUSED>
-__global__ void __launch_bounds__(TC * NWB) physics_prestep_kernel(const __grid_constant__ PhysArgs A) {
+__global__ void __launch_bounds__(TC * NWB, 2) physics_prestep_kernel(const __grid_constant__ PhysArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   PreSmem<NKMAX>& S = *reinterpret_cast<PreSmem<NKMAX>*>(smem_raw);
   const int nxf = A.nx + 2 * A.hx, nyf = A.ny + 2 * A.hx;
@@ -251,12 +254,10 @@ __global__ void __launch_bounds__(TC * NWB) physics_prestep_kernel(const __grid_
       const double pt = rd(PT, D_PT, k);
       const double qv = rd(QV, D_QV, k);
       if (FUSED && strip) {
-        // DycoreToPhysics' copy of this interface column
-        double v[N_D2P];
-#pragma unroll
-        for (int d = 0; d < N_D2P; ++d) v[d] = (d == D_PT) ? pt : (d == D_QV) ? qv : A.dsrc[d].at(i, j, k);
-#pragma unroll
-        for (int d = 0; d < N_D2P; ++d) A.ddst[d].at(i, j, k) = v[d];
+        // DycoreToPhysics' copy of this interface column (a few columns:
+        // one field at a time, to keep the registers for the compute path)
+#pragma unroll 1
+        for (int d = 0; d < N_D2P; ++d) A.ddst[d].at(i, j, k) = A.dsrc[d].at(i, j, k);
       }
       const double p = S.p[k][lane], pn = S.p[k + 1][lane];
       const double ph_k = S.ph[k][lane], ph1 = S.ph[k + 1][lane];

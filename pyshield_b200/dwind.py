@@ -123,7 +123,7 @@ class AGrid2DGridPhysics:
             self._geom = G
         load()
 
-    def __call__(self, u, v, u_dt, v_dt, stream=None):
+    def _winds(self, u, v, u_dt, v_dt):
         nx, ny, nz, h = self.nx, self.ny, self.nz, self.n_halo
         # u: j in [0, ny]; v: i in [0, nx]; the tendencies: one halo point
         fu = field3d(u, (nx, ny + 1, nz))
@@ -134,8 +134,33 @@ class AGrid2DGridPhysics:
                 raise ValueError("u_dt / v_dt need one halo point around the compute domain")
         fudt = field3d(u_dt, (nx + 1, ny + 1, nz))
         fvdt = field3d(v_dt, (nx + 1, ny + 1, nz))
+        return fu, fv, fudt, fvdt
+
+    def __call__(self, u, v, u_dt, v_dt, stream=None):
+        nx, ny, nz = self.nx, self.ny, self.nz
+        fu, fv, fudt, fvdt = self._winds(u, v, u_dt, v_dt)
         plan = ctypes.byref(self._plan) if self._plan is not None else None
         geom = ctypes.byref(self._geom) if self._geom is not None else None
         rc = load().shield_agrid_to_dgrid(nx, ny, nz, self._grid_type, float(self._dt5), plan, geom, fu, fv, fudt, fvdt,
                                           ctypes.c_void_p(_current_stream(stream)))
         check(rc, None, "shield_agrid_to_dgrid")
+
+
+def agrid_to_dgrid_tiles(calls, stream=None):
+    """Several ``AGrid2DGridPhysics.__call__`` at once: ``calls`` is a list
+    of (a2d, u, v, u_dt, v_dt), one per tile this GPU holds (1 to 6,
+    cube-sphere grids). Two launches in all (``shield_agrid_to_dgrid_tiles``)
+    instead of two per tile; every tile's results are its own call's."""
+    from ._lib import ShieldDwindTile
+
+    if not 1 <= len(calls) <= 6:
+        raise ValueError("1 to 6 tiles")
+    arr = (ShieldDwindTile * len(calls))()
+    for T, (a2d, u, v, u_dt, v_dt) in zip(arr, calls):
+        if a2d._grid_type > 3:
+            raise ValueError("agrid_to_dgrid_tiles takes cube-sphere tiles (grid_type <= 3)")
+        T.nx, T.ny, T.nz, T.grid_type, T.dt5 = a2d.nx, a2d.ny, a2d.nz, a2d._grid_type, float(a2d._dt5)
+        T.plan, T.geometry = a2d._plan, a2d._geom
+        T.u, T.v, T.u_dt, T.v_dt = a2d._winds(u, v, u_dt, v_dt)
+    rc = load().shield_agrid_to_dgrid_tiles(len(calls), arr, ctypes.c_void_p(_current_stream(stream)))
+    check(rc, None, "shield_agrid_to_dgrid_tiles")

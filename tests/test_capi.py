@@ -119,3 +119,41 @@ def test_argument_checks_on_the_cpu():
     assert "use_ppm" in _lib.last_error()
     assert lib.shield_mp_step(None, None, 150.0, 0, None) == -1
     assert lib.shield_update_physics_state(0, 1, 1, None, None, None, 1.0, None) == -1
+
+
+def test_ctypes_structs_match_the_header(tmp_path):
+    """The ctypes mirrors of the header's structs have the C sizes and field
+    offsets (a mismatch would hand the kernels shifted pointers)."""
+    import ctypes
+    import subprocess
+
+    from pyshield_b200 import _lib
+
+    checks = {
+        "ShieldMpFields": (_lib.ShieldMpFields, ["land", "rain", "graupel"]),
+        "ShieldMpCotangents": (_lib.ShieldMpCotangents, ["qaz", "rain"]),
+        "ShieldMpGradients": (_lib.ShieldMpGradients, ["qaz"]),
+        "ShieldMpMember": (_lib.ShieldMpMember, ["nx", "timestep", "area"]),
+        "ShieldPhysicsFields": (_lib.ShieldPhysicsFields, ["wmp", "vdt"]),
+        "ShieldEdgePlan": (_lib.ShieldEdgePlan, ["r"]),
+        "ShieldDwindGeometry": (_lib.ShieldDwindGeometry, ["edge_vect_s", "edge_stride"]),
+        "ShieldDwindTile": (_lib.ShieldDwindTile, ["dt5", "plan", "geometry", "u", "v_dt"]),
+        "ShieldMpConfig": (_lib.ShieldMpConfig, ["clin"]),
+    }
+    src = ['#include <stdio.h>', '#include <stddef.h>', '#include "shield_mp.h"', "int main(void) {"]
+    for name, (_, fields) in checks.items():
+        src.append(f'  printf("{name} %zu\\n", sizeof({name}));')
+        for f in fields:
+            src.append(f'  printf("{name}.{f} %zu\\n", offsetof({name}, {f}));')
+    src.append("  return 0;\n}")
+    c = tmp_path / "sizes.c"
+    c.write_text("\n".join(src))
+    exe = tmp_path / "sizes"
+    r = subprocess.run(["gcc", "-I", os.path.dirname(HEADER), str(c), "-o", str(exe)], capture_output=True,
+                       text=True)
+    assert r.returncode == 0, r.stderr
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True).stdout.splitlines())
+    for name, (cls, fields) in checks.items():
+        assert int(got[name]) == ctypes.sizeof(cls), name
+        for f in fields:
+            assert int(got[f"{name}.{f}"]) == getattr(cls, f).offset, f"{name}.{f}"

@@ -175,3 +175,98 @@ def test_doubly_periodic_matches_oracle(order):
     doubly_periodic(ref["u"], ref["v"], ref["u_dt"], ref["v_dt"], nx, ny, L, h, 0.5 * dt)
     for k in f:
         np.testing.assert_array_equal(t[k].cpu().numpy(), ref[k], err_msg=k)
+
+
+@pytest.mark.gpu
+def test_tiles_in_one_launch_equal_separate_calls():
+    """agrid_to_dgrid_tiles (two launches for all tiles) leaves every
+    storage of every tile bit for bit as each tile's own call does: six
+    tiles of unequal size, layouts and ranks (whole tiles and subtiles)."""
+    from types import SimpleNamespace
+
+    import torch
+
+    from pyshield_b200.dwind import AGrid2DGridPhysics, agrid_to_dgrid_tiles
+    from pyshield_b200.grid import GridIndexing, StencilFactory
+    from pyshield_b200.quantity import Quantity
+
+    h, L = 3, 9
+    cases = [(40, (1, 1), 0), (34, (1, 1), 0), (66, (2, 2), 3), (66, (2, 2), 0), (48, (2, 1), 1), (20, (1, 1), 0)]
+
+    def build(seed):
+        rng = np.random.default_rng(seed)
+        out = []
+        for t, (n, layout, rank) in enumerate(cases):
+            nx, ny = n // layout[0], n // layout[1]
+            sy, sx = rank // layout[0], rank % layout[0]
+            gi = GridIndexing(nx, ny, L, h)
+            gi.south_edge, gi.north_edge = sy == 0, sy == layout[1] - 1
+            gi.west_edge, gi.east_edge = sx == 0, sx == layout[0] - 1
+            shape3 = (nx + 2 * h + 1, ny + 2 * h + 1, L + 1)
+            dev3 = lambda a: torch.from_numpy(np.ascontiguousarray(a.transpose(2, 1, 0))).cuda().permute(2, 1, 0)  # noqa: E731
+            dev2 = lambda a: torch.from_numpy(np.ascontiguousarray(a.T)).cuda().t()  # noqa: E731
+            geom = {g: dev2(rng.uniform(-1.0, 1.0, shape3[:2])) for g in (
+                "vlon1", "vlon2", "vlon3", "vlat1", "vlat2", "vlat3", "es1_1", "es1_2", "es1_3", "ew2_1", "ew2_2",
+                "ew2_3")}
+            geom["edge_vect_w"] = dev2(rng.uniform(0.0, 1.0, shape3[:2]))
+            geom["edge_vect_e"] = dev2(rng.uniform(0.0, 1.0, shape3[:2]))
+            geom["edge_vect_s"] = torch.from_numpy(rng.uniform(0.0, 1.0, shape3[0])).cuda()
+            geom["edge_vect_n"] = torch.from_numpy(rng.uniform(0.0, 1.0, shape3[0])).cuda()
+            part = SimpleNamespace(subtile_index=lambda r, s=(sy, sx): s)
+            nl = SimpleNamespace(dt_atmos=225.0, npx=n + 1, npy=n + 1, layout=layout)
+            a2d = AGrid2DGridPhysics(StencilFactory(gi), None, part, rank, nl, SimpleNamespace(grid_type=0, **geom))
+            q = {k: Quantity(dev3(rng.normal(0.0, s, shape3)), ("x", "y", "z"), "", (h, h, 0), (nx, ny, L))
+                 for k, s in (("u", 20.0), ("v", 20.0), ("u_dt", 1e-3), ("v_dt", 1e-3))}
+            out.append((a2d, q))
+        return out
+
+    sep, bat = build(7), build(7)
+    for a2d, q in sep:
+        a2d(q["u"], q["v"], q["u_dt"], q["v_dt"])
+    agrid_to_dgrid_tiles([(a2d, q["u"], q["v"], q["u_dt"], q["v_dt"]) for a2d, q in bat])
+    torch.cuda.synchronize()
+    for t, ((_, qa), (_, qb)) in enumerate(zip(sep, bat)):
+        for k in ("u", "v", "u_dt", "v_dt"):
+            np.testing.assert_array_equal(qa[k].data.cpu().numpy(), qb[k].data.cpu().numpy(), err_msg=f"tile {t} {k}")
+
+
+@pytest.mark.gpu
+def test_wind_update_with_periodic_halo():
+    """DGridWindUpdate on one rank of a doubly periodic plane: the halo
+    exchange fills the one-point halo of u_dt / v_dt from the opposite edges
+    (this rank is its own neighbour), then the doubly periodic D-grid update
+    runs; against the oracle's update on storages whose halos were filled by
+    hand, bit for bit."""
+    from types import SimpleNamespace
+
+    import torch
+
+    from oracle.dwind import doubly_periodic
+    from pyshield_b200.coupling import DGridWindUpdate
+    from pyshield_b200.dwind import AGrid2DGridPhysics
+    from pyshield_b200.grid import GridIndexing, StencilFactory
+    from pyshield_b200.halo import doubly_periodic as periodic_table
+    from pyshield_b200.quantity import Quantity
+
+    nx, ny, L, h, dt = 40, 24, 7, 3, 180.0
+    rng = np.random.default_rng(9)
+    shape3 = (nx + 2 * h + 1, ny + 2 * h + 1, L + 1)
+    f = {"u": rng.uniform(-30.0, 30.0, shape3), "v": rng.uniform(-30.0, 30.0, shape3),
+         "u_dt": rng.normal(0.0, 1e-3, shape3), "v_dt": rng.normal(0.0, 1e-3, shape3)}
+    t = {k: torch.from_numpy(np.ascontiguousarray(a.T)).cuda().permute(2, 1, 0) for k, a in f.items()}
+    q = {k: Quantity(v, ("x", "y", "z"), "", (h, h, 0), (nx, ny, L)) for k, v in t.items()}
+    namelist = SimpleNamespace(dt_atmos=dt, npx=nx + 1, npy=ny + 1, layout=(1, 1))
+    a2d = AGrid2DGridPhysics(StencilFactory(GridIndexing(nx, ny, L, h)), None, None, 0, namelist,
+                             SimpleNamespace(grid_type=4))
+    DGridWindUpdate(a2d, periodic_table((1, 1)), 0)(q["u"], q["v"], q["u_dt"], q["v_dt"])
+    torch.cuda.synchronize()
+    ref = {k: v.copy() for k, v in f.items()}
+    for k in ("u_dt", "v_dt"):  # the periodic one-point halo, corners excluded
+        a = ref[k]
+        a[h - 1, h:h + ny, :L] = a[h + nx - 1, h:h + ny, :L]
+        a[h + nx, h:h + ny, :L] = a[h, h:h + ny, :L]
+        a[h:h + nx, h - 1, :L] = a[h:h + nx, h + ny - 1, :L]
+        a[h:h + nx, h + ny, :L] = a[h:h + nx, h, :L]
+    doubly_periodic(ref["u"], ref["v"], ref["u_dt"], ref["v_dt"], nx, ny, L, h, 0.5 * dt)
+    for k in f:
+        np.testing.assert_array_equal(t[k].cpu().numpy(), ref[k], err_msg=k)

@@ -206,18 +206,32 @@ __global__ void __launch_bounds__(DT_X * DT_Y, 4) dwind_update_kernel(const __gr
 // Several tiles (the ranks' subtiles a GPU holds, at most DW_MAXT) in one
 // launch: blockIdx.z is (tile, level block); a tile smaller than the grid's
 // largest leaves the blocks beyond its points idle.
-constexpr int DW_MAXT = 6;
+constexpr int DW_MAXT = 6;  // the batch kernels' switches name tiles 0 .. 5
 struct DwindBatch {
   DwindArgs t[DW_MAXT];
   int n, nkz;
 };
 
+// One tile of the batch; T is a compile-time index, so that every read of
+// the tile's arguments is a fixed offset into the kernel parameters.
+template <int T>
+__device__ __forceinline__ void dwind_update_batch_tile(const DwindBatch& B) {
+  const DwindArgs& A = B.t[T];
+  const int bz = blockIdx.z % B.nkz;
+  if ((int)blockIdx.x * DT_X > A.nx || (int)blockIdx.y * DT_Y > A.ny || bz * DT_K >= A.nz) return;
+  dwind_update_tile(A, blockIdx.x, blockIdx.y, bz);
+}
+
 __global__ void __launch_bounds__(DT_X * DT_Y, 4) dwind_update_batch_kernel(const __grid_constant__ DwindBatch B) {
-  const int t = blockIdx.z / B.nkz;
-  const DwindArgs& A = B.t[t];
-  if ((int)blockIdx.x * DT_X > A.nx || (int)blockIdx.y * DT_Y > A.ny || (int)(blockIdx.z % B.nkz) * DT_K >= A.nz)
-    return;
-  dwind_update_tile(A, blockIdx.x, blockIdx.y, blockIdx.z % B.nkz);
+  switch (blockIdx.z / B.nkz) {
+    case 0: dwind_update_batch_tile<0>(B); break;
+    case 1: dwind_update_batch_tile<1>(B); break;
+    case 2: dwind_update_batch_tile<2>(B); break;
+    case 3: dwind_update_batch_tile<3>(B); break;
+    case 4: dwind_update_batch_tile<4>(B); break;
+    case 5: dwind_update_batch_tile<5>(B); break;
+    default: break;
+  }
 }
 
 // set_winds_zero on the prep domain: i, j in [-1, n + 1), DW_KB levels per thread
@@ -240,7 +254,17 @@ __device__ __forceinline__ void dwind_zero_tile(const DwindArgs& A) {
 __global__ void dwind_zero_kernel(const __grid_constant__ DwindArgs A) { dwind_zero_tile(A); }
 
 // every tile of a batch: blockIdx.z is the tile
-__global__ void dwind_zero_batch_kernel(const __grid_constant__ DwindBatch B) { dwind_zero_tile(B.t[blockIdx.z]); }
+__global__ void dwind_zero_batch_kernel(const __grid_constant__ DwindBatch B) {
+  switch (blockIdx.z) {
+    case 0: dwind_zero_tile(B.t[0]); break;
+    case 1: dwind_zero_tile(B.t[1]); break;
+    case 2: dwind_zero_tile(B.t[2]); break;
+    case 3: dwind_zero_tile(B.t[3]); break;
+    case 4: dwind_zero_tile(B.t[4]); break;
+    case 5: dwind_zero_tile(B.t[5]); break;
+    default: break;
+  }
+}
 
 // doubly_periodic_wind_update (update_dwind_phys.py:153-161) on the compute domain
 __global__ void dwind_periodic_kernel(const __grid_constant__ DwindArgs A) {

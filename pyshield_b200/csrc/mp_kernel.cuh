@@ -1591,7 +1591,13 @@ cudaError_t launch_step(const MpArgs& A, cudaStream_t st) {
 #ifndef SHIELD_PACK_MINB
 #define SHIELD_PACK_MINB 1
 #endif
-using Packed80 = PackedLayout<5, 2, SHIELD_PACK_NGRP>;
+#ifndef SHIELD_PACK_NWG
+#define SHIELD_PACK_NWG 5
+#endif
+#ifndef SHIELD_PACK_P
+#define SHIELD_PACK_P 2
+#endif
+using Packed80 = PackedLayout<SHIELD_PACK_NWG, SHIELD_PACK_P, SHIELD_PACK_NGRP>;
 constexpr int PACK80_MINB = SHIELD_PACK_MINB;
 constexpr int PACK80_LMIN = 65, PACK80_LMAX = 80;
 

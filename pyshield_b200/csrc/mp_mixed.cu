@@ -28,7 +28,7 @@ cudaError_t launch_nw(const MpArgs& A, cudaStream_t st) {
 #ifndef SHIELD_PACK_PERSIST
 #define SHIELD_PACK_PERSIST 0
 #endif
-using Packed80Mixed = PackedLayout<5, 2, SHIELD_PACK_NGRP_MIXED>;
+using Packed80Mixed = PackedLayout<SHIELD_PACK_NWG, SHIELD_PACK_P, SHIELD_PACK_NGRP_MIXED>;
 constexpr bool kPersist80 = SHIELD_PACK_PERSIST && SmemP<Packed80Mixed, N_IN>::bytes <= 220 * 1024;
 // 97..128 levels, mixed form: columns per block. C96 L127 (ms): 4 columns
 // 4.17, 5 columns 3.70, 6 columns (768 threads, 80 registers) 3.57.

@@ -141,6 +141,19 @@ __global__ void __launch_bounds__(TC * NWB, 2) physics_prestep_kernel(const __gr
   // ---- A: statein's prelude (PARALLEL interval(...)): tracers * delp, dpn
   for (int k = w; k < nk; k += NWB) {
     if (compute) {
+      if constexpr (FUSED) {
+        // the copied fields statein leaves alone, moved here where the
+        // level loop has few loads of its own
+        if (k < nk - 1) {
+          const double cz = A.dsrc[D_DELZ].at(i, j, k), ca = A.dsrc[D_QCLD].at(i, j, k);
+          const double cu = A.dsrc[D_UA].at(i, j, k), cv = A.dsrc[D_VA].at(i, j, k), cw = A.dsrc[D_W].at(i, j, k);
+          A.ddst[D_DELZ].at(i, j, k) = cz;
+          A.ddst[D_QCLD].at(i, j, k) = ca;
+          A.ddst[D_UA].at(i, j, k) = cu;
+          A.ddst[D_VA].at(i, j, k) = cv;
+          A.ddst[D_W].at(i, j, k) = cw;
+        }
+      }
       if (k < nk - 1) S.ph[k][lane] = rd(DELZ, D_DELZ, k) * A.GRAV;
       const double dp0 = rd(DELP, D_DELP, k);
       double q[N_TRACER];
@@ -199,15 +212,6 @@ __global__ void __launch_bounds__(TC * NWB, 2) physics_prestep_kernel(const __gr
       const double tke = rd(TKE, D_TKE, k);
       const double pt = rd(PT, D_PT, k);
       const double om = (A.prepare || FUSED) ? rd(OMGA, D_OMGA, k) : 0.0;
-      // the copied fields statein leaves alone
-      double cp[5];
-      if constexpr (FUSED) {
-        cp[0] = A.dsrc[D_QCLD].at(i, j, k);
-        cp[1] = A.dsrc[D_DELZ].at(i, j, k);
-        cp[2] = A.dsrc[D_UA].at(i, j, k);
-        cp[3] = A.dsrc[D_VA].at(i, j, k);
-        cp[4] = A.dsrc[D_W].at(i, j, k);
-      }
       // statein
       const double pn = S.p[k + 1][lane];
       const double ph_k = S.ph[k][lane], ph1 = S.ph[k + 1][lane];
@@ -236,11 +240,6 @@ __global__ void __launch_bounds__(TC * NWB, 2) physics_prestep_kernel(const __gr
       f[DELP].at(i, j, k) = d;
       f[DELPRSI].at(i, j, k) = pn - p;
       if constexpr (FUSED) {
-        A.ddst[D_QCLD].at(i, j, k) = cp[0];
-        A.ddst[D_DELZ].at(i, j, k) = cp[1];
-        A.ddst[D_UA].at(i, j, k) = cp[2];
-        A.ddst[D_VA].at(i, j, k) = cp[3];
-        A.ddst[D_W].at(i, j, k) = cp[4];
         A.ddst[D_PT].at(i, j, k) = pt;
         A.ddst[D_OMGA].at(i, j, k) = om;
       }

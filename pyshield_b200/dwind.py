@@ -108,6 +108,11 @@ class AGrid2DGridPhysics:
                     P.r[s][q].line, P.r[s][q].lo, P.r[s][q].hi, P.r[s][q].dir = line - h, lo - h, hi - h, d
             self._plan = P
             G = ShieldDwindGeometry()
+            # the geometry table holds raw device pointers: keep the arrays
+            # alive as long as this object (a caller may drop grid_info)
+            self._geom_arrays = [getattr(grid_info, name) for name in (
+                "vlon1", "vlon2", "vlon3", "vlat1", "vlat2", "vlat3", "es1_1", "es1_2", "es1_3", "ew2_1", "ew2_2",
+                "ew2_3", "edge_vect_w", "edge_vect_e", "edge_vect_s", "edge_vect_n")]
             for name in ("vlon1", "vlon2", "vlon3", "vlat1", "vlat2", "vlat3", "es1_1", "es1_2", "es1_3", "ew2_1",
                          "ew2_2", "ew2_3", "edge_vect_w", "edge_vect_e"):
                 ptr, st = _origin_ptr(getattr(grid_info, name), h, 2)

@@ -104,6 +104,17 @@ struct Column {
   // column here (control flow around vertical operations must be uniform
   // over the barrier's threads)
   SHD bool group_any(bool p) { return any(p); }
+  // any() with the group's any() from the same exchange (one column here)
+  SHD bool any_group(bool p, bool& g) {
+    g = any(p);
+    return g;
+  }
+  SHD void any3_group(bool a, bool b, bool c, bool& ra, bool& rb, bool& rc, bool& ga, bool& gb, bool& gc) {
+    any3(a, b, c, ra, rb, rc);
+    ga = ra;
+    gb = rb;
+    gc = rc;
+  }
   SHD int min_int(int v) {
     v = __reduce_min_sync(FULLMASK, v);
     if (NW == 1) return v;
@@ -564,8 +575,26 @@ struct PackedColumn {
     rb = m[1] != 0;
     rc = m[2] != 0;
   }
+  // the column's any() and, from the same exchange, the group's (every
+  // warp's parts ORed)
+  SHD bool any_group(bool p, bool& g) {
+    unsigned m[1] = {p ? 1u : 0u}, gm = 0;
+    anyN<1>(m, &gm);
+    g = gm != 0;
+    return m[0] != 0;
+  }
+  SHD void any3_group(bool a, bool b, bool c3, bool& ra, bool& rb, bool& rc, bool& ga, bool& gb, bool& gc) {
+    unsigned m[3] = {a ? 1u : 0u, b ? 1u : 0u, c3 ? 1u : 0u}, gm = 0;
+    anyN<3>(m, &gm);
+    ra = m[0] != 0;
+    rb = m[1] != 0;
+    rc = m[2] != 0;
+    ga = (gm & 1u) != 0;
+    gb = (gm & 2u) != 0;
+    gc = (gm & 4u) != 0;
+  }
   template <int N>
-  SHD void anyN(unsigned (&m)[N]) {
+  SHD void anyN(unsigned (&m)[N], unsigned* group = nullptr) {
     const unsigned sm_ = segmask();
     unsigned bits = 0;
 #pragma unroll
@@ -576,6 +605,12 @@ struct PackedColumn {
     sync();
     unsigned r = 0;
     for (int u = wfirst(); u <= wlast(); ++u) r |= s[part(u)];
+    if (group) {
+      unsigned gr = 0;
+#pragma unroll
+      for (int u = 0; u < NWG; ++u) gr |= s[2 * u] | s[2 * u + 1];
+      *group = gr;
+    }
 #pragma unroll
     for (int n = 0; n < N; ++n) m[n] = (r >> n) & 1u;
   }
@@ -1048,14 +1083,15 @@ SHD void warm_rain(Col& C, const MpConst& K, const MpConstF& KF, bool valid, Lev
   double &qv = S.qv, &ql = S.ql, &qr = S.qr, &qi = S.qi, &qs = S.qs, &qg = S.qg, &tz = S.tz, &w = S.w;
   const double dt5 = 0.5 * K.dt_rain;
   m1_rain = 0.0;
-  const bool fall = C.any(valid && (qr > QRMIN));
+  bool gfall;
+  const bool fall = C.any_group(valid && (qr > QRMIN), gfall);
   if (falls) *falls = fall;
   r1 = 0.0;
   if (!fall) vtr = VF_MIN;
   // The fall's vertical operations run whenever a column sharing the
   // barrier has falling rain; a column without it takes part with no mass
   // (valid false), which leaves its state unchanged and its flux zero.
-  if (C.group_any(fall)) {
+  if (gfall) {
     const bool vf = valid && fall;
     if (fall) {
       if constexpr (MIXED) {
@@ -1124,16 +1160,17 @@ SHD void sedimentation(Col& C, const MpConst& K, const MpConstF& KF, bool valid,
   // implicit falls are independent of one another, so the three share
   // each column exchange; the vertical-velocity updates, which the
   // reference applies species after species, stay in that order.
-  bool fi, fs, fg;
-  C.any3(valid && (qi > QRMIN), valid && (qs > QRMIN), valid && (qg > QRMIN), fi, fs, fg);
+  bool fi, fs, fg, gi, gs, gg;
+  C.any3_group(valid && (qi > QRMIN), valid && (qs > QRMIN), valid && (qg > QRMIN), fi, fs, fg, gi, gs, gg);
   fi = fi && (K.vi_fac >= 1.0e-5);
+  gi = gi && (K.vi_fac >= 1.0e-5);
   if (flags)
     *flags |= (fi ? FLAG_ICE_FALLS : 0u) | (fs ? FLAG_SNOW_FALLS : 0u) | (fg ? FLAG_GRAUPEL_FALLS : 0u) |
               ((unsigned)min(first, L - 1) << FLAG_MELT_SHIFT);
   double mp = 0.0;  // m1_sol at the level above, for the heating
   // taken by every column sharing the barrier when one of them has a
   // falling species; each species' results apply only where it falls
-  if (C.group_any(fi || fs || fg)) {
+  if (gi || gs || gg) {
     const double dd[3] = {K.dts * vti, K.dts * vts, K.dts * vtg};
     double ddp[3];
     C.template prevN<3>(dd, ddp);

@@ -145,52 +145,96 @@ def cpu_baseline(domain, steps, warmup=1):
 
 # ------------------------------------------------------------ clocks
 class ClockSampler:
+    """nvidia-smi clock samples every 20 ms from a reader thread, each with its
+    host time, so that the samples of a short timed region can be picked out:
+    ``start()`` waits for the first sample (nvidia-smi takes a moment to come
+    up), ``mark()`` brackets the timed region, ``stop()`` summarises the samples
+    inside it (the nearest ones if the region was shorter than the interval)."""
+
     FIELDS = (
         "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
         "clocks_event_reasons.sw_power_cap"
     )
+    INTERVAL_MS = 20
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.lines = []
+        self.window = [None, None]
+        self.thread = None
 
-    def start(self):
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.monotonic(), line))
+
+    def start(self, wait_s=5.0):
+        import threading
+
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"],
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", str(self.INTERVAL_MS)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True,
             )
         except OSError:
             self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+        t_end = time.monotonic() + wait_s
+        while not self.lines and time.monotonic() < t_end and self.proc.poll() is None:
+            time.sleep(0.01)
+
+    def mark(self, which):
+        self.window[0 if which == "begin" else 1] = time.monotonic()
+
+    @staticmethod
+    def _parse(line):
+        parts = [p.strip() for p in line.split(",")]
+        if len(parts) < 7:
+            return None
+        try:
+            return float(parts[0]), float(parts[1]), parts[3:7]
+        except ValueError:
+            return None
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
         try:
-            out, _ = self.proc.communicate(timeout=5)
+            self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-            out, _ = self.proc.communicate()
-        sm, smax, reasons = [], [], set()
+            self.proc.wait()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+        rows = [(t, r) for t, r in ((t, self._parse(x)) for t, x in self.lines) if r is not None]
+        t0, t1 = self.window
+        inside = rows
+        if t0 is not None and t1 is not None:
+            # a sample printed within one interval after the region still
+            # describes it
+            inside = [x for x in rows if t0 <= x[0] <= t1 + self.INTERVAL_MS / 1000.0]
+            if not inside and rows:
+                mid = 0.5 * (t0 + t1)
+                inside = sorted(rows, key=lambda x: abs(x[0] - mid))[:2]
+        sm = [r[0] for _, r in inside]
+        smax = [r[1] for _, r in inside]
+        reasons = set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for line in out.strip().splitlines():
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 7:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                smax.append(float(parts[1]))
-            except ValueError:
-                continue
-            for name, v in zip(names, parts[3:7]):
+        for _, r in inside:
+            for name, v in zip(names, r[2]):
                 if v.lower() == "active":
                     reasons.add(name)
         return {
             "sm_mhz": statistics.median(sm) if sm else None,
             "sm_max_mhz": max(smax) if smax else None,
             "samples": len(sm),
+            "samples_total": len(rows),
+            "interval_ms": self.INTERVAL_MS,
             "reasons": sorted(reasons),
         }
 
@@ -993,6 +1037,7 @@ def run_ours(args, rank, world, local_rank):
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
+    clocks.mark("begin")
     t_start.record(stream)
     for s in range(args.steps):
         ev[s][0].record(stream)
@@ -1000,6 +1045,7 @@ def run_ours(args, rank, world, local_rank):
         ev[s][1].record(stream)
     t_end.record(stream)
     torch.cuda.synchronize()
+    clocks.mark("end")
     barrier()
     torch.cuda.synchronize()
     clk = clocks.stop()

@@ -134,8 +134,10 @@ int shield_mp_last_error(void* handle, char* buf, size_t n);
 /* ---------------------------------------------------------------------------
  * Adjoint of the step. pySHiELD has no adjoint; this is the vector-Jacobian
  * product (VJP) of one Microphysics.__call__ (microphysics.py:1981-2263),
- * evaluated in FP64 by a hand-written reverse kernel that replays the step
- * from its inputs.
+ * evaluated in FP64 by hand-written reverse kernels after a replay of the
+ * step from its inputs. The replay's records live in a workspace the handle
+ * allocates on the first call (about 100 doubles per grid point and
+ * sub-step) and keeps, grown as needed, until shield_mp_destroy.
  *
  * Outputs of the step, whose cotangents are given: the ten tendencies
  * (as written by the step: udt and vdt for levels k >= 1 only), wmp (which
@@ -148,8 +150,8 @@ int shield_mp_last_error(void* handle, char* buf, size_t n);
  * to the outputs and are not differentiated.
  *
  * Branches follow the forward at the given input. Supported: the plain form
- * and configurations without do_sedi_heat and de_ice, with at most 4
- * sub-steps (SHIELD_ELAYOUT otherwise). */
+ * and configurations without do_sedi_heat and de_ice (SHIELD_ELAYOUT
+ * otherwise), any number of sub-steps. */
 typedef struct {
   ShieldField3D pt_dt, qv_dt, ql_dt, qr_dt, qi_dt, qs_dt, qg_dt, qa_dt, udt, vdt, wmp, qaz; /* NULL ptr: zero */
   const double *rain, *snow, *ice, *graupel; /* ncol each (column c = j*nx + i), or NULL for zero */

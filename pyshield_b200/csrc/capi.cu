@@ -27,6 +27,8 @@ struct Handle {
   double* area = nullptr;  // device copy of grid_data.area (ncol)
   double* qaz = nullptr;   // persistent accumulator, nz * ncol, level-major
   int* err = nullptr;
+  double* vjp_ws = nullptr;  // the adjoint's workspace, allocated by its first call and grown as needed
+  int64_t vjp_ws_doubles = 0;
   MpConst K;
   bool have_ts = false;
   std::string last_error;
@@ -203,9 +205,18 @@ extern "C" int shield_mp_step_vjp(void* handle, const ShieldMpFields* F, const S
     std::string why;
     if (set_timestep(h->cfg, K, timestep, why) != SHIELD_OK) return fail(h, SHIELD_EINVAL, why);
   }
-  if (K.ntimes > mp_vjp_max_substeps())
-    return fail(h, SHIELD_ELAYOUT, "the adjoint supports at most " + std::to_string(mp_vjp_max_substeps()) +
-                                       " sub-steps (timestep / mp_time)");
+  const int64_t need = mp_vjp_workspace_doubles(K.ntimes, (int64_t)h->nz * h->ncol, h->ncol);
+  if (need > h->vjp_ws_doubles) {
+    cudaFree(h->vjp_ws);
+    h->vjp_ws = nullptr;
+    h->vjp_ws_doubles = 0;
+    cudaError_t e = cudaMalloc(&h->vjp_ws, sizeof(double) * (size_t)need);
+    if (e != cudaSuccess) {
+      h->vjp_ws = nullptr;
+      return cuda_fail(h, e, "allocating the adjoint's workspace");
+    }
+    h->vjp_ws_doubles = need;
+  }
   VjpArgs A;
   std::memset(&A, 0, sizeof(A));
   A.K = K;
@@ -234,6 +245,7 @@ extern "C" int shield_mp_step_vjp(void* handle, const ShieldMpFields* F, const S
   A.snow_b = cot->snow;
   A.ice_b = cot->ice;
   A.graupel_b = cot->graupel;
+  A.ws = h->vjp_ws;
   cudaError_t e = mp_launch_vjp(A, static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(h, e, "adjoint launch");
   return SHIELD_OK;
@@ -267,6 +279,7 @@ extern "C" int shield_mp_destroy(void* handle) {
   cudaFree(h->qaz);
   cudaFree(h->area);
   cudaFree(h->err);
+  cudaFree(h->vjp_ws);
   delete h;
   return SHIELD_OK;
 }

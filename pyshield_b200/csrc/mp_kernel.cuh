@@ -1072,13 +1072,25 @@ SHD void substep_geometry(Col& C, const MpConst& K, bool valid, double t0, doubl
   P.dz = C.heights(valid ? -P.dz1 : 0.0, K.zs);
 }
 
+// Recorder of a stage's intermediate states. The forward kernels pass
+// NoRec (every call compiles away); the adjoint's replay passes one that
+// stores the states the reverse sweeps start from.
+struct NoRec {
+  SHD void state(int, const LevState&) const {}
+  SHD void value(int, double) const {}
+  SHD void flag(bool) const {}
+};
+
 // warm_rain (:280-653) after the geometry: rain evaporation and accretion,
 // implicit rain fall with the vertical-velocity transport and heating, then
 // autoconversion. Returns the rain flux m1_rain at this level and the
 // surface flux r1.
-template <bool MIXED, class Col>
+// A recorder gets the states after the first evaporation (slot 0), after the
+// fall (1) and after the second evaporation (2), the liquid slope (value 0)
+// and the column's rain-fall decision.
+template <bool MIXED, class Col, class Rec = NoRec>
 SHD void warm_rain(Col& C, const MpConst& K, const MpConstF& KF, bool valid, LevState& S, const StepGeom& P,
-                   double& vtr, double& m1_rain, double& r1, bool* falls = nullptr) {
+                   double& vtr, double& m1_rain, double& r1, bool* falls = nullptr, const Rec& rec = Rec()) {
   const int k = C.k, L = C.L;
   double &qv = S.qv, &ql = S.ql, &qr = S.qr, &qi = S.qi, &qs = S.qs, &qg = S.qg, &tz = S.tz, &w = S.w;
   const double dt5 = 0.5 * K.dt_rain;
@@ -1086,6 +1098,7 @@ SHD void warm_rain(Col& C, const MpConst& K, const MpConstF& KF, bool valid, Lev
   bool gfall;
   const bool fall = C.any_group(valid && (qr > QRMIN), gfall);
   if (falls) *falls = fall;
+  rec.flag(fall);
   r1 = 0.0;
   if (!fall) vtr = VF_MIN;
   // The fall's vertical operations run whenever a column sharing the
@@ -1102,6 +1115,7 @@ SHD void warm_rain(Col& C, const MpConst& K, const MpConstF& KF, bool valid, Lev
         revap_racc(K, dt5, P.h_var, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac);
       }
     }
+    rec.state(0, S);
     const double dm = P.dp1 * (1.0 + qv + ql + qr + qi + qs + qg);
     m1_rain = implicit_fall(C, qr, vtr, P.dz, P.dp1, vf, K.dt_rain);
     double fv[2] = {m1_rain, vtr}, pv[2];
@@ -1109,12 +1123,18 @@ SHD void warm_rain(Col& C, const MpConst& K, const MpConstF& KF, bool valid, Lev
     r1 = C.bcast(m1_rain, L - 1);
     if (fall && K.do_sedi_w) w = w_update(k, w, dm, m1_rain, vtr, pv[0], pv[1]);
     if (K.do_sedi_heat) sedi_heat(C, K, tz, P.dz1, P.dp1, qv, ql, qr, qi, qs, qg, m1_rain, pv[0], vf, K.C_LIQ);
+    rec.state(1, S);
     if (fall) {
       if constexpr (MIXED)
         revap_racc_m(K, KF, dt5, P.h_var, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac);
       else
         revap_racc(K, dt5, P.h_var, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac);
     }
+    rec.state(2, S);
+  } else {
+    rec.state(0, S);
+    rec.state(1, S);
+    rec.state(2, S);
   }
   if (K.irain_f != 0) {
     if constexpr (MIXED)
@@ -1125,6 +1145,7 @@ SHD void warm_rain(Col& C, const MpConst& K, const MpConstF& KF, bool valid, Lev
     double dl;
     if (K.z_slope_liq) {
       dl = mono_slope(C, ql);
+      rec.value(0, dl);
       dl = fmax(dl, fmax(QVMIN, P.h_var * ql));
     } else {
       dl = fmax(QVMIN, P.h_var * ql);
@@ -1225,17 +1246,20 @@ SHD void sedimentation(Col& C, const MpConst& K, const MpConstF& KF, bool valid,
 }
 
 // icloud (:1220-1449): instant melting or freezing, the ice slope, the ice
-// processes and the saturation adjustment. The adjoint's replay passes rec
-// to keep the state between the ice processes and the adjustment.
-template <bool MIXED, class Col>
+// processes and the saturation adjustment. A recorder gets the state between
+// the ice processes and the adjustment (slot 0), the ice slope (value 0) and
+// the cloud ice after melting and freezing (value 1).
+template <bool MIXED, class Col, class Rec = NoRec>
 SHD void icloud(Col& C, const MpConst& K, const MpConstF& KF, bool valid, LevState& S, const StepGeom& P,
-                double& qa, double vtg, double vtr, double vts, LevState* rec = nullptr) {
+                double& qa, double vtg, double vtr, double vts, const Rec& rec = Rec()) {
   double &qv = S.qv, &ql = S.ql, &qr = S.qr, &qi = S.qi, &qs = S.qs, &qg = S.qg, &tz = S.tz;
   double q_liq, q_sol, cvm;
   icloud_melt_freeze(K, qv, ql, qr, qi, qs, qg, tz, P.den, q_liq, q_sol, cvm);
+  rec.value(1, qi);
   double di;
   if (K.z_slope_ice) {
     di = mono_slope(C, qi);
+    rec.value(0, di);
     di = fmax(di, fmax(QVMIN, P.h_var * qi));
   } else {
     di = fmax(QVMIN, P.h_var * qi);
@@ -1246,7 +1270,7 @@ SHD void icloud(Col& C, const MpConst& K, const MpConstF& KF, bool valid, LevSta
                          cvm);
     else
       icloud_processes(K, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac, vtg, vtr, vts, P.p1, di, q_liq, q_sol, cvm);
-    if (rec) *rec = S;
+    rec.state(0, S);
     if constexpr (MIXED)
       subgrid_z_proc<double, float>(K, P.h_var, P.rh_adj, P.rh_rain, qa, qg, qi, ql, qr, qs, qv, tz, P.den, P.denfac,
                                     P.p1, &KF);

@@ -110,6 +110,8 @@ struct VjpArgs {
   Fld3 grad[N_VJP_GRAD];
   Fld2 land, area;
   const double *rain_b, *snow_b, *ice_b, *graupel_b;
+  // workspace of mp_vjp_workspace_doubles(ntimes, nz * ncol, ncol) doubles
+  double* ws;
 };
 
 }  // namespace shield

@@ -5,19 +5,22 @@
 // the accumulator), for pySHiELD's Microphysics.__call__
 // (pySHiELD/stencils/microphysics.py:1981-2263).
 //
-// One thread per level and one group of NW warps per column, as in the
-// forward kernel. Each group
-//  1. replays the step with the forward's own stage functions, keeping the
-//     level's state at the entry of every stage of every sub-step in a
-//     small per-thread store (local memory);
-//  2. reverses fields_update (including the momentum scan);
-//  3. for each sub-step from the last, recomputes the sub-step geometry and
-//     reverses icloud, the second warm_rain pass, sedimentation and the
-//     first pass, each from its stored entry state (pointwise processes
-//     through the hand-written adjoints of mp_adjoint.cuh, vertical
-//     recurrences through bottom-up scans, level exchanges through their
-//     transposes);
-//  4. reverses fields_init.
+// A sequence of launches over a workspace in global memory:
+//  1. the replay (one thread per level, NW warps per column, as the forward
+//     kernel) runs the step with the forward's own stage functions and
+//     stores, per sub-step and level, the state at the entry of every
+//     stage and inside warm_rain and icloud, the sub-step geometry, the fall
+//     speeds and slopes, and each column's rain-fall decisions; it then
+//     reverses fields_update (including the momentum scan);
+//  2. per sub-step, from the last: the pointwise reverses run one thread per
+//     (level, column) point with consecutive columns on consecutive lanes,
+//     so that a warp's 32 points take the same physics branches far more
+//     often than the levels of one column do, and every warp of the launch
+//     runs the same short code. The reverses of the vertical recurrences
+//     (the rain fall, sedimentation) run on the column layout between them.
+//     The transposes of the slopes' three-point stencils are gathered at the
+//     start of the next point launch;
+//  3. the reverse of fields_init, on the column layout, writes the gradients.
 // Branches follow the forward at the given input (the VJP of the piecewise
 // smooth map on the branch it takes).
 #include <cuda_runtime.h>
@@ -27,31 +30,110 @@
 #include "mp_launch.h"
 
 namespace shield {
+
+// ------------------------------------------------------------- workspace
+// Every array holds one double per point p = k * ncol + col (level-major,
+// consecutive columns adjacent) or per column.
+//
+// per sub-step and point: the states (8 doubles each) at
+enum VjpCkSlot {
+  CK_E0,   // the first warm_rain pass's entry
+  CK_W1A,  // its state after the first evaporation,
+  CK_W2A,  // after the fall,
+  CK_W3A,  // after the second evaporation
+  CK_E1,   // sedimentation's entry
+  CK_E2,   // the second warm_rain pass's entry
+  CK_W1B, CK_W2B, CK_W3B,
+  CK_E3,   // icloud's entry
+  CK_E4,   // the state between the ice processes and the adjustment
+  N_CK
+};
+// per sub-step and point: scalars
+enum VjpSubScalar {
+  SS_DEN, SS_DENFAC, SS_DZ, SS_DZ1,  // the sub-step geometry
+  SS_VTR_A, SS_VTR_B,                // rain fall speed of each pass
+  SS_VTG, SS_VTS,                    // graupel and snow fall speeds of sedimentation
+  SS_SL_A, SS_SL_B,                  // liquid slope of each pass's autoconversion
+  SS_SL_I, SS_S1QI,                  // icloud's ice slope and cloud ice after melting / freezing
+  N_SS
+};
+// per sub-step and column: the rain-fall decisions of the two passes (0 / 1)
+enum VjpSubColumn { SCC_FALL_A, SCC_FALL_B, N_SCC };
+// per point, once: fields_init's dry mass and pressure
+enum VjpStepPoint { SP_DP1, SP_P1, N_SP };
+// per column, once: fields_init's column values
+enum VjpStepColumn { SC_HVAR, SC_RHADJ, SC_RHRAIN, SC_CCN, SC_CPRAUT, N_SC };
+// per point: the adjoint state carried between the launches
+enum VjpAdjField {
+  AS_QV, AS_QL, AS_QR, AS_QI, AS_QS, AS_QG, AS_TZ, AS_W,  // the state's cotangent
+  AS_DEN, AS_DENFAC, AS_DZ,                               // of the sub-step geometry
+  AS_DP1, AS_P1, AS_CCN, AS_CPRAUT,                       // of fields_init's values
+  AS_PT, AS_DELP, AS_DZ0, AS_QIN0,                        // of the inputs (six species from AS_QIN0)
+  AS_QA = AS_QIN0 + 6,                                    // of the accumulator (passes through)
+  AS_QA0, AS_U0, AS_V0,                                   // final: qcld, ua, va
+  AS_M1,                                                  // of the precipitation flux at the level
+  AS_VTR, AS_VTG, AS_VTS,                                 // of icloud's fall speeds
+  AS_VTT,                                                 // of a pass's rain fall speed (fall to evaporation)
+  AS_QLIQ, AS_QSOL, AS_CVM,                               // of icloud's melting / freezing outputs
+  AS_SLI, AS_SLL,                                         // of the ice and liquid slopes
+  N_AS
+};
+
+int64_t mp_vjp_workspace_doubles(int nt, int64_t npts, int64_t ncol) {
+  return npts * ((int64_t)nt * (8 * N_CK + N_SS) + N_SP + N_AS) + ncol * ((int64_t)nt * N_SCC + N_SC);
+}
+
 namespace {
 
-constexpr int VJP_MAXNT = 4;  // sub-steps whose stage states fit the store
-
-// launch shape: columns per block for 65-96 levels, and the minimum
-// resident blocks per SM given to __launch_bounds__
-#ifndef SHIELD_VJP_G3
-#define SHIELD_VJP_G3 4
-#endif
-#ifndef SHIELD_VJP_MINB
-#define SHIELD_VJP_MINB 1
-#endif
-constexpr int NT_IN = N_VJP_IN + N_VJP_COT;
-
-// Shared memory: NT_IN input tiles (inputs, then cotangents), N_VJP_GRAD
-// gradient tiles, G x 2 x SCR exchange scratch, G x 4 x RP work rows.
-template <int NW, int G>
-struct VjpSmem {
-  static constexpr int RP = Tiles<NW>::RP;
-  static constexpr size_t out = (size_t)NT_IN * G * RP;
-  static constexpr size_t scratch = out + (size_t)N_VJP_GRAD * G * RP;
-  static constexpr size_t work = scratch + (size_t)G * 2 * Tiles<NW>::SCR;
-  static constexpr size_t total = work + (size_t)G * 4 * RP;
-  static constexpr size_t bytes = total * sizeof(double);
+struct Ws {
+  double* base;
+  int64_t npts, ncol;
+  int nt;
+  SHD double* ck(int it, int slot) const { return base + ((int64_t)it * N_CK + slot) * 8 * npts; }
+  SHD double* ss(int it, int s) const { return base + ((int64_t)nt * 8 * N_CK + (int64_t)it * N_SS + s) * npts; }
+  SHD double* sp(int s) const { return base + ((int64_t)nt * (8 * N_CK + N_SS) + s) * npts; }
+  SHD double* as(int f) const { return base + ((int64_t)nt * (8 * N_CK + N_SS) + N_SP + f) * npts; }
+  SHD double* cbase() const { return base + ((int64_t)nt * (8 * N_CK + N_SS) + N_SP + N_AS) * npts; }
+  SHD double* scc(int it, int s) const { return cbase() + ((int64_t)it * N_SCC + s) * ncol; }
+  SHD double* sc(int s) const { return cbase() + ((int64_t)nt * N_SCC + s) * ncol; }
 };
+
+SHD Ws workspace(const VjpArgs& A) { return Ws{A.ws, (int64_t)A.nz * A.ncol, A.ncol, A.K.ntimes}; }
+
+// a state's 8 fields, npts apart from p
+SHD LevState load_lev(const double* q, int64_t npts) {
+  return LevState{q[0], q[npts], q[2 * npts], q[3 * npts], q[4 * npts], q[5 * npts], q[6 * npts], q[7 * npts]};
+}
+SHD void store_lev(double* q, int64_t npts, const LevState& S) {
+  q[0] = S.qv;
+  q[npts] = S.ql;
+  q[2 * npts] = S.qr;
+  q[3 * npts] = S.qi;
+  q[4 * npts] = S.qs;
+  q[5 * npts] = S.qg;
+  q[6 * npts] = S.tz;
+  q[7 * npts] = S.w;
+}
+
+// The replay's recorder (NoRec's interface, mp_kernel.cuh): states to
+// consecutive checkpoint slots from `st`, values to consecutive sub-step
+// scalars from `val`, the column decision to `flg` (written by level 0).
+struct VjpRec {
+  double *st, *val, *flg;
+  int64_t npts;
+  bool valid, head;
+  SHD void state(int s, const LevState& S) const {
+    if (valid) store_lev(st + (int64_t)s * 8 * npts, npts, S);
+  }
+  SHD void value(int s, double v) const {
+    if (valid) val[(int64_t)s * npts] = v;
+  }
+  SHD void flag(bool f) const {
+    if (head && flg) *flg = f ? 1.0 : 0.0;
+  }
+};
+
+constexpr int NT_IN = N_VJP_IN + N_VJP_COT;
 
 // load NF fields into tiles [f * G + g][k] (all loads issued before any
 // store); a field with a null pointer reads as zero
@@ -137,52 +219,64 @@ SHD void w_update_b(int k, double w, double dm, double flux, double vt, double f
   }
 }
 
-// mono_slope: v_b is the adjoint of the slope at this level; adds the
-// adjoints of q at k - 1, k and k + 1 into the owning levels' q_b
-template <int NW>
-SHD void mono_slope_b(Column<NW>& C, double q, double v_b, double& q_b, bool valid) {
-  double qp, qn;
-  C.nbrs(q, qp, qn);
-  const int k = C.k;
-  double cq = 0.0, cp = 0.0, cn = 0.0;
-  if (valid && k >= 1 && k <= C.L - 2) {
-    const double dq = 0.5 * (q - qp);
-    const double dqn = 0.5 * (qn - q);
-    const double s = dq + dqn;
-    const double A1 = fabs(s), A2 = 0.5 * q;
-    const double v0 = 0.5 * fmin(A1, A2);
-    double v0_b = 0.0, dq_b = 0.0, dqn_b = 0.0;
-    if (dq * dqn <= 0.0) {
-      if (dq > 0.0) {
-        const double m2 = fmin(dq, -dqn);
-        if (min_first(v0, m2))
-          v0_b = v_b;
-        else if (min_first(dq, -dqn))
-          dq_b += v_b;
-        else
-          dqn_b -= v_b;
-      }
-    } else {
-      v0_b = v_b;
+// mono_slope's derivative at a level with neighbours qp (above) and qn
+// (below), times the slope's cotangent v_b: the contributions to q there
+// (cq), above (cp) and below (cn). Zero outside 1 <= k <= L - 2.
+SHD void mono_slope_coeffs(double qp, double q, double qn, int k, int L, double v_b, double& cp, double& cq,
+                           double& cn) {
+  cp = cq = cn = 0.0;
+  if (k < 1 || k > L - 2) return;
+  const double dq = 0.5 * (q - qp);
+  const double dqn = 0.5 * (qn - q);
+  const double s = dq + dqn;
+  const double A1 = fabs(s), A2 = 0.5 * q;
+  const double v0 = 0.5 * fmin(A1, A2);
+  double v0_b = 0.0, dq_b = 0.0, dqn_b = 0.0;
+  if (dq * dqn <= 0.0) {
+    if (dq > 0.0) {
+      const double m2 = fmin(dq, -dqn);
+      if (min_first(v0, m2))
+        v0_b = v_b;
+      else if (min_first(dq, -dqn))
+        dq_b += v_b;
+      else
+        dqn_b -= v_b;
     }
-    if (min_first(A1, A2)) {
-      const double s_b = 0.5 * v0_b * (s >= 0.0 ? 1.0 : -1.0);
-      dq_b += s_b;
-      dqn_b += s_b;
-    } else {
-      cq += 0.25 * v0_b;
-    }
-    cq += 0.5 * dq_b - 0.5 * dqn_b;
-    cp = -0.5 * dq_b;
-    cn = 0.5 * dqn_b;
+  } else {
+    v0_b = v_b;
   }
-  double from_prev, from_next;
-  C.prev_next(cn, cp, from_prev, from_next);
-  if (valid) {
-    q_b += cq;
-    if (k >= 1) q_b += from_prev;
-    if (k <= C.L - 2) q_b += from_next;
+  if (min_first(A1, A2)) {
+    const double s_b = 0.5 * v0_b * (s >= 0.0 ? 1.0 : -1.0);
+    dq_b += s_b;
+    dqn_b += s_b;
+  } else {
+    cq += 0.25 * v0_b;
   }
+  cq += 0.5 * dq_b - 0.5 * dqn_b;
+  cp = -0.5 * dq_b;
+  cn = 0.5 * dqn_b;
+}
+
+// The transpose of the slope stencil gathered at level k of point p: q holds
+// the slope's input field and vb the slopes' cotangents (level-major, ncol
+// apart); the sum over the levels k - 1, k, k + 1 of their contribution to
+// q at k.
+SHD double slope_gather(const double* q, const double* vb, int64_t p, int64_t ncol, int k, int L) {
+  double qq[5];
+#pragma unroll
+  for (int d = -2; d <= 2; ++d) qq[d + 2] = (k + d >= 0 && k + d < L) ? q[p + d * ncol] : 0.0;
+  double cp, cq, cn, r = 0.0;
+  mono_slope_coeffs(qq[1], qq[2], qq[3], k, L, vb[p], cp, cq, cn);
+  r += cq;
+  if (k >= 1) {
+    mono_slope_coeffs(qq[0], qq[1], qq[2], k - 1, L, vb[p - ncol], cp, cq, cn);
+    r += cn;
+  }
+  if (k <= L - 2) {
+    mono_slope_coeffs(qq[2], qq[3], qq[4], k + 1, L, vb[p + ncol], cp, cq, cn);
+    r += cp;
+  }
+  return r;
 }
 
 // implicit_fall replayed with its intermediates kept
@@ -248,89 +342,6 @@ SHD void implicit_fall_b(Column<NW>& C, const FallRec& R, double q, double dz, d
 struct StepAdj {
   double den, denfac, dz, dp1, p1, ccn, c_praut;
 };
-
-// warm_rain reverse from its entry state S0. m1r_b: adjoint of the rain flux
-// at this level; rain_c: cotangent of the surface rain total; vtr_b: adjoint
-// of the pass's output fall speed.
-template <int NW>
-static __device__ __noinline__ void warm_rain_b(Column<NW>& C, const MpConst& K, bool valid, const LevState& S0, const StepGeom& P, double m1r_b,
-                     double rain_c, double vtr_b, LevState& Sb, StepAdj& Ab) {
-  const int k = C.k, L = C.L;
-  const double dt5 = 0.5 * K.dt_rain;
-  const bool fall = C.any(valid && (S0.qr > QRMIN));
-  LevState S1 = S0, S2 = S0, S3 = S0;
-  double vtr = VF_MIN, dm = 0.0, pv[2] = {0.0, 0.0};
-  FallRec R{};
-  if (fall) {
-    vtr = rain_fspeed(K, S0.qr, P.den);
-    revap_racc(K, dt5, P.h_var, S1.qg, S1.qi, S1.ql, S1.qr, S1.qs, S1.qv, S1.tz, P.den, P.denfac);
-    dm = P.dp1 * (1.0 + S1.qv + S1.ql + S1.qr + S1.qi + S1.qs + S1.qg);
-    R = implicit_fall_rec<NW>(C, S1.qr, vtr, P.dz, P.dp1, valid, K.dt_rain);
-    S2 = S1;
-    S2.qr = R.q1;
-    double fv[2] = {R.flux, vtr};
-    C.template prevN<2>(fv, pv);
-    if (K.do_sedi_w) S2.w = w_update(k, S1.w, dm, R.flux, vtr, pv[0], pv[1]);
-    S3 = S2;
-    revap_racc(K, dt5, P.h_var, S3.qg, S3.qi, S3.ql, S3.qr, S3.qs, S3.qv, S3.tz, P.den, P.denfac);
-  }
-  // autoconversion
-  if (K.irain_f != 0) {
-    if (valid)
-      autoconv_no_subgrid_var_b(K, S3.ql, S3.qr, S3.tz, P.den, P.ccn, P.c_praut, Sb.ql, Sb.qr, Ab.den, Ab.ccn,
-                                Ab.c_praut);
-  } else {
-    const double hq = P.h_var * S3.ql;
-    const double inner = fmax(QVMIN, hq);
-    double sl = 0.0, dl = inner;
-    if (K.z_slope_liq) {
-      sl = mono_slope(C, S3.ql);
-      dl = fmax(sl, inner);
-    }
-    double dl_b = 0.0;
-    if (valid)
-      autoconv_subgrid_var_b(K, S3.ql, S3.qr, S3.tz, P.den, P.ccn, P.c_praut, dl, Sb.ql, Sb.qr, Ab.den, Ab.ccn,
-                             Ab.c_praut, dl_b);
-    double sl_b = 0.0;
-    if (K.z_slope_liq && max_first(sl, inner))
-      sl_b = dl_b;
-    else if (!max_first(QVMIN, hq))
-      Sb.ql += dl_b * P.h_var;
-    if (K.z_slope_liq) mono_slope_b<NW>(C, S3.ql, sl_b, Sb.ql, valid);
-  }
-  if (!fall) return;  // vtr = VF_MIN: no adjoint
-  // second evaporation / accretion
-  if (valid)
-    revap_racc_b(K, dt5, P.h_var, S2.qg, S2.qi, S2.ql, S2.qr, S2.qs, S2.qv, S2.tz, P.den, P.denfac, Sb.qg, Sb.qi,
-                 Sb.ql, Sb.qr, Sb.qs, Sb.qv, Sb.tz, Ab.den, Ab.denfac);
-  double flux_b = m1r_b, vt_b = vtr_b, dm_b = 0.0, pv_b[2] = {0.0, 0.0};
-  if (K.do_sedi_w && valid)
-    w_update_b(k, S1.w, dm, R.flux, vtr, pv[0], pv[1], Sb.w, dm_b, flux_b, vt_b, pv_b[0], pv_b[1]);
-  if (k == L - 1) flux_b += rain_c;  // rain += the surface flux
-  double pn[2];
-  C.template nextN<2>(pv_b, pn);
-  if (valid && k < L - 1) {
-    flux_b += pn[0];
-    vt_b += pn[1];
-  }
-  double qr_b = Sb.qr;
-  implicit_fall_b<NW>(C, R, S1.qr, P.dz, P.dp1, valid, K.dt_rain, qr_b, flux_b, vt_b, Ab.dz, Ab.dp1);
-  Sb.qr = qr_b;
-  if (valid) {
-    // dm = dp1 (1 + qv + ql + qr + qi + qs + qg)
-    Ab.dp1 += dm_b * (1.0 + S1.qv + S1.ql + S1.qr + S1.qi + S1.qs + S1.qg);
-    const double t = dm_b * P.dp1;
-    Sb.qv += t;
-    Sb.ql += t;
-    Sb.qr += t;
-    Sb.qi += t;
-    Sb.qs += t;
-    Sb.qg += t;
-    revap_racc_b(K, dt5, P.h_var, S0.qg, S0.qi, S0.ql, S0.qr, S0.qs, S0.qv, S0.tz, P.den, P.denfac, Sb.qg, Sb.qi,
-                 Sb.ql, Sb.qr, Sb.qs, Sb.qv, Sb.tz, Ab.den, Ab.denfac);
-    rain_fspeed_b(K, S0.qr, P.den, vt_b, Sb.qr, Ab.den);
-  }
-}
 
 // sedimentation reverse from its entry state S0. m1s_b: adjoint of the
 // solid flux at this level; ice_c, snow_c, graupel_c: cotangents of the
@@ -509,69 +520,81 @@ static __device__ __noinline__ void sedimentation_b(Column<NW>& C, const MpConst
   if (valid)
     fall_speed_b(K, S0.qg, S0.qi, S0.qs, S0.tz, P.den, vt_b[2], vt_b[0], vt_b[1], Sb.qg, Sb.qi, Sb.qs, Sb.tz, Ab.den);
 }
-
-// icloud reverse from its entry state S0 and the state S2 between the ice
-// processes and the saturation adjustment; qa_b: adjoint of the level's
-// cloud-fraction accumulator
+// The rain fall of a warm_rain pass reversed (microphysics.py:459-515), from
+// W1, the state after the first evaporation: the vertical-velocity update,
+// the implicit fall and the fall's dm. m1r_b: cotangent of the rain flux at
+// this level; rain_c: of the surface rain total; vt_b: of the pass's fall
+// speed on entry, with the fall's own part added on return.
 template <int NW>
-static __device__ __noinline__ void icloud_b(Column<NW>& C, const MpConst& K, bool valid, const LevState& S0,
-                                             const LevState& S2, const StepGeom& P, double vtg, double vtr,
-                                             double vts, double qa_b, LevState& Sb, StepAdj& Ab, double& vtg_b,
-                                             double& vtr_b, double& vts_b) {
-  LevState S1 = S0;
-  double q_liq, q_sol, cvm;
-  icloud_melt_freeze(K, S1.qv, S1.ql, S1.qr, S1.qi, S1.qs, S1.qg, S1.tz, P.den, q_liq, q_sol, cvm);
-  const double hq = P.h_var * S1.qi;
-  const double inner = fmax(QVMIN, hq);
-  double sl = 0.0, di = inner;
-  if (K.z_slope_ice) {
-    sl = mono_slope(C, S1.qi);
-    di = fmax(sl, inner);
+SHD void rain_fall_b(Column<NW>& C, const MpConst& K, bool valid, const LevState& W1, const StepGeom& P,
+                     double vtr, double m1r_b, double rain_c, LevState& Sb, StepAdj& Ab, double& vt_b) {
+  const int k = C.k, L = C.L;
+  const double dm = P.dp1 * (1.0 + W1.qv + W1.ql + W1.qr + W1.qi + W1.qs + W1.qg);
+  const FallRec R = implicit_fall_rec<NW>(C, W1.qr, vtr, P.dz, P.dp1, valid, K.dt_rain);
+  double fv[2] = {R.flux, vtr}, pv[2];
+  C.template prevN<2>(fv, pv);
+  double flux_b = m1r_b, dm_b = 0.0, pv_b[2] = {0.0, 0.0};
+  if (K.do_sedi_w && valid)
+    w_update_b(k, W1.w, dm, R.flux, vtr, pv[0], pv[1], Sb.w, dm_b, flux_b, vt_b, pv_b[0], pv_b[1]);
+  if (k == L - 1) flux_b += rain_c;  // rain += the surface flux
+  double pn[2];
+  C.template nextN<2>(pv_b, pn);
+  if (valid && k < L - 1) {
+    flux_b += pn[0];
+    vt_b += pn[1];
   }
-  double di_b = 0.0, qliq_b = 0.0, qsol_b = 0.0, cvm_b = 0.0;
+  double qr_b = Sb.qr;
+  implicit_fall_b<NW>(C, R, W1.qr, P.dz, P.dp1, valid, K.dt_rain, qr_b, flux_b, vt_b, Ab.dz, Ab.dp1);
+  Sb.qr = qr_b;
   if (valid) {
-    subgrid_z_proc_b(K, P.h_var, P.rh_adj, P.rh_rain, qa_b, S2.qg, S2.qi, S2.ql, S2.qr, S2.qs, S2.qv, S2.tz, P.den,
-                     P.denfac, P.p1, Sb.qg, Sb.qi, Sb.ql, Sb.qr, Sb.qs, Sb.qv, Sb.tz, Ab.den, Ab.denfac);
-    const IcState Z0{S1.qg, S1.qi, S1.ql, S1.qr, S1.qs, S1.tz, q_liq, q_sol, cvm};
-    const IcIn I{S1.qv, P.den, P.denfac, vtg, vtr, vts, P.p1, di};
-    IcState Zb{Sb.qg, Sb.qi, Sb.ql, Sb.qr, Sb.qs, Sb.tz, 0.0, 0.0, 0.0};
-    IcIn Ib{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    icloud_processes_b(K, Z0, I, Zb, Ib);
-    Sb.qg = Zb.qg;
-    Sb.qi = Zb.qi;
-    Sb.ql = Zb.ql;
-    Sb.qr = Zb.qr;
-    Sb.qs = Zb.qs;
-    Sb.tz = Zb.tz;
-    Sb.qv += Ib.qv;
-    Ab.den += Ib.den;
-    Ab.denfac += Ib.denfac;
-    Ab.p1 += Ib.p1;
-    vtg_b += Ib.vtg;
-    vtr_b += Ib.vtr;
-    vts_b += Ib.vts;
-    di_b = Ib.di;
-    qliq_b = Zb.q_liq;
-    qsol_b = Zb.q_sol;
-    cvm_b = Zb.cvm;
+    // dm = dp1 (1 + qv + ql + qr + qi + qs + qg)
+    Ab.dp1 += dm_b * (1.0 + W1.qv + W1.ql + W1.qr + W1.qi + W1.qs + W1.qg);
+    const double t = dm_b * P.dp1;
+    Sb.qv += t;
+    Sb.ql += t;
+    Sb.qr += t;
+    Sb.qi += t;
+    Sb.qs += t;
+    Sb.qg += t;
   }
-  double sl_b = 0.0;
-  if (K.z_slope_ice && max_first(sl, inner))
-    sl_b = di_b;
-  else if (valid && !max_first(QVMIN, hq))
-    Sb.qi += di_b * P.h_var;
-  if (K.z_slope_ice) mono_slope_b<NW>(C, S1.qi, sl_b, Sb.qi, valid);
-  if (valid)
-    icloud_melt_freeze_b(K, S0.qv, S0.ql, S0.qr, S0.qi, S0.qs, S0.qg, S0.tz, P.den, qliq_b, qsol_b, cvm_b, Sb.qv,
-                         Sb.ql, Sb.qr, Sb.qi, Sb.qs, Sb.qg, Sb.tz, Ab.den);
+}
+
+// ------------------------------------------------------- column launches
+// Shared memory of the column launches: NTILE field tiles (G rows of RP
+// each), then G x 2 x SCR exchange scratch and G x NWORK work rows.
+template <int NW, int G, int NTILE, int NWORK>
+struct ColSmem {
+  static constexpr int RP = Tiles<NW>::RP;
+  static constexpr size_t scratch = (size_t)NTILE * G * RP;
+  static constexpr size_t work = scratch + (size_t)G * 2 * Tiles<NW>::SCR;
+  static constexpr size_t total = work + (size_t)G * NWORK * RP;
+  static constexpr size_t bytes = total * sizeof(double);
+};
+
+// this thread's column group g and its level operations
+template <int NW, int G, int NTILE, int NWORK>
+SHD Column<NW> column_of(double* sm, int L, int& g) {
+  using SM = ColSmem<NW, G, NTILE, NWORK>;
+  const int tid = threadIdx.x;
+  g = tid / (32 * NW);
+  Column<NW> C;
+  C.w = (tid >> 5) % NW;
+  C.lane = tid & 31;
+  C.k = 32 * C.w + C.lane;
+  C.L = L;
+  C.bar = 1 + g;
+  C.scr = sm + SM::scratch + (size_t)g * 2 * Tiles<NW>::SCR;
+  C.work = sm + SM::work + (size_t)g * NWORK * Tiles<NW>::RP;
+  C.par = 0;
+  return C;
 }
 
 // forward stages of the replay, out of line (one copy each)
 template <int NW>
 static __device__ __noinline__ void fwd_warm_rain(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid,
                                                   LevState& S, const StepGeom& P, double& vtr, double& m1r,
-                                                  double& r1) {
-  warm_rain<false>(C, K, KF, valid, S, P, vtr, m1r, r1);
+                                                  double& r1, VjpRec rec) {
+  warm_rain<false>(C, K, KF, valid, S, P, vtr, m1r, r1, nullptr, rec);
 }
 template <int NW>
 static __device__ __noinline__ void fwd_sedimentation(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid,
@@ -582,219 +605,538 @@ static __device__ __noinline__ void fwd_sedimentation(Column<NW>& C, const MpCon
 template <int NW>
 static __device__ __noinline__ void fwd_icloud(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid,
                                                LevState& S, const StepGeom& P, double& qa, double vtg, double vtr,
-                                               double vts, LevState& rec) {
-  icloud<false>(C, K, KF, valid, S, P, qa, vtg, vtr, vts, &rec);
+                                               double vts, VjpRec rec) {
+  icloud<false>(C, K, KF, valid, S, P, qa, vtg, vtr, vts, rec);
 }
 
+// 1. The replay with its records, then the reverse of fields_update.
 template <int NW, int G, int MINB>
-__global__ void __launch_bounds__(32 * NW * G, MINB) mp_vjp_kernel(const __grid_constant__ VjpArgs A) {
+__global__ void __launch_bounds__(32 * NW * G, MINB) vjp_replay_kernel(const __grid_constant__ VjpArgs A) {
   extern __shared__ double sm[];
-  using SM = VjpSmem<NW, G>;
   constexpr int RP = Tiles<NW>::RP;
   const MpConst& K = A.K;
   const MpConstF& KF = A.KF;
   const int L = A.nz;
-  const int tid = threadIdx.x;
-  const int g = tid / (32 * NW);
   const int64_t c0 = (int64_t)blockIdx.x * G;
   load_tiles<NW, G, N_VJP_IN>(A.in, sm, A.ncol, A.nx, L, c0);
   load_tiles<NW, G, N_VJP_COT>(A.cot, sm + (size_t)N_VJP_IN * G * RP, A.ncol, A.nx, L, c0);
   __syncthreads();
-
+  int g;
+  Column<NW> C = column_of<NW, G, NT_IN, 2>(sm, L, g);
   const int64_t col = c0 + g;
-  Column<NW> C;
-  C.w = (tid >> 5) % NW;
-  C.lane = tid & 31;
-  C.k = 32 * C.w + C.lane;
-  C.L = L;
-  C.bar = 1 + g;
-  C.scr = sm + SM::scratch + (size_t)g * 2 * Tiles<NW>::SCR;
-  C.work = sm + SM::work + (size_t)g * 4 * RP;
-  C.par = 0;
   const int k = C.k;
   const bool valid = k < L;
   const double* tile = sm + (size_t)g * RP + k;
   auto TI = [&](int f, double dflt) -> double { return valid ? tile[(size_t)f * G * RP] : dflt; };
   auto TC = [&](int f) -> double { return valid ? tile[(size_t)(N_VJP_IN + f) * G * RP] : 0.0; };
-  double* gtile = sm + SM::out + (size_t)g * RP + k;
-  auto TG = [&](int f) -> double& { return gtile[(size_t)f * G * RP]; };
+  if (col >= A.ncol) return;  // the whole column group (no block-wide barrier follows)
+  const Ws W = workspace(A);
+  const int64_t np = W.npts;
+  const int64_t p = (int64_t)(valid ? k : 0) * A.ncol + col;
+  const int64_t ci = col % A.nx, cj = col / A.nx;
+  const double land = A.land.p[ci * A.land.si + cj * A.land.sj];
+  const double area = A.area.p[ci * A.area.si + cj * A.area.sj];
+  const double pt = TI(IN_PT, 250.0), delp = TI(IN_DELP, 1.0), dz0 = TI(IN_DELZ, -100.0);
+  const double qin[6] = {TI(IN_QV, 0.0), TI(IN_QL, 0.0), TI(IN_QR, 0.0), TI(IN_QI, 0.0), TI(IN_QS, 0.0),
+                         TI(IN_QG, 0.0)};
+  // ------------------------------------------------------ forward replay
+  LevState S;
+  StepGeom P;
+  P.den = 1.0;
+  P.denfac = 1.0;
+  P.dz1 = -100.0;
+  P.dz = 100.0;
+  fields_init(C, K, valid, pt, qin[0], qin[1], qin[2], qin[3], qin[4], qin[5], delp, TI(IN_W, 0.0), dz0, land, area,
+              S, P);
+  if (valid) {
+    W.sp(SP_DP1)[p] = P.dp1;
+    W.sp(SP_P1)[p] = P.p1;
+  }
+  if (k == 0) {
+    W.sc(SC_HVAR)[col] = P.h_var;
+    W.sc(SC_RHADJ)[col] = P.rh_adj;
+    W.sc(SC_RHRAIN)[col] = P.rh_rain;
+    W.sc(SC_CCN)[col] = P.ccn;
+    W.sc(SC_CPRAUT)[col] = P.c_praut;
+  }
+  double m1 = 0.0, m1_sol = 0.0, vtr = VF_MIN, vtg = VF_MIN, vts = VF_MIN, qa = 0.0, ice = 0.0, snow = 0.0,
+         graupel = 0.0;
+  const int nt = K.ntimes;
+#pragma unroll 1
+  for (int it = 0; it < nt; ++it) {
+    substep_geometry(C, K, valid, pt, dz0, S, P);
+    if (valid) {
+      W.ss(it, SS_DEN)[p] = P.den;
+      W.ss(it, SS_DENFAC)[p] = P.denfac;
+      W.ss(it, SS_DZ)[p] = P.dz;
+      W.ss(it, SS_DZ1)[p] = P.dz1;
+      store_lev(W.ck(it, CK_E0) + p, np, S);
+    }
+    double m1r, r1;
+    fwd_warm_rain<NW>(C, K, KF, valid, S, P, vtr, m1r, r1,
+                      VjpRec{W.ck(it, CK_W1A) + p, W.ss(it, SS_SL_A) + p, W.scc(it, SCC_FALL_A) + col, np, valid,
+                             k == 0});
+    m1 = m1 + m1r;
+    if (valid) {
+      W.ss(it, SS_VTR_A)[p] = vtr;
+      store_lev(W.ck(it, CK_E1) + p, np, S);
+    }
+    fwd_sedimentation<NW>(C, K, KF, valid, S, P, vtg, vts, m1_sol, ice, snow, graupel);
+    if (valid) {
+      W.ss(it, SS_VTG)[p] = vtg;
+      W.ss(it, SS_VTS)[p] = vts;
+      store_lev(W.ck(it, CK_E2) + p, np, S);
+    }
+    fwd_warm_rain<NW>(C, K, KF, valid, S, P, vtr, m1r, r1,
+                      VjpRec{W.ck(it, CK_W1B) + p, W.ss(it, SS_SL_B) + p, W.scc(it, SCC_FALL_B) + col, np, valid,
+                             k == 0});
+    m1 = m1 + m1r + m1_sol;
+    if (valid) {
+      W.ss(it, SS_VTR_B)[p] = vtr;
+      store_lev(W.ck(it, CK_E3) + p, np, S);
+    }
+    fwd_icloud<NW>(C, K, KF, valid, S, P, qa, vtg, vtr, vts,
+                   VjpRec{W.ck(it, CK_E4) + p, W.ss(it, SS_SL_I) + p, nullptr, np, valid, false});
+  }
 
+  // ------------------------------------------------- fields_update reverse
+  const double rdt = K.rdt;
+  LevState Sb{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  double dp1_b = 0.0, pt_b = 0.0, delp_b = 0.0, u0_b = 0.0, v0_b = 0.0, qa0_b = 0.0, qa_b = 0.0;
+  double qin_b[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  if (valid) {
+    const double cq[6] = {TC(OUT_QV_DT), TC(OUT_QL_DT), TC(OUT_QR_DT), TC(OUT_QI_DT), TC(OUT_QS_DT), TC(OUT_QG_DT)};
+    const double qf[6] = {S.qv, S.ql, S.qr, S.qi, S.qs, S.qg};
+    const double dp1 = P.dp1, dp0 = delp;
+    const double omq0 = dp0 / dp1, omq = dp1 / dp0;
+    double qfb[6], omq_b = 0.0, omq0_b = 0.0;
+#pragma unroll
+    for (int n = 0; n < 6; ++n) {
+      const double q0 = qin[n] * omq0;
+      qfb[n] = cq[n] * rdt * omq;
+      const double q0_b = -cq[n] * rdt * omq;
+      omq_b += cq[n] * rdt * (qf[n] - q0);
+      qin_b[n] += q0_b * omq0;
+      omq0_b += q0_b * qin[n];
+    }
+    const double cvm = K.c_air + S.qv * K.c_vap + (S.qr + S.ql) * K.C_LIQ + (S.qi + S.qs + S.qg) * K.C_ICE;
+    const double gpt = TC(OUT_PT_DT) * rdt / K.CP_AIR;
+    Sb.tz = gpt * cvm;
+    pt_b -= gpt * cvm;
+    const double cvm_b = gpt * (S.tz - pt);
+    qfb[0] += cvm_b * K.c_vap;
+    qfb[1] += cvm_b * K.C_LIQ;
+    qfb[2] += cvm_b * K.C_LIQ;
+    qfb[3] += cvm_b * K.C_ICE;
+    qfb[4] += cvm_b * K.C_ICE;
+    qfb[5] += cvm_b * K.C_ICE;
+    Sb.qv = qfb[0], Sb.ql = qfb[1], Sb.qr = qfb[2], Sb.qi = qfb[3], Sb.qs = qfb[4], Sb.qg = qfb[5];
+    dp1_b += omq_b / dp0 - omq0_b * omq0 / dp1;
+    delp_b += -omq_b * omq / dp0 + omq0_b / dp1;
+    // the accumulator: qaz_out = qaz_in + the step's increments, and
+    // qa_dt = rdt (qaz_out / ntimes - qa0) (without do_qa, which leaves
+    // both alone)
+    qa_b = TC(OUT_QAZ);
+    if (!K.do_qa) {
+      qa_b += TC(OUT_QA_DT) * rdt / (double)K.ntimes;
+      qa0_b = -TC(OUT_QA_DT) * rdt;
+    }
+    Sb.w = TC(OUT_W);  // without do_sedi_w, wmp passes through unchanged
+  }
+  double m1_b = 0.0;
+  if (K.sedi_transport) {
+    const double u0 = TI(IN_UA, 0.0), v0 = TI(IN_VA, 0.0);
+    const double mp = C.prev(m1);
+    double au, av, b, D = 1.0;
+    if (k == 0 || !valid) {
+      au = u0;
+      av = v0;
+      b = 0.0;
+    } else {
+      D = delp + mp;
+      au = delp * u0 / D;
+      av = delp * v0 / D;
+      b = mp / D;
+    }
+    double u1, v1;
+    C.scan_affine2(au, b, av, b, u1, v1);
+    const bool out_k = valid && k >= 1;  // udt, vdt are written for k >= 1 only
+    const double cu = out_k ? TC(OUT_UDT) * rdt : 0.0, cv = out_k ? TC(OUT_VDT) * rdt : 0.0;
+    u0_b -= cu;
+    v0_b -= cv;
+    double bv[1] = {b}, bn[1];
+    C.template nextN<1>(bv, bn);
+    const double cn = (valid && k < L - 1) ? bn[0] : 0.0;
+    const double aa[2] = {cu, cv}, cc[2] = {cn, cn};
+    double lam[2];
+    C.template scanN_rev<2>(aa, cc, lam);
+    const double pu[2] = {u1, v1};
+    double pp[2];
+    C.template prevN<2>(pu, pp);
+    double mp_b = 0.0;
+    if (valid) {
+      if (k == 0) {
+        u0_b += lam[0];
+        v0_b += lam[1];
+      } else {
+        const double b_b = lam[0] * pp[0] + lam[1] * pp[1];
+        u0_b += lam[0] * delp / D;
+        v0_b += lam[1] * delp / D;
+        delp_b += lam[0] * u0 / D + lam[1] * v0 / D;
+        const double D_b = -lam[0] * au / D - lam[1] * av / D - b_b * b / D;
+        delp_b += D_b;
+        mp_b = b_b / D + D_b;
+      }
+    }
+    double mv[1] = {mp_b}, mn[1];
+    C.template nextN<1>(mv, mn);
+    m1_b = (valid && k < L - 1) ? mn[0] : 0.0;
+  }
+  if (valid) {
+    store_lev(W.as(AS_QV) + p, np, Sb);
+    W.as(AS_DP1)[p] = dp1_b;
+    W.as(AS_P1)[p] = 0.0;
+    W.as(AS_CCN)[p] = 0.0;
+    W.as(AS_CPRAUT)[p] = 0.0;
+    W.as(AS_PT)[p] = pt_b;
+    W.as(AS_DELP)[p] = delp_b;
+    W.as(AS_DZ0)[p] = 0.0;
+#pragma unroll
+    for (int n = 0; n < 6; ++n) W.as(AS_QIN0 + n)[p] = qin_b[n];
+    W.as(AS_QA)[p] = qa_b;
+    W.as(AS_QA0)[p] = qa0_b;
+    W.as(AS_U0)[p] = u0_b;
+    W.as(AS_V0)[p] = v0_b;
+    W.as(AS_M1)[p] = m1_b;
+  }
+}
+
+// ------------------------------------------------------- point launches
+// One thread per point p = k * ncol + col: consecutive columns of one level
+// on consecutive lanes.
+#ifndef SHIELD_VJP_PT_THREADS
+#define SHIELD_VJP_PT_THREADS 128
+#endif
+#ifndef SHIELD_VJP_PT_MINB
+#define SHIELD_VJP_PT_MINB 4
+#endif
+constexpr int PT_THREADS = SHIELD_VJP_PT_THREADS;
+
+struct PointIdx {
+  int64_t p, col;
+  int k;
+};
+SHD bool point_of(const Ws& W, PointIdx& q) {
+  q.p = (int64_t)blockIdx.x * PT_THREADS + threadIdx.x;
+  if (q.p >= W.npts) return false;
+  q.k = (int)(q.p / W.ncol);
+  q.col = q.p - (int64_t)q.k * W.ncol;
+  return true;
+}
+
+// 2a. icloud reversed from its recorded states: the saturation adjustment
+// and the ice processes. Leaves the state's cotangent with respect to the
+// melted / frozen state without the ice slope's part, the cotangents of
+// melting / freezing's other outputs and of the slope, and the fall speeds'.
+// Starts the sub-step's geometry cotangents.
+__global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_icloud_pt(const __grid_constant__ VjpArgs A,
+                                                                                int it) {
+  const Ws W = workspace(A);
+  PointIdx q;
+  if (!point_of(W, q)) return;
+  const int64_t p = q.p, np = W.npts, col = q.col;
+  const MpConst& K = A.K;
+  const LevState E3 = load_lev(W.ck(it, CK_E3) + p, np);
+  const LevState E4 = load_lev(W.ck(it, CK_E4) + p, np);
+  const double den = W.ss(it, SS_DEN)[p], denfac = W.ss(it, SS_DENFAC)[p], p1 = W.sp(SP_P1)[p];
+  const double h_var = W.sc(SC_HVAR)[col], rh_adj = W.sc(SC_RHADJ)[col], rh_rain = W.sc(SC_RHRAIN)[col];
+  const double vtg = W.ss(it, SS_VTG)[p], vtr = W.ss(it, SS_VTR_B)[p], vts = W.ss(it, SS_VTS)[p];
+  LevState Sb = load_lev(W.as(AS_QV) + p, np);
+  const double qa_b = W.as(AS_QA)[p];
+  double den_b = 0.0, denfac_b = 0.0;
+  LevState S1 = E3;
+  double q_liq, q_sol, cvm;
+  icloud_melt_freeze(K, S1.qv, S1.ql, S1.qr, S1.qi, S1.qs, S1.qg, S1.tz, den, q_liq, q_sol, cvm);
+  const double hq = h_var * S1.qi;
+  const double inner = fmax(QVMIN, hq);
+  double sl = 0.0, di = inner;
+  if (K.z_slope_ice) {
+    sl = W.ss(it, SS_SL_I)[p];
+    di = fmax(sl, inner);
+  }
+  subgrid_z_proc_b(K, h_var, rh_adj, rh_rain, qa_b, E4.qg, E4.qi, E4.ql, E4.qr, E4.qs, E4.qv, E4.tz, den, denfac, p1,
+                   Sb.qg, Sb.qi, Sb.ql, Sb.qr, Sb.qs, Sb.qv, Sb.tz, den_b, denfac_b);
+  const IcState Z0{S1.qg, S1.qi, S1.ql, S1.qr, S1.qs, S1.tz, q_liq, q_sol, cvm};
+  const IcIn I{S1.qv, den, denfac, vtg, vtr, vts, p1, di};
+  IcState Zb{Sb.qg, Sb.qi, Sb.ql, Sb.qr, Sb.qs, Sb.tz, 0.0, 0.0, 0.0};
+  IcIn Ib{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  icloud_processes_b(K, Z0, I, Zb, Ib);
+  Sb.qg = Zb.qg;
+  Sb.qi = Zb.qi;
+  Sb.ql = Zb.ql;
+  Sb.qr = Zb.qr;
+  Sb.qs = Zb.qs;
+  Sb.tz = Zb.tz;
+  Sb.qv += Ib.qv;
+  double sl_b = 0.0;
+  if (K.z_slope_ice && max_first(sl, inner))
+    sl_b = Ib.di;
+  else if (!max_first(QVMIN, hq))
+    Sb.qi += Ib.di * h_var;
+  store_lev(W.as(AS_QV) + p, np, Sb);
+  W.as(AS_DEN)[p] = den_b + Ib.den;
+  W.as(AS_DENFAC)[p] = denfac_b + Ib.denfac;
+  W.as(AS_DZ)[p] = 0.0;
+  W.as(AS_P1)[p] += Ib.p1;
+  W.as(AS_VTR)[p] = Ib.vtr;
+  W.as(AS_VTG)[p] = Ib.vtg;
+  W.as(AS_VTS)[p] = Ib.vts;
+  W.as(AS_QLIQ)[p] = Zb.q_liq;
+  W.as(AS_QSOL)[p] = Zb.q_sol;
+  W.as(AS_CVM)[p] = Zb.cvm;
+  W.as(AS_SLI)[p] = sl_b;
+}
+
+// 2b. Autoconversion of a warm_rain pass reversed (microphysics.py:559-653),
+// without the liquid slope's transpose; for the second pass, first the end
+// of icloud's reverse: the ice slope's transpose and melting / freezing.
+template <int PASS>
+__global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_autoconv_pt(const __grid_constant__ VjpArgs A,
+                                                                                  int it) {
+  const Ws W = workspace(A);
+  PointIdx q;
+  if (!point_of(W, q)) return;
+  const int64_t p = q.p, np = W.npts, col = q.col;
+  const MpConst& K = A.K;
+  LevState Sb = load_lev(W.as(AS_QV) + p, np);
+  const double den = W.ss(it, SS_DEN)[p];
+  double den_b = 0.0;
+  if (PASS == 1) {
+    if (K.z_slope_ice) Sb.qi += slope_gather(W.ss(it, SS_S1QI), W.as(AS_SLI), p, W.ncol, q.k, A.nz);
+    const LevState E3 = load_lev(W.ck(it, CK_E3) + p, np);
+    icloud_melt_freeze_b(K, E3.qv, E3.ql, E3.qr, E3.qi, E3.qs, E3.qg, E3.tz, den, W.as(AS_QLIQ)[p],
+                         W.as(AS_QSOL)[p], W.as(AS_CVM)[p], Sb.qv, Sb.ql, Sb.qr, Sb.qi, Sb.qs, Sb.qg, Sb.tz, den_b);
+  }
+  const LevState W3 = load_lev(W.ck(it, PASS ? CK_W3B : CK_W3A) + p, np);
+  const double h_var = W.sc(SC_HVAR)[col], ccn = W.sc(SC_CCN)[col], c_praut = W.sc(SC_CPRAUT)[col];
+  double ccn_b = 0.0, cpr_b = 0.0, sl_b = 0.0;
+  if (K.irain_f != 0) {
+    autoconv_no_subgrid_var_b(K, W3.ql, W3.qr, W3.tz, den, ccn, c_praut, Sb.ql, Sb.qr, den_b, ccn_b, cpr_b);
+  } else {
+    const double hq = h_var * W3.ql;
+    const double inner = fmax(QVMIN, hq);
+    double sl = 0.0, dl = inner;
+    if (K.z_slope_liq) {
+      sl = W.ss(it, PASS ? SS_SL_B : SS_SL_A)[p];
+      dl = fmax(sl, inner);
+    }
+    double dl_b = 0.0;
+    autoconv_subgrid_var_b(K, W3.ql, W3.qr, W3.tz, den, ccn, c_praut, dl, Sb.ql, Sb.qr, den_b, ccn_b, cpr_b, dl_b);
+    if (K.z_slope_liq && max_first(sl, inner))
+      sl_b = dl_b;
+    else if (!max_first(QVMIN, hq))
+      Sb.ql += dl_b * h_var;
+  }
+  store_lev(W.as(AS_QV) + p, np, Sb);
+  W.as(AS_DEN)[p] += den_b;
+  W.as(AS_CCN)[p] += ccn_b;
+  W.as(AS_CPRAUT)[p] += cpr_b;
+  W.as(AS_SLL)[p] = sl_b;
+}
+
+// 2c. The liquid slope's transpose, then the second evaporation / accretion
+// of a warm_rain pass reversed (columns with falling rain).
+__global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_revap2_pt(const __grid_constant__ VjpArgs A,
+                                                                                int it, int pass) {
+  const Ws W = workspace(A);
+  PointIdx q;
+  if (!point_of(W, q)) return;
+  const int64_t p = q.p, np = W.npts, col = q.col;
+  const MpConst& K = A.K;
+  LevState Sb = load_lev(W.as(AS_QV) + p, np);
+  if (K.irain_f == 0 && K.z_slope_liq)
+    Sb.ql += slope_gather(W.ck(it, pass ? CK_W3B : CK_W3A) + np, W.as(AS_SLL), p, W.ncol, q.k, A.nz);
+  if (W.scc(it, pass ? SCC_FALL_B : SCC_FALL_A)[col] != 0.0) {
+    const LevState W2 = load_lev(W.ck(it, pass ? CK_W2B : CK_W2A) + p, np);
+    const double den = W.ss(it, SS_DEN)[p], denfac = W.ss(it, SS_DENFAC)[p], h_var = W.sc(SC_HVAR)[col];
+    double den_b = 0.0, denfac_b = 0.0;
+    revap_racc_b(K, 0.5 * K.dt_rain, h_var, W2.qg, W2.qi, W2.ql, W2.qr, W2.qs, W2.qv, W2.tz, den, denfac, Sb.qg,
+                 Sb.qi, Sb.ql, Sb.qr, Sb.qs, Sb.qv, Sb.tz, den_b, denfac_b);
+    W.as(AS_DEN)[p] += den_b;
+    W.as(AS_DENFAC)[p] += denfac_b;
+  }
+  store_lev(W.as(AS_QV) + p, np, Sb);
+}
+
+// 2e. The first evaporation / accretion and the fall speed of a warm_rain
+// pass reversed (columns with falling rain); after the first pass, the
+// reverse of the sub-step geometry (density, fall factor, layer thickness
+// from the entry temperature: warm_rain with is_first, :349-380).
+__global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_revap1_pt(const __grid_constant__ VjpArgs A,
+                                                                                int it, int pass) {
+  const Ws W = workspace(A);
+  PointIdx q;
+  if (!point_of(W, q)) return;
+  const int64_t p = q.p, np = W.npts, col = q.col;
+  const MpConst& K = A.K;
+  LevState Sb = load_lev(W.as(AS_QV) + p, np);
+  const double den = W.ss(it, SS_DEN)[p], denfac = W.ss(it, SS_DENFAC)[p];
+  double den_b = 0.0, denfac_b = 0.0;
+  if (W.scc(it, pass ? SCC_FALL_B : SCC_FALL_A)[col] != 0.0) {
+    const LevState W0 = load_lev(W.ck(it, pass ? CK_E2 : CK_E0) + p, np);
+    const double h_var = W.sc(SC_HVAR)[col];
+    revap_racc_b(K, 0.5 * K.dt_rain, h_var, W0.qg, W0.qi, W0.ql, W0.qr, W0.qs, W0.qv, W0.tz, den, denfac, Sb.qg,
+                 Sb.qi, Sb.ql, Sb.qr, Sb.qs, Sb.qv, Sb.tz, den_b, denfac_b);
+    rain_fspeed_b(K, W0.qr, den, W.as(AS_VTT)[p], Sb.qr, den_b);
+  }
+  if (pass == 0) {
+    // den = den0 dz0 / dz1, den0 = -dp1 / (g dz0), denfac = sqrt(SFCRHO / den),
+    // dz1 = dz0 tz / t0, dz = heights(-dz1) (= -dz1 in exact arithmetic)
+    const int64_t i = col % A.nx, j = col / A.nx;
+    const Fld3& fp = A.in[IN_PT];
+    const Fld3& fz = A.in[IN_DELZ];
+    const double pt = fp.p[i * fp.si + j * fp.sj + (int64_t)q.k * fp.sk];
+    const double dz0 = fz.p[i * fz.si + j * fz.sj + (int64_t)q.k * fz.sk];
+    const double dp1 = W.sp(SP_DP1)[p], dz1 = W.ss(it, SS_DZ1)[p], tz0 = W.ck(it, CK_E0)[6 * np + p];
+    const double aden = W.as(AS_DEN)[p] + den_b, adenfac = W.as(AS_DENFAC)[p] + denfac_b;
+    const double den0 = -dp1 / (K.GRAV * dz0);
+    const double dn_b = aden - adenfac * 0.5 * denfac / den;
+    double dz1_b = -W.as(AS_DZ)[p];
+    const double den0_b = dn_b * dz0 / dz1;
+    double dz0_b = dn_b * den0 / dz1;
+    dz1_b -= dn_b * den / dz1;
+    dz0_b += dz1_b * tz0 / pt;
+    Sb.tz += dz1_b * dz0 / pt;
+    const double pt_b = -dz1_b * dz1 / pt;
+    const double dp1_b = -den0_b / (K.GRAV * dz0);
+    dz0_b += den0_b * dp1 / (K.GRAV * dz0 * dz0);
+    W.as(AS_DZ0)[p] += dz0_b;
+    W.as(AS_PT)[p] += pt_b;
+    W.as(AS_DP1)[p] += dp1_b;
+  } else {
+    W.as(AS_DEN)[p] += den_b;
+    W.as(AS_DENFAC)[p] += denfac_b;
+  }
+  store_lev(W.as(AS_QV) + p, np, Sb);
+}
+
+// ------------------------------------------------------- column launches
+// The values the column reverses take on a padding level k >= L (finite, so
+// that a zero cotangent stays zero through the scans).
+SHD LevState pad_state() { return LevState{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 250.0, 0.0}; }
+
+// 2d. The rain fall of a warm_rain pass reversed (columns with falling rain).
+template <int NW, int G, int MINB>
+__global__ void __launch_bounds__(32 * NW * G, MINB) vjp_fall_kernel(const __grid_constant__ VjpArgs A, int it,
+                                                                     int pass) {
+  extern __shared__ double sm[];
+  const int L = A.nz;
+  int g;
+  Column<NW> C = column_of<NW, G, 0, 0>(sm, L, g);
+  const int64_t col = (int64_t)blockIdx.x * G + g;
+  if (col >= A.ncol) return;  // the whole column group
+  const Ws W = workspace(A);
+  if (W.scc(it, pass ? SCC_FALL_B : SCC_FALL_A)[col] == 0.0) return;  // the whole column group
+  const MpConst& K = A.K;
+  const int k = C.k;
+  const bool valid = k < L;
+  const int64_t np = W.npts, p = (int64_t)(valid ? k : 0) * A.ncol + col;
+  const LevState W1 = valid ? load_lev(W.ck(it, pass ? CK_W1B : CK_W1A) + p, np) : pad_state();
+  StepGeom P;
+  P.dp1 = valid ? W.sp(SP_DP1)[p] : 1.0;
+  P.dz = valid ? W.ss(it, SS_DZ)[p] : 100.0;
+  const double vtr = valid ? W.ss(it, pass ? SS_VTR_B : SS_VTR_A)[p] : VF_MIN;
+  LevState Sb = valid ? load_lev(W.as(AS_QV) + p, np) : LevState{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  StepAdj Ab{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  const double m1_b = valid ? W.as(AS_M1)[p] : 0.0;
+  const double rain_c = A.rain_b ? A.rain_b[col] * (86400.0 * K.rdt * K.RGRAV) : 0.0;
+  double vt_b = (pass == 1 && valid) ? W.as(AS_VTR)[p] : 0.0;
+  rain_fall_b<NW>(C, K, valid, W1, P, vtr, m1_b, rain_c, Sb, Ab, vt_b);
+  if (valid) {
+    store_lev(W.as(AS_QV) + p, np, Sb);
+    W.as(AS_DZ)[p] += Ab.dz;
+    W.as(AS_DP1)[p] += Ab.dp1;
+    W.as(AS_VTT)[p] = vt_b;
+  }
+}
+
+// 2f. sedimentation reversed (fall speeds, cloud ice melting, the falls of
+// ice, snow and graupel with the vertical-velocity transport).
+template <int NW, int G, int MINB>
+__global__ void __launch_bounds__(32 * NW * G, MINB) vjp_sed_kernel(const __grid_constant__ VjpArgs A, int it) {
+  extern __shared__ double sm[];
+  const int L = A.nz;
+  int g;
+  Column<NW> C = column_of<NW, G, 0, 0>(sm, L, g);
+  const int64_t col = (int64_t)blockIdx.x * G + g;
+  if (col >= A.ncol) return;  // the whole column group
+  const Ws W = workspace(A);
+  const MpConst& K = A.K;
+  const int k = C.k;
+  const bool valid = k < L;
+  const int64_t np = W.npts, p = (int64_t)(valid ? k : 0) * A.ncol + col;
+  const LevState E1 = valid ? load_lev(W.ck(it, CK_E1) + p, np) : pad_state();
+  StepGeom P;
+  P.dp1 = valid ? W.sp(SP_DP1)[p] : 1.0;
+  P.dz = valid ? W.ss(it, SS_DZ)[p] : 100.0;
+  P.den = valid ? W.ss(it, SS_DEN)[p] : 1.0;
+  LevState Sb = valid ? load_lev(W.as(AS_QV) + p, np) : LevState{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  StepAdj Ab{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  const double convt = 86400.0 * K.rdt * K.RGRAV;
+  const double snow_c = A.snow_b ? A.snow_b[col] * convt : 0.0;
+  const double ice_c = A.ice_b ? A.ice_b[col] * convt : 0.0;
+  const double graupel_c = A.graupel_b ? A.graupel_b[col] * convt : 0.0;
+  const double m1_b = valid ? W.as(AS_M1)[p] : 0.0;
+  const double vtg_b = valid ? W.as(AS_VTG)[p] : 0.0, vts_b = valid ? W.as(AS_VTS)[p] : 0.0;
+  sedimentation_b<NW>(C, K, valid, E1, P, m1_b, ice_c, snow_c, graupel_c, vtg_b, vts_b, Sb, Ab);
+  if (valid) {
+    store_lev(W.as(AS_QV) + p, np, Sb);
+    W.as(AS_DEN)[p] += Ab.den;
+    W.as(AS_DZ)[p] += Ab.dz;
+    W.as(AS_DP1)[p] += Ab.dp1;
+  }
+}
+
+// 3. fields_init reversed (:27-276), then the gradients written through the
+// shared-memory tiles.
+template <int NW, int G, int MINB>
+__global__ void __launch_bounds__(32 * NW * G, MINB) vjp_init_kernel(const __grid_constant__ VjpArgs A) {
+  extern __shared__ double sm[];
+  constexpr int RP = Tiles<NW>::RP;
+  constexpr int NTILE = N_VJP_IN + N_VJP_GRAD;
+  const MpConst& K = A.K;
+  const int L = A.nz;
+  const int64_t c0 = (int64_t)blockIdx.x * G;
+  load_tiles<NW, G, N_VJP_IN>(A.in, sm, A.ncol, A.nx, L, c0);
+  __syncthreads();
+  int g;
+  Column<NW> C = column_of<NW, G, NTILE, 4>(sm, L, g);
+  const int64_t col = c0 + g;
+  const int k = C.k;
+  const bool valid = k < L;
+  const double* tile = sm + (size_t)g * RP + k;
+  auto TI = [&](int f, double dflt) -> double { return valid ? tile[(size_t)f * G * RP] : dflt; };
+  double* gtile = sm + (size_t)N_VJP_IN * G * RP + (size_t)g * RP + k;
+  auto TG = [&](int f) -> double& { return gtile[(size_t)f * G * RP]; };
   if (col < A.ncol) {
-    const int64_t ci = col % A.nx, cj = col / A.nx;
-    const double land = A.land.p[ci * A.land.si + cj * A.land.sj];
-    const double area = A.area.p[ci * A.area.si + cj * A.area.sj];
+    const Ws W = workspace(A);
+    const int64_t np = W.npts, p = (int64_t)(valid ? k : 0) * A.ncol + col;
+    auto AS = [&](int f) -> double { return valid ? W.as(f)[p] : 0.0; };
     const double pt = TI(IN_PT, 250.0), delp = TI(IN_DELP, 1.0), dz0 = TI(IN_DELZ, -100.0);
     const double qin[6] = {TI(IN_QV, 0.0), TI(IN_QL, 0.0), TI(IN_QR, 0.0), TI(IN_QI, 0.0), TI(IN_QS, 0.0),
                            TI(IN_QG, 0.0)};
-    // ------------------------------------------------------ forward replay
-    LevState S;
     StepGeom P;
-    P.den = 1.0;
-    P.denfac = 1.0;
-    P.dz1 = -100.0;
-    P.dz = 100.0;
-    fields_init(C, K, valid, pt, qin[0], qin[1], qin[2], qin[3], qin[4], qin[5], delp, TI(IN_W, 0.0), dz0, land,
-                    area, S, P);
-    LevState ck[VJP_MAXNT][5];  // entries of the four stages, and the state before the adjustment
-    double ckv[VJP_MAXNT][3];
-    double m1 = 0.0, m1_sol = 0.0, vtr = VF_MIN, vtg = VF_MIN, vts = VF_MIN, qa = 0.0, ice = 0.0, snow = 0.0,
-           graupel = 0.0;
-    const int nt = K.ntimes;
-#pragma unroll 1
-    for (int it = 0; it < nt; ++it) {
-      substep_geometry(C, K, valid, pt, dz0, S, P);
-#pragma unroll 1
-      for (int pass = 0; pass < 2; ++pass) {
-        double m1r, r1;
-        ck[it][2 * pass] = S;
-        fwd_warm_rain<NW>(C, K, KF, valid, S, P, vtr, m1r, r1);
-        m1 = (pass == 0) ? m1 + m1r : m1 + m1r + m1_sol;
-        ck[it][2 * pass + 1] = S;
-        if (pass == 1) break;
-        fwd_sedimentation<NW>(C, K, KF, valid, S, P, vtg, vts, m1_sol, ice, snow, graupel);
-      }
-      ckv[it][0] = vtr;
-      ckv[it][1] = vtg;
-      ckv[it][2] = vts;
-      fwd_icloud<NW>(C, K, KF, valid, S, P, qa, vtg, vtr, vts, ck[it][4]);
-    }
-
-    // ------------------------------------------------- fields_update reverse
-    const double rdt = K.rdt;
-    LevState Sb{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    StepAdj Ab{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    double pt_b = 0.0, delp_b = 0.0, dz0_b = 0.0, u0_b = 0.0, v0_b = 0.0, qa0_b = 0.0, qa_b = 0.0;
-    double qin_b[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    if (valid) {
-      const double cq[6] = {TC(OUT_QV_DT), TC(OUT_QL_DT), TC(OUT_QR_DT), TC(OUT_QI_DT), TC(OUT_QS_DT), TC(OUT_QG_DT)};
-      const double qf[6] = {S.qv, S.ql, S.qr, S.qi, S.qs, S.qg};
-      const double dp1 = P.dp1, dp0 = delp;
-      const double omq0 = dp0 / dp1, omq = dp1 / dp0;
-      double qfb[6], omq_b = 0.0, omq0_b = 0.0;
+    P.dp1 = valid ? W.sp(SP_DP1)[p] : 1.0;
+    P.p1 = valid ? W.sp(SP_P1)[p] : 1.0e5;
+    P.ccn = W.sc(SC_CCN)[col];
+    P.c_praut = W.sc(SC_CPRAUT)[col];
+    LevState Sb = valid ? load_lev(W.as(AS_QV) + p, np) : LevState{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    StepAdj Ab{0.0, 0.0, 0.0, AS(AS_DP1), AS(AS_P1), AS(AS_CCN), AS(AS_CPRAUT)};
+    double pt_b = AS(AS_PT), delp_b = AS(AS_DELP), dz0_b = AS(AS_DZ0);
+    double qin_b[6];
 #pragma unroll
-      for (int n = 0; n < 6; ++n) {
-        const double q0 = qin[n] * omq0;
-        qfb[n] = cq[n] * rdt * omq;
-        const double q0_b = -cq[n] * rdt * omq;
-        omq_b += cq[n] * rdt * (qf[n] - q0);
-        qin_b[n] += q0_b * omq0;
-        omq0_b += q0_b * qin[n];
-      }
-      const double cvm = K.c_air + S.qv * K.c_vap + (S.qr + S.ql) * K.C_LIQ + (S.qi + S.qs + S.qg) * K.C_ICE;
-      const double gpt = TC(OUT_PT_DT) * rdt / K.CP_AIR;
-      Sb.tz = gpt * cvm;
-      pt_b -= gpt * cvm;
-      const double cvm_b = gpt * (S.tz - pt);
-      qfb[0] += cvm_b * K.c_vap;
-      qfb[1] += cvm_b * K.C_LIQ;
-      qfb[2] += cvm_b * K.C_LIQ;
-      qfb[3] += cvm_b * K.C_ICE;
-      qfb[4] += cvm_b * K.C_ICE;
-      qfb[5] += cvm_b * K.C_ICE;
-      Sb.qv = qfb[0], Sb.ql = qfb[1], Sb.qr = qfb[2], Sb.qi = qfb[3], Sb.qs = qfb[4], Sb.qg = qfb[5];
-      Ab.dp1 += omq_b / dp0 - omq0_b * omq0 / dp1;
-      delp_b += -omq_b * omq / dp0 + omq0_b / dp1;
-      // the accumulator: qaz_out = qaz_in + the step's increments, and
-      // qa_dt = rdt (qaz_out / ntimes - qa0) (without do_qa, which leaves
-      // both alone)
-      qa_b = TC(OUT_QAZ);
-      if (!K.do_qa) {
-        qa_b += TC(OUT_QA_DT) * rdt / (double)K.ntimes;
-        qa0_b = -TC(OUT_QA_DT) * rdt;
-      }
-      Sb.w = TC(OUT_W);  // without do_sedi_w, wmp passes through unchanged
-    }
-    double m1_b = 0.0;
-    if (K.sedi_transport) {
-      const double u0 = TI(IN_UA, 0.0), v0 = TI(IN_VA, 0.0);
-      const double mp = C.prev(m1);
-      double au, av, b, D = 1.0;
-      if (k == 0 || !valid) {
-        au = u0;
-        av = v0;
-        b = 0.0;
-      } else {
-        D = delp + mp;
-        au = delp * u0 / D;
-        av = delp * v0 / D;
-        b = mp / D;
-      }
-      double u1, v1;
-      C.scan_affine2(au, b, av, b, u1, v1);
-      const bool out_k = valid && k >= 1;  // udt, vdt are written for k >= 1 only
-      const double cu = out_k ? TC(OUT_UDT) * rdt : 0.0, cv = out_k ? TC(OUT_VDT) * rdt : 0.0;
-      u0_b -= cu;
-      v0_b -= cv;
-      double bv[1] = {b}, bn[1];
-      C.template nextN<1>(bv, bn);
-      const double cn = (valid && k < L - 1) ? bn[0] : 0.0;
-      const double aa[2] = {cu, cv}, cc[2] = {cn, cn};
-      double lam[2];
-      C.template scanN_rev<2>(aa, cc, lam);
-      const double pu[2] = {u1, v1};
-      double pp[2];
-      C.template prevN<2>(pu, pp);
-      double mp_b = 0.0;
-      if (valid) {
-        if (k == 0) {
-          u0_b += lam[0];
-          v0_b += lam[1];
-        } else {
-          const double b_b = lam[0] * pp[0] + lam[1] * pp[1];
-          u0_b += lam[0] * delp / D;
-          v0_b += lam[1] * delp / D;
-          delp_b += lam[0] * u0 / D + lam[1] * v0 / D;
-          const double D_b = -lam[0] * au / D - lam[1] * av / D - b_b * b / D;
-          delp_b += D_b;
-          mp_b = b_b / D + D_b;
-        }
-      }
-      double mv[1] = {mp_b}, mn[1];
-      C.template nextN<1>(mv, mn);
-      m1_b = (valid && k < L - 1) ? mn[0] : 0.0;
-    }
-    // surface totals: out = total * 86400 rdt / g
-    const double convt = 86400.0 * K.rdt * K.RGRAV;
-    const double rain_c = A.rain_b ? A.rain_b[col] * convt : 0.0;
-    const double snow_c = A.snow_b ? A.snow_b[col] * convt : 0.0;
-    const double ice_c = A.ice_b ? A.ice_b[col] * convt : 0.0;
-    const double graupel_c = A.graupel_b ? A.graupel_b[col] * convt : 0.0;
-
-    // ------------------------------------------------------ sub-steps, reversed
-#pragma unroll 1
-    for (int it = nt - 1; it >= 0; --it) {
-      StepGeom Pg = P;
-      substep_geometry(C, K, valid, pt, dz0, ck[it][0], Pg);
-      Ab.den = 0.0;
-      Ab.denfac = 0.0;
-      Ab.dz = 0.0;
-      double vtg_b = 0.0, vtr_b = 0.0, vts_b = 0.0;
-      icloud_b<NW>(C, K, valid, ck[it][3], ck[it][4], Pg, ckv[it][1], ckv[it][0], ckv[it][2], qa_b, Sb, Ab, vtg_b,
-                   vtr_b, vts_b);
-#pragma unroll 1
-      for (int pass = 1; pass >= 0; --pass) {
-        warm_rain_b<NW>(C, K, valid, ck[it][2 * pass], Pg, m1_b, rain_c, pass == 1 ? vtr_b : 0.0, Sb, Ab);
-        if (pass == 1)
-          sedimentation_b<NW>(C, K, valid, ck[it][1], Pg, m1_b, ice_c, snow_c, graupel_c, vtg_b, vts_b, Sb, Ab);
-      }
-      // geometry: denfac = sqrt(SFCRHO / den), den = den0 dz0 / dz1,
-      // dz1 = dz0 tz / t0, dz = heights(-dz1), den0 = -dp1 / (g dz0)
-      if (valid) {
-        const double den0 = -Pg.dp1 / (K.GRAV * dz0);
-        const double den_b = Ab.den - Ab.denfac * 0.5 * Pg.denfac / Pg.den;
-        double dz1_b = -Ab.dz;
-        const double den0_b = den_b * dz0 / Pg.dz1;
-        dz0_b += den_b * den0 / Pg.dz1;
-        dz1_b -= den_b * Pg.den / Pg.dz1;
-        dz0_b += dz1_b * ck[it][0].tz / pt;
-        Sb.tz += dz1_b * dz0 / pt;
-        pt_b -= dz1_b * Pg.dz1 / pt;
-        Ab.dp1 -= den0_b / (K.GRAV * dz0);
-        dz0_b += den0_b * Pg.dp1 / (K.GRAV * dz0 * dz0);
-      }
-    }
-
-    // ----------------------------------------------------- fields_init reverse
+    for (int n = 0; n < 6; ++n) qin_b[n] = AS(AS_QIN0 + n);
+    const double qa0_b = AS(AS_QA0), u0_b = AS(AS_U0), v0_b = AS(AS_V0), qa_b = AS(AS_QA);
     // replay to the state before fix_negative, then reverse the fix
     const double omq = delp / P.dp1;
     LevState S0{qin[0] * omq, qin[1] * omq, qin[2] * omq, qin[3] * omq, qin[4] * omq, qin[5] * omq, pt,
@@ -932,31 +1274,51 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) mp_vjp_kernel(const __grid_
     }
   }
   __syncthreads();
-  store_tiles<NW, G, N_VJP_GRAD>(A.grad, sm + SM::out, A.ncol, A.nx, L, c0);
+  store_tiles<NW, G, N_VJP_GRAD>(A.grad, sm + (size_t)N_VJP_IN * G * RP, A.ncol, A.nx, L, c0);
 }
 
+// ---------------------------------------------------------------- launch
 template <int NW, int G, int MINB>
 cudaError_t launch_vjp(const VjpArgs& A, cudaStream_t st) {
-  auto kern = mp_vjp_kernel<NW, G, MINB>;
-  const size_t smem = VjpSmem<NW, G>::bytes;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  using SR = ColSmem<NW, G, NT_IN, 2>;
+  using SC = ColSmem<NW, G, 0, 0>;
+  using SI = ColSmem<NW, G, N_VJP_IN + N_VJP_GRAD, 4>;
+  cudaError_t e = cudaFuncSetAttribute(vjp_replay_kernel<NW, G, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)SR::bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(vjp_init_kernel<NW, G, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)SI::bytes);
   if (e != cudaSuccess) return e;
-  const int64_t nblk = (A.ncol + G - 1) / G;
-  kern<<<(unsigned)nblk, 32 * NW * G, smem, st>>>(A);
+  const unsigned nblk = (unsigned)((A.ncol + G - 1) / G);
+  const int64_t npts = (int64_t)A.nz * A.ncol;
+  const unsigned pblk = (unsigned)((npts + PT_THREADS - 1) / PT_THREADS);
+  constexpr int T = 32 * NW * G;
+  vjp_replay_kernel<NW, G, MINB><<<nblk, T, SR::bytes, st>>>(A);
+  for (int it = A.K.ntimes - 1; it >= 0; --it) {
+    vjp_icloud_pt<<<pblk, PT_THREADS, 0, st>>>(A, it);
+    vjp_autoconv_pt<1><<<pblk, PT_THREADS, 0, st>>>(A, it);
+    vjp_revap2_pt<<<pblk, PT_THREADS, 0, st>>>(A, it, 1);
+    vjp_fall_kernel<NW, G, MINB><<<nblk, T, SC::bytes, st>>>(A, it, 1);
+    vjp_revap1_pt<<<pblk, PT_THREADS, 0, st>>>(A, it, 1);
+    vjp_sed_kernel<NW, G, MINB><<<nblk, T, SC::bytes, st>>>(A, it);
+    vjp_autoconv_pt<0><<<pblk, PT_THREADS, 0, st>>>(A, it);
+    vjp_revap2_pt<<<pblk, PT_THREADS, 0, st>>>(A, it, 0);
+    vjp_fall_kernel<NW, G, MINB><<<nblk, T, SC::bytes, st>>>(A, it, 0);
+    vjp_revap1_pt<<<pblk, PT_THREADS, 0, st>>>(A, it, 0);
+  }
+  vjp_init_kernel<NW, G, MINB><<<nblk, T, SI::bytes, st>>>(A);
   return cudaGetLastError();
 }
 
 }  // namespace
 
-int mp_vjp_max_substeps() { return VJP_MAXNT; }
+int mp_vjp_launches(int ntimes) { return 2 + 10 * ntimes; }
 
 cudaError_t mp_launch_vjp(const VjpArgs& A, cudaStream_t st) {
   const int L = A.nz;
-  if (L <= 32) return launch_vjp<1, 2, SHIELD_VJP_MINB>(A, st);
-  if (L <= 64) return launch_vjp<2, 2, SHIELD_VJP_MINB>(A, st);
-  if (L <= 96) return launch_vjp<3, SHIELD_VJP_G3, SHIELD_VJP_MINB>(A, st);
-  // 3 columns of 4 warps: 12 warps share each instruction fetch, as at L79
-  // (C48 L127: 14.2 ms against 25.9 ms with one column per block)
+  if (L <= 32) return launch_vjp<1, 2, 1>(A, st);
+  if (L <= 64) return launch_vjp<2, 2, 1>(A, st);
+  if (L <= 96) return launch_vjp<3, 4, 1>(A, st);
   if (L <= 128) return launch_vjp<4, 3, 1>(A, st);
   return launch_vjp<8, 1, 1>(A, st);
 }

@@ -277,6 +277,9 @@ def test_vjp_rejects_unsupported_configs():
     mp, pc, x, land, area = _setup(4, 4, 79, 150.0, 18, do_sedi_heat=True)
     with pytest.raises(ShieldError, match="do_sedi_heat"):
         step_vjp(mp, x, land, [None] * len(OUTPUTS), 150.0)
-    mp, pc, x, land, area = _setup(4, 4, 79, 750.0, 18, mp_time=150.0)
-    with pytest.raises(ShieldError, match="sub-steps"):
-        step_vjp(mp, x, land, [None] * len(OUTPUTS), 750.0)
+
+
+def test_exact_five_substeps():
+    # dt = 750 s with mp_time = 150 s: five sub-steps, whose records the
+    # workspace holds like any other count
+    _assert_exact(exact_check(6, 4, 79, 750.0, 19, mp_time=150.0))

@@ -60,7 +60,9 @@ enum VjpSubScalar {
 // per sub-step and column: the rain-fall decisions of the two passes (0 / 1)
 enum VjpSubColumn { SCC_FALL_A, SCC_FALL_B, N_SCC };
 // per point, once: fields_init's dry mass and pressure
-enum VjpStepPoint { SP_DP1, SP_P1, N_SP };
+// per point, once: fields_init's dry mass and pressure, the precipitation
+// flux summed over the sub-steps, and the final state (8)
+enum VjpStepPoint { SP_DP1, SP_P1, SP_M1, SP_FIN, N_SP = SP_FIN + 8 };
 // per column, once: fields_init's column values
 enum VjpStepColumn { SC_HVAR, SC_RHADJ, SC_RHRAIN, SC_CCN, SC_CPRAUT, N_SC };
 // per point: the adjoint state carried between the launches
@@ -134,6 +136,7 @@ struct VjpRec {
 };
 
 constexpr int NT_IN = N_VJP_IN + N_VJP_COT;
+constexpr int NT_UPD = NT_IN + 10;  // the update launch's tiles: inputs, cotangents, final state, dp1, m1
 
 // load NF fields into tiles [f * G + g][k] (all loads issued before any
 // store); a field with a null pointer reads as zero
@@ -589,75 +592,121 @@ SHD Column<NW> column_of(double* sm, int L, int& g) {
   return C;
 }
 
-// forward stages of the replay, out of line (one copy each)
-template <int NW>
-static __device__ __noinline__ void fwd_warm_rain(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid,
-                                                  LevState& S, const StepGeom& P, double& vtr, double& m1r,
-                                                  double& r1, VjpRec rec) {
-  warm_rain<false>(C, K, KF, valid, S, P, vtr, m1r, r1, nullptr, rec);
+// The column launches move their workspace fields through shared-memory
+// tiles (field f, block column g, level k at (f * G + g) * RP + k):
+// consecutive threads take consecutive columns of one level, so that a warp
+// reads or writes whole sectors, and every load of a launch is issued before
+// any of its arithmetic. 32 NW G >= G L threads: one element per thread and
+// field. A null source reads as zero; a null destination is not written.
+template <int NW, int G, int NF>
+SHD void ws_gather(const double* const (&src)[NF], double* tiles, int64_t ncol, int L, int64_t c0) {
+  constexpr int RP = Tiles<NW>::RP;
+  const int tid = threadIdx.x, g = tid % G, k = tid / G;
+  const bool ok = k < L && c0 + g < ncol;
+  const int64_t o = (int64_t)k * ncol + c0 + g;
+  double v[NF];
+#pragma unroll
+  for (int f = 0; f < NF; ++f) v[f] = (ok && src[f]) ? src[f][o] : 0.0;
+  if (ok) {
+#pragma unroll
+    for (int f = 0; f < NF; ++f) tiles[(f * G + g) * RP + k] = v[f];
+  }
 }
-template <int NW>
-static __device__ __noinline__ void fwd_sedimentation(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid,
-                                                      LevState& S, const StepGeom& P, double& vtg, double& vts,
-                                                      double& m1s, double& ice, double& snow, double& graupel) {
-  sedimentation<false>(C, K, KF, valid, S, P, vtg, vts, m1s, ice, snow, graupel);
-}
-template <int NW>
-static __device__ __noinline__ void fwd_icloud(Column<NW>& C, const MpConst& K, const MpConstF& KF, bool valid,
-                                               LevState& S, const StepGeom& P, double& qa, double vtg, double vtr,
-                                               double vts, VjpRec rec) {
-  icloud<false>(C, K, KF, valid, S, P, qa, vtg, vtr, vts, rec);
+template <int NW, int G, int NF>
+SHD void ws_scatter(double* const (&dst)[NF], const double* tiles, int64_t ncol, int L, int64_t c0) {
+  constexpr int RP = Tiles<NW>::RP;
+  const int tid = threadIdx.x, g = tid % G, k = tid / G;
+  if (!(k < L && c0 + g < ncol)) return;
+  const int64_t o = (int64_t)k * ncol + c0 + g;
+#pragma unroll
+  for (int f = 0; f < NF; ++f)
+    if (dst[f]) dst[f][o] = tiles[(f * G + g) * RP + k];
 }
 
-// 1. The replay with its records, then the reverse of fields_update.
-template <int NW, int G, int MINB>
-__global__ void __launch_bounds__(32 * NW * G, MINB) vjp_replay_kernel(const __grid_constant__ VjpArgs A) {
+// 1a. The replay with its records, on the forward step's own thread layout
+// LY (so that its vertical sums round as the forward's do): one block's G
+// columns staged into shared memory as the forward kernel stages them.
+template <class LY>
+struct ReplaySmem {
+  static constexpr size_t scratch = (size_t)N_VJP_IN * LY::G * LY::RP;
+  static constexpr size_t work = scratch + (size_t)LY::NGRP * 2 * LY::SCR;
+  static constexpr size_t bytes = (work + (size_t)LY::NGRP * LY::WORK) * sizeof(double);
+};
+
+template <class LY, int MINB>
+__global__ void __launch_bounds__(LY::THREADS, MINB) vjp_replay_kernel(const __grid_constant__ VjpArgs A) {
   extern __shared__ double sm[];
-  constexpr int RP = Tiles<NW>::RP;
+  using SM = ReplaySmem<LY>;
+  constexpr int RP = LY::RP, G = LY::G;
   const MpConst& K = A.K;
   const MpConstF& KF = A.KF;
   const int L = A.nz;
   const int64_t c0 = (int64_t)blockIdx.x * G;
-  load_tiles<NW, G, N_VJP_IN>(A.in, sm, A.ncol, A.nx, L, c0);
-  load_tiles<NW, G, N_VJP_COT>(A.cot, sm + (size_t)N_VJP_IN * G * RP, A.ncol, A.nx, L, c0);
+  {
+    // element e < G L of each input tile (i-fastest storages: consecutive
+    // columns on consecutive threads; k-fastest: consecutive levels)
+    const int tid = threadIdx.x;
+    const int g = tid % G, k = tid / G, gk = tid / L, kk = tid % L;
+    const bool ok = c0 + g < A.ncol && k < L, okk = gk < G && c0 + gk < A.ncol;
+    const int64_t i = ok ? (c0 + g) % A.nx : 0, j = ok ? (c0 + g) / A.nx : 0;
+    const int64_t ik = okk ? (c0 + gk) % A.nx : 0, jk = okk ? (c0 + gk) / A.nx : 0;
+    double v[N_VJP_IN];
+#pragma unroll
+    for (int f = 0; f < N_VJP_IN; ++f) {
+      const Fld3 F = A.in[f];
+      v[f] = 0.0;
+      if (F.sk == 1) {
+        if (okk) v[f] = F.p[ik * F.si + jk * F.sj + kk];
+      } else if (ok) {
+        v[f] = F.p[i * F.si + j * F.sj + (int64_t)k * F.sk];
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < N_VJP_IN; ++f) {
+      if (A.in[f].sk == 1) {
+        if (okk) sm[(f * G + gk) * RP + kk] = v[f];
+      } else if (ok) {
+        sm[(f * G + g) * RP + k] = v[f];
+      }
+    }
+  }
   __syncthreads();
-  int g;
-  Column<NW> C = column_of<NW, G, NT_IN, 2>(sm, L, g);
-  const int64_t col = c0 + g;
+  typename LY::Col C;
+  const int g = LY::setup(C, threadIdx.x, L, sm + SM::scratch, sm + SM::work);
+  const bool slot_ok = g < G;
+  const int64_t col = c0 + (slot_ok ? g : 0);
+  const bool col_ok = slot_ok && col < A.ncol;
   const int k = C.k;
-  const bool valid = k < L;
-  const double* tile = sm + (size_t)g * RP + k;
+  const bool valid = col_ok && k < L;
+  const double* tile = sm + (size_t)(slot_ok ? g : 0) * RP + (valid ? k : 0);
   auto TI = [&](int f, double dflt) -> double { return valid ? tile[(size_t)f * G * RP] : dflt; };
-  auto TC = [&](int f) -> double { return valid ? tile[(size_t)(N_VJP_IN + f) * G * RP] : 0.0; };
-  if (col >= A.ncol) return;  // the whole column group (no block-wide barrier follows)
   const Ws W = workspace(A);
   const int64_t np = W.npts;
-  const int64_t p = (int64_t)(valid ? k : 0) * A.ncol + col;
-  const int64_t ci = col % A.nx, cj = col / A.nx;
+  const int64_t cc = col_ok ? col : 0;
+  const int64_t p = (int64_t)(valid ? k : 0) * A.ncol + cc;
+  const bool head = col_ok && k == 0;
+  const int64_t ci = cc % A.nx, cj = cc / A.nx;
   const double land = A.land.p[ci * A.land.si + cj * A.land.sj];
   const double area = A.area.p[ci * A.area.si + cj * A.area.sj];
-  const double pt = TI(IN_PT, 250.0), delp = TI(IN_DELP, 1.0), dz0 = TI(IN_DELZ, -100.0);
-  const double qin[6] = {TI(IN_QV, 0.0), TI(IN_QL, 0.0), TI(IN_QR, 0.0), TI(IN_QI, 0.0), TI(IN_QS, 0.0),
-                         TI(IN_QG, 0.0)};
-  // ------------------------------------------------------ forward replay
+  const double pt = TI(IN_PT, 250.0), dz0 = TI(IN_DELZ, -100.0);
   LevState S;
   StepGeom P;
   P.den = 1.0;
   P.denfac = 1.0;
   P.dz1 = -100.0;
   P.dz = 100.0;
-  fields_init(C, K, valid, pt, qin[0], qin[1], qin[2], qin[3], qin[4], qin[5], delp, TI(IN_W, 0.0), dz0, land, area,
-              S, P);
+  fields_init(C, K, valid, pt, TI(IN_QV, 0.0), TI(IN_QL, 0.0), TI(IN_QR, 0.0), TI(IN_QI, 0.0), TI(IN_QS, 0.0),
+              TI(IN_QG, 0.0), TI(IN_DELP, 1.0), TI(IN_W, 0.0), dz0, land, area, S, P);
   if (valid) {
     W.sp(SP_DP1)[p] = P.dp1;
     W.sp(SP_P1)[p] = P.p1;
   }
-  if (k == 0) {
-    W.sc(SC_HVAR)[col] = P.h_var;
-    W.sc(SC_RHADJ)[col] = P.rh_adj;
-    W.sc(SC_RHRAIN)[col] = P.rh_rain;
-    W.sc(SC_CCN)[col] = P.ccn;
-    W.sc(SC_CPRAUT)[col] = P.c_praut;
+  if (head) {
+    W.sc(SC_HVAR)[cc] = P.h_var;
+    W.sc(SC_RHADJ)[cc] = P.rh_adj;
+    W.sc(SC_RHRAIN)[cc] = P.rh_rain;
+    W.sc(SC_CCN)[cc] = P.ccn;
+    W.sc(SC_CPRAUT)[cc] = P.c_praut;
   }
   double m1 = 0.0, m1_sol = 0.0, vtr = VF_MIN, vtg = VF_MIN, vts = VF_MIN, qa = 0.0, ice = 0.0, snow = 0.0,
          graupel = 0.0;
@@ -672,33 +721,79 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_replay_kernel(const __g
       W.ss(it, SS_DZ1)[p] = P.dz1;
       store_lev(W.ck(it, CK_E0) + p, np, S);
     }
-    double m1r, r1;
-    fwd_warm_rain<NW>(C, K, KF, valid, S, P, vtr, m1r, r1,
-                      VjpRec{W.ck(it, CK_W1A) + p, W.ss(it, SS_SL_A) + p, W.scc(it, SCC_FALL_A) + col, np, valid,
-                             k == 0});
-    m1 = m1 + m1r;
-    if (valid) {
-      W.ss(it, SS_VTR_A)[p] = vtr;
-      store_lev(W.ck(it, CK_E1) + p, np, S);
+    // the first warm_rain pass, sedimentation, the second pass (one copy of
+    // the warm_rain code, run twice, as in the forward kernel)
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass) {
+      double m1r, r1;
+      warm_rain<false>(C, K, KF, valid, S, P, vtr, m1r, r1, nullptr,
+                       VjpRec{W.ck(it, pass ? CK_W1B : CK_W1A) + p, W.ss(it, pass ? SS_SL_B : SS_SL_A) + p,
+                              W.scc(it, pass ? SCC_FALL_B : SCC_FALL_A) + cc, np, valid, head});
+      m1 = (pass == 0) ? m1 + m1r : m1 + m1r + m1_sol;
+      if (valid) {
+        W.ss(it, pass ? SS_VTR_B : SS_VTR_A)[p] = vtr;
+        store_lev(W.ck(it, pass ? CK_E3 : CK_E1) + p, np, S);
+      }
+      if (pass == 1) break;
+      sedimentation<false>(C, K, KF, valid, S, P, vtg, vts, m1_sol, ice, snow, graupel);
+      if (valid) {
+        W.ss(it, SS_VTG)[p] = vtg;
+        W.ss(it, SS_VTS)[p] = vts;
+        store_lev(W.ck(it, CK_E2) + p, np, S);
+      }
     }
-    fwd_sedimentation<NW>(C, K, KF, valid, S, P, vtg, vts, m1_sol, ice, snow, graupel);
-    if (valid) {
-      W.ss(it, SS_VTG)[p] = vtg;
-      W.ss(it, SS_VTS)[p] = vts;
-      store_lev(W.ck(it, CK_E2) + p, np, S);
-    }
-    fwd_warm_rain<NW>(C, K, KF, valid, S, P, vtr, m1r, r1,
-                      VjpRec{W.ck(it, CK_W1B) + p, W.ss(it, SS_SL_B) + p, W.scc(it, SCC_FALL_B) + col, np, valid,
-                             k == 0});
-    m1 = m1 + m1r + m1_sol;
-    if (valid) {
-      W.ss(it, SS_VTR_B)[p] = vtr;
-      store_lev(W.ck(it, CK_E3) + p, np, S);
-    }
-    fwd_icloud<NW>(C, K, KF, valid, S, P, qa, vtg, vtr, vts,
-                   VjpRec{W.ck(it, CK_E4) + p, W.ss(it, SS_SL_I) + p, nullptr, np, valid, false});
+    icloud<false>(C, K, KF, valid, S, P, qa, vtg, vtr, vts,
+                  VjpRec{W.ck(it, CK_E4) + p, W.ss(it, SS_SL_I) + p, nullptr, np, valid, false});
   }
+  if (valid) {
+    W.sp(SP_M1)[p] = m1;
+    store_lev(W.sp(SP_FIN) + p, np, S);
+  }
+}
 
+// 1b. fields_update reversed (:1452-1553), including the momentum scan,
+// from the replay's final state; starts the adjoint state.
+template <int NW, int G, int MINB>
+__global__ void __launch_bounds__(32 * NW * G, MINB) vjp_update_kernel(const __grid_constant__ VjpArgs A) {
+  extern __shared__ double sm[];
+  constexpr int RP = Tiles<NW>::RP;
+  const MpConst& K = A.K;
+  const int L = A.nz;
+  const int64_t c0 = (int64_t)blockIdx.x * G;
+  load_tiles<NW, G, N_VJP_IN>(A.in, sm, A.ncol, A.nx, L, c0);
+  load_tiles<NW, G, N_VJP_COT>(A.cot, sm + (size_t)N_VJP_IN * G * RP, A.ncol, A.nx, L, c0);
+  const Ws W = workspace(A);
+  const int64_t np = W.npts;
+  {
+    const double* fin = W.sp(SP_FIN);
+    const double* src[10] = {fin, fin + np, fin + 2 * np, fin + 3 * np, fin + 4 * np, fin + 5 * np, fin + 6 * np,
+                             fin + 7 * np, W.sp(SP_DP1), W.sp(SP_M1)};
+    ws_gather<NW, G, 10>(src, sm + (size_t)NT_IN * G * RP, A.ncol, L, c0);
+  }
+  __syncthreads();
+  int g;
+  Column<NW> C = column_of<NW, G, NT_UPD, 0>(sm, L, g);
+  const int64_t col = c0 + g;
+  const int k = C.k;
+  const bool valid = k < L;
+  const double* tile = sm + (size_t)g * RP + k;
+  auto TI = [&](int f, double dflt) -> double { return valid ? tile[(size_t)f * G * RP] : dflt; };
+  auto TC = [&](int f) -> double { return valid ? tile[(size_t)(N_VJP_IN + f) * G * RP] : 0.0; };
+  // the adjoint state's fields AS_QV .. AS_M1, written through tiles 0 ..
+  // N_UPD_OUT - 1 once every tile has been read
+  constexpr int N_UPD_OUT = AS_M1 + 1;
+  double outv[N_UPD_OUT];
+#pragma unroll
+  for (int f = 0; f < N_UPD_OUT; ++f) outv[f] = 0.0;
+  if (col < A.ncol) {  // uniform over the column group
+  auto TW = [&](int f, double dflt) -> double { return valid ? tile[(size_t)(NT_IN + f) * G * RP] : dflt; };
+  const double pt = TI(IN_PT, 250.0), delp = TI(IN_DELP, 1.0);
+  const double qin[6] = {TI(IN_QV, 0.0), TI(IN_QL, 0.0), TI(IN_QR, 0.0), TI(IN_QI, 0.0), TI(IN_QS, 0.0),
+                         TI(IN_QG, 0.0)};
+  const LevState S{TW(0, 0.0), TW(1, 0.0), TW(2, 0.0), TW(3, 0.0), TW(4, 0.0), TW(5, 0.0), TW(6, 250.0), TW(7, 0.0)};
+  StepGeom P;
+  P.dp1 = TW(8, 1.0);
+  const double m1 = TW(9, 0.0);
   // ------------------------------------------------- fields_update reverse
   const double rdt = K.rdt;
   LevState Sb{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -792,23 +887,36 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_replay_kernel(const __g
     C.template nextN<1>(mv, mn);
     m1_b = (valid && k < L - 1) ? mn[0] : 0.0;
   }
-  if (valid) {
-    store_lev(W.as(AS_QV) + p, np, Sb);
-    W.as(AS_DP1)[p] = dp1_b;
-    W.as(AS_P1)[p] = 0.0;
-    W.as(AS_CCN)[p] = 0.0;
-    W.as(AS_CPRAUT)[p] = 0.0;
-    W.as(AS_PT)[p] = pt_b;
-    W.as(AS_DELP)[p] = delp_b;
-    W.as(AS_DZ0)[p] = 0.0;
+  outv[AS_QV] = Sb.qv;
+  outv[AS_QL] = Sb.ql;
+  outv[AS_QR] = Sb.qr;
+  outv[AS_QI] = Sb.qi;
+  outv[AS_QS] = Sb.qs;
+  outv[AS_QG] = Sb.qg;
+  outv[AS_TZ] = Sb.tz;
+  outv[AS_W] = Sb.w;
+  outv[AS_DP1] = dp1_b;
+  outv[AS_PT] = pt_b;
+  outv[AS_DELP] = delp_b;
 #pragma unroll
-    for (int n = 0; n < 6; ++n) W.as(AS_QIN0 + n)[p] = qin_b[n];
-    W.as(AS_QA)[p] = qa_b;
-    W.as(AS_QA0)[p] = qa0_b;
-    W.as(AS_U0)[p] = u0_b;
-    W.as(AS_V0)[p] = v0_b;
-    W.as(AS_M1)[p] = m1_b;
+  for (int n = 0; n < 6; ++n) outv[AS_QIN0 + n] = qin_b[n];
+  outv[AS_QA] = qa_b;
+  outv[AS_QA0] = qa0_b;
+  outv[AS_U0] = u0_b;
+  outv[AS_V0] = v0_b;
+  outv[AS_M1] = m1_b;
   }
+  __syncthreads();
+  if (col < A.ncol && valid) {
+    double* t = sm + (size_t)g * RP + k;
+#pragma unroll
+    for (int f = 0; f < N_UPD_OUT; ++f) t[(size_t)f * G * RP] = outv[f];
+  }
+  __syncthreads();
+  double* dst[N_UPD_OUT];
+#pragma unroll
+  for (int f = 0; f < N_UPD_OUT; ++f) dst[f] = W.as(f);
+  ws_scatter<NW, G, N_UPD_OUT>(dst, sm, A.ncol, L, c0);
 }
 
 // ------------------------------------------------------- point launches
@@ -834,11 +942,36 @@ SHD bool point_of(const Ws& W, PointIdx& q) {
   return true;
 }
 
-// 2a. icloud reversed from its recorded states: the saturation adjustment
-// and the ice processes. Leaves the state's cotangent with respect to the
-// melted / frozen state without the ice slope's part, the cotangents of
-// melting / freezing's other outputs and of the slope, and the fall speeds'.
+// 2a. icloud's saturation adjustment reversed (subgrid_z_proc,
+// microphysics_funcs.py:431-850) from the recorded state before it. Its own
+// launch, ahead of the ice processes': each launch's code is half as long
+// (C48 L79: 0.81 + 0.33 ms, against 1.46 ms for the two in one launch).
 // Starts the sub-step's geometry cotangents.
+__global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_subgrid_pt(const __grid_constant__ VjpArgs A,
+                                                                                 int it) {
+  const Ws W = workspace(A);
+  PointIdx q;
+  if (!point_of(W, q)) return;
+  const int64_t p = q.p, np = W.npts, col = q.col;
+  const MpConst& K = A.K;
+  const LevState E4 = load_lev(W.ck(it, CK_E4) + p, np);
+  const double den = W.ss(it, SS_DEN)[p], denfac = W.ss(it, SS_DENFAC)[p], p1 = W.sp(SP_P1)[p];
+  const double h_var = W.sc(SC_HVAR)[col], rh_adj = W.sc(SC_RHADJ)[col], rh_rain = W.sc(SC_RHRAIN)[col];
+  LevState Sb = load_lev(W.as(AS_QV) + p, np);
+  const double qa_b = W.as(AS_QA)[p];
+  double den_b = 0.0, denfac_b = 0.0;
+  subgrid_z_proc_b(K, h_var, rh_adj, rh_rain, qa_b, E4.qg, E4.qi, E4.ql, E4.qr, E4.qs, E4.qv, E4.tz, den, denfac, p1,
+                   Sb.qg, Sb.qi, Sb.ql, Sb.qr, Sb.qs, Sb.qv, Sb.tz, den_b, denfac_b);
+  store_lev(W.as(AS_QV) + p, np, Sb);
+  W.as(AS_DEN)[p] = den_b;
+  W.as(AS_DENFAC)[p] = denfac_b;
+}
+
+// 2b. icloud's melting / freezing and ice processes reversed
+// (microphysics.py:1220-1449, icloud_main: microphysics_funcs.py:853-1260).
+// Leaves the state's cotangent with respect to the melted / frozen state
+// without the ice slope's part, the cotangents of melting / freezing's
+// other outputs, of the slope and of the fall speeds.
 __global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_icloud_pt(const __grid_constant__ VjpArgs A,
                                                                                 int it) {
   const Ws W = workspace(A);
@@ -847,13 +980,11 @@ __global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_icloud_pt(
   const int64_t p = q.p, np = W.npts, col = q.col;
   const MpConst& K = A.K;
   const LevState E3 = load_lev(W.ck(it, CK_E3) + p, np);
-  const LevState E4 = load_lev(W.ck(it, CK_E4) + p, np);
   const double den = W.ss(it, SS_DEN)[p], denfac = W.ss(it, SS_DENFAC)[p], p1 = W.sp(SP_P1)[p];
-  const double h_var = W.sc(SC_HVAR)[col], rh_adj = W.sc(SC_RHADJ)[col], rh_rain = W.sc(SC_RHRAIN)[col];
+  const double h_var = W.sc(SC_HVAR)[col];
   const double vtg = W.ss(it, SS_VTG)[p], vtr = W.ss(it, SS_VTR_B)[p], vts = W.ss(it, SS_VTS)[p];
   LevState Sb = load_lev(W.as(AS_QV) + p, np);
-  const double qa_b = W.as(AS_QA)[p];
-  double den_b = 0.0, denfac_b = 0.0;
+  const double den_b = W.as(AS_DEN)[p], denfac_b = W.as(AS_DENFAC)[p];
   LevState S1 = E3;
   double q_liq, q_sol, cvm;
   icloud_melt_freeze(K, S1.qv, S1.ql, S1.qr, S1.qi, S1.qs, S1.qg, S1.tz, den, q_liq, q_sol, cvm);
@@ -864,8 +995,6 @@ __global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_icloud_pt(
     sl = W.ss(it, SS_SL_I)[p];
     di = fmax(sl, inner);
   }
-  subgrid_z_proc_b(K, h_var, rh_adj, rh_rain, qa_b, E4.qg, E4.qi, E4.ql, E4.qr, E4.qs, E4.qv, E4.tz, den, denfac, p1,
-                   Sb.qg, Sb.qi, Sb.ql, Sb.qr, Sb.qs, Sb.qv, Sb.tz, den_b, denfac_b);
   const IcState Z0{S1.qg, S1.qi, S1.ql, S1.qr, S1.qs, S1.tz, q_liq, q_sol, cvm};
   const IcIn I{S1.qv, den, denfac, vtg, vtr, vts, p1, di};
   IcState Zb{Sb.qg, Sb.qi, Sb.ql, Sb.qr, Sb.qs, Sb.tz, 0.0, 0.0, 0.0};
@@ -897,7 +1026,7 @@ __global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_icloud_pt(
   W.as(AS_SLI)[p] = sl_b;
 }
 
-// 2b. Autoconversion of a warm_rain pass reversed (microphysics.py:559-653),
+// 2c. Autoconversion of a warm_rain pass reversed (microphysics.py:559-653),
 // without the liquid slope's transpose; for the second pass, first the end
 // of icloud's reverse: the ice slope's transpose and melting / freezing.
 template <int PASS>
@@ -944,7 +1073,7 @@ __global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_autoconv_p
   W.as(AS_SLL)[p] = sl_b;
 }
 
-// 2c. The liquid slope's transpose, then the second evaporation / accretion
+// 2d. The liquid slope's transpose, then the second evaporation / accretion
 // of a warm_rain pass reversed (columns with falling rain).
 __global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_revap2_pt(const __grid_constant__ VjpArgs A,
                                                                                 int it, int pass) {
@@ -968,7 +1097,7 @@ __global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_revap2_pt(
   store_lev(W.as(AS_QV) + p, np, Sb);
 }
 
-// 2e. The first evaporation / accretion and the fall speed of a warm_rain
+// 2f. The first evaporation / accretion and the fall speed of a warm_rain
 // pass reversed (columns with falling rain); after the first pass, the
 // reverse of the sub-step geometry (density, fall factor, layer thickness
 // from the entry temperature: warm_rain with is_first, :349-380).
@@ -1025,76 +1154,152 @@ __global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_revap1_pt(
 // that a zero cotangent stays zero through the scans).
 SHD LevState pad_state() { return LevState{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 250.0, 0.0}; }
 
-// 2d. The rain fall of a warm_rain pass reversed (columns with falling rain).
+// 2e. The rain fall of a warm_rain pass reversed (columns with falling rain).
+// Tiles, read-only first: W1 (8), dp1, dz, the fall speed, the flux's
+// cotangent, icloud's fall-speed cotangent; then read and written: the
+// state's cotangent (8), the geometry's dz and dp1 cotangents, the fall
+// speed's cotangent (written only).
+enum FallTile { FT_W1 = 0, FT_DP1 = 8, FT_DZ, FT_VTR, FT_M1, FT_VTRB, FT_OUT, FT_SB = FT_OUT, FT_ADZ = FT_SB + 8,
+                FT_ADP1, FT_VTT, N_FT };
 template <int NW, int G, int MINB>
 __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_fall_kernel(const __grid_constant__ VjpArgs A, int it,
                                                                      int pass) {
   extern __shared__ double sm[];
+  constexpr int RP = Tiles<NW>::RP;
   const int L = A.nz;
-  int g;
-  Column<NW> C = column_of<NW, G, 0, 0>(sm, L, g);
-  const int64_t col = (int64_t)blockIdx.x * G + g;
-  if (col >= A.ncol) return;  // the whole column group
+  const int64_t c0 = (int64_t)blockIdx.x * G;
   const Ws W = workspace(A);
-  if (W.scc(it, pass ? SCC_FALL_B : SCC_FALL_A)[col] == 0.0) return;  // the whole column group
-  const MpConst& K = A.K;
-  const int k = C.k;
-  const bool valid = k < L;
-  const int64_t np = W.npts, p = (int64_t)(valid ? k : 0) * A.ncol + col;
-  const LevState W1 = valid ? load_lev(W.ck(it, pass ? CK_W1B : CK_W1A) + p, np) : pad_state();
-  StepGeom P;
-  P.dp1 = valid ? W.sp(SP_DP1)[p] : 1.0;
-  P.dz = valid ? W.ss(it, SS_DZ)[p] : 100.0;
-  const double vtr = valid ? W.ss(it, pass ? SS_VTR_B : SS_VTR_A)[p] : VF_MIN;
-  LevState Sb = valid ? load_lev(W.as(AS_QV) + p, np) : LevState{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  StepAdj Ab{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  const double m1_b = valid ? W.as(AS_M1)[p] : 0.0;
-  const double rain_c = A.rain_b ? A.rain_b[col] * (86400.0 * K.rdt * K.RGRAV) : 0.0;
-  double vt_b = (pass == 1 && valid) ? W.as(AS_VTR)[p] : 0.0;
-  rain_fall_b<NW>(C, K, valid, W1, P, vtr, m1_b, rain_c, Sb, Ab, vt_b);
-  if (valid) {
-    store_lev(W.as(AS_QV) + p, np, Sb);
-    W.as(AS_DZ)[p] += Ab.dz;
-    W.as(AS_DP1)[p] += Ab.dp1;
-    W.as(AS_VTT)[p] = vt_b;
+  const int64_t np = W.npts;
+  const double* w1 = W.ck(it, pass ? CK_W1B : CK_W1A);
+  double* sb = W.as(AS_QV);
+  {
+    const double* src[N_FT] = {w1, w1 + np, w1 + 2 * np, w1 + 3 * np, w1 + 4 * np, w1 + 5 * np, w1 + 6 * np,
+                               w1 + 7 * np, W.sp(SP_DP1), W.ss(it, SS_DZ), W.ss(it, pass ? SS_VTR_B : SS_VTR_A),
+                               W.as(AS_M1), pass ? W.as(AS_VTR) : nullptr, sb, sb + np, sb + 2 * np, sb + 3 * np,
+                               sb + 4 * np, sb + 5 * np, sb + 6 * np, sb + 7 * np, W.as(AS_DZ), W.as(AS_DP1),
+                               nullptr};
+    ws_gather<NW, G, N_FT>(src, sm, A.ncol, L, c0);
   }
+  __syncthreads();
+  int g;
+  Column<NW> C = column_of<NW, G, N_FT, 0>(sm, L, g);
+  const int64_t col = c0 + g;
+  // uniform over the column group
+  if (col < A.ncol && W.scc(it, pass ? SCC_FALL_B : SCC_FALL_A)[col] != 0.0) {
+    const MpConst& K = A.K;
+    const int k = C.k;
+    const bool valid = k < L;
+    double* tile = sm + (size_t)g * RP + (valid ? k : 0);
+    auto T = [&](int f) -> double& { return tile[(size_t)f * G * RP]; };
+    const LevState W1 = valid ? LevState{T(FT_W1), T(FT_W1 + 1), T(FT_W1 + 2), T(FT_W1 + 3), T(FT_W1 + 4),
+                                         T(FT_W1 + 5), T(FT_W1 + 6), T(FT_W1 + 7)}
+                              : pad_state();
+    StepGeom P;
+    P.dp1 = valid ? T(FT_DP1) : 1.0;
+    P.dz = valid ? T(FT_DZ) : 100.0;
+    const double vtr = valid ? T(FT_VTR) : VF_MIN;
+    LevState Sb{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (valid)
+      Sb = LevState{T(FT_SB), T(FT_SB + 1), T(FT_SB + 2), T(FT_SB + 3), T(FT_SB + 4), T(FT_SB + 5), T(FT_SB + 6),
+                    T(FT_SB + 7)};
+    StepAdj Ab{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const double m1_b = valid ? T(FT_M1) : 0.0;
+    const double rain_c = A.rain_b ? A.rain_b[col] * (86400.0 * K.rdt * K.RGRAV) : 0.0;
+    double vt_b = valid ? T(FT_VTRB) : 0.0;
+    rain_fall_b<NW>(C, K, valid, W1, P, vtr, m1_b, rain_c, Sb, Ab, vt_b);
+    if (valid) {
+      T(FT_SB) = Sb.qv;
+      T(FT_SB + 1) = Sb.ql;
+      T(FT_SB + 2) = Sb.qr;
+      T(FT_SB + 3) = Sb.qi;
+      T(FT_SB + 4) = Sb.qs;
+      T(FT_SB + 5) = Sb.qg;
+      T(FT_SB + 6) = Sb.tz;
+      T(FT_SB + 7) = Sb.w;
+      T(FT_ADZ) += Ab.dz;
+      T(FT_ADP1) += Ab.dp1;
+      T(FT_VTT) = vt_b;
+    }
+  }
+  __syncthreads();
+  // a column without falling rain writes back what it read (its fall-speed
+  // cotangent is not read)
+  double* dst[N_FT - FT_OUT] = {sb, sb + np, sb + 2 * np, sb + 3 * np, sb + 4 * np, sb + 5 * np, sb + 6 * np,
+                                sb + 7 * np, W.as(AS_DZ), W.as(AS_DP1), W.as(AS_VTT)};
+  ws_scatter<NW, G, N_FT - FT_OUT>(dst, sm + (size_t)FT_OUT * G * RP, A.ncol, L, c0);
 }
 
-// 2f. sedimentation reversed (fall speeds, cloud ice melting, the falls of
-// ice, snow and graupel with the vertical-velocity transport).
+// 2g. sedimentation reversed (fall speeds, cloud ice melting, the falls of
+// ice, snow and graupel with the vertical-velocity transport). Tiles,
+// read-only first: E1 (8), dp1, dz, den, the flux's cotangent, icloud's
+// graupel and snow fall-speed cotangents; then read and written: the state's
+// cotangent (8), the geometry's den, dz and dp1 cotangents.
+enum SedTile { ST_E1 = 0, ST_DP1 = 8, ST_DZ, ST_DEN, ST_M1, ST_VTG, ST_VTS, ST_OUT, ST_SB = ST_OUT,
+               ST_ADEN = ST_SB + 8, ST_ADZ, ST_ADP1, N_ST };
 template <int NW, int G, int MINB>
 __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_sed_kernel(const __grid_constant__ VjpArgs A, int it) {
   extern __shared__ double sm[];
+  constexpr int RP = Tiles<NW>::RP;
   const int L = A.nz;
-  int g;
-  Column<NW> C = column_of<NW, G, 0, 0>(sm, L, g);
-  const int64_t col = (int64_t)blockIdx.x * G + g;
-  if (col >= A.ncol) return;  // the whole column group
+  const int64_t c0 = (int64_t)blockIdx.x * G;
   const Ws W = workspace(A);
-  const MpConst& K = A.K;
-  const int k = C.k;
-  const bool valid = k < L;
-  const int64_t np = W.npts, p = (int64_t)(valid ? k : 0) * A.ncol + col;
-  const LevState E1 = valid ? load_lev(W.ck(it, CK_E1) + p, np) : pad_state();
-  StepGeom P;
-  P.dp1 = valid ? W.sp(SP_DP1)[p] : 1.0;
-  P.dz = valid ? W.ss(it, SS_DZ)[p] : 100.0;
-  P.den = valid ? W.ss(it, SS_DEN)[p] : 1.0;
-  LevState Sb = valid ? load_lev(W.as(AS_QV) + p, np) : LevState{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  StepAdj Ab{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  const double convt = 86400.0 * K.rdt * K.RGRAV;
-  const double snow_c = A.snow_b ? A.snow_b[col] * convt : 0.0;
-  const double ice_c = A.ice_b ? A.ice_b[col] * convt : 0.0;
-  const double graupel_c = A.graupel_b ? A.graupel_b[col] * convt : 0.0;
-  const double m1_b = valid ? W.as(AS_M1)[p] : 0.0;
-  const double vtg_b = valid ? W.as(AS_VTG)[p] : 0.0, vts_b = valid ? W.as(AS_VTS)[p] : 0.0;
-  sedimentation_b<NW>(C, K, valid, E1, P, m1_b, ice_c, snow_c, graupel_c, vtg_b, vts_b, Sb, Ab);
-  if (valid) {
-    store_lev(W.as(AS_QV) + p, np, Sb);
-    W.as(AS_DEN)[p] += Ab.den;
-    W.as(AS_DZ)[p] += Ab.dz;
-    W.as(AS_DP1)[p] += Ab.dp1;
+  const int64_t np = W.npts;
+  const double* e1 = W.ck(it, CK_E1);
+  double* sb = W.as(AS_QV);
+  {
+    const double* src[N_ST] = {e1, e1 + np, e1 + 2 * np, e1 + 3 * np, e1 + 4 * np, e1 + 5 * np, e1 + 6 * np,
+                               e1 + 7 * np, W.sp(SP_DP1), W.ss(it, SS_DZ), W.ss(it, SS_DEN), W.as(AS_M1),
+                               W.as(AS_VTG), W.as(AS_VTS), sb, sb + np, sb + 2 * np, sb + 3 * np, sb + 4 * np,
+                               sb + 5 * np, sb + 6 * np, sb + 7 * np, W.as(AS_DEN), W.as(AS_DZ), W.as(AS_DP1)};
+    ws_gather<NW, G, N_ST>(src, sm, A.ncol, L, c0);
   }
+  __syncthreads();
+  int g;
+  Column<NW> C = column_of<NW, G, N_ST, 0>(sm, L, g);
+  const int64_t col = c0 + g;
+  if (col < A.ncol) {
+    const MpConst& K = A.K;
+    const int k = C.k;
+    const bool valid = k < L;
+    double* tile = sm + (size_t)g * RP + (valid ? k : 0);
+    auto T = [&](int f) -> double& { return tile[(size_t)f * G * RP]; };
+    const LevState E1 = valid ? LevState{T(ST_E1), T(ST_E1 + 1), T(ST_E1 + 2), T(ST_E1 + 3), T(ST_E1 + 4),
+                                         T(ST_E1 + 5), T(ST_E1 + 6), T(ST_E1 + 7)}
+                              : pad_state();
+    StepGeom P;
+    P.dp1 = valid ? T(ST_DP1) : 1.0;
+    P.dz = valid ? T(ST_DZ) : 100.0;
+    P.den = valid ? T(ST_DEN) : 1.0;
+    LevState Sb{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (valid)
+      Sb = LevState{T(ST_SB), T(ST_SB + 1), T(ST_SB + 2), T(ST_SB + 3), T(ST_SB + 4), T(ST_SB + 5), T(ST_SB + 6),
+                    T(ST_SB + 7)};
+    StepAdj Ab{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const double convt = 86400.0 * K.rdt * K.RGRAV;
+    const double snow_c = A.snow_b ? A.snow_b[col] * convt : 0.0;
+    const double ice_c = A.ice_b ? A.ice_b[col] * convt : 0.0;
+    const double graupel_c = A.graupel_b ? A.graupel_b[col] * convt : 0.0;
+    const double m1_b = valid ? T(ST_M1) : 0.0;
+    const double vtg_b = valid ? T(ST_VTG) : 0.0, vts_b = valid ? T(ST_VTS) : 0.0;
+    sedimentation_b<NW>(C, K, valid, E1, P, m1_b, ice_c, snow_c, graupel_c, vtg_b, vts_b, Sb, Ab);
+    if (valid) {
+      T(ST_SB) = Sb.qv;
+      T(ST_SB + 1) = Sb.ql;
+      T(ST_SB + 2) = Sb.qr;
+      T(ST_SB + 3) = Sb.qi;
+      T(ST_SB + 4) = Sb.qs;
+      T(ST_SB + 5) = Sb.qg;
+      T(ST_SB + 6) = Sb.tz;
+      T(ST_SB + 7) = Sb.w;
+      T(ST_ADEN) += Ab.den;
+      T(ST_ADZ) += Ab.dz;
+      T(ST_ADP1) += Ab.dp1;
+    }
+  }
+  __syncthreads();
+  double* dst[N_ST - ST_OUT] = {sb, sb + np, sb + 2 * np, sb + 3 * np, sb + 4 * np, sb + 5 * np, sb + 6 * np,
+                                sb + 7 * np, W.as(AS_DEN), W.as(AS_DZ), W.as(AS_DP1)};
+  ws_scatter<NW, G, N_ST - ST_OUT>(dst, sm + (size_t)ST_OUT * G * RP, A.ncol, L, c0);
 }
 
 // 3. fields_init reversed (:27-276), then the gradients written through the
@@ -1103,11 +1308,22 @@ template <int NW, int G, int MINB>
 __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_init_kernel(const __grid_constant__ VjpArgs A) {
   extern __shared__ double sm[];
   constexpr int RP = Tiles<NW>::RP;
-  constexpr int NTILE = N_VJP_IN + N_VJP_GRAD;
+  constexpr int WT = N_VJP_IN + N_VJP_GRAD;  // the workspace tiles: AS_QV .. AS_QA0 + 1, then dp1 and p1
+  constexpr int NWS = AS_V0 + 1 + 2;
+  constexpr int NTILE = WT + NWS;
   const MpConst& K = A.K;
   const int L = A.nz;
   const int64_t c0 = (int64_t)blockIdx.x * G;
   load_tiles<NW, G, N_VJP_IN>(A.in, sm, A.ncol, A.nx, L, c0);
+  const Ws W = workspace(A);
+  {
+    const double* src[NWS];
+#pragma unroll
+    for (int f = 0; f <= AS_V0; ++f) src[f] = (f == AS_DEN || f == AS_DENFAC || f == AS_DZ) ? nullptr : W.as(f);
+    src[AS_V0 + 1] = W.sp(SP_DP1);
+    src[AS_V0 + 2] = W.sp(SP_P1);
+    ws_gather<NW, G, NWS>(src, sm + (size_t)WT * G * RP, A.ncol, L, c0);
+  }
   __syncthreads();
   int g;
   Column<NW> C = column_of<NW, G, NTILE, 4>(sm, L, g);
@@ -1119,18 +1335,16 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_init_kernel(const __gri
   double* gtile = sm + (size_t)N_VJP_IN * G * RP + (size_t)g * RP + k;
   auto TG = [&](int f) -> double& { return gtile[(size_t)f * G * RP]; };
   if (col < A.ncol) {
-    const Ws W = workspace(A);
-    const int64_t np = W.npts, p = (int64_t)(valid ? k : 0) * A.ncol + col;
-    auto AS = [&](int f) -> double { return valid ? W.as(f)[p] : 0.0; };
+    auto AS = [&](int f) -> double { return valid ? tile[(size_t)(WT + f) * G * RP] : 0.0; };
     const double pt = TI(IN_PT, 250.0), delp = TI(IN_DELP, 1.0), dz0 = TI(IN_DELZ, -100.0);
     const double qin[6] = {TI(IN_QV, 0.0), TI(IN_QL, 0.0), TI(IN_QR, 0.0), TI(IN_QI, 0.0), TI(IN_QS, 0.0),
                            TI(IN_QG, 0.0)};
     StepGeom P;
-    P.dp1 = valid ? W.sp(SP_DP1)[p] : 1.0;
-    P.p1 = valid ? W.sp(SP_P1)[p] : 1.0e5;
+    P.dp1 = valid ? AS(AS_V0 + 1) : 1.0;
+    P.p1 = valid ? AS(AS_V0 + 2) : 1.0e5;
     P.ccn = W.sc(SC_CCN)[col];
     P.c_praut = W.sc(SC_CPRAUT)[col];
-    LevState Sb = valid ? load_lev(W.as(AS_QV) + p, np) : LevState{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    LevState Sb{AS(AS_QV), AS(AS_QL), AS(AS_QR), AS(AS_QI), AS(AS_QS), AS(AS_QG), AS(AS_TZ), AS(AS_W)};
     StepAdj Ab{0.0, 0.0, 0.0, AS(AS_DP1), AS(AS_P1), AS(AS_CCN), AS(AS_CPRAUT)};
     double pt_b = AS(AS_PT), delp_b = AS(AS_DELP), dz0_b = AS(AS_DZ0);
     double qin_b[6];
@@ -1278,49 +1492,65 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_init_kernel(const __gri
 }
 
 // ---------------------------------------------------------------- launch
-template <int NW, int G, int MINB>
+// The replay on layout RL (the forward step's), the column reverses on NW
+// warps per column, G columns per block.
+template <class RL, int RMINB, int NW, int G>
 cudaError_t launch_vjp(const VjpArgs& A, cudaStream_t st) {
-  using SR = ColSmem<NW, G, NT_IN, 2>;
-  using SC = ColSmem<NW, G, 0, 0>;
-  using SI = ColSmem<NW, G, N_VJP_IN + N_VJP_GRAD, 4>;
-  cudaError_t e = cudaFuncSetAttribute(vjp_replay_kernel<NW, G, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)SR::bytes);
+  using SU = ColSmem<NW, G, NT_UPD, 0>;
+  using SF = ColSmem<NW, G, N_FT, 0>;
+  using SS = ColSmem<NW, G, N_ST, 0>;
+  using SI = ColSmem<NW, G, N_VJP_IN + N_VJP_GRAD + AS_V0 + 3, 4>;
+  cudaError_t e = cudaFuncSetAttribute(vjp_replay_kernel<RL, RMINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)ReplaySmem<RL>::bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(vjp_init_kernel<NW, G, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(vjp_update_kernel<NW, G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)SU::bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(vjp_init_kernel<NW, G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)SI::bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(vjp_fall_kernel<NW, G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SF::bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(vjp_sed_kernel<NW, G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SS::bytes);
   if (e != cudaSuccess) return e;
+  const unsigned rblk = (unsigned)((A.ncol + RL::G - 1) / RL::G);
   const unsigned nblk = (unsigned)((A.ncol + G - 1) / G);
   const int64_t npts = (int64_t)A.nz * A.ncol;
   const unsigned pblk = (unsigned)((npts + PT_THREADS - 1) / PT_THREADS);
   constexpr int T = 32 * NW * G;
-  vjp_replay_kernel<NW, G, MINB><<<nblk, T, SR::bytes, st>>>(A);
+  vjp_replay_kernel<RL, RMINB><<<rblk, RL::THREADS, ReplaySmem<RL>::bytes, st>>>(A);
+  vjp_update_kernel<NW, G, 1><<<nblk, T, SU::bytes, st>>>(A);
   for (int it = A.K.ntimes - 1; it >= 0; --it) {
+    vjp_subgrid_pt<<<pblk, PT_THREADS, 0, st>>>(A, it);
     vjp_icloud_pt<<<pblk, PT_THREADS, 0, st>>>(A, it);
     vjp_autoconv_pt<1><<<pblk, PT_THREADS, 0, st>>>(A, it);
     vjp_revap2_pt<<<pblk, PT_THREADS, 0, st>>>(A, it, 1);
-    vjp_fall_kernel<NW, G, MINB><<<nblk, T, SC::bytes, st>>>(A, it, 1);
+    vjp_fall_kernel<NW, G, 1><<<nblk, T, SF::bytes, st>>>(A, it, 1);
     vjp_revap1_pt<<<pblk, PT_THREADS, 0, st>>>(A, it, 1);
-    vjp_sed_kernel<NW, G, MINB><<<nblk, T, SC::bytes, st>>>(A, it);
+    vjp_sed_kernel<NW, G, 1><<<nblk, T, SS::bytes, st>>>(A, it);
     vjp_autoconv_pt<0><<<pblk, PT_THREADS, 0, st>>>(A, it);
     vjp_revap2_pt<<<pblk, PT_THREADS, 0, st>>>(A, it, 0);
-    vjp_fall_kernel<NW, G, MINB><<<nblk, T, SC::bytes, st>>>(A, it, 0);
+    vjp_fall_kernel<NW, G, 1><<<nblk, T, SF::bytes, st>>>(A, it, 0);
     vjp_revap1_pt<<<pblk, PT_THREADS, 0, st>>>(A, it, 0);
   }
-  vjp_init_kernel<NW, G, MINB><<<nblk, T, SI::bytes, st>>>(A);
+  vjp_init_kernel<NW, G, 1><<<nblk, T, SI::bytes, st>>>(A);
   return cudaGetLastError();
 }
 
 }  // namespace
 
-int mp_vjp_launches(int ntimes) { return 2 + 10 * ntimes; }
+int mp_vjp_launches(int ntimes) { return 3 + 11 * ntimes; }
 
+// The replay takes the plain step's launch shape for each level range
+// (mp_plain.cu), so that it repeats the step's arithmetic exactly.
 cudaError_t mp_launch_vjp(const VjpArgs& A, cudaStream_t st) {
   const int L = A.nz;
-  if (L <= 32) return launch_vjp<1, 2, 1>(A, st);
-  if (L <= 64) return launch_vjp<2, 2, 1>(A, st);
-  if (L <= 96) return launch_vjp<3, 4, 1>(A, st);
-  if (L <= 128) return launch_vjp<4, 3, 1>(A, st);
-  return launch_vjp<8, 1, 1>(A, st);
+  if (L <= 32) return launch_vjp<ColumnLayout<1, 4>, 2, 1, 2>(A, st);
+  if (L <= 64) return launch_vjp<ColumnLayout<2, 2>, 2, 2, 2>(A, st);
+  if (L <= PACK80_LMAX) return launch_vjp<Packed80, PACK80_MINB, 3, 4>(A, st);
+  if (L <= 96) return launch_vjp<ColumnLayout<3, 4>, 1, 3, 4>(A, st);
+  if (L <= 128) return launch_vjp<ColumnLayout<4, 5>, 1, 4, 3>(A, st);
+  return launch_vjp<ColumnLayout<8, 1>, 2, 8, 1>(A, st);
 }
 
 }  // namespace shield

@@ -149,9 +149,13 @@ int shield_mp_last_error(void* handle, char* buf, size_t n);
  * delprsi, delz, wmp) and the accumulator. The incoming tendencies only add
  * to the outputs and are not differentiated.
  *
- * Branches follow the forward at the given input. Supported: the plain form
- * and configurations without do_sedi_heat and de_ice (SHIELD_ELAYOUT
- * otherwise), any number of sub-steps. */
+ * Branches follow the forward at the given input. Supported: the plain form,
+ * every configuration of the step (do_sedi_heat and de_ice included) and any
+ * number of sub-steps. The state fields of `state` are the step's inputs as
+ * they were before the step; with de_ice, state->qi_dt (NULL: zero) is the
+ * incoming qi_dt the step read (de_ice rewrites qice, qsnow, qi_dt and
+ * qs_dt in place, so pass copies taken before the step). No other tendency
+ * is read. */
 typedef struct {
   ShieldField3D pt_dt, qv_dt, ql_dt, qr_dt, qi_dt, qs_dt, qg_dt, qa_dt, udt, vdt, wmp, qaz; /* NULL ptr: zero */
   const double *rain, *snow, *ice, *graupel; /* ncol each (column c = j*nx + i), or NULL for zero */

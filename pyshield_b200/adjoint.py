@@ -73,9 +73,14 @@ def _state_fields(mp, state, land):
     return F
 
 
-def step_forward(mp, state, land, timestep, stream=None):
+def step_forward(mp, state, land, timestep, stream=None, tendencies=None):
     """Outputs of one step from the 14 inputs: the ten increments, the
-    updated wmp and accumulator, and the four surface totals (mm/day)."""
+    updated wmp and accumulator, and the four surface totals (mm/day).
+
+    ``tendencies`` (dict of tendency name -> field, missing ones zero): the
+    incoming tendencies the step adds its increments to, which the outputs
+    then include; with ``de_ice`` the step reads ``qi_dt`` and rewrites
+    ``qi_dt``, ``qs_dt``, qice and qsnow (state copies are used here)."""
     import torch
 
     _check_state(mp, state)
@@ -86,7 +91,17 @@ def step_forward(mp, state, land, timestep, stream=None):
     F.wmp = field3d(w_out, (mp.nx, mp.ny, mp.nz))
     tend = [_empty3(state[0]) for _ in MP_TENDENCY_FIELDS]
     for name, t in zip(MP_TENDENCY_FIELDS, tend):
+        if tendencies is not None and tendencies.get(name) is not None:
+            t.copy_(tendencies[name])
         setattr(F, name, field3d(t, (mp.nx, mp.ny, mp.nz)))
+    if tendencies is not None:
+        # de_ice writes the step's input qi and qs in place
+        keep_q = []
+        for name in ("qice", "qsnow"):
+            q = _empty3(state[0])
+            q.copy_(state[STATE.index(name)])
+            keep_q.append(q)
+            setattr(F, name, field3d(q, (mp.nx, mp.ny, mp.nz)))
     pr = torch.zeros((4, mp.ny, mp.nx), dtype=torch.float64, device=state[0].device)
     base, plane = pr.data_ptr(), mp.nx * mp.ny * 8
     F.rain, F.snow, F.ice, F.graupel = base, base + plane, base + 2 * plane, base + 3 * plane
@@ -97,14 +112,18 @@ def step_forward(mp, state, land, timestep, stream=None):
     return tuple(tend) + (w_out, qaz) + tuple(pr[i].t() for i in range(4))
 
 
-def step_vjp(mp, state, land, cot, timestep, stream=None):
+def step_vjp(mp, state, land, cot, timestep, stream=None, tendencies=None):
     """Input adjoints (14 fields, ``STATE`` order) of one step at ``state``
-    for the output cotangents ``cot`` (``OUTPUTS`` order; None = zero)."""
+    for the output cotangents ``cot`` (``OUTPUTS`` order; None = zero).
+    ``tendencies``: the incoming tendencies of the forward (``step_forward``);
+    only de_ice reads one (``qi_dt``)."""
     _check_state(mp, state)
     if len(cot) != len(OUTPUTS):
         raise ValueError(f"expected {len(OUTPUTS)} cotangents {OUTPUTS}")
     ext = (mp.nx, mp.ny, mp.nz)
     F = _state_fields(mp, state, land)
+    if tendencies is not None and tendencies.get("qi_dt") is not None:
+        F.qi_dt = field3d(tendencies["qi_dt"], ext)
     C = ShieldMpCotangents()
     keep = []
     for name, c in zip(OUT3, cot[: len(OUT3)]):

@@ -198,8 +198,6 @@ extern "C" int shield_mp_step_vjp(void* handle, const ShieldMpFields* F, const S
   Handle* h = static_cast<Handle*>(handle);
   if (!h) return fail(nullptr, SHIELD_EINVAL, "null handle");
   if (!F || !cot || !grad) return fail(h, SHIELD_EINVAL, "null fields, cotangents or gradients");
-  if (h->cfg.do_sedi_heat || h->cfg.de_ice)
-    return fail(h, SHIELD_ELAYOUT, "the adjoint does not support do_sedi_heat or de_ice");
   MpConst K = h->K;
   if (timestep != K.timestep) {
     std::string why;
@@ -246,6 +244,7 @@ extern "C" int shield_mp_step_vjp(void* handle, const ShieldMpFields* F, const S
   A.ice_b = cot->ice;
   A.graupel_b = cot->graupel;
   A.ws = h->vjp_ws;
+  A.de_ice_qi_dt = f3(F->qi_dt);
   cudaError_t e = mp_launch_vjp(A, static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return cuda_fail(h, e, "adjoint launch");
   return SHIELD_OK;

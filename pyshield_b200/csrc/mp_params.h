@@ -112,6 +112,8 @@ struct VjpArgs {
   const double *rain_b, *snow_b, *ice_b, *graupel_b;
   // workspace of mp_vjp_workspace_doubles(ntimes, nz * ncol, ncol) doubles
   double* ws;
+  // the incoming qi_dt that de_ice reads (null: zero)
+  Fld3 de_ice_qi_dt;
 };
 
 }  // namespace shield

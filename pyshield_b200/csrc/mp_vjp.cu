@@ -346,6 +346,72 @@ struct StepAdj {
   double den, denfac, dz, dp1, p1, ccn, c_praut;
 };
 
+// sedi_heat reversed (microphysics.py:516-557 with C_LIQ, :1176-1217 with
+// C_ICE) from the temperature tz before the heating and the species it saw.
+// Sb.tz holds the heated temperature's cotangent on entry and the entry
+// temperature's on return; the species' cotangents (through the heat
+// capacity), flux_b (the flux leaving this level), dz1_b and dp1_b are added
+// to; fp_b is set to the cotangent of fp, the flux entering from above,
+// which the caller hands to the level above.
+template <int NW>
+SHD void sedi_heat_b(Column<NW>& C, const MpConst& K, double tz, double dz1, double dp1, double qv, double ql,
+                     double qr, double qi, double qs, double qg, double flux, double fp, bool valid, double c_cond,
+                     LevState& Sb, double& flux_b, double& fp_b, double& dz1_b, double& dp1_b) {
+  const int k = C.k, L = C.L;
+  const double dgz = -0.5 * K.GRAV * dz1;
+  const double cs = K.CV_AIR + qv * K.CV_VAP + (qr + ql) * K.C_LIQ + (qi + qs + qg) * K.C_ICE;
+  const double cvn = dp1 * cs;
+  double a, b, D = 1.0, tmp = 1.0;
+  if (k == 0) {
+    tmp = cvn + flux * c_cond;
+    a = tz + flux * dgz / tmp;
+    b = 0.0;
+  } else {
+    D = cvn + c_cond * flux;
+    a = ((cvn + c_cond * (flux - fp)) * tz + dgz * (fp + flux)) / D;
+    b = fp * c_cond / D;
+  }
+  if (!valid) {
+    a = tz;
+    b = 0.0;
+  }
+  const double x = C.scan_affine(a, b);
+  double bv[1] = {b}, bn[1];
+  C.template nextN<1>(bv, bn);
+  const double cn = (valid && k < L - 1) ? bn[0] : 0.0;
+  const double lam = C.scan_affine_rev(valid ? Sb.tz : 0.0, cn);
+  const double xp = C.prev(x);
+  fp_b = 0.0;
+  if (!valid) return;
+  double cvn_b = 0.0, dgz_b = 0.0;
+  if (k == 0) {
+    const double u = flux * dgz;
+    const double u_b = lam / tmp, tmp_b = -lam * u / (tmp * tmp);
+    Sb.tz = lam;
+    flux_b += u_b * dgz + tmp_b * c_cond;
+    dgz_b += u_b * flux;
+    cvn_b += tmp_b;
+  } else {
+    const double b_b = lam * xp;
+    const double N_b = lam / D;
+    const double D_b = -lam * a / D - b_b * b / D;
+    Sb.tz = N_b * (cvn + c_cond * (flux - fp));
+    cvn_b += N_b * tz + D_b;
+    flux_b += N_b * (c_cond * tz + dgz) + D_b * c_cond;
+    fp_b += N_b * (dgz - c_cond * tz) + b_b * c_cond / D;
+    dgz_b += N_b * (fp + flux);
+  }
+  dz1_b += -0.5 * K.GRAV * dgz_b;
+  dp1_b += cvn_b * cs;
+  const double t = cvn_b * dp1;
+  Sb.qv += t * K.CV_VAP;
+  Sb.ql += t * K.C_LIQ;
+  Sb.qr += t * K.C_LIQ;
+  Sb.qi += t * K.C_ICE;
+  Sb.qs += t * K.C_ICE;
+  Sb.qg += t * K.C_ICE;
+}
+
 // sedimentation reverse from its entry state S0. m1s_b: adjoint of the
 // solid flux at this level; ice_c, snow_c, graupel_c: cotangents of the
 // surface totals; vtg_b, vts_b: adjoints of the output fall speeds.
@@ -398,8 +464,36 @@ static __device__ __noinline__ void sedimentation_b(Column<NW>& C, const MpConst
     const double w0 = S1.w;
     const double w1 = (fi && K.do_sedi_w) ? w_update(k, w0, dm_i, flux[0], vti, pv[0], pv[1]) : w0;
     const double w2 = (fs && K.do_sedi_w) ? w_update(k, w1, dm_s, flux[1], vts, pv[2], pv[3]) : w1;
-    // reverse: vertical velocity, in the reverse species order
+    // reverse: the heating by the falling species, which saw the fallen
+    // state and their summed fluxes (do_sedi_heat) ...
     double flux_b[3] = {0.0, 0.0, 0.0}, dm_b[3] = {0.0, 0.0, 0.0}, pv_b[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (K.do_sedi_heat) {
+      double m1s = 0.0, mp = 0.0;
+      if (fi) {
+        m1s = flux[0];
+        mp = pv[0];
+      }
+      if (fs) {
+        m1s = m1s + flux[1];
+        mp = mp + pv[2];
+      }
+      if (fg) {
+        m1s = m1s + flux[2];
+        mp = mp + pv[4];
+      }
+      double hflux_b = 0.0, hmp_b = 0.0, dz1_b = 0.0;
+      sedi_heat_b<NW>(C, K, S1.tz, P.dz1, dp1, S1.qv, S1.ql, S1.qr, qi2, qs2, qg2, m1s, mp, valid, K.C_ICE, Sb,
+                      hflux_b, hmp_b, dz1_b, Ab.dp1);
+      Ab.dz -= dz1_b;  // dz = -dz1 in exact arithmetic: the geometry's reverse takes -dz_b as dz1's cotangent
+#pragma unroll
+      for (int n = 0; n < 3; ++n) {
+        if ((n == 0 && fi) || (n == 1 && fs) || (n == 2 && fg)) {
+          flux_b[n] += hflux_b;
+          pv_b[2 * n] += hmp_b;
+        }
+      }
+    }
+    // ... then the vertical velocity, in the reverse species order
     double wb = Sb.w;
     if (valid) {
       if (fg) {
@@ -516,6 +610,12 @@ static __device__ __noinline__ void sedimentation_b(Column<NW>& C, const MpConst
         vt_b[n] += dd_b[n] * K.dts;
       }
     }
+  } else if (K.do_sedi_heat) {
+    // no species falls: the heating with zero fluxes
+    double hflux_b = 0.0, hmp_b = 0.0, dz1_b = 0.0;
+    sedi_heat_b<NW>(C, K, S1.tz, P.dz1, dp1, S1.qv, S1.ql, S1.qr, S1.qi, S1.qs, S1.qg, 0.0, 0.0, valid, K.C_ICE, Sb,
+                    hflux_b, hmp_b, dz1_b, Ab.dp1);
+    Ab.dz -= dz1_b;
   }
   if (melt_lev)
     sedi_ice_melt_b(K, S0.qv, S0.ql, S0.qr, S0.qi, S0.qs, S0.qg, S0.tz, Sb.qv, Sb.ql, Sb.qr, Sb.qi, Sb.qs, Sb.qg,
@@ -537,6 +637,14 @@ SHD void rain_fall_b(Column<NW>& C, const MpConst& K, bool valid, const LevState
   double fv[2] = {R.flux, vtr}, pv[2];
   C.template prevN<2>(fv, pv);
   double flux_b = m1r_b, dm_b = 0.0, pv_b[2] = {0.0, 0.0};
+  if (K.do_sedi_heat) {
+    // the heating by the falling rain, which saw the fallen state
+    double fp_b = 0.0, dz1_b = 0.0;
+    sedi_heat_b<NW>(C, K, W1.tz, P.dz1, P.dp1, W1.qv, W1.ql, R.q1, W1.qi, W1.qs, W1.qg, R.flux, pv[0], valid,
+                    K.C_LIQ, Sb, flux_b, fp_b, dz1_b, Ab.dp1);
+    Ab.dz -= dz1_b;  // dz = -dz1 in exact arithmetic: the geometry's reverse takes -dz_b as dz1's cotangent
+    pv_b[0] += fp_b;
+  }
   if (K.do_sedi_w && valid)
     w_update_b(k, W1.w, dm, R.flux, vtr, pv[0], pv[1], Sb.w, dm_b, flux_b, vt_b, pv_b[0], pv_b[1]);
   if (k == L - 1) flux_b += rain_c;  // rain += the surface flux
@@ -623,6 +731,38 @@ SHD void ws_scatter(double* const (&dst)[NF], const double* tiles, int64_t ncol,
     if (dst[f]) dst[f][o] = tiles[(f * G + g) * RP + k];
 }
 
+// de_ice (microphysics.py:110-120; the forward's de_ice_kernel) at one
+// point, with the incoming qi_dt: qi and qs become the step's input state.
+// Returns 0 when it leaves them, 1 when qi becomes qi - timestep qi_dt, 2
+// when qi becomes qi0_max.
+SHD int de_ice_point(const MpConst& K, double& qi, double& qs, double qi_dt) {
+  const double qio = qi - K.timestep * qi_dt;
+  const double qin = fmax(qio, K.qi0_max);
+  if (!(qi > qin)) return 0;
+  qs = qs + qi - qin;
+  qi = qin;
+  return max_first(qio, K.qi0_max) ? 1 : 2;
+}
+SHD double de_ice_qi_dt(const VjpArgs& A, int64_t col, int k) {
+  const Fld3& f = A.de_ice_qi_dt;
+  if (!f.p) return 0.0;
+  return f.p[(col % A.nx) * f.si + (col / A.nx) * f.sj + (int64_t)k * f.sk];
+}
+
+// With de_ice, the block's staged qi and qs tiles (tiles[(f * G + g) * RP +
+// k]) become the step's input state; then a block barrier.
+template <int G, int RP>
+SHD void de_ice_tiles(const VjpArgs& A, double* tiles, int64_t c0) {
+  if (!A.K.de_ice) return;  // uniform over the block
+  for (int e = threadIdx.x; e < G * A.nz; e += blockDim.x) {
+    const int g = e % G, k = e / G;
+    const int64_t col = c0 + g;
+    if (col >= A.ncol) continue;
+    de_ice_point(A.K, tiles[(IN_QI * G + g) * RP + k], tiles[(IN_QS * G + g) * RP + k], de_ice_qi_dt(A, col, k));
+  }
+  __syncthreads();
+}
+
 // 1a. The replay with its records, on the forward step's own thread layout
 // LY (so that its vertical sums round as the forward's do): one block's G
 // columns staged into shared memory as the forward kernel stages them.
@@ -671,6 +811,7 @@ __global__ void __launch_bounds__(LY::THREADS, MINB) vjp_replay_kernel(const __g
     }
   }
   __syncthreads();
+  de_ice_tiles<G, RP>(A, sm, c0);
   typename LY::Col C;
   const int g = LY::setup(C, threadIdx.x, L, sm + SM::scratch, sm + SM::work);
   const bool slot_ok = g < G;
@@ -771,6 +912,7 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_update_kernel(const __g
     ws_gather<NW, G, 10>(src, sm + (size_t)NT_IN * G * RP, A.ncol, L, c0);
   }
   __syncthreads();
+  de_ice_tiles<G, RP>(A, sm, c0);
   int g;
   Column<NW> C = column_of<NW, G, NT_UPD, 0>(sm, L, g);
   const int64_t col = c0 + g;
@@ -1159,7 +1301,7 @@ SHD LevState pad_state() { return LevState{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 250.0, 
 // cotangent, icloud's fall-speed cotangent; then read and written: the
 // state's cotangent (8), the geometry's dz and dp1 cotangents, the fall
 // speed's cotangent (written only).
-enum FallTile { FT_W1 = 0, FT_DP1 = 8, FT_DZ, FT_VTR, FT_M1, FT_VTRB, FT_OUT, FT_SB = FT_OUT, FT_ADZ = FT_SB + 8,
+enum FallTile { FT_W1 = 0, FT_DP1 = 8, FT_DZ, FT_DZ1, FT_VTR, FT_M1, FT_VTRB, FT_OUT, FT_SB = FT_OUT, FT_ADZ = FT_SB + 8,
                 FT_ADP1, FT_VTT, N_FT };
 template <int NW, int G, int MINB>
 __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_fall_kernel(const __grid_constant__ VjpArgs A, int it,
@@ -1174,7 +1316,8 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_fall_kernel(const __gri
   double* sb = W.as(AS_QV);
   {
     const double* src[N_FT] = {w1, w1 + np, w1 + 2 * np, w1 + 3 * np, w1 + 4 * np, w1 + 5 * np, w1 + 6 * np,
-                               w1 + 7 * np, W.sp(SP_DP1), W.ss(it, SS_DZ), W.ss(it, pass ? SS_VTR_B : SS_VTR_A),
+                               w1 + 7 * np, W.sp(SP_DP1), W.ss(it, SS_DZ), A.K.do_sedi_heat ? W.ss(it, SS_DZ1) : nullptr,
+                               W.ss(it, pass ? SS_VTR_B : SS_VTR_A),
                                W.as(AS_M1), pass ? W.as(AS_VTR) : nullptr, sb, sb + np, sb + 2 * np, sb + 3 * np,
                                sb + 4 * np, sb + 5 * np, sb + 6 * np, sb + 7 * np, W.as(AS_DZ), W.as(AS_DP1),
                                nullptr};
@@ -1197,6 +1340,7 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_fall_kernel(const __gri
     StepGeom P;
     P.dp1 = valid ? T(FT_DP1) : 1.0;
     P.dz = valid ? T(FT_DZ) : 100.0;
+    P.dz1 = valid ? T(FT_DZ1) : -100.0;
     const double vtr = valid ? T(FT_VTR) : VF_MIN;
     LevState Sb{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (valid)
@@ -1234,7 +1378,7 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_fall_kernel(const __gri
 // read-only first: E1 (8), dp1, dz, den, the flux's cotangent, icloud's
 // graupel and snow fall-speed cotangents; then read and written: the state's
 // cotangent (8), the geometry's den, dz and dp1 cotangents.
-enum SedTile { ST_E1 = 0, ST_DP1 = 8, ST_DZ, ST_DEN, ST_M1, ST_VTG, ST_VTS, ST_OUT, ST_SB = ST_OUT,
+enum SedTile { ST_E1 = 0, ST_DP1 = 8, ST_DZ, ST_DZ1, ST_DEN, ST_M1, ST_VTG, ST_VTS, ST_OUT, ST_SB = ST_OUT,
                ST_ADEN = ST_SB + 8, ST_ADZ, ST_ADP1, N_ST };
 template <int NW, int G, int MINB>
 __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_sed_kernel(const __grid_constant__ VjpArgs A, int it) {
@@ -1248,7 +1392,8 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_sed_kernel(const __grid
   double* sb = W.as(AS_QV);
   {
     const double* src[N_ST] = {e1, e1 + np, e1 + 2 * np, e1 + 3 * np, e1 + 4 * np, e1 + 5 * np, e1 + 6 * np,
-                               e1 + 7 * np, W.sp(SP_DP1), W.ss(it, SS_DZ), W.ss(it, SS_DEN), W.as(AS_M1),
+                               e1 + 7 * np, W.sp(SP_DP1), W.ss(it, SS_DZ), A.K.do_sedi_heat ? W.ss(it, SS_DZ1) : nullptr,
+                               W.ss(it, SS_DEN), W.as(AS_M1),
                                W.as(AS_VTG), W.as(AS_VTS), sb, sb + np, sb + 2 * np, sb + 3 * np, sb + 4 * np,
                                sb + 5 * np, sb + 6 * np, sb + 7 * np, W.as(AS_DEN), W.as(AS_DZ), W.as(AS_DP1)};
     ws_gather<NW, G, N_ST>(src, sm, A.ncol, L, c0);
@@ -1269,6 +1414,7 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_sed_kernel(const __grid
     StepGeom P;
     P.dp1 = valid ? T(ST_DP1) : 1.0;
     P.dz = valid ? T(ST_DZ) : 100.0;
+    P.dz1 = valid ? T(ST_DZ1) : -100.0;
     P.den = valid ? T(ST_DEN) : 1.0;
     LevState Sb{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (valid)
@@ -1325,6 +1471,7 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_init_kernel(const __gri
     ws_gather<NW, G, NWS>(src, sm + (size_t)WT * G * RP, A.ncol, L, c0);
   }
   __syncthreads();
+  de_ice_tiles<G, RP>(A, sm, c0);
   int g;
   Column<NW> C = column_of<NW, G, NTILE, 4>(sm, L, g);
   const int64_t col = c0 + g;
@@ -1485,6 +1632,22 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_init_kernel(const __gri
       TG(IN_DELZ) = dz0_b;
       TG(IN_W) = Sb.w;
       TG(IN_QAZ) = qa_b;
+      if (K.de_ice) {
+        // de_ice reversed: where qi became qi0_max, the input qi moves qs
+        // (qs + qi - qi0_max) and the tendencies it sets (qi_dt = dqi,
+        // qs_dt += qi_dt - dqi, dqi = (qi0_max - qi + timestep qi_dt) rdt);
+        // elsewhere qi and qs pass through
+        double qi0 = A.in[IN_QI].p[(col % A.nx) * A.in[IN_QI].si + (col / A.nx) * A.in[IN_QI].sj +
+                                   (int64_t)k * A.in[IN_QI].sk];
+        double qs0 = 0.0;
+        if (de_ice_point(K, qi0, qs0, de_ice_qi_dt(A, col, k)) == 2) {
+          auto cot = [&](int o) -> double {
+            const Fld3& f = A.cot[o];
+            return f.p ? f.p[(col % A.nx) * f.si + (col / A.nx) * f.sj + (int64_t)k * f.sk] : 0.0;
+          };
+          TG(IN_QI) = TG(IN_QS) + (cot(OUT_QS_DT) - cot(OUT_QI_DT)) * K.rdt;
+        }
+      }
     }
   }
   __syncthreads();
@@ -1494,7 +1657,17 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_init_kernel(const __gri
 // ---------------------------------------------------------------- launch
 // The replay on layout RL (the forward step's), the column reverses on NW
 // warps per column, G columns per block.
-template <class RL, int RMINB, int NW, int G>
+// Resident blocks per SM of the column reverses (__launch_bounds__): the
+// rain fall's short code gains from two (C48 L79: 0.22 -> 0.16 ms per
+// launch, 80 registers); sedimentation's and the update's did not, and the
+// init launch's shared memory holds one.
+#ifndef SHIELD_VJP_COL_MINB
+#define SHIELD_VJP_COL_MINB 1
+#endif
+#ifndef SHIELD_VJP_FALL_MINB
+#define SHIELD_VJP_FALL_MINB 2
+#endif
+template <class RL, int RMINB, int NW, int G, int CMINB = SHIELD_VJP_COL_MINB, int FMINB = SHIELD_VJP_FALL_MINB>
 cudaError_t launch_vjp(const VjpArgs& A, cudaStream_t st) {
   using SU = ColSmem<NW, G, NT_UPD, 0>;
   using SF = ColSmem<NW, G, N_FT, 0>;
@@ -1503,15 +1676,15 @@ cudaError_t launch_vjp(const VjpArgs& A, cudaStream_t st) {
   cudaError_t e = cudaFuncSetAttribute(vjp_replay_kernel<RL, RMINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)ReplaySmem<RL>::bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(vjp_update_kernel<NW, G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(vjp_update_kernel<NW, G, CMINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)SU::bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(vjp_init_kernel<NW, G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(vjp_init_kernel<NW, G, CMINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)SI::bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(vjp_fall_kernel<NW, G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SF::bytes);
+    e = cudaFuncSetAttribute(vjp_fall_kernel<NW, G, FMINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SF::bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(vjp_sed_kernel<NW, G, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SS::bytes);
+    e = cudaFuncSetAttribute(vjp_sed_kernel<NW, G, CMINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SS::bytes);
   if (e != cudaSuccess) return e;
   const unsigned rblk = (unsigned)((A.ncol + RL::G - 1) / RL::G);
   const unsigned nblk = (unsigned)((A.ncol + G - 1) / G);
@@ -1519,21 +1692,21 @@ cudaError_t launch_vjp(const VjpArgs& A, cudaStream_t st) {
   const unsigned pblk = (unsigned)((npts + PT_THREADS - 1) / PT_THREADS);
   constexpr int T = 32 * NW * G;
   vjp_replay_kernel<RL, RMINB><<<rblk, RL::THREADS, ReplaySmem<RL>::bytes, st>>>(A);
-  vjp_update_kernel<NW, G, 1><<<nblk, T, SU::bytes, st>>>(A);
+  vjp_update_kernel<NW, G, CMINB><<<nblk, T, SU::bytes, st>>>(A);
   for (int it = A.K.ntimes - 1; it >= 0; --it) {
     vjp_subgrid_pt<<<pblk, PT_THREADS, 0, st>>>(A, it);
     vjp_icloud_pt<<<pblk, PT_THREADS, 0, st>>>(A, it);
     vjp_autoconv_pt<1><<<pblk, PT_THREADS, 0, st>>>(A, it);
     vjp_revap2_pt<<<pblk, PT_THREADS, 0, st>>>(A, it, 1);
-    vjp_fall_kernel<NW, G, 1><<<nblk, T, SF::bytes, st>>>(A, it, 1);
+    vjp_fall_kernel<NW, G, FMINB><<<nblk, T, SF::bytes, st>>>(A, it, 1);
     vjp_revap1_pt<<<pblk, PT_THREADS, 0, st>>>(A, it, 1);
-    vjp_sed_kernel<NW, G, 1><<<nblk, T, SS::bytes, st>>>(A, it);
+    vjp_sed_kernel<NW, G, CMINB><<<nblk, T, SS::bytes, st>>>(A, it);
     vjp_autoconv_pt<0><<<pblk, PT_THREADS, 0, st>>>(A, it);
     vjp_revap2_pt<<<pblk, PT_THREADS, 0, st>>>(A, it, 0);
-    vjp_fall_kernel<NW, G, 1><<<nblk, T, SF::bytes, st>>>(A, it, 0);
+    vjp_fall_kernel<NW, G, FMINB><<<nblk, T, SF::bytes, st>>>(A, it, 0);
     vjp_revap1_pt<<<pblk, PT_THREADS, 0, st>>>(A, it, 0);
   }
-  vjp_init_kernel<NW, G, 1><<<nblk, T, SI::bytes, st>>>(A);
+  vjp_init_kernel<NW, G, CMINB><<<nblk, T, SI::bytes, st>>>(A);
   return cudaGetLastError();
 }
 

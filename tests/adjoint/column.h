@@ -64,6 +64,33 @@ T w_update_t(int k, T w, T dm, T flux, T vt, T fp, T vp) {
   return (dm * w - fp * vp + flux * vt) / (dm + fp - flux);
 }
 
+// Implicit heating by falling condensate (microphysics.py:516-557 with
+// C_LIQ, :1176-1217 with C_ICE), level by level: flux[k] leaves level k,
+// fp[k] enters it from above.
+template <class T>
+struct Col;
+template <class T>
+void sedi_heat(const MpConst& K, int L, Col<T>& c, const T* flux, const T* fp, double c_cond) {
+  T xprev = 0.0;
+  for (int k = 0; k < L; ++k) {
+    const T dgz = -0.5 * K.GRAV * c.dz1[k];
+    const T cvn =
+        c.dp1[k] * (K.CV_AIR + c.qv[k] * K.CV_VAP + (c.qr[k] + c.ql[k]) * K.C_LIQ + (c.qi[k] + c.qs[k] + c.qg[k]) * K.C_ICE);
+    T x;
+    if (k == 0) {
+      const T tmp = cvn + flux[k] * c_cond;
+      x = c.tz[k] + flux[k] * dgz / tmp;
+    } else {
+      const T D = cvn + c_cond * flux[k];
+      const T a = ((cvn + c_cond * (flux[k] - fp[k])) * c.tz[k] + dgz * (fp[k] + flux[k])) / D;
+      const T b = fp[k] * c_cond / D;
+      x = a + b * xprev;
+    }
+    c.tz[k] = x;
+    xprev = x;
+  }
+}
+
 template <class T>
 struct Col {
   T qv[LMAX], ql[LMAX], qr[LMAX], qi[LMAX], qs[LMAX], qg[LMAX], tz[LMAX], w[LMAX];
@@ -95,6 +122,11 @@ void warm_rain(const MpConst& K, int L, Col<T>& c, T* vtr, T* m1r, T& r1) {
       for (int k = 0; k < L; ++k)
         c.w[k] = w_update_t<T>(k, c.w[k], dm[k], m1r[k], vtr[k], k > 0 ? m1r[k - 1] : T(0.0),
                                k > 0 ? vtr[k - 1] : T(0.0));
+    if (K.do_sedi_heat) {
+      T fp[LMAX];
+      for (int k = 0; k < L; ++k) fp[k] = k > 0 ? m1r[k - 1] : T(0.0);
+      sedi_heat<T>(K, L, c, m1r, fp, K.C_LIQ);
+    }
     for (int k = 0; k < L; ++k)
       revap_racc<T>(K, dt5, c.h_var, c.qg[k], c.qi[k], c.ql[k], c.qr[k], c.qs[k], c.qv[k], c.tz[k], c.den[k],
                     c.denfac[k]);
@@ -130,7 +162,12 @@ void sedimentation(const MpConst& K, int L, Col<T>& c, T* vtg, T* vts, T* m1s, T
   }
   fi = fi && (K.vi_fac >= 1.0e-5);
   for (int k = 0; k < L; ++k) m1s[k] = 0.0;
-  if (!(fi || fs || fg)) return;
+  T mp[LMAX];  // the falling species' flux entering each level from above
+  for (int k = 0; k < L; ++k) mp[k] = 0.0;
+  if (!(fi || fs || fg)) {
+    if (K.do_sedi_heat) sedi_heat<T>(K, L, c, m1s, mp, K.C_ICE);
+    return;
+  }
   T* vt[3] = {vti, vts, vtg};
   T qq[3][LMAX], flux[3][LMAX];
   for (int k = 0; k < L; ++k) {
@@ -150,6 +187,10 @@ void sedimentation(const MpConst& K, int L, Col<T>& c, T* vtg, T* vts, T* m1s, T
   }
   for (int k = 0; k < L; ++k) {
     const int p = k > 0 ? k - 1 : 0;
+    const T z = 0.0;
+    if (fi) mp[k] = k > 0 ? flux[0][p] : z;
+    if (fs) mp[k] = mp[k] + (k > 0 ? flux[1][p] : z);
+    if (fg) mp[k] = mp[k] + (k > 0 ? flux[2][p] : z);
     if (fi) {
       m1s[k] = flux[0][k];
       if (K.do_sedi_w) c.w[k] = w_update_t<T>(k, c.w[k], dmi[k], flux[0][k], vti[k], flux[0][p], vti[p]);
@@ -163,6 +204,7 @@ void sedimentation(const MpConst& K, int L, Col<T>& c, T* vtg, T* vts, T* m1s, T
       if (K.do_sedi_w) c.w[k] = w_update_t<T>(k, c.w[k], dmg[k], flux[2][k], vtg[k], flux[2][p], vtg[p]);
     }
   }
+  if (K.do_sedi_heat) sedi_heat<T>(K, L, c, m1s, mp, K.C_ICE);
   if (fi) sfc[0] = sfc[0] + flux[0][L - 1];
   if (fs) sfc[1] = sfc[1] + flux[1][L - 1];
   if (fg) sfc[2] = sfc[2] + flux[2][L - 1];

@@ -141,7 +141,8 @@ def test_exact_two_substeps():
 
 @pytest.mark.parametrize("cfg", [{"fix_negative": False, "z_slope_liq": False, "z_slope_ice": False},
                                  {"irain_f": 1, "prog_ccn": True, "do_qa": True},
-                                 {"do_sedi_w": False, "sedi_transport": False, "fast_sat_adj": False}])
+                                 {"do_sedi_w": False, "sedi_transport": False, "fast_sat_adj": False},
+                                 {"do_sedi_heat": True}])
 def test_exact_config_variants(cfg):
     _assert_exact(exact_check(8, 3, 79, 150.0, 13, **cfg))
 
@@ -270,13 +271,53 @@ def test_autograd_function_matches_vjp():
         assert torch.equal(a, b), name
 
 
-def test_vjp_rejects_unsupported_configs():
-    from pyshield_b200._lib import ShieldError
-    from pyshield_b200.adjoint import OUTPUTS, step_vjp
+def test_de_ice_composes_with_the_step():
+    """de_ice (microphysics.py:110-120) with incoming qi_dt: the adjoint equals
+    the adjoint of the step without de_ice taken at the de-iced state, chained
+    with de_ice's own derivative. Where qi becomes qi0_max, the input qi
+    reaches the outputs through qs (qs + qi - qi0_max) and through the
+    tendencies de_ice sets (qi_dt = dqi, qs_dt += qi_dt - dqi with
+    dqi = (qi0_max - qi + dt qi_dt) / dt); elsewhere qi and qs pass through.
+    With zero incoming tendencies de_ice changes nothing."""
+    import torch
 
-    mp, pc, x, land, area = _setup(4, 4, 79, 150.0, 18, do_sedi_heat=True)
-    with pytest.raises(ShieldError, match="do_sedi_heat"):
-        step_vjp(mp, x, land, [None] * len(OUTPUTS), 150.0)
+    from pyshield_b200.adjoint import OUTPUTS, STATE, step_forward, step_vjp
+
+    dt = 150.0
+    mp, pc, x, land, area = _setup(6, 4, 79, dt, 23, de_ice=True)
+    iqi, iqs = STATE.index("qice"), STATE.index("qsnow")
+    qi = x[iqi]
+    g = torch.Generator(device="cuda").manual_seed(5)
+    # half the points with ice above qi0_max lose it to the floor, a quarter
+    # keep qi - dt qi_dt, the rest get no tendency
+    u = torch.rand(qi.shape, generator=g, device="cuda", dtype=torch.float64)
+    qi_dt = torch.where(u < 0.5, (qi + 1e-4) / dt, torch.where(u < 0.75, 0.2 * qi / dt, torch.zeros_like(qi)))
+    x[iqi] = torch.where(qi > pc.qi0_max, qi, qi + 2.0 * pc.qi0_max)  # plenty of points above the threshold
+    qi = x[iqi]
+    tend = {"qi_dt": qi_dt}
+    y = step_forward(mp, x, land, dt, tendencies=tend)
+    ybar = _cotangents(y, 31)
+    got = step_vjp(mp, x, land, ybar, dt, tendencies=tend)
+    # the step without de_ice at the de-iced state
+    qio = qi - dt * qi_dt
+    qin = torch.maximum(qio, torch.full_like(qio, pc.qi0_max))
+    hit = qi > qin
+    floor = hit & ~(qio >= pc.qi0_max)
+    assert int(floor.sum()) > 100 and int((hit & ~floor).sum()) > 100
+    xd = [t.clone() for t in x]
+    xd[iqs] = torch.where(hit, x[iqs] + qi - qin, x[iqs])
+    xd[iqi] = torch.where(hit, qin, qi)
+    mp0 = _setup(6, 4, 79, dt, 23)[0]  # the same domain without de_ice
+    ref = list(step_vjp(mp0, xd, land, ybar, dt))
+    c_qi, c_qs = ybar[OUTPUTS.index("qi_dt")], ybar[OUTPUTS.index("qs_dt")]
+    ref[iqi] = torch.where(floor, ref[iqs] + (c_qs - c_qi) / dt, ref[iqi])
+    for name, a, b in zip(STATE, got, ref):
+        scale = float(b.abs().max()) or 1.0
+        assert float((a - b).abs().max()) <= 1e-12 * scale, name
+    # zero incoming tendencies: de_ice leaves the step alone
+    plain = step_vjp(mp0, x, land, ybar, dt)
+    for name, a, b in zip(STATE, step_vjp(mp, x, land, ybar, dt), plain):
+        assert torch.equal(a, b), name
 
 
 def test_exact_five_substeps():

@@ -272,7 +272,8 @@ def column_ref(lib, cfg, ts, X, land, area, DX=None, YB=None):
 
 @pytest.mark.parametrize("kw", [{}, {"mp_time": 75.0}, {"fix_negative": False, "z_slope_liq": False},
                                 {"irain_f": 1, "prog_ccn": True, "do_qa": True},
-                                {"do_sedi_w": False, "sedi_transport": False, "fast_sat_adj": False}])
+                                {"do_sedi_w": False, "sedi_transport": False, "fast_sat_adj": False},
+                                {"do_sedi_heat": True}])
 def test_column_reference_matches_oracle(harness, kw):
     """The sequential column step that serves as the exact reference for the
     adjoint computes the oracle's step: every output within the plain-form

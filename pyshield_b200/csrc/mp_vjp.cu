@@ -35,7 +35,7 @@ namespace shield {
 // Every array holds one double per point p = k * ncol + col (level-major,
 // consecutive columns adjacent) or per column.
 //
-// per sub-step and point: the states (8 doubles each) at
+// per sub-step and point: the states at
 enum VjpCkSlot {
   CK_E0,   // the first warm_rain pass's entry
   CK_W1A,  // its state after the first evaporation,
@@ -48,6 +48,15 @@ enum VjpCkSlot {
   CK_E4,   // the state between the ice processes and the adjustment
   N_CK
 };
+// Of these, only the fields a stage changes are stored (N_CKF per sub-step
+// and point): the entry of each warm_rain pass in full (qv ql qr qi qs qg tz
+// w), then the pass's block: after the first evaporation qv ql qr tz (+0),
+// after the fall qr w tz (+4), after the second evaporation qv ql qr tz
+// (+7), after autoconversion ql qr (+11); icloud's adjustment entry in full.
+// Evaporation / accretion changes qv ql qr tz, the fall qr w (and tz with
+// the heating), autoconversion ql qr.
+enum VjpCkField { CKF_E0 = 0, CKF_PASS = 21, CKF_BLOCK = 8, CKF_E4 = 42, N_CKF = 50 };
+
 // per sub-step and point: scalars
 enum VjpSubScalar {
   SS_DEN, SS_DENFAC, SS_DZ, SS_DZ1,  // the sub-step geometry
@@ -82,7 +91,7 @@ enum VjpAdjField {
 };
 
 int64_t mp_vjp_workspace_doubles(int nt, int64_t npts, int64_t ncol) {
-  return npts * ((int64_t)nt * (8 * N_CK + N_SS) + N_SP + N_AS) + ncol * ((int64_t)nt * N_SCC + N_SC);
+  return npts * ((int64_t)nt * (N_CKF + N_SS) + N_SP + N_AS) + ncol * ((int64_t)nt * N_SCC + N_SC);
 }
 
 namespace {
@@ -91,11 +100,40 @@ struct Ws {
   double* base;
   int64_t npts, ncol;
   int nt;
-  SHD double* ck(int it, int slot) const { return base + ((int64_t)it * N_CK + slot) * 8 * npts; }
-  SHD double* ss(int it, int s) const { return base + ((int64_t)nt * 8 * N_CK + (int64_t)it * N_SS + s) * npts; }
-  SHD double* sp(int s) const { return base + ((int64_t)nt * (8 * N_CK + N_SS) + s) * npts; }
-  SHD double* as(int f) const { return base + ((int64_t)nt * (8 * N_CK + N_SS) + N_SP + f) * npts; }
-  SHD double* cbase() const { return base + ((int64_t)nt * (8 * N_CK + N_SS) + N_SP + N_AS) * npts; }
+  // stored checkpoint field f of sub-step it (VjpCkField offsets)
+  SHD double* ckf(int it, int f) const { return base + ((int64_t)it * N_CKF + f) * npts; }
+  SHD double* ss(int it, int s) const { return base + ((int64_t)nt * N_CKF + (int64_t)it * N_SS + s) * npts; }
+  SHD double* sp(int s) const { return base + ((int64_t)nt * (N_CKF + N_SS) + s) * npts; }
+  SHD double* as(int f) const { return base + ((int64_t)nt * (N_CKF + N_SS) + N_SP + f) * npts; }
+  SHD double* cbase() const { return base + ((int64_t)nt * (N_CKF + N_SS) + N_SP + N_AS) * npts; }
+  // the 8 field arrays (qv ql qr qi qs qg tz w) of the state at slot s of
+  // sub-step it, from the fields stored there and at the slots before it
+  SHD void ck(int it, int s, const double* (&f)[8]) const {
+    if (s == CK_E4) {
+      for (int n = 0; n < 8; ++n) f[n] = ckf(it, CKF_E4 + n);
+      return;
+    }
+    const int pass = s >= CK_E2;
+    const int b = pass * CKF_PASS, w = b + CKF_BLOCK;
+    const int st = s - (pass ? CK_E2 : CK_E0);  // 0 entry, 1..3 W1..W3, 4 after autoconversion
+    for (int n = 0; n < 8; ++n) f[n] = ckf(it, b + n);
+    if (st == 1) {
+      f[0] = ckf(it, w), f[1] = ckf(it, w + 1), f[2] = ckf(it, w + 2), f[6] = ckf(it, w + 3);
+    } else if (st >= 2) {
+      f[7] = ckf(it, w + 5);  // w after the fall
+      if (st == 2) {
+        f[0] = ckf(it, w), f[1] = ckf(it, w + 1), f[2] = ckf(it, w + 4), f[6] = ckf(it, w + 6);
+      } else {
+        f[0] = ckf(it, w + 7), f[1] = ckf(it, w + 8), f[2] = ckf(it, w + 9), f[6] = ckf(it, w + 10);
+        if (st == 4) f[1] = ckf(it, w + 11), f[2] = ckf(it, w + 12);
+      }
+    }
+  }
+  SHD LevState ck_state(int it, int s, int64_t p) const {
+    const double* f[8];
+    ck(it, s, f);
+    return LevState{f[0][p], f[1][p], f[2][p], f[3][p], f[4][p], f[5][p], f[6][p], f[7][p]};
+  }
   SHD double* scc(int it, int s) const { return cbase() + ((int64_t)it * N_SCC + s) * ncol; }
   SHD double* sc(int s) const { return cbase() + ((int64_t)nt * N_SCC + s) * ncol; }
 };
@@ -120,12 +158,27 @@ SHD void store_lev(double* q, int64_t npts, const LevState& S) {
 // The replay's recorder (NoRec's interface, mp_kernel.cuh): states to
 // consecutive checkpoint slots from `st`, values to consecutive sub-step
 // scalars from `val`, the column decision to `flg` (written by level 0).
+// A warm_rain recorder (full false) stores the fields its stage changed
+// into the pass's block at `st`; icloud's (full true) the whole state.
 struct VjpRec {
   double *st, *val, *flg;
   int64_t npts;
-  bool valid, head;
+  bool valid, head, full;
   SHD void state(int s, const LevState& S) const {
-    if (valid) store_lev(st + (int64_t)s * 8 * npts, npts, S);
+    if (!valid) return;
+    if (full) {
+      store_lev(st, npts, S);
+    } else if (s == 1) {
+      st[4 * npts] = S.qr;
+      st[5 * npts] = S.w;
+      st[6 * npts] = S.tz;
+    } else {
+      double* q = st + (s == 0 ? 0 : 7) * npts;
+      q[0] = S.qv;
+      q[npts] = S.ql;
+      q[2 * npts] = S.qr;
+      q[3 * npts] = S.tz;
+    }
   }
   SHD void value(int s, double v) const {
     if (valid) val[(int64_t)s * npts] = v;
@@ -860,7 +913,7 @@ __global__ void __launch_bounds__(LY::THREADS, MINB) vjp_replay_kernel(const __g
       W.ss(it, SS_DENFAC)[p] = P.denfac;
       W.ss(it, SS_DZ)[p] = P.dz;
       W.ss(it, SS_DZ1)[p] = P.dz1;
-      store_lev(W.ck(it, CK_E0) + p, np, S);
+      store_lev(W.ckf(it, CKF_E0) + p, np, S);
     }
     // the first warm_rain pass, sedimentation, the second pass (one copy of
     // the warm_rain code, run twice, as in the forward kernel)
@@ -868,23 +921,25 @@ __global__ void __launch_bounds__(LY::THREADS, MINB) vjp_replay_kernel(const __g
     for (int pass = 0; pass < 2; ++pass) {
       double m1r, r1;
       warm_rain<false>(C, K, KF, valid, S, P, vtr, m1r, r1, nullptr,
-                       VjpRec{W.ck(it, pass ? CK_W1B : CK_W1A) + p, W.ss(it, pass ? SS_SL_B : SS_SL_A) + p,
-                              W.scc(it, pass ? SCC_FALL_B : SCC_FALL_A) + cc, np, valid, head});
+                       VjpRec{W.ckf(it, pass * CKF_PASS + CKF_BLOCK) + p, W.ss(it, pass ? SS_SL_B : SS_SL_A) + p,
+                              W.scc(it, pass ? SCC_FALL_B : SCC_FALL_A) + cc, np, valid, head, false});
       m1 = (pass == 0) ? m1 + m1r : m1 + m1r + m1_sol;
       if (valid) {
         W.ss(it, pass ? SS_VTR_B : SS_VTR_A)[p] = vtr;
-        store_lev(W.ck(it, pass ? CK_E3 : CK_E1) + p, np, S);
+        // autoconversion changed ql and qr
+        W.ckf(it, pass * CKF_PASS + CKF_BLOCK + 11)[p] = S.ql;
+        W.ckf(it, pass * CKF_PASS + CKF_BLOCK + 12)[p] = S.qr;
       }
       if (pass == 1) break;
       sedimentation<false>(C, K, KF, valid, S, P, vtg, vts, m1_sol, ice, snow, graupel);
       if (valid) {
         W.ss(it, SS_VTG)[p] = vtg;
         W.ss(it, SS_VTS)[p] = vts;
-        store_lev(W.ck(it, CK_E2) + p, np, S);
+        store_lev(W.ckf(it, CKF_PASS) + p, np, S);
       }
     }
     icloud<false>(C, K, KF, valid, S, P, qa, vtg, vtr, vts,
-                  VjpRec{W.ck(it, CK_E4) + p, W.ss(it, SS_SL_I) + p, nullptr, np, valid, false});
+                  VjpRec{W.ckf(it, CKF_E4) + p, W.ss(it, SS_SL_I) + p, nullptr, np, valid, false, true});
   }
   if (valid) {
     W.sp(SP_M1)[p] = m1;
@@ -1096,7 +1151,7 @@ __global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_subgrid_pt
   if (!point_of(W, q)) return;
   const int64_t p = q.p, np = W.npts, col = q.col;
   const MpConst& K = A.K;
-  const LevState E4 = load_lev(W.ck(it, CK_E4) + p, np);
+  const LevState E4 = W.ck_state(it, CK_E4, p);
   const double den = W.ss(it, SS_DEN)[p], denfac = W.ss(it, SS_DENFAC)[p], p1 = W.sp(SP_P1)[p];
   const double h_var = W.sc(SC_HVAR)[col], rh_adj = W.sc(SC_RHADJ)[col], rh_rain = W.sc(SC_RHRAIN)[col];
   LevState Sb = load_lev(W.as(AS_QV) + p, np);
@@ -1121,7 +1176,7 @@ __global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_icloud_pt(
   if (!point_of(W, q)) return;
   const int64_t p = q.p, np = W.npts, col = q.col;
   const MpConst& K = A.K;
-  const LevState E3 = load_lev(W.ck(it, CK_E3) + p, np);
+  const LevState E3 = W.ck_state(it, CK_E3, p);
   const double den = W.ss(it, SS_DEN)[p], denfac = W.ss(it, SS_DENFAC)[p], p1 = W.sp(SP_P1)[p];
   const double h_var = W.sc(SC_HVAR)[col];
   const double vtg = W.ss(it, SS_VTG)[p], vtr = W.ss(it, SS_VTR_B)[p], vts = W.ss(it, SS_VTS)[p];
@@ -1184,11 +1239,11 @@ __global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_autoconv_p
   double den_b = 0.0;
   if (PASS == 1) {
     if (K.z_slope_ice) Sb.qi += slope_gather(W.ss(it, SS_S1QI), W.as(AS_SLI), p, W.ncol, q.k, A.nz);
-    const LevState E3 = load_lev(W.ck(it, CK_E3) + p, np);
+    const LevState E3 = W.ck_state(it, CK_E3, p);
     icloud_melt_freeze_b(K, E3.qv, E3.ql, E3.qr, E3.qi, E3.qs, E3.qg, E3.tz, den, W.as(AS_QLIQ)[p],
                          W.as(AS_QSOL)[p], W.as(AS_CVM)[p], Sb.qv, Sb.ql, Sb.qr, Sb.qi, Sb.qs, Sb.qg, Sb.tz, den_b);
   }
-  const LevState W3 = load_lev(W.ck(it, PASS ? CK_W3B : CK_W3A) + p, np);
+  const LevState W3 = W.ck_state(it, PASS ? CK_W3B : CK_W3A, p);
   const double h_var = W.sc(SC_HVAR)[col], ccn = W.sc(SC_CCN)[col], c_praut = W.sc(SC_CPRAUT)[col];
   double ccn_b = 0.0, cpr_b = 0.0, sl_b = 0.0;
   if (K.irain_f != 0) {
@@ -1226,9 +1281,9 @@ __global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_revap2_pt(
   const MpConst& K = A.K;
   LevState Sb = load_lev(W.as(AS_QV) + p, np);
   if (K.irain_f == 0 && K.z_slope_liq)
-    Sb.ql += slope_gather(W.ck(it, pass ? CK_W3B : CK_W3A) + np, W.as(AS_SLL), p, W.ncol, q.k, A.nz);
+    Sb.ql += slope_gather(W.ckf(it, pass * CKF_PASS + CKF_BLOCK + 8), W.as(AS_SLL), p, W.ncol, q.k, A.nz);
   if (W.scc(it, pass ? SCC_FALL_B : SCC_FALL_A)[col] != 0.0) {
-    const LevState W2 = load_lev(W.ck(it, pass ? CK_W2B : CK_W2A) + p, np);
+    const LevState W2 = W.ck_state(it, pass ? CK_W2B : CK_W2A, p);
     const double den = W.ss(it, SS_DEN)[p], denfac = W.ss(it, SS_DENFAC)[p], h_var = W.sc(SC_HVAR)[col];
     double den_b = 0.0, denfac_b = 0.0;
     revap_racc_b(K, 0.5 * K.dt_rain, h_var, W2.qg, W2.qi, W2.ql, W2.qr, W2.qs, W2.qv, W2.tz, den, denfac, Sb.qg,
@@ -1254,7 +1309,7 @@ __global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_revap1_pt(
   const double den = W.ss(it, SS_DEN)[p], denfac = W.ss(it, SS_DENFAC)[p];
   double den_b = 0.0, denfac_b = 0.0;
   if (W.scc(it, pass ? SCC_FALL_B : SCC_FALL_A)[col] != 0.0) {
-    const LevState W0 = load_lev(W.ck(it, pass ? CK_E2 : CK_E0) + p, np);
+    const LevState W0 = W.ck_state(it, pass ? CK_E2 : CK_E0, p);
     const double h_var = W.sc(SC_HVAR)[col];
     revap_racc_b(K, 0.5 * K.dt_rain, h_var, W0.qg, W0.qi, W0.ql, W0.qr, W0.qs, W0.qv, W0.tz, den, denfac, Sb.qg,
                  Sb.qi, Sb.ql, Sb.qr, Sb.qs, Sb.qv, Sb.tz, den_b, denfac_b);
@@ -1268,7 +1323,7 @@ __global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_revap1_pt(
     const Fld3& fz = A.in[IN_DELZ];
     const double pt = fp.p[i * fp.si + j * fp.sj + (int64_t)q.k * fp.sk];
     const double dz0 = fz.p[i * fz.si + j * fz.sj + (int64_t)q.k * fz.sk];
-    const double dp1 = W.sp(SP_DP1)[p], dz1 = W.ss(it, SS_DZ1)[p], tz0 = W.ck(it, CK_E0)[6 * np + p];
+    const double dp1 = W.sp(SP_DP1)[p], dz1 = W.ss(it, SS_DZ1)[p], tz0 = W.ckf(it, CKF_E0 + 6)[p];
     const double aden = W.as(AS_DEN)[p] + den_b, adenfac = W.as(AS_DENFAC)[p] + denfac_b;
     const double den0 = -dp1 / (K.GRAV * dz0);
     const double dn_b = aden - adenfac * 0.5 * denfac / den;
@@ -1312,11 +1367,11 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_fall_kernel(const __gri
   const int64_t c0 = (int64_t)blockIdx.x * G;
   const Ws W = workspace(A);
   const int64_t np = W.npts;
-  const double* w1 = W.ck(it, pass ? CK_W1B : CK_W1A);
+  const double* w1[8];
+  W.ck(it, pass ? CK_W1B : CK_W1A, w1);
   double* sb = W.as(AS_QV);
   {
-    const double* src[N_FT] = {w1, w1 + np, w1 + 2 * np, w1 + 3 * np, w1 + 4 * np, w1 + 5 * np, w1 + 6 * np,
-                               w1 + 7 * np, W.sp(SP_DP1), W.ss(it, SS_DZ), A.K.do_sedi_heat ? W.ss(it, SS_DZ1) : nullptr,
+    const double* src[N_FT] = {w1[0], w1[1], w1[2], w1[3], w1[4], w1[5], w1[6], w1[7], W.sp(SP_DP1), W.ss(it, SS_DZ), A.K.do_sedi_heat ? W.ss(it, SS_DZ1) : nullptr,
                                W.ss(it, pass ? SS_VTR_B : SS_VTR_A),
                                W.as(AS_M1), pass ? W.as(AS_VTR) : nullptr, sb, sb + np, sb + 2 * np, sb + 3 * np,
                                sb + 4 * np, sb + 5 * np, sb + 6 * np, sb + 7 * np, W.as(AS_DZ), W.as(AS_DP1),
@@ -1388,11 +1443,11 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_sed_kernel(const __grid
   const int64_t c0 = (int64_t)blockIdx.x * G;
   const Ws W = workspace(A);
   const int64_t np = W.npts;
-  const double* e1 = W.ck(it, CK_E1);
+  const double* e1[8];
+  W.ck(it, CK_E1, e1);
   double* sb = W.as(AS_QV);
   {
-    const double* src[N_ST] = {e1, e1 + np, e1 + 2 * np, e1 + 3 * np, e1 + 4 * np, e1 + 5 * np, e1 + 6 * np,
-                               e1 + 7 * np, W.sp(SP_DP1), W.ss(it, SS_DZ), A.K.do_sedi_heat ? W.ss(it, SS_DZ1) : nullptr,
+    const double* src[N_ST] = {e1[0], e1[1], e1[2], e1[3], e1[4], e1[5], e1[6], e1[7], W.sp(SP_DP1), W.ss(it, SS_DZ), A.K.do_sedi_heat ? W.ss(it, SS_DZ1) : nullptr,
                                W.ss(it, SS_DEN), W.as(AS_M1),
                                W.as(AS_VTG), W.as(AS_VTS), sb, sb + np, sb + 2 * np, sb + 3 * np, sb + 4 * np,
                                sb + 5 * np, sb + 6 * np, sb + 7 * np, W.as(AS_DEN), W.as(AS_DZ), W.as(AS_DP1)};

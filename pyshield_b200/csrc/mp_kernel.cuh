@@ -1161,10 +1161,11 @@ SHD void warm_rain(Col& C, const MpConst& K, const MpConstF& KF, bool valid, Lev
 // implicit falls of ice, snow and graupel with their vertical-velocity
 // transport and heating. Returns the solid flux m1_sol at this level and
 // adds the surface fluxes to ice, snow and graupel.
-template <bool MIXED, class Col>
+// A recorder gets the cloud ice fall speed (value 0).
+template <bool MIXED, class Col, class Rec = NoRec>
 SHD void sedimentation(Col& C, const MpConst& K, const MpConstF& KF, bool valid, LevState& S,
                        const StepGeom& P, double& vtg, double& vts, double& m1_sol, double& ice, double& snow,
-                       double& graupel, unsigned* flags = nullptr) {
+                       double& graupel, unsigned* flags = nullptr, const Rec& rec = Rec()) {
   const int k = C.k, L = C.L;
   double &qv = S.qv, &ql = S.ql, &qr = S.qr, &qi = S.qi, &qs = S.qs, &qg = S.qg, &tz = S.tz, &w = S.w;
   const double dp1 = P.dp1, dz = P.dz;
@@ -1173,6 +1174,7 @@ SHD void sedimentation(Col& C, const MpConst& K, const MpConstF& KF, bool valid,
     fall_speed_m(K, KF, qg, qi, qs, tz, P.den, vtg, vti, vts);
   else
     fall_speed(K, qg, qi, qs, tz, P.den, vtg, vti, vts);
+  rec.value(0, vti);
   m1_sol = 0.0;
   // cloud ice melting at and below the first level warmer than tice (:702-746)
   const int first = C.min_int((valid && tz > K.tice) ? k : (1 << 30));

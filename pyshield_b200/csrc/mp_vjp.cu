@@ -61,7 +61,7 @@ enum VjpCkField { CKF_E0 = 0, CKF_PASS = 21, CKF_BLOCK = 8, CKF_E4 = 42, N_CKF =
 enum VjpSubScalar {
   SS_DEN, SS_DENFAC, SS_DZ, SS_DZ1,  // the sub-step geometry
   SS_VTR_A, SS_VTR_B,                // rain fall speed of each pass
-  SS_VTG, SS_VTS,                    // graupel and snow fall speeds of sedimentation
+  SS_VTG, SS_VTS, SS_VTI,            // graupel, snow and cloud ice fall speeds of sedimentation
   SS_SL_A, SS_SL_B,                  // liquid slope of each pass's autoconversion
   SS_SL_I, SS_S1QI,                  // icloud's ice slope and cloud ice after melting / freezing
   N_SS
@@ -87,6 +87,8 @@ enum VjpAdjField {
   AS_VTT,                                                 // of a pass's rain fall speed (fall to evaporation)
   AS_QLIQ, AS_QSOL, AS_CVM,                               // of icloud's melting / freezing outputs
   AS_SLI, AS_SLL,                                         // of the ice and liquid slopes
+  AS_VTI,                                                 // of sedimentation's cloud ice fall speed
+  AS_MELT,                                                // 1 where sedimentation melted cloud ice
   N_AS
 };
 
@@ -465,25 +467,28 @@ SHD void sedi_heat_b(Column<NW>& C, const MpConst& K, double tz, double dz1, dou
   Sb.qg += t * K.C_ICE;
 }
 
-// sedimentation reverse from its entry state S0. m1s_b: adjoint of the
-// solid flux at this level; ice_c, snow_c, graupel_c: cotangents of the
-// surface totals; vtg_b, vts_b: adjoints of the output fall speeds.
+// sedimentation's falls reversed from its entry state S0 and the fall speeds
+// the forward computed there: the ice, snow and graupel falls with their
+// vertical-velocity transport and heating. m1s_b: cotangent of the solid
+// flux at this level; ice_c, snow_c, graupel_c: of the surface totals; vt_b:
+// the fall speeds' (vti, vts, vtg) cotangents, added to. Leaves Sb with
+// respect to the state after cloud ice melting, which happened where
+// melt_lev is set (the reverses of the melting and of the fall speeds are
+// pointwise and run in their own launch).
 template <int NW>
-static __device__ __noinline__ void sedimentation_b(Column<NW>& C, const MpConst& K, bool valid, const LevState& S0, const StepGeom& P,
-                         double m1s_b, double ice_c, double snow_c, double graupel_c, double vtg_b, double vts_b,
-                         LevState& Sb, StepAdj& Ab) {
+static __device__ __noinline__ void sedimentation_b(Column<NW>& C, const MpConst& K, bool valid, const LevState& S0,
+                                                    const StepGeom& P, double vtg, double vti, double vts,
+                                                    double m1s_b, double ice_c, double snow_c, double graupel_c,
+                                                    double (&vt_b)[3], LevState& Sb, StepAdj& Ab, bool& melt_lev) {
   const int k = C.k, L = C.L;
   const double dp1 = P.dp1, dz = P.dz;
-  double vtg, vti, vts;
-  fall_speed(K, S0.qg, S0.qi, S0.qs, S0.tz, P.den, vtg, vti, vts);
   const int first = C.min_int((valid && S0.tz > K.tice) ? k : (1 << 30));
-  const bool melt_lev = (k >= first || k == L - 1) && valid;
+  melt_lev = (k >= first || k == L - 1) && valid;
   LevState S1 = S0;
   if (melt_lev) sedi_ice_melt(K, S1.qv, S1.ql, S1.qr, S1.qi, S1.qs, S1.qg, S1.tz);
   bool fi, fs, fg;
   C.any3(valid && (S1.qi > QRMIN), valid && (S1.qs > QRMIN), valid && (S1.qg > QRMIN), fi, fs, fg);
   fi = fi && (K.vi_fac >= 1.0e-5);
-  double vt_b[3] = {0.0, vts_b, vtg_b};  // vti, vts, vtg
   if (fi || fs || fg) {
     const double dd[3] = {K.dts * vti, K.dts * vts, K.dts * vtg};
     double ddp[3];
@@ -670,11 +675,6 @@ static __device__ __noinline__ void sedimentation_b(Column<NW>& C, const MpConst
                     hflux_b, hmp_b, dz1_b, Ab.dp1);
     Ab.dz -= dz1_b;
   }
-  if (melt_lev)
-    sedi_ice_melt_b(K, S0.qv, S0.ql, S0.qr, S0.qi, S0.qs, S0.qg, S0.tz, Sb.qv, Sb.ql, Sb.qr, Sb.qi, Sb.qs, Sb.qg,
-                    Sb.tz);
-  if (valid)
-    fall_speed_b(K, S0.qg, S0.qi, S0.qs, S0.tz, P.den, vt_b[2], vt_b[0], vt_b[1], Sb.qg, Sb.qi, Sb.qs, Sb.tz, Ab.den);
 }
 // The rain fall of a warm_rain pass reversed (microphysics.py:459-515), from
 // W1, the state after the first evaporation: the vertical-velocity update,
@@ -931,7 +931,8 @@ __global__ void __launch_bounds__(LY::THREADS, MINB) vjp_replay_kernel(const __g
         W.ckf(it, pass * CKF_PASS + CKF_BLOCK + 12)[p] = S.qr;
       }
       if (pass == 1) break;
-      sedimentation<false>(C, K, KF, valid, S, P, vtg, vts, m1_sol, ice, snow, graupel);
+      sedimentation<false>(C, K, KF, valid, S, P, vtg, vts, m1_sol, ice, snow, graupel, nullptr,
+                           VjpRec{nullptr, W.ss(it, SS_VTI) + p, nullptr, np, valid, false, false});
       if (valid) {
         W.ss(it, SS_VTG)[p] = vtg;
         W.ss(it, SS_VTS)[p] = vts;
@@ -1428,13 +1429,14 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_fall_kernel(const __gri
   ws_scatter<NW, G, N_FT - FT_OUT>(dst, sm + (size_t)FT_OUT * G * RP, A.ncol, L, c0);
 }
 
-// 2g. sedimentation reversed (fall speeds, cloud ice melting, the falls of
-// ice, snow and graupel with the vertical-velocity transport). Tiles,
-// read-only first: E1 (8), dp1, dz, den, the flux's cotangent, icloud's
-// graupel and snow fall-speed cotangents; then read and written: the state's
-// cotangent (8), the geometry's den, dz and dp1 cotangents.
-enum SedTile { ST_E1 = 0, ST_DP1 = 8, ST_DZ, ST_DZ1, ST_DEN, ST_M1, ST_VTG, ST_VTS, ST_OUT, ST_SB = ST_OUT,
-               ST_ADEN = ST_SB + 8, ST_ADZ, ST_ADP1, N_ST };
+// 2g. sedimentation's falls reversed (the ice, snow and graupel falls with
+// their vertical-velocity transport and heating). Tiles, read-only first:
+// E1 (8), dp1, dz, dz1, the flux's cotangent; then read and written: the
+// state's cotangent (8), the geometry's dz and dp1 cotangents, the fall
+// speeds (replaced by their cotangents: icloud's in, the totals out), the
+// melting flag (written only).
+enum SedTile { ST_E1 = 0, ST_DP1 = 8, ST_DZ, ST_DZ1, ST_M1, ST_OUT, ST_SB = ST_OUT, ST_ADZ = ST_SB + 8, ST_ADP1,
+               ST_VTI, ST_VTS, ST_VTG, ST_MELT, N_ST };
 template <int NW, int G, int MINB>
 __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_sed_kernel(const __grid_constant__ VjpArgs A, int it) {
   extern __shared__ double sm[];
@@ -1447,10 +1449,10 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_sed_kernel(const __grid
   W.ck(it, CK_E1, e1);
   double* sb = W.as(AS_QV);
   {
-    const double* src[N_ST] = {e1[0], e1[1], e1[2], e1[3], e1[4], e1[5], e1[6], e1[7], W.sp(SP_DP1), W.ss(it, SS_DZ), A.K.do_sedi_heat ? W.ss(it, SS_DZ1) : nullptr,
-                               W.ss(it, SS_DEN), W.as(AS_M1),
-                               W.as(AS_VTG), W.as(AS_VTS), sb, sb + np, sb + 2 * np, sb + 3 * np, sb + 4 * np,
-                               sb + 5 * np, sb + 6 * np, sb + 7 * np, W.as(AS_DEN), W.as(AS_DZ), W.as(AS_DP1)};
+    const double* src[N_ST] = {e1[0], e1[1], e1[2], e1[3], e1[4], e1[5], e1[6], e1[7], W.sp(SP_DP1), W.ss(it, SS_DZ),
+                               A.K.do_sedi_heat ? W.ss(it, SS_DZ1) : nullptr, W.as(AS_M1), sb, sb + np, sb + 2 * np,
+                               sb + 3 * np, sb + 4 * np, sb + 5 * np, sb + 6 * np, sb + 7 * np, W.as(AS_DZ),
+                               W.as(AS_DP1), nullptr, W.as(AS_VTS), W.as(AS_VTG), nullptr};
     ws_gather<NW, G, N_ST>(src, sm, A.ncol, L, c0);
   }
   __syncthreads();
@@ -1463,6 +1465,7 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_sed_kernel(const __grid
     const bool valid = k < L;
     double* tile = sm + (size_t)g * RP + (valid ? k : 0);
     auto T = [&](int f) -> double& { return tile[(size_t)f * G * RP]; };
+    const int64_t p = (int64_t)(valid ? k : 0) * A.ncol + col;
     const LevState E1 = valid ? LevState{T(ST_E1), T(ST_E1 + 1), T(ST_E1 + 2), T(ST_E1 + 3), T(ST_E1 + 4),
                                          T(ST_E1 + 5), T(ST_E1 + 6), T(ST_E1 + 7)}
                               : pad_state();
@@ -1470,7 +1473,9 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_sed_kernel(const __grid
     P.dp1 = valid ? T(ST_DP1) : 1.0;
     P.dz = valid ? T(ST_DZ) : 100.0;
     P.dz1 = valid ? T(ST_DZ1) : -100.0;
-    P.den = valid ? T(ST_DEN) : 1.0;
+    // the forward's fall speeds at sedimentation's entry
+    const double vtg = valid ? W.ss(it, SS_VTG)[p] : VF_MIN, vts = valid ? W.ss(it, SS_VTS)[p] : VF_MIN,
+                 vti = valid ? W.ss(it, SS_VTI)[p] : VF_MIN;
     LevState Sb{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (valid)
       Sb = LevState{T(ST_SB), T(ST_SB + 1), T(ST_SB + 2), T(ST_SB + 3), T(ST_SB + 4), T(ST_SB + 5), T(ST_SB + 6),
@@ -1481,8 +1486,9 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_sed_kernel(const __grid
     const double ice_c = A.ice_b ? A.ice_b[col] * convt : 0.0;
     const double graupel_c = A.graupel_b ? A.graupel_b[col] * convt : 0.0;
     const double m1_b = valid ? T(ST_M1) : 0.0;
-    const double vtg_b = valid ? T(ST_VTG) : 0.0, vts_b = valid ? T(ST_VTS) : 0.0;
-    sedimentation_b<NW>(C, K, valid, E1, P, m1_b, ice_c, snow_c, graupel_c, vtg_b, vts_b, Sb, Ab);
+    double vt_b[3] = {0.0, valid ? T(ST_VTS) : 0.0, valid ? T(ST_VTG) : 0.0};
+    bool melt_lev;
+    sedimentation_b<NW>(C, K, valid, E1, P, vtg, vti, vts, m1_b, ice_c, snow_c, graupel_c, vt_b, Sb, Ab, melt_lev);
     if (valid) {
       T(ST_SB) = Sb.qv;
       T(ST_SB + 1) = Sb.ql;
@@ -1492,15 +1498,41 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_sed_kernel(const __grid
       T(ST_SB + 5) = Sb.qg;
       T(ST_SB + 6) = Sb.tz;
       T(ST_SB + 7) = Sb.w;
-      T(ST_ADEN) += Ab.den;
       T(ST_ADZ) += Ab.dz;
       T(ST_ADP1) += Ab.dp1;
+      T(ST_VTI) = vt_b[0];
+      T(ST_VTS) = vt_b[1];
+      T(ST_VTG) = vt_b[2];
+      T(ST_MELT) = melt_lev ? 1.0 : 0.0;
     }
   }
   __syncthreads();
-  double* dst[N_ST - ST_OUT] = {sb, sb + np, sb + 2 * np, sb + 3 * np, sb + 4 * np, sb + 5 * np, sb + 6 * np,
-                                sb + 7 * np, W.as(AS_DEN), W.as(AS_DZ), W.as(AS_DP1)};
+  double* dst[N_ST - ST_OUT] = {sb,          sb + np,     sb + 2 * np, sb + 3 * np,  sb + 4 * np,  sb + 5 * np,
+                                sb + 6 * np, sb + 7 * np, W.as(AS_DZ), W.as(AS_DP1), W.as(AS_VTI), W.as(AS_VTS),
+                                W.as(AS_VTG), W.as(AS_MELT)};
   ws_scatter<NW, G, N_ST - ST_OUT>(dst, sm + (size_t)ST_OUT * G * RP, A.ncol, L, c0);
+}
+
+// 2h. The pointwise end of sedimentation's reverse: cloud ice melting
+// (:702-746) where it happened, then the fall speeds (microphysics_funcs.py:
+// 269-341) at the entry state.
+__global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_sed_tail_pt(const __grid_constant__ VjpArgs A,
+                                                                                  int it) {
+  const Ws W = workspace(A);
+  PointIdx q;
+  if (!point_of(W, q)) return;
+  const int64_t p = q.p, np = W.npts;
+  const MpConst& K = A.K;
+  LevState Sb = load_lev(W.as(AS_QV) + p, np);
+  const LevState E1 = W.ck_state(it, CK_E1, p);
+  if (W.as(AS_MELT)[p] != 0.0)
+    sedi_ice_melt_b(K, E1.qv, E1.ql, E1.qr, E1.qi, E1.qs, E1.qg, E1.tz, Sb.qv, Sb.ql, Sb.qr, Sb.qi, Sb.qs, Sb.qg,
+                    Sb.tz);
+  double den_b = 0.0;
+  fall_speed_b(K, E1.qg, E1.qi, E1.qs, E1.tz, W.ss(it, SS_DEN)[p], W.as(AS_VTG)[p], W.as(AS_VTI)[p],
+               W.as(AS_VTS)[p], Sb.qg, Sb.qi, Sb.qs, Sb.tz, den_b);
+  store_lev(W.as(AS_QV) + p, np, Sb);
+  W.as(AS_DEN)[p] += den_b;
 }
 
 // 3. fields_init reversed (:27-276), then the gradients written through the
@@ -1722,7 +1754,11 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_init_kernel(const __gri
 #ifndef SHIELD_VJP_FALL_MINB
 #define SHIELD_VJP_FALL_MINB 2
 #endif
-template <class RL, int RMINB, int NW, int G, int CMINB = SHIELD_VJP_COL_MINB, int FMINB = SHIELD_VJP_FALL_MINB>
+#ifndef SHIELD_VJP_SED_MINB
+#define SHIELD_VJP_SED_MINB 1
+#endif
+template <class RL, int RMINB, int NW, int G, int CMINB = SHIELD_VJP_COL_MINB, int FMINB = SHIELD_VJP_FALL_MINB,
+          int SMINB = SHIELD_VJP_SED_MINB>
 cudaError_t launch_vjp(const VjpArgs& A, cudaStream_t st) {
   using SU = ColSmem<NW, G, NT_UPD, 0>;
   using SF = ColSmem<NW, G, N_FT, 0>;
@@ -1739,7 +1775,7 @@ cudaError_t launch_vjp(const VjpArgs& A, cudaStream_t st) {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(vjp_fall_kernel<NW, G, FMINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SF::bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(vjp_sed_kernel<NW, G, CMINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SS::bytes);
+    e = cudaFuncSetAttribute(vjp_sed_kernel<NW, G, SMINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SS::bytes);
   if (e != cudaSuccess) return e;
   const unsigned rblk = (unsigned)((A.ncol + RL::G - 1) / RL::G);
   const unsigned nblk = (unsigned)((A.ncol + G - 1) / G);
@@ -1755,7 +1791,8 @@ cudaError_t launch_vjp(const VjpArgs& A, cudaStream_t st) {
     vjp_revap2_pt<<<pblk, PT_THREADS, 0, st>>>(A, it, 1);
     vjp_fall_kernel<NW, G, FMINB><<<nblk, T, SF::bytes, st>>>(A, it, 1);
     vjp_revap1_pt<<<pblk, PT_THREADS, 0, st>>>(A, it, 1);
-    vjp_sed_kernel<NW, G, CMINB><<<nblk, T, SS::bytes, st>>>(A, it);
+    vjp_sed_kernel<NW, G, SMINB><<<nblk, T, SS::bytes, st>>>(A, it);
+    vjp_sed_tail_pt<<<pblk, PT_THREADS, 0, st>>>(A, it);
     vjp_autoconv_pt<0><<<pblk, PT_THREADS, 0, st>>>(A, it);
     vjp_revap2_pt<<<pblk, PT_THREADS, 0, st>>>(A, it, 0);
     vjp_fall_kernel<NW, G, FMINB><<<nblk, T, SF::bytes, st>>>(A, it, 0);
@@ -1767,7 +1804,7 @@ cudaError_t launch_vjp(const VjpArgs& A, cudaStream_t st) {
 
 }  // namespace
 
-int mp_vjp_launches(int ntimes) { return 3 + 11 * ntimes; }
+int mp_vjp_launches(int ntimes) { return 3 + 12 * ntimes; }
 
 // The replay takes the plain step's launch shape for each level range
 // (mp_plain.cu), so that it repeats the step's arithmetic exactly.

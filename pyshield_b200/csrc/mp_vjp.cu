@@ -73,7 +73,8 @@ enum VjpSubColumn { SCC_FALL_A, SCC_FALL_B, N_SCC };
 // flux summed over the sub-steps, and the final state (8)
 enum VjpStepPoint { SP_DP1, SP_P1, SP_M1, SP_FIN, N_SP = SP_FIN + 8 };
 // per column, once: fields_init's column values
-enum VjpStepColumn { SC_HVAR, SC_RHADJ, SC_RHRAIN, SC_CCN, SC_CPRAUT, N_SC };
+// (SC_CCNB: the CCN cotangent's column total, set by the fields_init reverse)
+enum VjpStepColumn { SC_HVAR, SC_RHADJ, SC_RHRAIN, SC_CCN, SC_CPRAUT, SC_CCNB, N_SC };
 // per point: the adjoint state carried between the launches
 enum VjpAdjField {
   AS_QV, AS_QL, AS_QR, AS_QI, AS_QS, AS_QG, AS_TZ, AS_W,  // the state's cotangent
@@ -190,8 +191,6 @@ struct VjpRec {
   }
 };
 
-constexpr int NT_IN = N_VJP_IN + N_VJP_COT;
-constexpr int NT_UPD = NT_IN + 10;  // the update launch's tiles: inputs, cotangents, final state, dp1, m1
 
 // load NF fields into tiles [f * G + g][k] (all loads issued before any
 // store); a field with a null pointer reads as zero
@@ -224,29 +223,6 @@ SHD void load_tiles(const Fld3* F, double* tiles, int64_t ncol, int nx, int L, i
       if (okk) tiles[(f * G + gk) * RP + kk] = v[f];
     } else if (ok) {
       tiles[(f * G + g) * RP + k] = v[f];
-    }
-  }
-}
-
-template <int NW, int G, int NF>
-SHD void store_tiles(const Fld3* F, const double* tiles, int64_t ncol, int nx, int L, int64_t c0) {
-  constexpr int RP = Tiles<NW>::RP;
-  const int tid = threadIdx.x;
-  const int g = tid % G, k = tid / G;
-  const int64_t col = c0 + g;
-  const bool ok = col < ncol && k < L;
-  const int64_t i = ok ? col % nx : 0, j = ok ? col / nx : 0;
-  const int gk = tid / (32 * NW), kk = tid % (32 * NW);
-  const int64_t colk = c0 + gk;
-  const bool okk = colk < ncol && kk < L;
-  const int64_t ik = okk ? colk % nx : 0, jk = okk ? colk / nx : 0;
-#pragma unroll
-  for (int f = 0; f < NF; ++f) {
-    if (!F[f].p) continue;
-    if (F[f].sk == 1) {
-      if (okk) F[f].p[ik * F[f].si + jk * F[f].sj + kk] = tiles[(f * G + gk) * RP + kk];
-    } else if (ok) {
-      F[f].p[i * F[f].si + j * F[f].sj + (int64_t)k * F[f].sk] = tiles[(f * G + g) * RP + k];
     }
   }
 }
@@ -948,97 +924,140 @@ __global__ void __launch_bounds__(LY::THREADS, MINB) vjp_replay_kernel(const __g
   }
 }
 
-// 1b. fields_update reversed (:1452-1553), including the momentum scan,
-// from the replay's final state; starts the adjoint state.
+// ------------------------------------------------------- point launches
+// One thread per point p = k * ncol + col: consecutive columns of one level
+// on consecutive lanes.
+#ifndef SHIELD_VJP_PT_THREADS
+#define SHIELD_VJP_PT_THREADS 128
+#endif
+#ifndef SHIELD_VJP_PT_MINB
+#define SHIELD_VJP_PT_MINB 4
+#endif
+constexpr int PT_THREADS = SHIELD_VJP_PT_THREADS;
+
+struct PointIdx {
+  int64_t p, col;
+  int k;
+};
+SHD bool point_of(const Ws& W, PointIdx& q) {
+  q.p = (int64_t)blockIdx.x * PT_THREADS + threadIdx.x;
+  if (q.p >= W.npts) return false;
+  q.k = (int)(q.p / W.ncol);
+  q.col = q.p - (int64_t)q.k * W.ncol;
+  return true;
+}
+
+// 1b. fields_update reversed (:1452-1553), pointwise part: the tendencies
+// and wmp from the replay's final state, the accumulator; starts the adjoint
+// state. One thread per point, consecutive columns on consecutive lanes.
+__global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_update_pt(const __grid_constant__ VjpArgs A) {
+  const Ws W = workspace(A);
+  PointIdx q;
+  if (!point_of(W, q)) return;
+  const int64_t p = q.p, np = W.npts, col = q.col;
+  const int k = q.k;
+  const MpConst& K = A.K;
+  const int64_t i = col % A.nx, j = col / A.nx;
+  auto in = [&](int f) -> double { return A.in[f].p[i * A.in[f].si + j * A.in[f].sj + (int64_t)k * A.in[f].sk]; };
+  auto cot = [&](int f) -> double {
+    const Fld3& F = A.cot[f];
+    return F.p ? F.p[i * F.si + j * F.sj + (int64_t)k * F.sk] : 0.0;
+  };
+  const double rdt = K.rdt;
+  const double pt = in(IN_PT), delp = in(IN_DELP);
+  double qin[6] = {in(IN_QV), in(IN_QL), in(IN_QR), in(IN_QI), in(IN_QS), in(IN_QG)};
+  if (K.de_ice) de_ice_point(K, qin[3], qin[4], de_ice_qi_dt(A, col, k));
+  const LevState S = load_lev(W.sp(SP_FIN) + p, np);
+  const double dp1 = W.sp(SP_DP1)[p];
+  // q_dt = rdt (q - q0 omq0) omq, pt_dt = rdt (tz - t0) cvm / cp_air
+  const double cq[6] = {cot(OUT_QV_DT), cot(OUT_QL_DT), cot(OUT_QR_DT), cot(OUT_QI_DT), cot(OUT_QS_DT), cot(OUT_QG_DT)};
+  const double qf[6] = {S.qv, S.ql, S.qr, S.qi, S.qs, S.qg};
+  const double dp0 = delp;
+  const double omq0 = dp0 / dp1, omq = dp1 / dp0;
+  double qfb[6], qin_b[6], omq_b = 0.0, omq0_b = 0.0;
+#pragma unroll
+  for (int n = 0; n < 6; ++n) {
+    const double q0 = qin[n] * omq0;
+    qfb[n] = cq[n] * rdt * omq;
+    const double q0_b = -cq[n] * rdt * omq;
+    omq_b += cq[n] * rdt * (qf[n] - q0);
+    qin_b[n] = q0_b * omq0;
+    omq0_b += q0_b * qin[n];
+  }
+  const double cvm = K.c_air + S.qv * K.c_vap + (S.qr + S.ql) * K.C_LIQ + (S.qi + S.qs + S.qg) * K.C_ICE;
+  const double gpt = cot(OUT_PT_DT) * rdt / K.CP_AIR;
+  LevState Sb;
+  Sb.tz = gpt * cvm;
+  const double pt_b = -gpt * cvm;
+  const double cvm_b = gpt * (S.tz - pt);
+  qfb[0] += cvm_b * K.c_vap;
+  qfb[1] += cvm_b * K.C_LIQ;
+  qfb[2] += cvm_b * K.C_LIQ;
+  qfb[3] += cvm_b * K.C_ICE;
+  qfb[4] += cvm_b * K.C_ICE;
+  qfb[5] += cvm_b * K.C_ICE;
+  Sb.qv = qfb[0], Sb.ql = qfb[1], Sb.qr = qfb[2], Sb.qi = qfb[3], Sb.qs = qfb[4], Sb.qg = qfb[5];
+  Sb.w = cot(OUT_W);  // without do_sedi_w, wmp passes through unchanged
+  // the accumulator: qaz_out = qaz_in + the step's increments, and
+  // qa_dt = rdt (qaz_out / ntimes - qa0) (without do_qa, which leaves both)
+  double qa_b = cot(OUT_QAZ), qa0_b = 0.0;
+  if (!K.do_qa) {
+    qa_b += cot(OUT_QA_DT) * rdt / (double)K.ntimes;
+    qa0_b = -cot(OUT_QA_DT) * rdt;
+  }
+  store_lev(W.as(AS_QV) + p, np, Sb);
+  W.as(AS_DP1)[p] = omq_b / dp0 - omq0_b * omq0 / dp1;
+  W.as(AS_P1)[p] = 0.0;
+  W.as(AS_CCN)[p] = 0.0;
+  W.as(AS_CPRAUT)[p] = 0.0;
+  W.as(AS_PT)[p] = pt_b;
+  W.as(AS_DELP)[p] = -omq_b * omq / dp0 + omq0_b / dp1;
+  W.as(AS_DZ0)[p] = 0.0;
+#pragma unroll
+  for (int n = 0; n < 6; ++n) W.as(AS_QIN0 + n)[p] = qin_b[n];
+  W.as(AS_QA)[p] = qa_b;
+  W.as(AS_QA0)[p] = qa0_b;
+  if (!K.sedi_transport) {
+    W.as(AS_U0)[p] = 0.0;
+    W.as(AS_V0)[p] = 0.0;
+    W.as(AS_M1)[p] = 0.0;
+  }
+}
+
+// 1c. (sedi_transport) the momentum transport reversed (:1466-1532): the
+// implicit recurrence of u and v by the precipitation flux, on the column
+// layout. Tiles: u0, v0, delp, the summed flux m1, the udt / vdt
+// cotangents; then the delp cotangent (read and written), the winds' and
+// m1's cotangents (written).
+enum MomTile { MT_U0 = 0, MT_V0, MT_DELP, MT_M1, MT_CU, MT_CV, MT_OUT, MT_ADELP = MT_OUT, MT_U0B, MT_V0B, MT_M1B, N_MT };
 template <int NW, int G, int MINB>
-__global__ void __launch_bounds__(32 * NW * G, MINB) vjp_update_kernel(const __grid_constant__ VjpArgs A) {
+__global__ void __launch_bounds__(32 * NW * G, MINB) vjp_momentum_kernel(const __grid_constant__ VjpArgs A) {
   extern __shared__ double sm[];
   constexpr int RP = Tiles<NW>::RP;
-  const MpConst& K = A.K;
   const int L = A.nz;
   const int64_t c0 = (int64_t)blockIdx.x * G;
-  load_tiles<NW, G, N_VJP_IN>(A.in, sm, A.ncol, A.nx, L, c0);
-  load_tiles<NW, G, N_VJP_COT>(A.cot, sm + (size_t)N_VJP_IN * G * RP, A.ncol, A.nx, L, c0);
   const Ws W = workspace(A);
-  const int64_t np = W.npts;
   {
-    const double* fin = W.sp(SP_FIN);
-    const double* src[10] = {fin, fin + np, fin + 2 * np, fin + 3 * np, fin + 4 * np, fin + 5 * np, fin + 6 * np,
-                             fin + 7 * np, W.sp(SP_DP1), W.sp(SP_M1)};
-    ws_gather<NW, G, 10>(src, sm + (size_t)NT_IN * G * RP, A.ncol, L, c0);
+    const Fld3 F[6] = {A.in[IN_UA], A.in[IN_VA], A.in[IN_DELP], Fld3{nullptr, 0, 0, 0}, A.cot[OUT_UDT], A.cot[OUT_VDT]};
+    load_tiles<NW, G, 6>(F, sm, A.ncol, A.nx, L, c0);
+    // the null fourth field's zero tile is overwritten by m1 (same thread, same element)
+    const double* sm1[1] = {W.sp(SP_M1)};
+    const double* sdp[1] = {W.as(AS_DELP)};
+    ws_gather<NW, G, 1>(sm1, sm + (size_t)MT_M1 * G * RP, A.ncol, L, c0);
+    ws_gather<NW, G, 1>(sdp, sm + (size_t)MT_ADELP * G * RP, A.ncol, L, c0);
   }
   __syncthreads();
-  de_ice_tiles<G, RP>(A, sm, c0);
   int g;
-  Column<NW> C = column_of<NW, G, NT_UPD, 0>(sm, L, g);
+  Column<NW> C = column_of<NW, G, N_MT, 0>(sm, L, g);
   const int64_t col = c0 + g;
-  const int k = C.k;
-  const bool valid = k < L;
-  const double* tile = sm + (size_t)g * RP + k;
-  auto TI = [&](int f, double dflt) -> double { return valid ? tile[(size_t)f * G * RP] : dflt; };
-  auto TC = [&](int f) -> double { return valid ? tile[(size_t)(N_VJP_IN + f) * G * RP] : 0.0; };
-  // the adjoint state's fields AS_QV .. AS_M1, written through tiles 0 ..
-  // N_UPD_OUT - 1 once every tile has been read
-  constexpr int N_UPD_OUT = AS_M1 + 1;
-  double outv[N_UPD_OUT];
-#pragma unroll
-  for (int f = 0; f < N_UPD_OUT; ++f) outv[f] = 0.0;
   if (col < A.ncol) {  // uniform over the column group
-  auto TW = [&](int f, double dflt) -> double { return valid ? tile[(size_t)(NT_IN + f) * G * RP] : dflt; };
-  const double pt = TI(IN_PT, 250.0), delp = TI(IN_DELP, 1.0);
-  const double qin[6] = {TI(IN_QV, 0.0), TI(IN_QL, 0.0), TI(IN_QR, 0.0), TI(IN_QI, 0.0), TI(IN_QS, 0.0),
-                         TI(IN_QG, 0.0)};
-  const LevState S{TW(0, 0.0), TW(1, 0.0), TW(2, 0.0), TW(3, 0.0), TW(4, 0.0), TW(5, 0.0), TW(6, 250.0), TW(7, 0.0)};
-  StepGeom P;
-  P.dp1 = TW(8, 1.0);
-  const double m1 = TW(9, 0.0);
-  // ------------------------------------------------- fields_update reverse
-  const double rdt = K.rdt;
-  LevState Sb{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  double dp1_b = 0.0, pt_b = 0.0, delp_b = 0.0, u0_b = 0.0, v0_b = 0.0, qa0_b = 0.0, qa_b = 0.0;
-  double qin_b[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  if (valid) {
-    const double cq[6] = {TC(OUT_QV_DT), TC(OUT_QL_DT), TC(OUT_QR_DT), TC(OUT_QI_DT), TC(OUT_QS_DT), TC(OUT_QG_DT)};
-    const double qf[6] = {S.qv, S.ql, S.qr, S.qi, S.qs, S.qg};
-    const double dp1 = P.dp1, dp0 = delp;
-    const double omq0 = dp0 / dp1, omq = dp1 / dp0;
-    double qfb[6], omq_b = 0.0, omq0_b = 0.0;
-#pragma unroll
-    for (int n = 0; n < 6; ++n) {
-      const double q0 = qin[n] * omq0;
-      qfb[n] = cq[n] * rdt * omq;
-      const double q0_b = -cq[n] * rdt * omq;
-      omq_b += cq[n] * rdt * (qf[n] - q0);
-      qin_b[n] += q0_b * omq0;
-      omq0_b += q0_b * qin[n];
-    }
-    const double cvm = K.c_air + S.qv * K.c_vap + (S.qr + S.ql) * K.C_LIQ + (S.qi + S.qs + S.qg) * K.C_ICE;
-    const double gpt = TC(OUT_PT_DT) * rdt / K.CP_AIR;
-    Sb.tz = gpt * cvm;
-    pt_b -= gpt * cvm;
-    const double cvm_b = gpt * (S.tz - pt);
-    qfb[0] += cvm_b * K.c_vap;
-    qfb[1] += cvm_b * K.C_LIQ;
-    qfb[2] += cvm_b * K.C_LIQ;
-    qfb[3] += cvm_b * K.C_ICE;
-    qfb[4] += cvm_b * K.C_ICE;
-    qfb[5] += cvm_b * K.C_ICE;
-    Sb.qv = qfb[0], Sb.ql = qfb[1], Sb.qr = qfb[2], Sb.qi = qfb[3], Sb.qs = qfb[4], Sb.qg = qfb[5];
-    dp1_b += omq_b / dp0 - omq0_b * omq0 / dp1;
-    delp_b += -omq_b * omq / dp0 + omq0_b / dp1;
-    // the accumulator: qaz_out = qaz_in + the step's increments, and
-    // qa_dt = rdt (qaz_out / ntimes - qa0) (without do_qa, which leaves
-    // both alone)
-    qa_b = TC(OUT_QAZ);
-    if (!K.do_qa) {
-      qa_b += TC(OUT_QA_DT) * rdt / (double)K.ntimes;
-      qa0_b = -TC(OUT_QA_DT) * rdt;
-    }
-    Sb.w = TC(OUT_W);  // without do_sedi_w, wmp passes through unchanged
-  }
-  double m1_b = 0.0;
-  if (K.sedi_transport) {
-    const double u0 = TI(IN_UA, 0.0), v0 = TI(IN_VA, 0.0);
+    const double rdt = A.K.rdt;
+    const int k = C.k;
+    const bool valid = k < L;
+    double* tile = sm + (size_t)g * RP + (valid ? k : 0);
+    auto T = [&](int f) -> double& { return tile[(size_t)f * G * RP]; };
+    const double u0 = valid ? T(MT_U0) : 0.0, v0 = valid ? T(MT_V0) : 0.0, delp = valid ? T(MT_DELP) : 1.0;
+    const double m1 = valid ? T(MT_M1) : 0.0;
     const double mp = C.prev(m1);
     double au, av, b, D = 1.0;
     if (k == 0 || !valid) {
@@ -1054,9 +1073,8 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_update_kernel(const __g
     double u1, v1;
     C.scan_affine2(au, b, av, b, u1, v1);
     const bool out_k = valid && k >= 1;  // udt, vdt are written for k >= 1 only
-    const double cu = out_k ? TC(OUT_UDT) * rdt : 0.0, cv = out_k ? TC(OUT_VDT) * rdt : 0.0;
-    u0_b -= cu;
-    v0_b -= cv;
+    const double cu = out_k ? T(MT_CU) * rdt : 0.0, cv = out_k ? T(MT_CV) * rdt : 0.0;
+    double u0_b = -cu, v0_b = -cv, delp_b = 0.0;
     double bv[1] = {b}, bn[1];
     C.template nextN<1>(bv, bn);
     const double cn = (valid && k < L - 1) ? bn[0] : 0.0;
@@ -1083,61 +1101,16 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_update_kernel(const __g
     }
     double mv[1] = {mp_b}, mn[1];
     C.template nextN<1>(mv, mn);
-    m1_b = (valid && k < L - 1) ? mn[0] : 0.0;
-  }
-  outv[AS_QV] = Sb.qv;
-  outv[AS_QL] = Sb.ql;
-  outv[AS_QR] = Sb.qr;
-  outv[AS_QI] = Sb.qi;
-  outv[AS_QS] = Sb.qs;
-  outv[AS_QG] = Sb.qg;
-  outv[AS_TZ] = Sb.tz;
-  outv[AS_W] = Sb.w;
-  outv[AS_DP1] = dp1_b;
-  outv[AS_PT] = pt_b;
-  outv[AS_DELP] = delp_b;
-#pragma unroll
-  for (int n = 0; n < 6; ++n) outv[AS_QIN0 + n] = qin_b[n];
-  outv[AS_QA] = qa_b;
-  outv[AS_QA0] = qa0_b;
-  outv[AS_U0] = u0_b;
-  outv[AS_V0] = v0_b;
-  outv[AS_M1] = m1_b;
+    if (valid) {
+      T(MT_ADELP) += delp_b;
+      T(MT_U0B) = u0_b;
+      T(MT_V0B) = v0_b;
+      T(MT_M1B) = k < L - 1 ? mn[0] : 0.0;
+    }
   }
   __syncthreads();
-  if (col < A.ncol && valid) {
-    double* t = sm + (size_t)g * RP + k;
-#pragma unroll
-    for (int f = 0; f < N_UPD_OUT; ++f) t[(size_t)f * G * RP] = outv[f];
-  }
-  __syncthreads();
-  double* dst[N_UPD_OUT];
-#pragma unroll
-  for (int f = 0; f < N_UPD_OUT; ++f) dst[f] = W.as(f);
-  ws_scatter<NW, G, N_UPD_OUT>(dst, sm, A.ncol, L, c0);
-}
-
-// ------------------------------------------------------- point launches
-// One thread per point p = k * ncol + col: consecutive columns of one level
-// on consecutive lanes.
-#ifndef SHIELD_VJP_PT_THREADS
-#define SHIELD_VJP_PT_THREADS 128
-#endif
-#ifndef SHIELD_VJP_PT_MINB
-#define SHIELD_VJP_PT_MINB 4
-#endif
-constexpr int PT_THREADS = SHIELD_VJP_PT_THREADS;
-
-struct PointIdx {
-  int64_t p, col;
-  int k;
-};
-SHD bool point_of(const Ws& W, PointIdx& q) {
-  q.p = (int64_t)blockIdx.x * PT_THREADS + threadIdx.x;
-  if (q.p >= W.npts) return false;
-  q.k = (int)(q.p / W.ncol);
-  q.col = q.p - (int64_t)q.k * W.ncol;
-  return true;
+  double* dst[N_MT - MT_OUT] = {W.as(AS_DELP), W.as(AS_U0), W.as(AS_V0), W.as(AS_M1)};
+  ws_scatter<NW, G, N_MT - MT_OUT>(dst, sm + (size_t)MT_OUT * G * RP, A.ncol, L, c0);
 }
 
 // 2a. icloud's saturation adjustment reversed (subgrid_z_proc,
@@ -1535,60 +1508,53 @@ __global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_sed_tail_p
   W.as(AS_DEN)[p] += den_b;
 }
 
-// 3. fields_init reversed (:27-276), then the gradients written through the
-// shared-memory tiles.
+// 3a. fields_init reversed (:27-276), column part: fix_negative's borrows
+// of vapour from the level above and by the bottom level (:229-276), and
+// the column sums of the CCN cotangents (their total per column goes to
+// SC_CCNB). Tiles: the inputs (those fields_init reads), dp1 and the CCN
+// cotangents; then the vapour's and dp1's cotangents (read and written).
+enum FixTile { XT_DP1 = N_VJP_IN, XT_CCN, XT_CPR, XT_OUT, XT_QVB = XT_OUT, XT_DP1B, N_XT };
 template <int NW, int G, int MINB>
-__global__ void __launch_bounds__(32 * NW * G, MINB) vjp_init_kernel(const __grid_constant__ VjpArgs A) {
+__global__ void __launch_bounds__(32 * NW * G, MINB) vjp_fixneg_kernel(const __grid_constant__ VjpArgs A) {
   extern __shared__ double sm[];
   constexpr int RP = Tiles<NW>::RP;
-  constexpr int WT = N_VJP_IN + N_VJP_GRAD;  // the workspace tiles: AS_QV .. AS_QA0 + 1, then dp1 and p1
-  constexpr int NWS = AS_V0 + 1 + 2;
-  constexpr int NTILE = WT + NWS;
   const MpConst& K = A.K;
   const int L = A.nz;
   const int64_t c0 = (int64_t)blockIdx.x * G;
-  load_tiles<NW, G, N_VJP_IN>(A.in, sm, A.ncol, A.nx, L, c0);
   const Ws W = workspace(A);
   {
-    const double* src[NWS];
-#pragma unroll
-    for (int f = 0; f <= AS_V0; ++f) src[f] = (f == AS_DEN || f == AS_DENFAC || f == AS_DZ) ? nullptr : W.as(f);
-    src[AS_V0 + 1] = W.sp(SP_DP1);
-    src[AS_V0 + 2] = W.sp(SP_P1);
-    ws_gather<NW, G, NWS>(src, sm + (size_t)WT * G * RP, A.ncol, L, c0);
+    Fld3 F[N_VJP_IN];
+    const Fld3 none{nullptr, 0, 0, 0};
+    for (int f = 0; f < N_VJP_IN; ++f) F[f] = (f <= IN_QG || f == IN_DELP) ? A.in[f] : none;
+    load_tiles<NW, G, N_VJP_IN>(F, sm, A.ncol, A.nx, L, c0);
+    const double* src[N_XT - N_VJP_IN] = {W.sp(SP_DP1), W.as(AS_CCN), W.as(AS_CPRAUT), W.as(AS_QV), W.as(AS_DP1)};
+    ws_gather<NW, G, N_XT - N_VJP_IN>(src, sm + (size_t)N_VJP_IN * G * RP, A.ncol, L, c0);
   }
   __syncthreads();
   de_ice_tiles<G, RP>(A, sm, c0);
   int g;
-  Column<NW> C = column_of<NW, G, NTILE, 4>(sm, L, g);
+  Column<NW> C = column_of<NW, G, N_XT, 4>(sm, L, g);
   const int64_t col = c0 + g;
-  const int k = C.k;
-  const bool valid = k < L;
-  const double* tile = sm + (size_t)g * RP + k;
-  auto TI = [&](int f, double dflt) -> double { return valid ? tile[(size_t)f * G * RP] : dflt; };
-  double* gtile = sm + (size_t)N_VJP_IN * G * RP + (size_t)g * RP + k;
-  auto TG = [&](int f) -> double& { return gtile[(size_t)f * G * RP]; };
-  if (col < A.ncol) {
-    auto AS = [&](int f) -> double { return valid ? tile[(size_t)(WT + f) * G * RP] : 0.0; };
-    const double pt = TI(IN_PT, 250.0), delp = TI(IN_DELP, 1.0), dz0 = TI(IN_DELZ, -100.0);
+  if (col < A.ncol) {  // uniform over the column group
+    const int k = C.k;
+    const bool valid = k < L;
+    double* tile = sm + (size_t)g * RP + (valid ? k : 0);
+    auto T = [&](int f) -> double& { return tile[(size_t)f * G * RP]; };
+    auto TI = [&](int f, double dflt) -> double { return valid ? T(f) : dflt; };
+    const double pt = TI(IN_PT, 250.0), delp = TI(IN_DELP, 1.0);
     const double qin[6] = {TI(IN_QV, 0.0), TI(IN_QL, 0.0), TI(IN_QR, 0.0), TI(IN_QI, 0.0), TI(IN_QS, 0.0),
                            TI(IN_QG, 0.0)};
     StepGeom P;
-    P.dp1 = valid ? AS(AS_V0 + 1) : 1.0;
-    P.p1 = valid ? AS(AS_V0 + 2) : 1.0e5;
-    P.ccn = W.sc(SC_CCN)[col];
-    P.c_praut = W.sc(SC_CPRAUT)[col];
-    LevState Sb{AS(AS_QV), AS(AS_QL), AS(AS_QR), AS(AS_QI), AS(AS_QS), AS(AS_QG), AS(AS_TZ), AS(AS_W)};
-    StepAdj Ab{0.0, 0.0, 0.0, AS(AS_DP1), AS(AS_P1), AS(AS_CCN), AS(AS_CPRAUT)};
-    double pt_b = AS(AS_PT), delp_b = AS(AS_DELP), dz0_b = AS(AS_DZ0);
-    double qin_b[6];
-#pragma unroll
-    for (int n = 0; n < 6; ++n) qin_b[n] = AS(AS_QIN0 + n);
-    const double qa0_b = AS(AS_QA0), u0_b = AS(AS_U0), v0_b = AS(AS_V0), qa_b = AS(AS_QA);
-    // replay to the state before fix_negative, then reverse the fix
+    P.dp1 = valid ? T(XT_DP1) : 1.0;
+    LevState Sb{valid ? T(XT_QVB) : 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    StepAdj Ab{0.0, 0.0, 0.0, valid ? T(XT_DP1B) : 0.0, 0.0, 0.0, 0.0};
+    // c_praut = cpaut (ccn RHOR)^(-1/3); ccn is one value per column
+    double ccn_b = C.colsum(valid ? T(XT_CCN) : 0.0);
+    const double cpr_b = C.colsum(valid ? T(XT_CPR) : 0.0);
+    if (!K.prog_ccn) ccn_b += cpr_b * W.sc(SC_CPRAUT)[col] * (-1.0 / 3.0) / W.sc(SC_CCN)[col];
+    if (k == 0) W.sc(SC_CCNB)[col] = ccn_b;
     const double omq = delp / P.dp1;
-    LevState S0{qin[0] * omq, qin[1] * omq, qin[2] * omq, qin[3] * omq, qin[4] * omq, qin[5] * omq, pt,
-                TI(IN_W, 0.0)};
+    const LevState S0{qin[0] * omq, qin[1] * omq, qin[2] * omq, qin[3] * omq, qin[4] * omq, qin[5] * omq, pt, 0.0};
     if (K.fix_negative) {
       LevState S1 = S0;
       fix_negative_point(K, S1.qv, S1.ql, S1.qr, S1.qi, S1.qs, S1.qg, S1.tz);
@@ -1666,79 +1632,95 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_init_kernel(const __gri
           Ab.dp1 += wdb[k];
         }
       }
-      if (valid)
-        fix_negative_point_b(K, S0.qv, S0.ql, S0.qr, S0.qi, S0.qs, S0.qg, S0.tz, Sb.qv, Sb.ql, Sb.qr, Sb.qi, Sb.qs,
-                             Sb.qg, Sb.tz);
-    }
-    // c_praut = cpaut (ccn RHOR)^(-1/3); ccn is one value per column
-    double ccn_b = C.colsum(valid ? Ab.ccn : 0.0);
-    const double cpr_b = C.colsum(valid ? Ab.c_praut : 0.0);
-    if (!K.prog_ccn) {
-      ccn_b += cpr_b * P.c_praut * (-1.0 / 3.0) / P.ccn;
-      if (K.use_ccn) {
-        // ccn = ccn0 RDGAS tz / p1 of the bottom level, tz = pt there
-        double tzb, p1b;
-        C.bcast2(pt, P.p1, L - 1, tzb, p1b);
-        if (k == L - 1) {
-          pt_b += ccn_b * P.ccn / tzb;
-          Ab.p1 -= ccn_b * P.ccn / p1b;
-        }
-      }
     }
     if (valid) {
-      // p1 = den0 RDGAS pt, den0 = -dp1 / (g dz0)
-      const double den0 = -P.dp1 / (K.GRAV * dz0);
-      const double den0_b = Ab.p1 * K.RDGAS * pt;
-      pt_b += Ab.p1 * den0 * K.RDGAS;
-      Ab.dp1 -= den0_b / (K.GRAV * dz0);
-      dz0_b += den0_b * P.dp1 / (K.GRAV * dz0 * dz0);
-      // q = q_in omq, omq = delp / dp1, dp1 = delp (1 - qv_in)
-      const double sq_b[6] = {Sb.qv, Sb.ql, Sb.qr, Sb.qi, Sb.qs, Sb.qg};
-      double omq_b = 0.0;
-#pragma unroll
-      for (int n = 0; n < 6; ++n) {
-        omq_b += sq_b[n] * qin[n];
-        qin_b[n] += sq_b[n] * omq;
-      }
-      delp_b += omq_b / P.dp1;
-      Ab.dp1 -= omq_b * omq / P.dp1;
-      delp_b += Ab.dp1 * (1.0 - qin[0]);
-      qin_b[0] -= Ab.dp1 * delp;
-      pt_b += Sb.tz;
-      TG(IN_PT) = pt_b;
-      TG(IN_QV) = qin_b[0];
-      TG(IN_QL) = qin_b[1];
-      TG(IN_QR) = qin_b[2];
-      TG(IN_QI) = qin_b[3];
-      TG(IN_QS) = qin_b[4];
-      TG(IN_QG) = qin_b[5];
-      TG(IN_QA) = qa0_b;
-      TG(IN_UA) = u0_b;
-      TG(IN_VA) = v0_b;
-      TG(IN_DELP) = delp_b;
-      TG(IN_DELZ) = dz0_b;
-      TG(IN_W) = Sb.w;
-      TG(IN_QAZ) = qa_b;
-      if (K.de_ice) {
-        // de_ice reversed: where qi became qi0_max, the input qi moves qs
-        // (qs + qi - qi0_max) and the tendencies it sets (qi_dt = dqi,
-        // qs_dt += qi_dt - dqi, dqi = (qi0_max - qi + timestep qi_dt) rdt);
-        // elsewhere qi and qs pass through
-        double qi0 = A.in[IN_QI].p[(col % A.nx) * A.in[IN_QI].si + (col / A.nx) * A.in[IN_QI].sj +
-                                   (int64_t)k * A.in[IN_QI].sk];
-        double qs0 = 0.0;
-        if (de_ice_point(K, qi0, qs0, de_ice_qi_dt(A, col, k)) == 2) {
-          auto cot = [&](int o) -> double {
-            const Fld3& f = A.cot[o];
-            return f.p ? f.p[(col % A.nx) * f.si + (col / A.nx) * f.sj + (int64_t)k * f.sk] : 0.0;
-          };
-          TG(IN_QI) = TG(IN_QS) + (cot(OUT_QS_DT) - cot(OUT_QI_DT)) * K.rdt;
-        }
-      }
+      T(XT_QVB) = Sb.qv;
+      T(XT_DP1B) = Ab.dp1;
     }
   }
   __syncthreads();
-  store_tiles<NW, G, N_VJP_GRAD>(A.grad, sm + (size_t)N_VJP_IN * G * RP, A.ncol, A.nx, L, c0);
+  double* dst[N_XT - XT_OUT] = {W.as(AS_QV), W.as(AS_DP1)};
+  ws_scatter<NW, G, N_XT - XT_OUT>(dst, sm + (size_t)XT_OUT * G * RP, A.ncol, L, c0);
+}
+
+// 3b. fields_init reversed, pointwise part: fix_negative's point step, the
+// bottom level's CCN (use_ccn), the pressure, the mixing-ratio conversion,
+// de_ice; writes the gradients.
+__global__ void __launch_bounds__(PT_THREADS, SHIELD_VJP_PT_MINB) vjp_init_pt(const __grid_constant__ VjpArgs A) {
+  const Ws W = workspace(A);
+  PointIdx q;
+  if (!point_of(W, q)) return;
+  const int64_t p = q.p, np = W.npts, col = q.col;
+  const int k = q.k, L = A.nz;
+  const MpConst& K = A.K;
+  const int64_t i = col % A.nx, j = col / A.nx;
+  auto at = [&](const Fld3& F) -> double { return F.p[i * F.si + j * F.sj + (int64_t)k * F.sk]; };
+  auto put = [&](const Fld3& F, double v) {
+    if (F.p) F.p[i * F.si + j * F.sj + (int64_t)k * F.sk] = v;
+  };
+  const double pt = at(A.in[IN_PT]), delp = at(A.in[IN_DELP]), dz0 = at(A.in[IN_DELZ]);
+  double qin[6] = {at(A.in[IN_QV]), at(A.in[IN_QL]), at(A.in[IN_QR]), at(A.in[IN_QI]), at(A.in[IN_QS]),
+                   at(A.in[IN_QG])};
+  int de_ice_branch = 0;
+  if (K.de_ice) de_ice_branch = de_ice_point(K, qin[3], qin[4], de_ice_qi_dt(A, col, k));
+  const double dp1 = W.sp(SP_DP1)[p];
+  LevState Sb = load_lev(W.as(AS_QV) + p, np);
+  double Ab_dp1 = W.as(AS_DP1)[p], Ab_p1 = W.as(AS_P1)[p];
+  double pt_b = W.as(AS_PT)[p], delp_b = W.as(AS_DELP)[p], dz0_b = W.as(AS_DZ0)[p];
+  double qin_b[6];
+#pragma unroll
+  for (int n = 0; n < 6; ++n) qin_b[n] = W.as(AS_QIN0 + n)[p];
+  const double omq = delp / dp1;
+  if (K.fix_negative)
+    fix_negative_point_b(K, qin[0] * omq, qin[1] * omq, qin[2] * omq, qin[3] * omq, qin[4] * omq, qin[5] * omq, pt,
+                         Sb.qv, Sb.ql, Sb.qr, Sb.qi, Sb.qs, Sb.qg, Sb.tz);
+  if (!K.prog_ccn && K.use_ccn && k == L - 1) {
+    // ccn = ccn0 RDGAS tz / p1 of the bottom level, tz = pt there
+    const double ccn_b = W.sc(SC_CCNB)[col], ccn = W.sc(SC_CCN)[col];
+    pt_b += ccn_b * ccn / pt;
+    Ab_p1 -= ccn_b * ccn / W.sp(SP_P1)[p];
+  }
+  // p1 = den0 RDGAS pt, den0 = -dp1 / (g dz0)
+  const double den0 = -dp1 / (K.GRAV * dz0);
+  const double den0_b = Ab_p1 * K.RDGAS * pt;
+  pt_b += Ab_p1 * den0 * K.RDGAS;
+  Ab_dp1 -= den0_b / (K.GRAV * dz0);
+  dz0_b += den0_b * dp1 / (K.GRAV * dz0 * dz0);
+  // q = q_in omq, omq = delp / dp1, dp1 = delp (1 - qv_in)
+  const double sq_b[6] = {Sb.qv, Sb.ql, Sb.qr, Sb.qi, Sb.qs, Sb.qg};
+  double omq_b = 0.0;
+#pragma unroll
+  for (int n = 0; n < 6; ++n) {
+    omq_b += sq_b[n] * qin[n];
+    qin_b[n] += sq_b[n] * omq;
+  }
+  delp_b += omq_b / dp1;
+  Ab_dp1 -= omq_b * omq / dp1;
+  delp_b += Ab_dp1 * (1.0 - qin[0]);
+  qin_b[0] -= Ab_dp1 * delp;
+  pt_b += Sb.tz;
+  if (de_ice_branch == 2) {
+    // de_ice reversed: where qi became qi0_max, the input qi moves qs
+    // (qs + qi - qi0_max) and the tendencies it sets (qi_dt = dqi,
+    // qs_dt += qi_dt - dqi, dqi = (qi0_max - qi + timestep qi_dt) rdt);
+    // elsewhere qi and qs pass through
+    auto cot = [&](int o) -> double { return A.cot[o].p ? at(A.cot[o]) : 0.0; };
+    qin_b[3] = qin_b[4] + (cot(OUT_QS_DT) - cot(OUT_QI_DT)) * K.rdt;
+  }
+  put(A.grad[IN_PT], pt_b);
+  put(A.grad[IN_QV], qin_b[0]);
+  put(A.grad[IN_QL], qin_b[1]);
+  put(A.grad[IN_QR], qin_b[2]);
+  put(A.grad[IN_QI], qin_b[3]);
+  put(A.grad[IN_QS], qin_b[4]);
+  put(A.grad[IN_QG], qin_b[5]);
+  put(A.grad[IN_QA], W.as(AS_QA0)[p]);
+  put(A.grad[IN_UA], W.as(AS_U0)[p]);
+  put(A.grad[IN_VA], W.as(AS_V0)[p]);
+  put(A.grad[IN_DELP], delp_b);
+  put(A.grad[IN_DELZ], dz0_b);
+  put(A.grad[IN_W], Sb.w);
+  put(A.grad[IN_QAZ], W.as(AS_QA)[p]);
 }
 
 // ---------------------------------------------------------------- launch
@@ -1760,17 +1742,17 @@ __global__ void __launch_bounds__(32 * NW * G, MINB) vjp_init_kernel(const __gri
 template <class RL, int RMINB, int NW, int G, int CMINB = SHIELD_VJP_COL_MINB, int FMINB = SHIELD_VJP_FALL_MINB,
           int SMINB = SHIELD_VJP_SED_MINB>
 cudaError_t launch_vjp(const VjpArgs& A, cudaStream_t st) {
-  using SU = ColSmem<NW, G, NT_UPD, 0>;
+  using SU = ColSmem<NW, G, N_MT, 0>;
   using SF = ColSmem<NW, G, N_FT, 0>;
   using SS = ColSmem<NW, G, N_ST, 0>;
-  using SI = ColSmem<NW, G, N_VJP_IN + N_VJP_GRAD + AS_V0 + 3, 4>;
+  using SI = ColSmem<NW, G, N_XT, 4>;
   cudaError_t e = cudaFuncSetAttribute(vjp_replay_kernel<RL, RMINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)ReplaySmem<RL>::bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(vjp_update_kernel<NW, G, CMINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(vjp_momentum_kernel<NW, G, CMINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)SU::bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(vjp_init_kernel<NW, G, CMINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(vjp_fixneg_kernel<NW, G, CMINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)SI::bytes);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(vjp_fall_kernel<NW, G, FMINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SF::bytes);
@@ -1783,7 +1765,8 @@ cudaError_t launch_vjp(const VjpArgs& A, cudaStream_t st) {
   const unsigned pblk = (unsigned)((npts + PT_THREADS - 1) / PT_THREADS);
   constexpr int T = 32 * NW * G;
   vjp_replay_kernel<RL, RMINB><<<rblk, RL::THREADS, ReplaySmem<RL>::bytes, st>>>(A);
-  vjp_update_kernel<NW, G, CMINB><<<nblk, T, SU::bytes, st>>>(A);
+  vjp_update_pt<<<pblk, PT_THREADS, 0, st>>>(A);
+  if (A.K.sedi_transport) vjp_momentum_kernel<NW, G, CMINB><<<nblk, T, SU::bytes, st>>>(A);
   for (int it = A.K.ntimes - 1; it >= 0; --it) {
     vjp_subgrid_pt<<<pblk, PT_THREADS, 0, st>>>(A, it);
     vjp_icloud_pt<<<pblk, PT_THREADS, 0, st>>>(A, it);
@@ -1798,13 +1781,14 @@ cudaError_t launch_vjp(const VjpArgs& A, cudaStream_t st) {
     vjp_fall_kernel<NW, G, FMINB><<<nblk, T, SF::bytes, st>>>(A, it, 0);
     vjp_revap1_pt<<<pblk, PT_THREADS, 0, st>>>(A, it, 0);
   }
-  vjp_init_kernel<NW, G, CMINB><<<nblk, T, SI::bytes, st>>>(A);
+  vjp_fixneg_kernel<NW, G, CMINB><<<nblk, T, SI::bytes, st>>>(A);
+  vjp_init_pt<<<pblk, PT_THREADS, 0, st>>>(A);
   return cudaGetLastError();
 }
 
 }  // namespace
 
-int mp_vjp_launches(int ntimes) { return 3 + 12 * ntimes; }
+int mp_vjp_launches(int ntimes) { return 5 + 12 * ntimes; }
 
 // The replay takes the plain step's launch shape for each level range
 // (mp_plain.cu), so that it repeats the step's arithmetic exactly.

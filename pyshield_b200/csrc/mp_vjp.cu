@@ -799,8 +799,28 @@ template <class LY>
 struct ReplaySmem {
   static constexpr size_t scratch = (size_t)N_VJP_IN * LY::G * LY::RP;
   static constexpr size_t work = scratch + (size_t)LY::NGRP * 2 * LY::SCR;
-  static constexpr size_t bytes = (work + (size_t)LY::NGRP * LY::WORK) * sizeof(double);
+  static constexpr size_t rec = work + (size_t)LY::NGRP * LY::WORK;
+  static constexpr int NREC = 15;  // record tiles: the largest group stored at once
+  static constexpr size_t bytes = (rec + (size_t)NREC * LY::G * LY::RP) * sizeof(double);
 };
+
+// The replay's records collect in shared-memory tiles (field f of block
+// column g at level k at (f * G + g) * RP + k) and go to their workspace
+// rows dst[f] at block-uniform points: consecutive threads take consecutive
+// columns of one level, so each warp stores whole sectors (stored where they
+// arise, each warp store touched about 30 sectors: a warp holds the levels
+// of one column). Block barriers on both sides.
+template <int G, int RP, int NMAX>
+SHD void flush_records(const double* rec, double* const (&dst)[NMAX], int n, int64_t ncol, int L, int64_t c0) {
+  __syncthreads();
+  for (int e = threadIdx.x; e < G * L; e += blockDim.x) {
+    const int g = e % G, k = e / G;
+    if (c0 + g >= ncol) continue;
+    const int64_t o = (int64_t)k * ncol + c0 + g;
+    for (int f = 0; f < n; ++f) dst[f][o] = rec[(f * G + g) * RP + k];
+  }
+  __syncthreads();
+}
 
 template <class LY, int MINB>
 __global__ void __launch_bounds__(LY::THREADS, MINB) vjp_replay_kernel(const __grid_constant__ VjpArgs A) {
@@ -851,7 +871,6 @@ __global__ void __launch_bounds__(LY::THREADS, MINB) vjp_replay_kernel(const __g
   const double* tile = sm + (size_t)(slot_ok ? g : 0) * RP + (valid ? k : 0);
   auto TI = [&](int f, double dflt) -> double { return valid ? tile[(size_t)f * G * RP] : dflt; };
   const Ws W = workspace(A);
-  const int64_t np = W.npts;
   const int64_t cc = col_ok ? col : 0;
   const int64_t p = (int64_t)(valid ? k : 0) * A.ncol + cc;
   const bool head = col_ok && k == 0;
@@ -880,47 +899,82 @@ __global__ void __launch_bounds__(LY::THREADS, MINB) vjp_replay_kernel(const __g
   }
   double m1 = 0.0, m1_sol = 0.0, vtr = VF_MIN, vtg = VF_MIN, vts = VF_MIN, qa = 0.0, ice = 0.0, snow = 0.0,
          graupel = 0.0;
+  constexpr int NREC = SM::NREC;
+  constexpr int64_t RS = (int64_t)G * RP;  // stride between record tiles
+  const double* rec = sm + SM::rec;
+  double* rt = sm + SM::rec + (size_t)(slot_ok ? g : 0) * RP + (valid ? k : 0);  // this thread's record slot
+  auto put = [&](int f, double v) {
+    if (valid) rt[f * RS] = v;
+  };
+  auto put_lev = [&](int f, const LevState& X) {
+    if (valid) store_lev(rt + f * RS, RS, X);
+  };
   const int nt = K.ntimes;
 #pragma unroll 1
   for (int it = 0; it < nt; ++it) {
     substep_geometry(C, K, valid, pt, dz0, S, P);
-    if (valid) {
-      W.ss(it, SS_DEN)[p] = P.den;
-      W.ss(it, SS_DENFAC)[p] = P.denfac;
-      W.ss(it, SS_DZ)[p] = P.dz;
-      W.ss(it, SS_DZ1)[p] = P.dz1;
-      store_lev(W.ckf(it, CKF_E0) + p, np, S);
+    put_lev(0, S);
+    put(8, P.den);
+    put(9, P.denfac);
+    put(10, P.dz);
+    put(11, P.dz1);
+    {
+      double* d[NREC] = {};
+      for (int f = 0; f < 8; ++f) d[f] = W.ckf(it, CKF_E0 + f);
+      d[8] = W.ss(it, SS_DEN), d[9] = W.ss(it, SS_DENFAC), d[10] = W.ss(it, SS_DZ), d[11] = W.ss(it, SS_DZ1);
+      flush_records<G, RP, NREC>(rec, d, 12, A.ncol, L, c0);
     }
     // the first warm_rain pass, sedimentation, the second pass (one copy of
     // the warm_rain code, run twice, as in the forward kernel)
 #pragma unroll 1
     for (int pass = 0; pass < 2; ++pass) {
       double m1r, r1;
+      // tiles 0 .. 12: the pass's block; 13: the fall speed; 14: the slope
       warm_rain<false>(C, K, KF, valid, S, P, vtr, m1r, r1, nullptr,
-                       VjpRec{W.ckf(it, pass * CKF_PASS + CKF_BLOCK) + p, W.ss(it, pass ? SS_SL_B : SS_SL_A) + p,
-                              W.scc(it, pass ? SCC_FALL_B : SCC_FALL_A) + cc, np, valid, head, false});
+                       VjpRec{rt, rt + 14 * RS, W.scc(it, pass ? SCC_FALL_B : SCC_FALL_A) + cc, RS, valid, head,
+                              false});
       m1 = (pass == 0) ? m1 + m1r : m1 + m1r + m1_sol;
-      if (valid) {
-        W.ss(it, pass ? SS_VTR_B : SS_VTR_A)[p] = vtr;
-        // autoconversion changed ql and qr
-        W.ckf(it, pass * CKF_PASS + CKF_BLOCK + 11)[p] = S.ql;
-        W.ckf(it, pass * CKF_PASS + CKF_BLOCK + 12)[p] = S.qr;
+      put(13, vtr);
+      put(11, S.ql);  // autoconversion changed ql and qr
+      put(12, S.qr);
+      {
+        double* d[NREC] = {};
+        for (int f = 0; f < 13; ++f) d[f] = W.ckf(it, pass * CKF_PASS + CKF_BLOCK + f);
+        d[13] = W.ss(it, pass ? SS_VTR_B : SS_VTR_A);
+        d[14] = W.ss(it, pass ? SS_SL_B : SS_SL_A);
+        flush_records<G, RP, NREC>(rec, d, 15, A.ncol, L, c0);
       }
       if (pass == 1) break;
+      // tiles 0 .. 7: the state after sedimentation; 8, 9, 10: vtg, vts, vti
       sedimentation<false>(C, K, KF, valid, S, P, vtg, vts, m1_sol, ice, snow, graupel, nullptr,
-                           VjpRec{nullptr, W.ss(it, SS_VTI) + p, nullptr, np, valid, false, false});
-      if (valid) {
-        W.ss(it, SS_VTG)[p] = vtg;
-        W.ss(it, SS_VTS)[p] = vts;
-        store_lev(W.ckf(it, CKF_PASS) + p, np, S);
+                           VjpRec{nullptr, rt + 10 * RS, nullptr, RS, valid, false, false});
+      put_lev(0, S);
+      put(8, vtg);
+      put(9, vts);
+      {
+        double* d[NREC] = {};
+        for (int f = 0; f < 8; ++f) d[f] = W.ckf(it, CKF_PASS + f);
+        d[8] = W.ss(it, SS_VTG), d[9] = W.ss(it, SS_VTS), d[10] = W.ss(it, SS_VTI);
+        flush_records<G, RP, NREC>(rec, d, 11, A.ncol, L, c0);
       }
     }
-    icloud<false>(C, K, KF, valid, S, P, qa, vtg, vtr, vts,
-                  VjpRec{W.ckf(it, CKF_E4) + p, W.ss(it, SS_SL_I) + p, nullptr, np, valid, false, true});
+    // tiles 0 .. 7: the state before the adjustment; 8, 9: the ice slope and
+    // the melted / frozen cloud ice
+    icloud<false>(C, K, KF, valid, S, P, qa, vtg, vtr, vts, VjpRec{rt, rt + 8 * RS, nullptr, RS, valid, false, true});
+    {
+      double* d[NREC] = {};
+      for (int f = 0; f < 8; ++f) d[f] = W.ckf(it, CKF_E4 + f);
+      d[8] = W.ss(it, SS_SL_I), d[9] = W.ss(it, SS_S1QI);
+      flush_records<G, RP, NREC>(rec, d, 10, A.ncol, L, c0);
+    }
   }
-  if (valid) {
-    W.sp(SP_M1)[p] = m1;
-    store_lev(W.sp(SP_FIN) + p, np, S);
+  put(0, m1);
+  put_lev(1, S);
+  {
+    double* d[NREC] = {};
+    d[0] = W.sp(SP_M1);
+    for (int f = 0; f < 8; ++f) d[1 + f] = W.sp(SP_FIN + f);
+    flush_records<G, RP, NREC>(rec, d, 9, A.ncol, L, c0);
   }
 }
 

@@ -1099,11 +1099,17 @@ def run_ours(args, rank, world, local_rank):
 
 
 def run_ensemble(args):
-    """64 members of sizes C24/C48/C96 (6 N^2 columns, the six tiles side by
-    side), dt ~ U(120, 225) s, per-member Ts offset N(0, 3) K and seed, L79.
-    Times 64 sequential launches (one Microphysics per member, FP64 and
+    """The ensemble workload on its own (``--ensemble``): one JSON line."""
+    emit(measure_ensemble(args.members, args.levels, args.steps))
+
+
+def measure_ensemble(nm, levels, steps):
+    """``nm`` members of sizes C24/C48/C96 (6 N^2 columns, the six tiles side
+    by side), dt ~ U(120, 225) s, per-member Ts offset N(0, 3) K and seed.
+    Times ``nm`` sequential launches (one Microphysics per member, FP64 and
     mixed) against one batched launch of the whole ensemble (autotuned
-    launch shape, replayed from a CUDA graph)."""
+    launch shape, replayed from a CUDA graph); mean of ``steps`` runs after
+    a warm-up, CUDA events."""
     import numpy as np
     import torch
 
@@ -1111,17 +1117,15 @@ def run_ensemble(args):
     from pyshield_b200.ensemble import MicrophysicsEnsemble
     from pyshield_b200.microphysics import Microphysics
 
-    torch.cuda.set_device(0)
     rng = np.random.default_rng(4)
-    nm = args.members
     sizes = rng.choice([24, 48, 96], nm)
     dts = rng.uniform(120.0, 225.0, nm)
     offs = rng.normal(0.0, 3.0, nm)
     cfg = PhysicsConfig(dt_atmos=150.0)
     built = []
     for m in range(nm):
-        ms, sf, qf, gd, host, land, (nx, ny, n) = build_state(args.levels, torch.device("cuda", 0), seed=7000 + m,
-                                                             n_cube=int(sizes[m]))
+        ms, sf, qf, gd, host, land, (nx, ny, n) = build_state(levels, torch.device("cuda", torch.cuda.current_device()),
+                                                             seed=7000 + m, n_cube=int(sizes[m]))
         host.clear()
         ms.pt.view.add_(float(offs[m]))
         built.append((ms, sf, qf, gd, n))
@@ -1148,14 +1152,14 @@ def run_ensemble(args):
             for mp_, b, dt in zip(mps, built, dts):
                 mp_(b[0], float(dt))
 
-        out[f"sequential_{form}_ms"] = timed(sequential, args.steps)
+        out[f"sequential_{form}_ms"] = timed(sequential, steps)
         del mps
     for form in ("mixed", "plain"):
         ens = MicrophysicsEnsemble(cfg, [b[0] for b in built], [b[3].area for b in built], [float(d) for d in dts],
                                    precision=form)
         tuned, timings = ens.autotune(reps=1)
         ens.capture()
-        out[f"batched_{form}_ms"] = timed(ens.replay, args.steps)
+        out[f"batched_{form}_ms"] = timed(ens.replay, steps)
         out[f"autotune_{form}"] = {f"{g}x{b}": round(ms, 3) for (g, b), ms in timings.items()}
         out[f"tuned_{form}"] = f"{tuned[0]} columns/block, {tuned[1]} blocks/SM"
         ens.graph = None
@@ -1163,16 +1167,19 @@ def run_ensemble(args):
     rec = {
         "metric": "GFDL MP column-steps/s, ensemble",
         "workload": f"{nm} members, sizes C24/C48/C96 ({int((sizes == 24).sum())}/{int((sizes == 48).sum())}/"
-                    f"{int((sizes == 96).sum())}), {total_cols} columns x L{args.levels}, dt U(120,225) s",
+                    f"{int((sizes == 96).sum())}), {total_cols} columns x L{levels}, dt U(120,225) s",
         "unit": "column-steps/s",
-        "steps": args.steps,
+        "steps": steps,
     }
     for k, v in list(out.items()):
         if k.endswith("_ms"):
             rec[k.replace("_ms", "_column_steps_per_s")] = total_cols / (v / 1000.0)
         rec[k] = v
     rec["batched_mixed_vs_sequential_plain"] = out["sequential_plain_ms"] / out["batched_mixed_ms"]
-    emit(rec)
+    rec["batched_mixed_vs_sequential_mixed"] = out["sequential_mixed_ms"] / out["batched_mixed_ms"]
+    del built
+    torch.cuda.empty_cache()
+    return rec
 
 
 def emit(rec):
@@ -1220,6 +1227,7 @@ def main():
     ap.add_argument("--no-c384", action="store_true", help="skip the C384 mixed-against-plain comparison")
     ap.add_argument("--ncube", type=int, default=N_CUBE, help="cube size N of the CN workload (default 96)")
     ap.add_argument("--ensemble", action="store_true", help="run the ensemble workload instead")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble measurement of the default line")
     ap.add_argument("--members", type=int, default=64)
     args = ap.parse_args()
     if args.warmup < 3:
@@ -1318,6 +1326,10 @@ def main():
                if (rank == 0 and world == 1 and not args.no_physics and args.form == "plain") else None)
     coupling = (run_coupling(n_cube=args.ncube, nlev=nlev)
                 if (rank == 0 and world == 1 and not args.no_coupling and args.form == "plain") else None)
+    # the ensemble of 64 members C24/C48/C96 at L79: sequential launches
+    # against one batched, graph-replayed launch
+    ensemble = (measure_ensemble(args.members, 79, 3)
+                if (rank == 0 and world == 1 and not args.no_ensemble and args.form == "plain") else None)
     fp64 = None
     if rank == 0:
         peak64 = fp64_peak()
@@ -1378,6 +1390,7 @@ def main():
             "dycore_to_physics": d2p,
             "agrid_to_dgrid": dwind,
             "c384_mixed": c384,
+            "ensemble": ensemble,
         }
         emit(rec)
 

@@ -452,10 +452,9 @@ SHD void sedi_heat_b(Column<NW>& C, const MpConst& K, double tz, double dz1, dou
 // melt_lev is set (the reverses of the melting and of the fall speeds are
 // pointwise and run in their own launch).
 template <int NW>
-static __device__ __noinline__ void sedimentation_b(Column<NW>& C, const MpConst& K, bool valid, const LevState& S0,
-                                                    const StepGeom& P, double vtg, double vti, double vts,
-                                                    double m1s_b, double ice_c, double snow_c, double graupel_c,
-                                                    double (&vt_b)[3], LevState& Sb, StepAdj& Ab, bool& melt_lev) {
+SHD void sedimentation_b(Column<NW>& C, const MpConst& K, bool valid, const LevState& S0, const StepGeom& P,
+                         double vtg, double vti, double vts, double m1s_b, double ice_c, double snow_c,
+                         double graupel_c, double (&vt_b)[3], LevState& Sb, StepAdj& Ab, bool& melt_lev) {
   const int k = C.k, L = C.L;
   const double dp1 = P.dp1, dz = P.dz;
   const int first = C.min_int((valid && S0.tz > K.tice) ? k : (1 << 30));

@@ -17,8 +17,6 @@ cudaError_t mp_launch_ensemble_plain(const MpArgs* members, const int64_t* offs,
 cudaError_t mp_launch_vjp(const VjpArgs& A, cudaStream_t st);
 // doubles of the adjoint's workspace for nt sub-steps over npts points and ncol columns
 int64_t mp_vjp_workspace_doubles(int nt, int64_t npts, int64_t ncol);
-// kernel launches of one adjoint call with nt sub-steps
-int mp_vjp_launches(int nt);
 cudaError_t mp_launch_ensemble_mixed(const MpArgs* members, const int64_t* offs, int nm, int nz, int G, int grid,
                                      unsigned long long* counter, cudaStream_t st);
 

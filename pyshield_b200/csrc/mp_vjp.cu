@@ -1841,8 +1841,6 @@ cudaError_t launch_vjp(const VjpArgs& A, cudaStream_t st) {
 
 }  // namespace
 
-int mp_vjp_launches(int ntimes) { return 5 + 12 * ntimes; }
-
 // The replay takes the plain step's launch shape for each level range
 // (mp_plain.cu), so that it repeats the step's arithmetic exactly.
 cudaError_t mp_launch_vjp(const VjpArgs& A, cudaStream_t st) {

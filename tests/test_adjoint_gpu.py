@@ -147,7 +147,7 @@ def test_exact_config_variants(cfg):
     _assert_exact(exact_check(8, 3, 79, 150.0, 13, **cfg))
 
 
-@pytest.mark.parametrize("nz", [31, 127])
+@pytest.mark.parametrize("nz", [31, 90, 127])
 def test_exact_column_heights(nz):
     _assert_exact(exact_check(6, 3, nz, 150.0, 14))
 

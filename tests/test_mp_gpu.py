@@ -67,9 +67,10 @@ CONFIGS = {
 
 
 @pytest.mark.parametrize("cname", sorted(CONFIGS))
-@pytest.mark.parametrize("nlev,dt", [(79, 150.0), (127, 180.0), (63, 450.0)])
+@pytest.mark.parametrize("nlev,dt", [(79, 150.0), (127, 180.0), (63, 450.0), (30, 150.0), (90, 180.0), (160, 150.0)])
 def test_c12_vs_oracle(cname, nlev, dt):
-    """C12 (6 x 12 x 12 = 864 columns) synthetic state, one step."""
+    """C12 (6 x 12 x 12 = 864 columns) synthetic state, one step; every launch
+    shape of the level ranges (up to 32, 64, 80, 96, 128 and 256 levels)."""
     from pyshield_b200._config import PhysicsConfig
     from pyshield_b200.inputs import make_state
 

@@ -137,7 +137,9 @@ int shield_mp_last_error(void* handle, char* buf, size_t n);
  * evaluated in FP64 by hand-written reverse kernels after a replay of the
  * step from its inputs. The replay's records live in a workspace the handle
  * allocates on the first call (about 100 doubles per grid point and
- * sub-step) and keeps, grown as needed, until shield_mp_destroy.
+ * sub-step) and keeps, grown as needed, until shield_mp_destroy. VJP calls
+ * on one handle share that workspace: calls that overlap on the GPU (other
+ * streams) race; calls on one stream, or on different handles, do not.
  *
  * Outputs of the step, whose cotangents are given: the ten tendencies
  * (as written by the step: udt and vdt for levels k >= 1 only), wmp (which

@@ -6,21 +6,24 @@
 // (pySHiELD/stencils/microphysics.py:1981-2263).
 //
 // A sequence of launches over a workspace in global memory:
-//  1. the replay (one thread per level, NW warps per column, as the forward
-//     kernel) runs the step with the forward's own stage functions and
-//     stores, per sub-step and level, the state at the entry of every
-//     stage and inside warm_rain and icloud, the sub-step geometry, the fall
-//     speeds and slopes, and each column's rain-fall decisions; it then
-//     reverses fields_update (including the momentum scan);
+//  1. the replay, on the forward step's own thread layout (one thread per
+//     level), runs the step with the forward's own stage functions and
+//     records, per sub-step and point, the fields each stage changes at the
+//     entry of every stage and inside warm_rain and icloud, the sub-step
+//     geometry, the fall speeds and slopes, and each column's rain-fall
+//     decisions (through shared-memory tiles, in whole-sector stores);
+//     fields_update's reverse follows as a point launch and a column launch
+//     of the momentum recurrence;
 //  2. per sub-step, from the last: the pointwise reverses run one thread per
 //     (level, column) point with consecutive columns on consecutive lanes,
 //     so that a warp's 32 points take the same physics branches far more
 //     often than the levels of one column do, and every warp of the launch
 //     runs the same short code. The reverses of the vertical recurrences
-//     (the rain fall, sedimentation) run on the column layout between them.
-//     The transposes of the slopes' three-point stencils are gathered at the
-//     start of the next point launch;
-//  3. the reverse of fields_init, on the column layout, writes the gradients.
+//     (the rain fall, sedimentation's falls) run on the column layout
+//     between them. The transposes of the slopes' three-point stencils are
+//     gathered at the start of the next point launch;
+//  3. fields_init's reverse: a column launch for fix_negative's borrows and
+//     the CCN sums, then a point launch that writes the gradients.
 // Branches follow the forward at the given input (the VJP of the piecewise
 // smooth map on the branch it takes).
 #include <cuda_runtime.h>

@@ -285,7 +285,9 @@ class Physics:
         """``Physics.__call__`` (physics.py:276-366). ``dycore_state``
         (optional, not in the reference's signature): run
         ``DycoreToPhysics``' copy from it inside the pre-step launch, in
-        place of a separate ``DycoreToPhysics.__call__`` before this call."""
+        place of a separate ``DycoreToPhysics.__call__`` before this call
+        (same results; measured slower at C96 L79 than the separate copy,
+        whose launch runs near the HBM bandwidth)."""
         ps = physics_state
         self.prestep(ps, stream, dycore_state)
         if self._gfs_microphysics:

@@ -271,6 +271,30 @@ def test_autograd_function_matches_vjp():
         assert torch.equal(a, b), name
 
 
+def test_workspace_grows_with_the_substeps():
+    """A handle's adjoint workspace, allocated for one sub-step by a first
+    call, grows for a later call with three sub-steps: the result equals a
+    fresh handle's, and a repeated call gives the same bits again."""
+    import torch
+
+    from pyshield_b200.adjoint import OUTPUTS, STATE, step_forward, step_vjp
+
+    mp, pc, x, land, area = _setup(6, 4, 79, 150.0, 21, mp_time=150.0)
+    y = step_forward(mp, x, land, 150.0)
+    ybar = _cotangents(y, 22)
+    step_vjp(mp, x, land, ybar, 150.0)  # one sub-step: the first workspace
+    y3 = step_forward(mp, x, land, 450.0)
+    ybar3 = _cotangents(y3, 23)
+    got = step_vjp(mp, x, land, ybar3, 450.0)  # three sub-steps on the same handle
+    again = step_vjp(mp, x, land, ybar3, 450.0)
+    fresh_mp = _setup(6, 4, 79, 450.0, 21, mp_time=150.0)[0]
+    ref = step_vjp(fresh_mp, x, land, ybar3, 450.0)
+    assert len(got) == len(STATE) and len(ybar3) == len(OUTPUTS)
+    for name, a, b, c in zip(STATE, got, again, ref):
+        assert torch.equal(a, c), name
+        assert torch.equal(a, b), name
+
+
 def test_de_ice_composes_with_the_step():
     """de_ice (microphysics.py:110-120) with incoming qi_dt: the adjoint equals
     the adjoint of the step without de_ice taken at the de-iced state, chained

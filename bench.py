@@ -328,12 +328,13 @@ def build_state(nlev, device, seed, n_cube=N_CUBE, sat_fraction=0.0):
     return ms, StencilFactory(gi), qf, GridData(area_q), host, land, (nx, ny, n)
 
 
-def run_adjoint(nsteps_window=8, reps=5, n_cube=48, nlev=79, dt=150.0):
-    """Adjoint cost at C48 L79: the device time of one VJP of the step
-    (shield_mp_step_vjp) against one forward step, and of an nsteps window
-    (forward steps with the state update, then the backward through
-    torch.autograd with per-step checkpointing) against the window's forward
-    alone. Each timing is the mean of ``reps`` runs after a warm-up."""
+def run_adjoint(nsteps_window=8, reps=5, n_cube=96, nlev=79, dt=150.0, window=True):
+    """Adjoint cost at C96 L79 (C48 without the window beside it): the device
+    time of one VJP of the step (shield_mp_step_vjp) against one forward step,
+    and of an nsteps window (forward steps with the state update, then the
+    backward through torch.autograd with per-step checkpointing) against the
+    window's forward alone. Each timing is the mean of ``reps`` runs after a
+    warm-up."""
     import torch
 
     from pyshield_b200._config import PhysicsConfig
@@ -364,6 +365,14 @@ def run_adjoint(nsteps_window=8, reps=5, n_cube=48, nlev=79, dt=150.0):
 
     fwd_ms = timed(lambda: mp(ms, dt))
     vjp_ms = timed(lambda: step_vjp(mp, x, lnd, ybar, dt))
+    res = {
+        "workload": f"GFDL microphysics step, C{n_cube} ({n} columns) x L{nlev}, dt {dt:g} s, FP64",
+        "forward_ms": fwd_ms,
+        "vjp_ms": vjp_ms,
+        "vjp_over_forward": vjp_ms / fwd_ms,
+    }
+    if not window:
+        return res
 
     def window_forward():
         with torch.no_grad():
@@ -377,17 +386,14 @@ def run_adjoint(nsteps_window=8, reps=5, n_cube=48, nlev=79, dt=150.0):
 
     wf_ms = timed(window_forward)
     wb_ms = timed(window_backward)
-    return {
-        "workload": f"GFDL microphysics step, C{n_cube} ({n} columns) x L{nlev}, dt {dt:g} s, FP64",
-        "forward_ms": fwd_ms,
-        "vjp_ms": vjp_ms,
-        "vjp_over_forward": vjp_ms / fwd_ms,
+    res.update({
         "window_steps": nsteps_window,
         "window_forward_ms": wf_ms,
         "window_forward_and_backward_ms": wb_ms,
         "window_backward_over_forward": (wb_ms - wf_ms) / wf_ms,
         "note": "device time (CUDA events); the window keeps each step's inputs and recomputes inside the step",
-    }
+    })
+    return res
 
 
 E2E_IN = ("pt", "qvapor", "qliquid", "qrain", "qice", "qsnow", "qgraupel", "qcld", "ua", "va", "delprsi", "delz",
@@ -1269,7 +1275,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
-    ap.add_argument("--no-adjoint", action="store_true", help="skip the C48 adjoint-cost measurement")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-cost measurement (C96 and C48)")
     ap.add_argument("--no-physics", action="store_true", help="skip the Physics.__call__ measurement")
     ap.add_argument("--no-coupling", action="store_true",
                     help="skip the UpdateAtmosphereState, DycoreToPhysics and AGrid2DGridPhysics measurements")
@@ -1370,7 +1376,10 @@ def main():
         cpu = {"value": v, "unit": "column-steps/s", "cores": cores, "kind": "port",
                "sample": sample + f"; {1000.0 * per:.0f} ms per step; one process alone on 3456 columns: "
                                   f"{v1:.4g} column-steps/s"}
-    adjoint = run_adjoint() if (rank == 0 and world == 1 and not args.no_adjoint and args.form == "plain") else None
+    adjoint = None
+    if rank == 0 and world == 1 and not args.no_adjoint and args.form == "plain":
+        adjoint = run_adjoint(n_cube=96)
+        adjoint["c48"] = run_adjoint(n_cube=48, window=False)
     physics = (run_physics(n_cube=args.ncube, nlev=nlev)
                if (rank == 0 and world == 1 and not args.no_physics and args.form == "plain") else None)
     coupling = (run_coupling(n_cube=args.ncube, nlev=nlev)

@@ -68,7 +68,9 @@ dim3 row_grid(int len, int64_t rows) {
 // computes each v3 once into shared memory, where the u and v points of the
 // level read it. Only A points in the prep domain [-1, nx] x [-1, ny] are
 // touched: every read of a D point lies there.
+// 16 levels per block measured the same as 8 (0.111 ms); 4 slower (0.128).
 constexpr int DT_X = 32, DT_Y = 8, DT_K = 8;
+constexpr int DW_MINB = 3;  // blocks per SM of the update kernels
 constexpr int AT_X = DT_X + 2, AT_Y = DT_Y + 2;
 // Levels per thread of the zeroing kernel.
 constexpr int DW_KB = 4;
@@ -78,10 +80,16 @@ constexpr int DW_KB = 4;
 // (west, east) stencils, on one tile. Each expression keeps the reference's
 // operand order; the loads of a level's u and v come before its stores.
 // The edge-plan tests and the points' addresses are worked out once, before
-// the level loop. Four blocks per SM (a 64-register cap, a few bytes
-// spilled) measured faster than three without the cap.
+// the level loop. The level loop is software-pipelined: the next level's
+// udt, vdt, u and v loads are issued before this level's barrier, and v3
+// alternates between two shared buffers, so one barrier per level orders
+// the writes of a buffer after every read of it two levels before. Six C96
+// tiles at L79 in one launch: 0.112 ms at three blocks per SM (80
+// registers), 0.127 ms at four (64 registers, more spilled), 0.133 ms at
+// two; 0.139 ms for the loop without the pipelining (load, barrier,
+// compute, barrier per level) at four.
 __device__ __forceinline__ void dwind_update_tile(const DwindArgs& A, int bx, int by, int bz) {
-  __shared__ double g_lon[3][AT_Y][AT_X], g_lat[3][AT_Y][AT_X], v3s[3][AT_Y][AT_X];
+  __shared__ double g_lon[3][AT_Y][AT_X], g_lat[3][AT_Y][AT_X], v3b[2][3][AT_Y][AT_X];
   constexpr int NT = DT_X * DT_Y;
   constexpr int NA = (AT_X * AT_Y + NT - 1) / NT;  // A points per thread
   const int tx = threadIdx.x % DT_X, ty = threadIdx.x / DT_X;
@@ -150,16 +158,34 @@ __device__ __forceinline__ void dwind_update_tile(const DwindArgs& A, int bx, in
   const bool any_u = fu[0] || fu[1] || fu[2] || fu[3], any_v = fv[0] || fv[1] || fv[2] || fv[3];
   double* pu = A.u.p + (up ? i * A.u.si + j * A.u.sj : 0);
   double* pv = A.v.p + (vp ? i * A.v.si + j * A.v.sj : 0);
+  // level k0's loads
+  double ut[NA], vt[NA];
+#pragma unroll
+  for (int n = 0; n < NA; ++n) {
+    ut[n] = ain[n] ? A.udt.p[ou[n] + k0 * A.udt.sk] : 0.0;
+    vt[n] = ain[n] ? A.vdt.p[ov[n] + k0 * A.vdt.sk] : 0.0;
+  }
+  double un = up && k0 < k1 ? pu[k0 * A.u.sk] : 0.0, vn = vp && k0 < k1 ? pv[k0 * A.v.sk] : 0.0;
   __syncthreads();
   for (int k = k0; k < k1; ++k) {
-    const double uk = up ? pu[k * A.u.sk] : 0.0, vk = vp ? pv[k * A.v.sk] : 0.0;
+    double(*v3s)[AT_Y][AT_X] = v3b[(k - k0) & 1];
 #pragma unroll
     for (int n = 0; n < NA; ++n) {
       if (!ain[n]) continue;
-      const double ut = A.udt.p[ou[n] + k * A.udt.sk], vt = A.vdt.p[ov[n] + k * A.vdt.sk];
 #pragma unroll
       for (int m = 0; m < 3; ++m)
-        v3s[m][ay[n]][ax[n]] = ut * g_lon[m][ay[n]][ax[n]] + vt * g_lat[m][ay[n]][ax[n]];
+        v3s[m][ay[n]][ax[n]] = ut[n] * g_lon[m][ay[n]][ax[n]] + vt[n] * g_lat[m][ay[n]][ax[n]];
+    }
+    const double uk = un, vk = vn;
+    if (k + 1 < k1) {
+#pragma unroll
+      for (int n = 0; n < NA; ++n) {
+        if (!ain[n]) continue;
+        ut[n] = A.udt.p[ou[n] + (k + 1) * A.udt.sk];
+        vt[n] = A.vdt.p[ov[n] + (k + 1) * A.vdt.sk];
+      }
+      if (up) un = pu[(k + 1) * A.u.sk];
+      if (vp) vn = pv[(k + 1) * A.v.sk];
     }
     __syncthreads();
     // A point (ai, aj) sits at v3s[.][aj - j0 + 1][ai - i0 + 1]
@@ -195,11 +221,10 @@ __device__ __forceinline__ void dwind_update_tile(const DwindArgs& A, int bx, in
       }
       pv[k * A.v.sk] = vk + A.dt5 * (w[0] * e2[0] + w[1] * e2[1] + w[2] * e2[2]);
     }
-    __syncthreads();  // every read of this level's v3s before the next level's
   }
 }
 
-__global__ void __launch_bounds__(DT_X * DT_Y, 4) dwind_update_kernel(const __grid_constant__ DwindArgs A) {
+__global__ void __launch_bounds__(DT_X * DT_Y, DW_MINB) dwind_update_kernel(const __grid_constant__ DwindArgs A) {
   dwind_update_tile(A, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
@@ -222,7 +247,7 @@ __device__ __forceinline__ void dwind_update_batch_tile(const DwindBatch& B) {
   dwind_update_tile(A, blockIdx.x, blockIdx.y, bz);
 }
 
-__global__ void __launch_bounds__(DT_X * DT_Y, 4) dwind_update_batch_kernel(const __grid_constant__ DwindBatch B) {
+__global__ void __launch_bounds__(DT_X * DT_Y, DW_MINB) dwind_update_batch_kernel(const __grid_constant__ DwindBatch B) {
   switch (blockIdx.z / B.nkz) {
     case 0: dwind_update_batch_tile<0>(B); break;
     case 1: dwind_update_batch_tile<1>(B); break;

@@ -349,7 +349,13 @@ def run_adjoint(nsteps_window=8, reps=5, n_cube=96, nlev=79, dt=150.0, window=Tr
     lnd = land.view.clone()
     y = step_forward(mp, x, lnd, dt)
     g = torch.Generator(device=device).manual_seed(1)
-    ybar = [torch.randn(v.shape, generator=g, device=device, dtype=torch.float64) for v in y]
+
+    def cotangent(v):
+        # a cotangent in its output's own layout (i fastest, as the step writes them)
+        t = torch.randn(tuple(reversed(v.shape)), generator=g, device=device, dtype=torch.float64)
+        return t.permute(*reversed(range(v.dim())))
+
+    ybar = [cotangent(v) for v in y]
     stream = torch.cuda.current_stream()
 
     def timed(fn):
